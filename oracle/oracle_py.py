@@ -1,0 +1,248 @@
+"""ctypes binding of the FP64 CPU oracle (test infrastructure only).
+
+Imported only by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
+leg, as the checker.  Arrays follow the oracle's layouts: particle arrays are
+structure-of-arrays (3, np); fields are (3, mz, my, mx).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
+RFD_REFERENCE, RFD_PAPER = 0, 1
+
+
+class OrcConfig(ctypes.Structure):
+    _fields_ = [
+        ("mx", ctypes.c_int32), ("my", ctypes.c_int32), ("mz", ctypes.c_int32),
+        ("kernel", ctypes.c_int32),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+        ("shearviscosity", ctypes.c_double), ("temperature", ctypes.c_double),
+        ("dt", ctypes.c_double), ("cutoff", ctypes.c_double),
+        ("extra_mobility", ctypes.c_double), ("soft_epsilon", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("pair", ctypes.c_int32), ("rfd", ctypes.c_int32),
+        ("nonbonded", ctypes.c_int32), ("pad_", ctypes.c_int32),
+    ]
+
+
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+_F = ctypes.POINTER(ctypes.c_float)
+_I = ctypes.POINTER(ctypes.c_int32)
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = os.path.join(HERE, "liboracle_fsl.so")
+    if not os.path.exists(path):
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("_orc_build", os.path.join(HERE, "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build_oracle()
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.orc_create.restype = vp
+    L.orc_create.argtypes = [ctypes.POINTER(OrcConfig), ctypes.c_int64, _D]
+    L.orc_destroy.argtypes = [vp]
+    L.orc_set_bonds.argtypes = [vp, ctypes.c_int64, _I, _I, _D, _D, ctypes.c_int64, _I, _D, _D, _D]
+    L.orc_step.argtypes = [vp, ctypes.c_int64]
+    for name in ("orc_get_positions", "orc_set_positions", "orc_get_predictor",
+                 "orc_get_forces", "orc_get_velocity"):
+        getattr(L, name).argtypes = [vp, _D]
+    L.orc_get_step.restype = ctypes.c_uint64
+    L.orc_get_step.argtypes = [vp]
+    L.orc_set_step.argtypes = [vp, ctypes.c_uint64]
+    L.orc_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, _D]
+    L.orc_neighbor_grid.argtypes = [vp, _I]
+    L.orc_cell_list.argtypes = [vp, _D, _I, _I, _I]
+    L.orc_forces.argtypes = [vp, _D, _D]
+    L.orc_spread.argtypes = [vp, _D, _D, _D]
+    L.orc_solve.argtypes = [vp, _D, _D]
+    L.orc_interp.argtypes = [vp, _D, _D, _D]
+    L.orc_build_W.argtypes = [vp, _D, ctypes.c_int, _D]
+    L.orc_fft3d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D]
+    L.orc_ljtable.argtypes = [vp, _F]
+    L.orc_tex_linear.restype = ctypes.c_float
+    L.orc_tex_linear.argtypes = [_F, ctypes.c_int, ctypes.c_float]
+    L.orc_delta3.restype = ctypes.c_double
+    L.orc_delta3.argtypes = [ctypes.c_double]
+    L.orc_delta4.restype = ctypes.c_double
+    L.orc_delta4.argtypes = [ctypes.c_double]
+    L.orc_num_threads.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def noise(seed, t, first, count):
+    out = np.empty(count, dtype=np.float64)
+    _load().orc_noise(seed, t, first, count, _dp(out))
+    return out
+
+
+def fft3d(a, sign):
+    """Unnormalised 3-D DFT of a complex (mz, my, mx) array, sign -1 or +1."""
+    z = np.ascontiguousarray(a, dtype=np.complex128).copy()
+    mz, my, mx = z.shape
+    _load().orc_fft3d(mx, my, mz, sign, z.ctypes.data_as(_D))
+    return z
+
+
+def delta3(x):
+    return _load().orc_delta3(float(x))
+
+
+def delta4(x):
+    return _load().orc_delta4(float(x))
+
+
+def tex_linear(table, x):
+    t = np.ascontiguousarray(table, dtype=np.float32)
+    return _load().orc_tex_linear(t.ctypes.data_as(_F), len(t), float(x))
+
+
+def num_threads():
+    return _load().orc_num_threads()
+
+
+class Oracle:
+    """One Stokes-limit instance on the CPU, FP64."""
+
+    def __init__(self, mx, my, mz, lx, ly, lz, q, eta=1.0, kT=0.01, dt=0.01, cutoff=1.5,
+                 kernel=3, pair=PAIR_SOFT, soft_epsilon=1.0, rfd=RFD_REFERENCE,
+                 nonbonded=1, extra_mobility=0.0, seed=1):
+        self.L = _load()
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(3, -1)
+        self.np = q.shape[1]
+        self.shape = (mz, my, mx)
+        self.nc = mx * my * mz
+        c = OrcConfig(mx=mx, my=my, mz=mz, kernel=kernel, lx=lx, ly=ly, lz=lz,
+                      shearviscosity=eta, temperature=kT, dt=dt, cutoff=cutoff,
+                      extra_mobility=extra_mobility, soft_epsilon=soft_epsilon,
+                      seed=seed, pair=pair, rfd=rfd, nonbonded=nonbonded, pad_=0)
+        self.cfg = c
+        self.h = self.L.orc_create(ctypes.byref(c), self.np, _dp(q))
+        if not self.h:
+            raise ValueError("orc_create rejected the configuration")
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.L.orc_destroy(h)
+            self.h = None
+
+    def set_bonds(self, bi, bj, k, r0, fi=None, fk=None, fr0=None, fxyz=None):
+        bi = np.ascontiguousarray(bi, dtype=np.int32)
+        bj = np.ascontiguousarray(bj, dtype=np.int32)
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        r0 = np.ascontiguousarray(r0, dtype=np.float64)
+        if fi is None:
+            fi = np.zeros(0, np.int32)
+            fk = fr0 = np.zeros(0)
+            fxyz = np.zeros((0, 3))
+        fi = np.ascontiguousarray(fi, dtype=np.int32)
+        fk = np.ascontiguousarray(fk, dtype=np.float64)
+        fr0 = np.ascontiguousarray(fr0, dtype=np.float64)
+        fxyz = np.ascontiguousarray(fxyz, dtype=np.float64).reshape(-1, 3)
+        rc = self.L.orc_set_bonds(self.h, len(bi), bi.ctypes.data_as(_I), bj.ctypes.data_as(_I),
+                                  _dp(k), _dp(r0), len(fi), fi.ctypes.data_as(_I), _dp(fk),
+                                  _dp(fr0), _dp(fxyz))
+        if rc != 0:
+            raise ValueError("bond index out of range")
+
+    def step(self, n=1):
+        self.L.orc_step(self.h, n)
+
+    def positions(self):
+        out = np.empty((3, self.np))
+        self.L.orc_get_positions(self.h, _dp(out))
+        return out
+
+    def set_positions(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(3, self.np)
+        self.L.orc_set_positions(self.h, _dp(q))
+
+    def predictor(self):
+        out = np.empty((3, self.np))
+        self.L.orc_get_predictor(self.h, _dp(out))
+        return out
+
+    def forces(self):
+        out = np.empty((3, self.np))
+        self.L.orc_get_forces(self.h, _dp(out))
+        return out
+
+    def velocity(self):
+        out = np.empty((3,) + self.shape)
+        self.L.orc_get_velocity(self.h, _dp(out))
+        return out
+
+    @property
+    def t(self):
+        return int(self.L.orc_get_step(self.h))
+
+    @t.setter
+    def t(self, value):
+        self.L.orc_set_step(self.h, int(value))
+
+    def neighbor_grid(self):
+        d = np.zeros(3, np.int32)
+        m = self.L.orc_neighbor_grid(self.h, d.ctypes.data_as(_I))
+        return tuple(int(x) for x in d), int(m)
+
+    def cell_list(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        (_, m) = self.neighbor_grid()
+        cell_of = np.empty(self.np, np.int32)
+        start = np.empty(m + 1, np.int32)
+        srt = np.empty(self.np, np.int32)
+        self.L.orc_cell_list(self.h, _dp(q), cell_of.ctypes.data_as(_I),
+                             start.ctypes.data_as(_I), srt.ctypes.data_as(_I))
+        return cell_of, start, srt
+
+    def compute_forces(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        F = np.empty((3, self.np))
+        self.L.orc_forces(self.h, _dp(q), _dp(F))
+        return F
+
+    def spread(self, q, F):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        f = np.empty((3,) + self.shape)
+        self.L.orc_spread(self.h, _dp(q), _dp(F), _dp(f))
+        return f
+
+    def solve(self, W):
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        v = np.empty((3,) + self.shape)
+        self.L.orc_solve(self.h, _dp(W), _dp(v))
+        return v
+
+    def interp(self, q, v):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        u = np.empty((3, self.np))
+        self.L.orc_interp(self.h, _dp(q), _dp(v), _dp(u))
+        return u
+
+    def build_W(self, f, second=False):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        W = np.empty((3,) + self.shape)
+        self.L.orc_build_W(self.h, _dp(f), 1 if second else 0, _dp(W))
+        return W
+
+    def ljtable(self):
+        out = np.empty(4096, np.float32)
+        self.L.orc_ljtable(self.h, out.ctypes.data_as(_F))
+        return out
