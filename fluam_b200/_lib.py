@@ -1,0 +1,125 @@
+"""ctypes binding of libfluamsl.so (the C ABI declared in include/fluamsl.h).
+
+The library is built in-tree by ``fluam_b200/build.py``.  There is no CPU
+fallback: if the shared library is missing or cannot be loaded, every entry
+point raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfluamsl.so")
+
+FSL_OK = 0
+ERRORS = {-1: "FSL_E_ARG", -2: "FSL_E_CUDA", -3: "FSL_E_NOMEM", -4: "FSL_E_KERNEL",
+          -5: "FSL_E_IO", -6: "FSL_E_INPUT"}
+PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
+RFD_REFERENCE, RFD_PAPER = 0, 1
+
+# Every symbol include/fluamsl.h declares.
+EXPORTS = [
+    "fsl_config_defaults", "fsl_create", "fsl_load_bonds", "fsl_step", "fsl_sync",
+    "fsl_get_positions", "fsl_set_positions", "fsl_get_forces", "fsl_get_velocity",
+    "fsl_get_status", "fsl_set_step", "fsl_clear_errors", "fsl_set_graph", "fsl_stream",
+    "fsl_profile", "fsl_profile_read",
+    "fsl_destroy", "fsl_last_error", "fsl_run_data_main", "fsl_parse_data_main",
+    "fsl_neighbor_grid", "fsl_cell_list", "fsl_compute_forces", "fsl_spread", "fsl_solve",
+    "fsl_interpolate", "fsl_noise",
+]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("mx", ctypes.c_int32), ("my", ctypes.c_int32), ("mz", ctypes.c_int32),
+        ("kernel", ctypes.c_int32),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+        ("shearviscosity", ctypes.c_double), ("temperature", ctypes.c_double),
+        ("dt", ctypes.c_double), ("cutoff", ctypes.c_double),
+        ("extra_mobility", ctypes.c_double), ("soft_epsilon", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("pair", ctypes.c_int32), ("rfd", ctypes.c_int32),
+        ("nonbonded", ctypes.c_int32), ("device", ctypes.c_int32),
+    ]
+
+
+class Status(ctypes.Structure):
+    _fields_ = [
+        ("step", ctypes.c_uint64), ("error_bits", ctypes.c_int32), ("np", ctypes.c_int32),
+        ("nc", ctypes.c_int64), ("graph", ctypes.c_int32), ("launches_per_step", ctypes.c_int32),
+    ]
+
+
+class StageTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_int64),
+                ("total_ms", ctypes.c_double)]
+
+
+class FslError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+_F = ctypes.POINTER(ctypes.c_float)
+_I = ctypes.POINTER(ctypes.c_int32)
+_VP = ctypes.c_void_p
+
+
+def load(path=None):
+    """Load libfluamsl.so (raises OSError if it is not built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise OSError(f"{p} is not built; run fluam_b200/build.py (nvcc, sm_100a)")
+    L = ctypes.CDLL(p)
+    L.fsl_config_defaults.argtypes = [ctypes.POINTER(Config)]
+    L.fsl_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int64, _D, ctypes.POINTER(_VP)]
+    L.fsl_load_bonds.argtypes = [_VP, ctypes.c_int64, _I, _I, _D, _D, ctypes.c_int64, _I, _D, _D, _D]
+    L.fsl_step.argtypes = [_VP, ctypes.c_int64]
+    L.fsl_sync.argtypes = [_VP]
+    L.fsl_get_positions.argtypes = [_VP, _D]
+    L.fsl_set_positions.argtypes = [_VP, _D]
+    L.fsl_get_forces.argtypes = [_VP, _D]
+    L.fsl_get_velocity.argtypes = [_VP, _F]
+    L.fsl_get_status.argtypes = [_VP, ctypes.POINTER(Status)]
+    L.fsl_set_step.argtypes = [_VP, ctypes.c_uint64]
+    L.fsl_clear_errors.argtypes = [_VP]
+    L.fsl_set_graph.argtypes = [_VP, ctypes.c_int]
+    L.fsl_stream.argtypes = [_VP]
+    L.fsl_stream.restype = _VP
+    L.fsl_profile.argtypes = [_VP, ctypes.c_int]
+    L.fsl_profile_read.argtypes = [_VP, ctypes.POINTER(StageTime), ctypes.c_int32,
+                                   ctypes.POINTER(ctypes.c_int32)]
+    L.fsl_destroy.argtypes = [_VP]
+    L.fsl_destroy.restype = None
+    L.fsl_last_error.restype = ctypes.c_char_p
+    L.fsl_run_data_main.argtypes = [ctypes.c_char_p]
+    L.fsl_parse_data_main.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config),
+                                      ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    L.fsl_neighbor_grid.argtypes = [_VP, _I]
+    L.fsl_cell_list.argtypes = [_VP, _I, _I, _I]
+    L.fsl_compute_forces.argtypes = [_VP, _D]
+    L.fsl_spread.argtypes = [_VP, _D, _D]
+    L.fsl_solve.argtypes = [_VP, _D, _D]
+    L.fsl_interpolate.argtypes = [_VP, _D, _D]
+    L.fsl_noise.argtypes = [_VP, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, _F]
+    if path is None:
+        _lib = L
+    return L
+
+
+def check(rc):
+    if rc != FSL_OK:
+        msg = load().fsl_last_error()
+        raise FslError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def last_error():
+    m = load().fsl_last_error()
+    return m.decode() if m else ""

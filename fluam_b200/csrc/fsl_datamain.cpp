@@ -1,0 +1,490 @@
+// fsl_datamain.cpp -- the drop-in driver: fluam's data.main input contract and
+// its particle output files, around the libfluamsl C ABI.
+//
+// Input  (src/loadDataMain.cu:173-683): whitespace-separated keywords, each
+//   followed by a fixed number of values; '#' starts a comment to end of line;
+//   an unknown keyword is an error ("ERROR INPUT FILE").  Every keyword of the
+//   reference parser is accepted and consumes the same tokens; the ones that
+//   the Stokes-limit path does not read are ignored.  Four keywords are new
+//   (the reference parser would reject them): pairPotential lj|soft|none,
+//   softEpsilon <eps>, kernelPoints 3|4, rfdMode reference|paper.
+// Output (src/saveFunctionsSchemeStokesLimit.cu, src/saveParticles.cu:32-82,
+//   src/saveSeed.cpp, src/saveTime.cpp, src/cudaDevice.cu):
+//   <out>.data.main echo, <out>.cuda, <out>.seed, <out>.time,
+//   <out>.particles and <out>.velocityParticles ("#NUMBER PARTICLES np", then
+//   per sample a line step*dt and np lines "x y z", precision 15).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/fluamsl.h"
+
+namespace {
+
+struct Run {
+  fsl_config cfg;
+  int64_t numsteps = 0, relax = 0, samplefreq = 0, np = 0;
+  bool have_seed = false;
+  int loadparticles = 0;
+  std::string coordinates, outputname, bondfile;
+  bool bonded = false;
+  // scheme flags that select another fluam scheme (src/main.cpp:36-105)
+  bool stokesLimit = false;
+  std::vector<std::string> other_schemes;
+  std::string wordfile;
+};
+
+// Number of values that follow each keyword of the reference parser.
+const std::map<std::string, int>& keyword_arity() {
+  static const std::map<std::string, int> m = {
+      {"particles", 1}, {"saffmanCutOffWaveNumber", 1}, {"saffmanLayerWidth", 1},
+      {"viscosityMeasureAmplitude", 1}, {"identity_prefactor", 1}, {"gradTemperature", 1},
+      {"soretCoefficient", 1}, {"backgroundvelocity", 3}, {"setDevice", 1},
+      {"particlesdata", 1}, {"boundary", 1}, {"velocityboundary", 1},
+      {"volumeboundaryconst", 1}, {"densfluid", 1}, {"shearviscosity", 1},
+      {"bulkviscosity", 1}, {"temperature", 1}, {"thermostat", 0}, {"numsteps", 1},
+      {"numstepsRelaxation", 1}, {"dt", 1}, {"samplefreq", 1}, {"savefreq", 1},
+      {"pressureparameters", 3}, {"outputname", 1}, {"seed", 1}, {"cells", 3},
+      {"celldimension", 3}, {"initfluid", 1}, {"checkVelocity", 1}, {"loadparticles", 1},
+      {"coordinates", 1}, {"velocities", 1}, {"fluid", 1}, {"numberparticles", 1},
+      {"mass", 1}, {"volumeParticle", 1}, {"cutoff", 1}, {"maxNumberPartInCell", 1},
+      {"maxNumberPartInCellNonBonded", 1}, {"dDensity", 1}, {"omega", 1},
+      {"waveSourceIndex", 1}, {"saveFluid", 1}, {"saveVTK", 1}, {"ghost", 0},
+      {"bondedForces", 1}, {"bondedForcesVersion", 1}, {"computeNonBondedForces", 1},
+      {"binaryMixture", 0}, {"diffusion", 1}, {"massSpecies0", 1}, {"massSpecies1", 1},
+      {"concentration", 1}, {"binaryMixtureWall", 0}, {"concentrationWall", 2},
+      {"vxWall", 2}, {"vyWall", 2}, {"vzWall", 2}, {"densityWall", 2},
+      {"giantFluctuations", 0}, {"continuousGradient", 0}, {"incompressible", 0},
+      {"incompressibleBoundaryRK2", 0}, {"quasiNeutrallyBuoyant", 0},
+      {"quasiNeutrallyBuoyant2D", 0}, {"quasiNeutrallyBuoyant4pt2D", 0}, {"quasi2D", 0},
+      {"hydrodynamicRadius", 1}, {"nDrift", 1}, {"stokesLimit2D", 0},
+      {"predictorCorrector", 1}, {"sampleHydroGrid", 1}, {"cellsHydroGrid", 2},
+      {"greenParticles", 2}, {"use_RFD", 1}, {"IMEXRK", 0},
+      {"incompressibleBinaryMixture", 0}, {"incompressibleBinaryMixtureMidPoint", 0},
+      {"particlesWall", 0}, {"freeEnergyCompressibleParticles", 0}, {"omega0", 1},
+      {"semiImplicitCompressibleParticles", 0}, {"momentumCoupling", 0},
+      {"stokesLimitFirstOrder", 0}, {"stokesLimit", 0}, {"extraMobility", 1},
+      // extensions of this build
+      {"pairPotential", 1}, {"softEpsilon", 1}, {"kernelPoints", 1}, {"rfdMode", 1},
+      {"savedensity", -1}};
+  return m;
+}
+
+int parse(const char* path, Run& r, std::string& err) {
+  fsl_config_defaults(&r.cfg);
+  std::ifstream in(path);
+  if (!in) {
+    err = std::string("cannot open ") + path;
+    return FSL_E_IO;
+  }
+  // wordfile echo exactly as src/loadDataMain.cu:313-317
+  {
+    std::string line;
+    while (!in.eof()) {
+      std::getline(in, line);
+      r.wordfile += line + "\n";
+    }
+  }
+  in.close();
+  in.open(path);
+  const auto& ar = keyword_arity();
+  std::string word, oldword;
+  int64_t thermostat = 0;
+  in >> word;
+  while (!in.eof()) {
+    if (!word.empty() && word[0] == '#') {
+      std::getline(in, word);
+    } else {
+      auto it = ar.find(word);
+      if (it == ar.end()) {
+        err = "ERROR INPUT FILE; LAST WORD READED: " + oldword + " (unknown keyword '" + word + "')";
+        return FSL_E_INPUT;
+      }
+      std::vector<std::string> vals;
+      int n = it->second;
+      if (word == "savedensity") {
+        std::string v;
+        in >> v;
+        if (v == "1") {
+          int64_t ns = 0;
+          in >> ns;
+          for (int64_t k = 0; k < ns; ++k) in >> v;
+        } else {
+          std::getline(in, v);
+        }
+        n = 0;
+      }
+      for (int k = 0; k < n; ++k) {
+        std::string v;
+        in >> v;
+        vals.push_back(v);
+      }
+      auto D = [&](int k) { return std::strtod(vals[k].c_str(), nullptr); };
+      auto I = [&](int k) { return (int64_t)std::strtoll(vals[k].c_str(), nullptr, 10); };
+      fsl_config& c = r.cfg;
+      if (word == "cells") {
+        c.mx = (int)I(0);
+        c.my = (int)I(1);
+        c.mz = (int)I(2);
+      } else if (word == "celldimension") {
+        c.lx = D(0);
+        c.ly = D(1);
+        c.lz = D(2);
+      } else if (word == "shearviscosity") {
+        c.shearviscosity = D(0);
+      } else if (word == "temperature") {
+        c.temperature = D(0);
+      } else if (word == "dt") {
+        c.dt = D(0);
+      } else if (word == "cutoff") {
+        c.cutoff = D(0);
+      } else if (word == "numsteps") {
+        r.numsteps = I(0);
+      } else if (word == "numstepsRelaxation") {
+        r.relax = I(0);
+      } else if (word == "samplefreq") {
+        r.samplefreq = I(0);
+      } else if (word == "seed") {
+        c.seed = (uint64_t)I(0);
+        r.have_seed = true;
+      } else if (word == "outputname") {
+        r.outputname = vals[0];
+      } else if (word == "numberparticles") {
+        r.np = I(0);
+      } else if (word == "loadparticles") {
+        r.loadparticles = (int)I(0);
+      } else if (word == "coordinates") {
+        r.coordinates = vals[0];
+      } else if (word == "bondedForces") {
+        r.bonded = true;
+        r.bondfile = vals[0];
+      } else if (word == "bondedForcesVersion") {
+        if (I(0) != 0) {
+          err = "bondedForcesVersion != 0 (old bond file format) is not supported";
+          return FSL_E_INPUT;
+        }
+      } else if (word == "computeNonBondedForces") {
+        c.nonbonded = (int)I(0);
+      } else if (word == "extraMobility") {
+        c.extra_mobility = D(0);
+      } else if (word == "setDevice") {
+        c.device = (int)I(0);
+      } else if (word == "stokesLimit") {
+        r.stokesLimit = true;
+      } else if (word == "thermostat") {
+        thermostat = 1;
+      } else if (word == "pairPotential") {
+        if (vals[0] == "lj") c.pair = FSL_PAIR_TABLE_LJ;
+        else if (vals[0] == "soft") c.pair = FSL_PAIR_SOFT;
+        else if (vals[0] == "none") c.pair = FSL_PAIR_NONE;
+        else {
+          err = "pairPotential must be lj, soft or none";
+          return FSL_E_INPUT;
+        }
+      } else if (word == "softEpsilon") {
+        c.soft_epsilon = D(0);
+      } else if (word == "kernelPoints") {
+        c.kernel = (int)I(0);
+      } else if (word == "rfdMode") {
+        if (vals[0] == "reference") c.rfd = FSL_RFD_REFERENCE;
+        else if (vals[0] == "paper") c.rfd = FSL_RFD_PAPER;
+        else {
+          err = "rfdMode must be reference or paper";
+          return FSL_E_INPUT;
+        }
+      } else if (word == "continuousGradient" || word == "giantFluctuations" ||
+                 word == "binaryMixtureWall" || word == "binaryMixture" ||
+                 word == "particlesWall" || word == "freeEnergyCompressibleParticles" ||
+                 word == "semiImplicitCompressibleParticles" || word == "momentumCoupling" ||
+                 word == "incompressible" || word == "incompressibleBinaryMixture" ||
+                 word == "incompressibleBinaryMixtureMidPoint" ||
+                 word == "quasiNeutrallyBuoyant" || word == "quasiNeutrallyBuoyant2D" ||
+                 word == "quasiNeutrallyBuoyant4pt2D" || word == "quasi2D" ||
+                 word == "stokesLimit2D" || word == "stokesLimitFirstOrder") {
+        r.other_schemes.push_back(word);
+      }
+    }
+    oldword = word;
+    in >> word;
+  }
+  // the reference's scheme precedence (src/main.cpp:36-99): all of these come
+  // before stokesLimit in its if-chain
+  if (thermostat) r.other_schemes.push_back("thermostat");
+  return FSL_OK;
+}
+
+bool read_coordinates(const std::string& file, std::vector<double>& q, int64_t& np) {
+  // src/createParticles.cpp:81-101: np then np lines "x y z"
+  std::ifstream f(file);
+  if (!f) return false;
+  f >> np;
+  if (!f || np < 0) return false;
+  std::vector<double> x(np), y(np), z(np);
+  for (int64_t i = 0; i < np; ++i) f >> x[i] >> y[i] >> z[i];
+  if (!f) return false;
+  q.resize(3 * np);
+  for (int64_t i = 0; i < np; ++i) {
+    q[i] = x[i];
+    q[np + i] = y[i];
+    q[2 * np + i] = z[i];
+  }
+  return true;
+}
+
+void simple_cubic(const fsl_config& c, int64_t np, std::vector<double>& q) {
+  // src/simpleCubic.cpp:25-63 (dimension 3)
+  double lx = c.lx, ly = c.ly, lz = c.lz;
+  double sigma = std::pow(lx * ly * lz / (np), 1. / 3.);
+  int nz = (int(lz / sigma) ? int(lz / sigma) : 1);
+  int nx = (int(lx / sigma) ? int(lx / sigma) : 1);
+  int ny = (int(ly / sigma) ? int(ly / sigma) : 1);
+  while ((int64_t)nx * ny * nz < np) {
+    if ((int64_t)nx * ny * nz < np) nx++;
+    if ((int64_t)nx * ny * nz < np) ny++;
+    if ((int64_t)nx * ny * nz < np) nz++;
+  }
+  double dx = lx / double(nx), dy = ly / double(ny), dz = lz / double(nz);
+  q.assign(3 * np, 0.0);
+  int64_t n = 0;
+  for (int i = 0; i <= nz - 1; i++)
+    for (int j = 0; j <= ny - 1; j++)
+      for (int k = 0; k <= nx - 1; k++)
+        if (n < np) {
+          n = n + 1;
+          q[n - 1] = (k + 0.5) * dx - lx / 2.;
+          q[np + n - 1] = (j + 0.5) * dy - ly / 2.;
+          q[2 * np + n - 1] = (i + 0.5) * dz - lz / 2.;
+        }
+}
+
+struct Bonds {
+  std::vector<int32_t> bi, bj, fi;
+  std::vector<double> k, r0, fk, fr0, fxyz;
+};
+
+bool read_bonds(const std::string& file, Bonds& b) {
+  // src/initializeBondedForces.cpp:31-150 (format in bin/inputfiles/README:60-108)
+  std::ifstream f(file);
+  if (!f) return false;
+  int64_t n = 0;
+  f >> n;
+  if (!f || n < 0) return false;
+  for (int64_t k = 0; k < n; ++k) {
+    int i1, i2;
+    double ks, r0;
+    f >> i1 >> i2 >> ks >> r0;
+    b.bi.push_back(i1);
+    b.bj.push_back(i2);
+    b.k.push_back(ks);
+    b.r0.push_back(r0);
+  }
+  int64_t nf = 0;
+  f >> nf;
+  if (!f || nf < 0) return false;
+  for (int64_t k = 0; k < nf; ++k) {
+    int i1;
+    double ks, r0, x, y, z;
+    f >> i1 >> ks >> r0 >> x >> y >> z;
+    b.fi.push_back(i1);
+    b.fk.push_back(ks);
+    b.fr0.push_back(r0);
+    b.fxyz.push_back(x);
+    b.fxyz.push_back(y);
+    b.fxyz.push_back(z);
+  }
+  return (bool)f;
+}
+
+void write_cuda_file(const std::string& out, int setDevice) {
+  // src/cudaDevice.cu:23-83
+  std::ofstream f(out + ".cuda");
+  int count = 0, drv = 0, rt = 0;
+  cudaGetDeviceCount(&count);
+  f << std::endl << "cudaGetDeviceCount     " << count << std::endl;
+  for (int i = 0; i < count; i++) {
+    cudaDeviceProp p;
+    cudaGetDeviceProperties(&p, i);
+    f << std::endl << "Device " << i << ": version " << p.major << " " << p.minor << std::endl;
+    f << p.name << std::endl;
+    cudaDriverGetVersion(&drv);
+    f << "Driver version                  " << drv << std::endl;
+    cudaRuntimeGetVersion(&rt);
+    f << "Runtime version                 " << rt << std::endl;
+    f << "Multiprocessors                 " << p.multiProcessorCount << std::endl;
+    f << "Global memory (bytes)           " << p.totalGlobalMem << std::endl;
+    f << "Constant memory (bytes)         " << p.totalConstMem << std::endl;
+    f << "Shared memory per block (bytes) " << p.sharedMemPerBlock << std::endl;
+    f << "Registers per block             " << p.regsPerBlock << std::endl;
+    f << "Warp size                       " << p.warpSize << std::endl;
+    f << "Maximum threads per block       " << p.maxThreadsPerBlock << std::endl;
+    int clk = 0;
+    cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, i);
+    f << "Clock rate (GHz)                " << clk * 1e-6 << std::endl;
+    int mode = 0;
+    cudaDeviceGetAttribute(&mode, cudaDevAttrComputeMode, i);
+    f << "Compute Mode                    " << mode << std::endl;
+  }
+  if (setDevice >= 0) {
+    cudaSetDevice(setDevice);
+    int d = 0;
+    cudaGetDevice(&d);
+    f << std::endl << std::endl << std::endl;
+    f << "Device selected " << d << std::endl;
+  }
+  f << std::endl;
+}
+
+void write_sample(std::ofstream& f, int64_t np, const std::vector<double>& a, double t) {
+  f << t << std::endl;
+  for (int64_t i = 0; i < np; ++i) f << a[i] << " " << a[np + i] << " " << a[2 * np + i] << std::endl;
+}
+
+}  // namespace
+
+extern "C" int fsl_parse_data_main(const char* path, fsl_config* cfg, int64_t* numsteps,
+                                   int64_t* samplefreq, int64_t* relax, int64_t* np) {
+  if (!path || !cfg) return FSL_E_ARG;
+  Run r;
+  std::string err;
+  int rc = parse(path, r, err);
+  if (rc) {
+    std::cerr << err << std::endl;
+    return rc;
+  }
+  *cfg = r.cfg;
+  if (numsteps) *numsteps = r.numsteps;
+  if (samplefreq) *samplefreq = r.samplefreq;
+  if (relax) *relax = r.relax;
+  if (np) *np = r.np;
+  return FSL_OK;
+}
+
+extern "C" int fsl_run_data_main(const char* path) {
+  Run r;
+  std::string err;
+  int rc = parse(path ? path : "data.main", r, err);
+  if (rc) {
+    std::cout << err << std::endl;
+    return rc;
+  }
+  // echo of the input (src/loadDataMain.cu:672-676)
+  {
+    std::ofstream fo(r.outputname + ".data.main");
+    fo << r.wordfile << std::endl;
+  }
+  std::cout << "READ " << (path ? path : "data.main") << " :                DONE" << std::endl;
+  if (!r.other_schemes.empty() || !r.stokesLimit) {
+    std::cout << "ERROR: this build runs the stokesLimit scheme only"
+              << (r.other_schemes.empty() ? std::string(" (keyword stokesLimit missing)")
+                                          : " (found " + r.other_schemes[0] + ")")
+              << std::endl;
+    return FSL_E_INPUT;
+  }
+  if (r.samplefreq <= 0) {
+    // the reference divides by samplefreq (src/runSchemeStokesLimit.cu:280)
+    std::cout << "ERROR: samplefreq must be > 0" << std::endl;
+    return FSL_E_INPUT;
+  }
+  write_cuda_file(r.outputname, r.cfg.device);
+  // src/initializeRandomNumber.cpp:23-36
+  if (!r.have_seed) {
+    uint64_t s = (uint64_t)time(0);
+    r.cfg.seed = s % 18671;
+  }
+  // particles (src/createParticles.cpp:39-102)
+  std::vector<double> q;
+  int64_t np = r.np;
+  if (r.loadparticles == 1) {
+    if (r.coordinates.empty()) {
+      std::cout << "ERROR NO PARTICLESCOOR FILE FOUND" << std::endl;
+      return FSL_E_INPUT;
+    }
+    if (!read_coordinates(r.coordinates, q, np)) {
+      std::cout << "ERROR reading coordinates file " << r.coordinates << std::endl;
+      return FSL_E_IO;
+    }
+  } else {
+    if (np <= 0) {
+      std::cout << "ERROR: numberparticles must be > 0" << std::endl;
+      return FSL_E_INPUT;
+    }
+    simple_cubic(r.cfg, np, q);
+  }
+  fsl_handle* h = nullptr;
+  rc = fsl_create(&r.cfg, np, q.data(), &h);
+  if (rc) {
+    std::cout << "ERROR: " << fsl_last_error() << std::endl;
+    return rc;
+  }
+  if (r.bonded) {
+    Bonds b;
+    if (!read_bonds(r.bondfile, b)) {
+      std::cout << "ERROR reading bondedForces file " << r.bondfile << std::endl;
+      fsl_destroy(h);
+      return FSL_E_IO;
+    }
+    rc = fsl_load_bonds(h, (int64_t)b.bi.size(), b.bi.data(), b.bj.data(), b.k.data(),
+                        b.r0.data(), (int64_t)b.fi.size(), b.fi.data(), b.fk.data(),
+                        b.fr0.data(), b.fxyz.data());
+    if (rc) {
+      std::cout << "ERROR: " << fsl_last_error() << std::endl;
+      fsl_destroy(h);
+      return rc;
+    }
+  }
+  {
+    std::ofstream fs(r.outputname + ".seed");
+    fs << r.cfg.seed << std::endl;
+  }
+  time_t t0 = time(NULL);
+  std::ofstream fp(r.outputname + ".particles"), fv(r.outputname + ".velocityParticles");
+  fp.precision(15);
+  fv.precision(15);
+  fp << "#NUMBER PARTICLES " << np << std::endl;
+  fv << "#NUMBER PARTICLES " << np << std::endl;
+  std::vector<double> pos(3 * np), frc(3 * np);
+  // src/runSchemeStokesLimit.cu:83, 163-285
+  int64_t step = -r.relax;
+  while (step < r.numsteps) {
+    // next step index s > step with s % samplefreq == 0 and s > 0, or the end
+    int64_t next = r.numsteps;
+    int64_t s0 = step + 1;
+    int64_t cand = ((s0 + r.samplefreq - 1) / r.samplefreq) * r.samplefreq;
+    if (s0 <= 0) cand = r.samplefreq;
+    if (cand < next) next = cand;
+    rc = fsl_step(h, next - step);
+    if (rc) break;
+    step = next;
+    if (!(step % r.samplefreq) && step > 0) {
+      std::cout << "Stokes Limit  " << step << std::endl;
+      rc = fsl_sync(h);
+      if (rc) {
+        std::cout << "ERROR IN KERNEL: " << fsl_last_error() << std::endl;
+        break;
+      }
+      if ((rc = fsl_get_positions(h, pos.data())) || (rc = fsl_get_forces(h, frc.data()))) break;
+      write_sample(fp, np, pos, step * r.cfg.dt);
+      write_sample(fv, np, frc, step * r.cfg.dt);
+    }
+  }
+  if (rc) std::cout << "ERROR: " << fsl_last_error() << std::endl;
+  if (!rc) rc = fsl_sync(h);
+  time_t t1 = time(NULL) - t0;
+  std::cout << std::endl << "TIME RUN_GPU                       " << t1 << std::endl << std::endl;
+  {
+    std::ofstream ft(r.outputname + ".time");
+    ft << "TIME RUN GPU     " << t1 << std::endl;
+  }
+  fsl_destroy(h);
+  if (!rc) std::cout << "END" << std::endl;
+  return rc;
+}

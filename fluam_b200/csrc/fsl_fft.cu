@@ -1,0 +1,513 @@
+// fsl_fft.cu -- the periodic Stokes solve of the Stokes-limit step:
+//   W = f + c div(Sigma)  ->  forward FFT  ->  shift, projection, 1/(eta k^2),
+//   unshift  ->  inverse FFT  ->  v
+// (src/runSchemeStokesLimit.cu:186-214 and 234-261; kernels
+// kernelConstructWstokesLimit(_2), kernelShift, kernelUpdateVstokesLimit,
+// doubleComplexToDoubleNormalized).  The reference runs 3 + 3 cuFFT Z2Z
+// transforms and 5 elementwise passes per solve in FP64; here the transform is
+// a hand-written FP32 mixed-radix Stockham FFT in shared memory, done as
+// three passes over the half spectrum:
+//   k_xfwd   builds W in registers from the fixed-point spread field and the
+//            noise, and transforms two real x-lines as one complex line;
+//   k_yfft   transforms along y (forward and inverse);
+//   k_zsolve transforms along z, applies the spectral multiplier to all three
+//            components of each mode, and transforms back along z;
+//   k_xinv   rebuilds two real x-lines from their half spectra.
+// The multiplier keeps Hermitian symmetry (the sign of sin(pi j/m) for
+// j > m/2 cancels between gradient and shift), so the real-to-complex form
+// equals the reference's Re(IFFT(...)) up to rounding.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "fsl_internal.cuh"
+
+namespace fsl {
+
+struct Radices {
+  int n;
+  int nst;
+  int r[14];
+};
+
+struct FftPlan {
+  Radices rx, ry, rz;
+  float2 *twx = nullptr, *twy = nullptr, *twz = nullptr;  // exp(-2 pi i t / m)
+  float *gx = nullptr, *gy = nullptr, *gz = nullptr;      // 2/h sin(pi j / m)
+  float2 *ex = nullptr, *ey = nullptr, *ez = nullptr;     // exp(+i pi j / m)
+  size_t smem_x = 0, smem_y = 0, smem_z = 0;
+  bool ok = false;
+};
+
+static bool factorize(int n, Radices& R) {
+  R.n = n;
+  R.nst = 0;
+  int m = n;
+  while (m % 4 == 0 && R.nst < 14) {
+    R.r[R.nst++] = 4;
+    m /= 4;
+  }
+  const int ps[5] = {2, 3, 5, 7, 11};
+  for (int pi = 0; pi < 5; ++pi)
+    while (m % ps[pi] == 0 && R.nst < 14) {
+      R.r[R.nst++] = ps[pi];
+      m /= ps[pi];
+    }
+  return m == 1;
+}
+
+// p-point DFT coefficients exp(-2 pi i t / p) for p = 5, 7, 11
+__constant__ float2 c_w5[5];
+__constant__ float2 c_w7[7];
+__constant__ float2 c_w11[11];
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// V[q] = sum_r v[r] exp(dir 2 pi i r q / P)
+template <int P>
+__device__ __forceinline__ void dft(float2 (&v)[P], int dir);
+
+template <>
+__device__ __forceinline__ void dft<2>(float2 (&v)[2], int) {
+  float2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+
+template <>
+__device__ __forceinline__ void dft<4>(float2 (&v)[4], int dir) {
+  float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+  float2 c = cadd(v[1], v[3]), e = csub(v[1], v[3]);
+  float2 d = make_float2(-dir * e.y, dir * e.x);  // (dir i) e
+  v[0] = cadd(a, c);
+  v[2] = csub(a, c);
+  v[1] = cadd(b, d);
+  v[3] = csub(b, d);
+}
+
+template <>
+__device__ __forceinline__ void dft<3>(float2 (&v)[3], int dir) {
+  const float s = 0.86602540378443864676f * dir;  // dir sqrt(3)/2
+  float2 t1 = cadd(v[1], v[2]);
+  float2 t2 = csub(v[1], v[2]);
+  float2 m = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+  float2 r = make_float2(-s * t2.y, s * t2.x);  // (i s) t2
+  v[0] = cadd(v[0], t1);
+  v[1] = cadd(m, r);
+  v[2] = csub(m, r);
+}
+
+template <int P>
+__device__ __forceinline__ void dft_generic(float2 (&v)[P], int dir, const float2* w) {
+  float2 out[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    float2 acc = v[0];
+#pragma unroll
+    for (int r = 1; r < P; ++r) {
+      float2 t = w[(r * q) % P];
+      if (dir > 0) t.y = -t.y;
+      acc = cadd(acc, cmul(v[r], t));
+    }
+    out[q] = acc;
+  }
+#pragma unroll
+  for (int q = 0; q < P; ++q) v[q] = out[q];
+}
+
+template <>
+__device__ __forceinline__ void dft<5>(float2 (&v)[5], int dir) { dft_generic<5>(v, dir, c_w5); }
+template <>
+__device__ __forceinline__ void dft<7>(float2 (&v)[7], int dir) { dft_generic<7>(v, dir, c_w7); }
+template <>
+__device__ __forceinline__ void dft<11>(float2 (&v)[11], int dir) { dft_generic<11>(v, dir, c_w11); }
+
+// One Stockham stage of radix P on nlines lines of length n stored in shared
+// memory with element k of line l at [k * LS + l]; Ns is the length of the
+// sub-transforms already done.  tw[t] = exp(-2 pi i t / n).
+template <int P>
+__device__ __forceinline__ void stage(const float2* __restrict__ A, float2* __restrict__ B, int n,
+                                      int LS, int nlines, int Ns, const float2* __restrict__ tw,
+                                      int dir) {
+  const int nbut = n / P;
+  const int tstride = n / (Ns * P);
+  const int total = nbut * nlines;
+  for (int w = threadIdx.x; w < total; w += blockDim.x) {
+    int l = w % nlines, j = w / nlines;
+    int k = j % Ns;
+    float2 v[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) v[r] = A[(j + r * nbut) * LS + l];
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < P; ++r) {
+        float2 t = tw[r * k * tstride];
+        if (dir > 0) t.y = -t.y;
+        v[r] = cmul(v[r], t);
+      }
+    }
+    dft<P>(v, dir);
+    int base = (j - k) * P + k;
+#pragma unroll
+    for (int r = 0; r < P; ++r) B[(base + r * Ns) * LS + l] = v[r];
+  }
+}
+
+// Full transform; returns the buffer (A or B) that holds the result.
+__device__ float2* fft_lines(float2* A, float2* B, int LS, int nlines, const Radices& R,
+                             const float2* tw, int dir) {
+  int Ns = 1;
+  for (int s = 0; s < R.nst; ++s) {
+    int p = R.r[s];
+    switch (p) {
+      case 4: stage<4>(A, B, R.n, LS, nlines, Ns, tw, dir); break;
+      case 2: stage<2>(A, B, R.n, LS, nlines, Ns, tw, dir); break;
+      case 3: stage<3>(A, B, R.n, LS, nlines, Ns, tw, dir); break;
+      case 5: stage<5>(A, B, R.n, LS, nlines, Ns, tw, dir); break;
+      case 7: stage<7>(A, B, R.n, LS, nlines, Ns, tw, dir); break;
+      default: stage<11>(A, B, R.n, LS, nlines, Ns, tw, dir); break;
+    }
+    __syncthreads();
+    float2* t = A;
+    A = B;
+    B = t;
+    Ns *= p;
+  }
+  return A;
+}
+
+constexpr int kXPairs = 16;  // x pass: row pairs (complex lines) per block
+constexpr int kYTile = 16;   // y pass: kx columns per block
+constexpr int kZTile = 8;    // z pass: kx columns per block (x 3 components)
+constexpr int kFftThreads = 512;
+
+// Noise terms of W for component comp at cell i (x,y,z) for one stress
+// sample d (src/stokesLimitFunctions.cu:2323-2367): the divergence of the
+// stochastic stress with diagonals at cell centres and off-diagonals on edges.
+__device__ __forceinline__ float stress_div(const Params& P, const float* __restrict__ d, int comp,
+                                            int x, int y, int z, int i, float a1x, float a1y,
+                                            float a1z, float a4x, float a4y, float a4z) {
+  const size_t nc = (size_t)P.nc;
+  const int mx = P.mx, my = P.my, mz = P.mz;
+  int xm = x == 0 ? mx - 1 : x - 1, xp = x == mx - 1 ? 0 : x + 1;
+  int ym = y == 0 ? my - 1 : y - 1, yp = y == my - 1 ? 0 : y + 1;
+  int zm = z == 0 ? mz - 1 : z - 1, zp = z == mz - 1 ? 0 : z + 1;
+  int rowyz = mx * (y + my * z);
+  if (comp == 0) {
+    int v3 = xp + rowyz, v1 = x + mx * (ym + my * z), v0 = x + mx * (y + my * zm);
+    return a1x * (__ldg(d + v3) - __ldg(d + i)) + a4y * (__ldg(d + nc + i) - __ldg(d + nc + v1)) +
+           a4z * (__ldg(d + 2 * nc + i) - __ldg(d + 2 * nc + v0));
+  } else if (comp == 1) {
+    int v4 = x + mx * (yp + my * z), v2 = xm + rowyz, v0 = x + mx * (y + my * zm);
+    return a1y * (__ldg(d + 3 * nc + v4) - __ldg(d + 3 * nc + i)) +
+           a4x * (__ldg(d + nc + i) - __ldg(d + nc + v2)) +
+           a4z * (__ldg(d + 4 * nc + i) - __ldg(d + 4 * nc + v0));
+  } else {
+    int v5 = x + mx * (y + my * zp), v2 = xm + rowyz, v1 = x + mx * (ym + my * z);
+    return a1z * (__ldg(d + 5 * nc + v5) - __ldg(d + 5 * nc + i)) +
+           a4x * (__ldg(d + 2 * nc + i) - __ldg(d + 2 * nc + v2)) +
+           a4y * (__ldg(d + 4 * nc + i) - __ldg(d + 4 * nc + v1));
+  }
+}
+
+// W build + real-to-complex transform along x.  Block (bx, comp) handles the
+// row pairs [bx*kXPairs, ...); row R = y + my z; the pair (2p, 2p+1) is
+// transformed as the complex line row_2p + i row_2p+1.
+__global__ void __launch_bounds__(kFftThreads)
+    k_xfwd(Params P, Radices R, const float2* __restrict__ tw,
+           const unsigned long long* __restrict__ grid, const float* __restrict__ noise,
+           int nsets, float nfac, const float* __restrict__ wext, float2* __restrict__ spec) {
+  extern __shared__ float2 smem[];
+  const int mx = P.mx, mxh = P.mxh;
+  const int LS = kXPairs + 1;
+  float2* A = smem;
+  float2* B = A + mx * LS;
+  float2* stw = B + mx * LS;
+  const int comp = blockIdx.y;
+  const int nrows = P.my * P.mz;
+  const int row0 = blockIdx.x * 2 * kXPairs;
+  for (int t = threadIdx.x; t < mx; t += blockDim.x) stw[t] = tw[t];
+
+  const float scale = (float)(kFixedInv / P.dV);
+  float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
+  float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
+  float a4x = (float)P.invdx * f4, a4y = (float)P.invdy * f4, a4z = (float)P.invdz * f4;
+  const size_t off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
+  float* Af = reinterpret_cast<float*>(A);
+  for (int e = threadIdx.x; e < 2 * kXPairs * mx; e += blockDim.x) {
+    int rl = e / mx, x = e - rl * mx;
+    int Rw = row0 + rl;
+    float w = 0.0f;
+    if (Rw < nrows) {
+      int i = x + mx * Rw;
+      if (wext) {
+        w = wext[(size_t)comp * P.nc + i];
+      } else {
+        int y = Rw % P.my, z = Rw / P.my;
+        long long g = (long long)grid[(size_t)comp * P.nc + i];
+        w = (float)((double)g * (double)scale);
+        w += stress_div(P, noise, comp, x, y, z, i, a1x, a1y, a1z, a4x, a4y, a4z);
+        if (nsets > 1)
+          w += stress_div(P, noise + off2, comp, x, y, z, i, a1x, a1y, a1z, a4x, a4y, a4z);
+      }
+    }
+    Af[2 * (x * LS + (rl >> 1)) + (rl & 1)] = w;
+  }
+  __syncthreads();
+  float2* Z = fft_lines(A, B, LS, kXPairs, R, stw, -1);
+  // split the two spectra: X_k = (Z_k + conj Z_-k)/2, Y_k = -i (Z_k - conj Z_-k)/2
+  for (int e = threadIdx.x; e < kXPairs * mxh; e += blockDim.x) {
+    int l = e / mxh, k = e - l * mxh;
+    int Rw = row0 + 2 * l;
+    if (Rw >= nrows) continue;
+    float2 zk = Z[k * LS + l];
+    float2 zm = Z[((mx - k) % mx) * LS + l];
+    float2 X = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    float2 Y = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    float2* out = spec + (size_t)comp * nrows * mxh;
+    out[(size_t)Rw * mxh + k] = X;
+    if (Rw + 1 < nrows) out[(size_t)(Rw + 1) * mxh + k] = Y;
+  }
+}
+
+// Complex transform along y of the half spectrum, in place.
+__global__ void __launch_bounds__(kFftThreads)
+    k_yfft(Params P, Radices R, const float2* __restrict__ tw, float2* __restrict__ spec, int dir) {
+  extern __shared__ float2 smem[];
+  const int my = P.my, mxh = P.mxh;
+  const int LS = kYTile;
+  float2* A = smem;
+  float2* B = A + my * LS;
+  float2* stw = B + my * LS;
+  const int kx0 = blockIdx.x * kYTile, z = blockIdx.y, comp = blockIdx.z;
+  for (int t = threadIdx.x; t < my; t += blockDim.x) stw[t] = tw[t];
+  float2* base = spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
+  for (int e = threadIdx.x; e < my * kYTile; e += blockDim.x) {
+    int l = e % kYTile, y = e / kYTile;
+    int kx = kx0 + l;
+    A[y * LS + l] = kx < mxh ? base[(size_t)y * mxh + kx] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2* Z = fft_lines(A, B, LS, kYTile, R, stw, dir);
+  for (int e = threadIdx.x; e < my * kYTile; e += blockDim.x) {
+    int l = e % kYTile, y = e / kYTile;
+    int kx = kx0 + l;
+    if (kx < mxh) base[(size_t)y * mxh + kx] = Z[y * LS + l];
+  }
+}
+
+// Transform along z, Stokes solve of every mode, inverse transform along z.
+// Per mode (src/stokesLimitFunctions.cu:2399-2451 with the shifts of
+// src/realToComplex.cu:263-303 and the 1/ncells of :40-59):
+//   W'_a = W_a e^{-i pi j_a/m_a};  G2 = |g|^2, g_a = 2/h_a sin(pi j_a/m_a)
+//   V'_a = (W'_a - g_a (g.W')/G2) / (eta G2);  v_a = V'_a e^{+i pi j_a/m_a}/nc
+//   and v = 0 for the zero mode.
+__global__ void __launch_bounds__(kFftThreads)
+    k_zsolve(Params P, Radices R, const float2* __restrict__ tw, const float* __restrict__ gx,
+             const float* __restrict__ gy, const float* __restrict__ gz,
+             const float2* __restrict__ ex, const float2* __restrict__ ey,
+             const float2* __restrict__ ez, float2* __restrict__ spec) {
+  extern __shared__ float2 smem[];
+  const int mz = P.mz, my = P.my, mxh = P.mxh;
+  const int NL = 3 * kZTile, LS = NL;
+  float2* A = smem;
+  float2* B = A + mz * LS;
+  float2* stw = B + mz * LS;
+  const int kx0 = blockIdx.x * kZTile, ky = blockIdx.y;
+  for (int t = threadIdx.x; t < mz; t += blockDim.x) stw[t] = tw[t];
+  const size_t cstride = (size_t)mz * my * mxh, zstride = (size_t)my * mxh;
+  for (int e = threadIdx.x; e < mz * NL; e += blockDim.x) {
+    int lx = e % kZTile, r = e / kZTile;
+    int z = r % mz, comp = r / mz;
+    int kx = kx0 + lx;
+    A[z * LS + comp * kZTile + lx] =
+        kx < mxh ? spec[comp * cstride + z * zstride + (size_t)ky * mxh + kx] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2* Z = fft_lines(A, B, LS, NL, R, stw, -1);
+  const float inv_eta = (float)(1.0 / P.eta);
+  const float inv_nc = 1.0f / (float)P.nc;
+  for (int e = threadIdx.x; e < mz * kZTile; e += blockDim.x) {
+    int lx = e % kZTile, kz = e / kZTile;
+    int kx = kx0 + lx;
+    if (kx >= mxh) continue;
+    float2* p = Z + kz * LS + lx;
+    float2 E[3] = {__ldg(ex + kx), __ldg(ey + ky), __ldg(ez + kz)};
+    float g[3] = {__ldg(gx + kx), __ldg(gy + ky), __ldg(gz + kz)};
+    float2 W[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float2 w = p[a * kZTile];
+      W[a] = make_float2(w.x * E[a].x + w.y * E[a].y, w.y * E[a].x - w.x * E[a].y);
+    }
+    float G2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+    if (kx == 0 && ky == 0 && kz == 0) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) p[a * kZTile] = make_float2(0.f, 0.f);
+      continue;
+    }
+    float invG2 = 1.0f / G2;
+    float2 GW = make_float2(g[0] * W[0].x + g[1] * W[1].x + g[2] * W[2].x,
+                            g[0] * W[0].y + g[1] * W[1].y + g[2] * W[2].y);
+    float fac = inv_eta * invG2 * inv_nc;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float2 V = make_float2((W[a].x - g[a] * GW.x * invG2) * fac, (W[a].y - g[a] * GW.y * invG2) * fac);
+      p[a * kZTile] = make_float2(V.x * E[a].x - V.y * E[a].y, V.y * E[a].x + V.x * E[a].y);
+    }
+  }
+  __syncthreads();
+  float2* other = (Z == A) ? B : A;
+  float2* Y = fft_lines(Z, other, LS, NL, R, stw, +1);
+  for (int e = threadIdx.x; e < mz * NL; e += blockDim.x) {
+    int lx = e % kZTile, r = e / kZTile;
+    int z = r % mz, comp = r / mz;
+    int kx = kx0 + lx;
+    if (kx < mxh) spec[comp * cstride + z * zstride + (size_t)ky * mxh + kx] = Y[z * LS + comp * kZTile + lx];
+  }
+}
+
+// Complex-to-real along x: Z_k = X_k + i Y_k (k <= mx/2) and its Hermitian
+// completion conj X_{m-k} + i conj Y_{m-k}; the inverse transform gives the
+// two real rows as real and imaginary parts.
+__global__ void __launch_bounds__(kFftThreads)
+    k_xinv(Params P, Radices R, const float2* __restrict__ tw, const float2* __restrict__ spec,
+           float* __restrict__ v) {
+  extern __shared__ float2 smem[];
+  const int mx = P.mx, mxh = P.mxh;
+  const int LS = kXPairs + 1;
+  float2* A = smem;
+  float2* B = A + mx * LS;
+  float2* stw = B + mx * LS;
+  const int comp = blockIdx.y;
+  const int nrows = P.my * P.mz;
+  const int row0 = blockIdx.x * 2 * kXPairs;
+  for (int t = threadIdx.x; t < mx; t += blockDim.x) stw[t] = tw[t];
+  const float2* in = spec + (size_t)comp * nrows * mxh;
+  for (int e = threadIdx.x; e < kXPairs * mxh; e += blockDim.x) {
+    int l = e / mxh, k = e - l * mxh;
+    int Rw = row0 + 2 * l;
+    float2 X = make_float2(0.f, 0.f), Y = make_float2(0.f, 0.f);
+    if (Rw < nrows) X = in[(size_t)Rw * mxh + k];
+    if (Rw + 1 < nrows) Y = in[(size_t)(Rw + 1) * mxh + k];
+    A[k * LS + l] = make_float2(X.x - Y.y, X.y + Y.x);
+    int km = mx - k;
+    if (k > 0 && km != k && km < mx) A[km * LS + l] = make_float2(X.x + Y.y, Y.x - X.y);
+  }
+  __syncthreads();
+  float2* Z = fft_lines(A, B, LS, kXPairs, R, stw, +1);
+  const float* Zf = reinterpret_cast<const float*>(Z);
+  float* out = v + (size_t)comp * P.nc;
+  for (int e = threadIdx.x; e < 2 * kXPairs * mx; e += blockDim.x) {
+    int rl = e / mx, x = e - rl * mx;
+    int Rw = row0 + rl;
+    if (Rw < nrows) out[(size_t)Rw * mx + x] = Zf[2 * (x * LS + (rl >> 1)) + (rl & 1)];
+  }
+}
+
+// ------------------------------------------------------------ host side ---
+static bool upload_table(const std::vector<float2>& h, float2** d) {
+  if (cudaMalloc(d, sizeof(float2) * h.size()) != cudaSuccess) return false;
+  return cudaMemcpy(*d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+}
+static bool upload_table(const std::vector<float>& h, float** d) {
+  if (cudaMalloc(d, sizeof(float) * h.size()) != cudaSuccess) return false;
+  return cudaMemcpy(*d, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
+FftPlan* fft_plan_create(const Params& P) {
+  FftPlan* fp = new FftPlan();
+  if (!factorize(P.mx, fp->rx) || !factorize(P.my, fp->ry) || !factorize(P.mz, fp->rz)) {
+    delete fp;
+    return nullptr;
+  }
+  // small-DFT coefficient tables (idempotent)
+  float2 w5[5], w7[7], w11[11];
+  for (int t = 0; t < 5; ++t) w5[t] = make_float2((float)cos(2 * M_PI * t / 5), (float)-sin(2 * M_PI * t / 5));
+  for (int t = 0; t < 7; ++t) w7[t] = make_float2((float)cos(2 * M_PI * t / 7), (float)-sin(2 * M_PI * t / 7));
+  for (int t = 0; t < 11; ++t) w11[t] = make_float2((float)cos(2 * M_PI * t / 11), (float)-sin(2 * M_PI * t / 11));
+  cudaMemcpyToSymbol(c_w5, w5, sizeof(w5));
+  cudaMemcpyToSymbol(c_w7, w7, sizeof(w7));
+  cudaMemcpyToSymbol(c_w11, w11, sizeof(w11));
+
+  const int m[3] = {P.mx, P.my, P.mz};
+  const double invd[3] = {P.invdx, P.invdy, P.invdz};
+  float2** tws[3] = {&fp->twx, &fp->twy, &fp->twz};
+  float** gs[3] = {&fp->gx, &fp->gy, &fp->gz};
+  float2** es[3] = {&fp->ex, &fp->ey, &fp->ez};
+  double pi = 4. * atan(1.);
+  for (int a = 0; a < 3; ++a) {
+    std::vector<float2> tw(m[a]), e(m[a]);
+    std::vector<float> g(m[a]);
+    for (int t = 0; t < m[a]; ++t) {
+      double ang = 2.0 * pi * (double)t / (double)m[a];
+      tw[t] = make_float2((float)cos(ang), (float)-sin(ang));
+      // src/initializePrefactorFourierSpace.cu:48-66
+      g[t] = (float)(2 * invd[a] * sin(pi * t / double(m[a])));
+      e[t] = make_float2((float)cos(pi * t / double(m[a])), (float)sin(pi * t / double(m[a])));
+    }
+    if (!upload_table(tw, tws[a]) || !upload_table(g, gs[a]) || !upload_table(e, es[a])) {
+      fft_plan_destroy(fp);
+      return nullptr;
+    }
+  }
+  fp->smem_x = sizeof(float2) * (2 * (size_t)P.mx * (kXPairs + 1) + P.mx);
+  fp->smem_y = sizeof(float2) * (2 * (size_t)P.my * kYTile + P.my);
+  fp->smem_z = sizeof(float2) * (2 * (size_t)P.mz * 3 * kZTile + P.mz);
+  size_t lim = 227 * 1024;
+  if (fp->smem_x > lim || fp->smem_y > lim || fp->smem_z > lim) {
+    fft_plan_destroy(fp);
+    return nullptr;
+  }
+  cudaFuncSetAttribute(k_xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_x);
+  cudaFuncSetAttribute(k_xinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_x);
+  cudaFuncSetAttribute(k_yfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_y);
+  cudaFuncSetAttribute(k_zsolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_z);
+  fp->ok = true;
+  return fp;
+}
+
+void fft_plan_destroy(FftPlan* fp) {
+  if (!fp) return;
+  cudaFree(fp->twx);
+  cudaFree(fp->twy);
+  cudaFree(fp->twz);
+  cudaFree(fp->gx);
+  cudaFree(fp->gy);
+  cudaFree(fp->gz);
+  cudaFree(fp->ex);
+  cudaFree(fp->ey);
+  cudaFree(fp->ez);
+  delete fp;
+}
+
+void launch_solve(const Params& P, FftPlan* fp, const unsigned long long* grid, const float* noise,
+                  int nsets, const float* wext, float2* spec, float* v, cudaStream_t s,
+                  Prof* prof) {
+  Prof dummy;
+  Prof& pr = prof ? *prof : dummy;
+  const int nrows = P.my * P.mz;
+  const int npairs = (nrows + 1) / 2;
+  dim3 gx((npairs + kXPairs - 1) / kXPairs, 3);
+  float nfac = nsets > 1 ? (float)sqrt(0.5) : (float)sqrt(2.0);
+  pr.mark(s, "xfwd");
+  k_xfwd<<<gx, kFftThreads, fp->smem_x, s>>>(P, fp->rx, fp->twx, grid, noise, nsets, nfac, wext, spec);
+  dim3 gy((P.mxh + kYTile - 1) / kYTile, P.mz, 3);
+  pr.mark(s, "yfft");
+  k_yfft<<<gy, kFftThreads, fp->smem_y, s>>>(P, fp->ry, fp->twy, spec, -1);
+  dim3 gz((P.mxh + kZTile - 1) / kZTile, P.my);
+  pr.mark(s, "zsolve");
+  k_zsolve<<<gz, kFftThreads, fp->smem_z, s>>>(P, fp->rz, fp->twz, fp->gx, fp->gy, fp->gz, fp->ex,
+                                               fp->ey, fp->ez, spec);
+  pr.mark(s, "yfft");
+  k_yfft<<<gy, kFftThreads, fp->smem_y, s>>>(P, fp->ry, fp->twy, spec, +1);
+  pr.mark(s, "xinv");
+  k_xinv<<<gx, kFftThreads, fp->smem_x, s>>>(P, fp->rx, fp->twx, spec, v);
+  pr.count(5);
+}
+
+}  // namespace fsl

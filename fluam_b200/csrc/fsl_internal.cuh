@@ -1,0 +1,242 @@
+// fsl_internal.cuh -- shared definitions of the sm_100a Stokes-limit path.
+//
+// Numerics of the CUDA path (the error against the FP64 oracle is checked by
+// the tests for each of these choices):
+//   * particle positions, their increments and the cell-index arithmetic are
+//     FP64, evaluated with explicitly rounded operations (__dmul_rn, ...), so
+//     cell lists and stencil choices are bit-identical to the FP64 oracle;
+//   * forces are FP64 (few per step);
+//   * spreading accumulates 64-bit fixed point (2^-40) with integer atomics,
+//     so the spread field is independent of the order of the atomics and the
+//     whole step is bit-reproducible run to run;
+//   * kernel weights, the noise, the fields, the FFTs and the spectral
+//     multiplier are FP32.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fsl {
+
+constexpr double kFixedScale = 1099511627776.0;      // 2^40
+constexpr double kFixedInv = 1.0 / 1099511627776.0;  // 2^-40
+constexpr double kFixedMax = 4611686018427387904.0;  // 2^62
+constexpr double kRfdDelta = 0.001;  // src/stokesLimitFunctions.cu:1719
+constexpr int kLjTableSize = 4096;   // src/initForcesNonBonded.cu:36
+
+enum { ERR_ANY = 0, ERR_BITS = 1 };
+
+// Everything a kernel needs about one instance, passed by value.
+struct Params {
+  // fluid grid
+  int mx, my, mz, mxh;  // mxh = mx/2 + 1 (half spectrum along x)
+  int nc;
+  double lx, ly, lz, dx, dy, dz;
+  double invdx, invdy, invdz, invlx, invly, invlz, dV;
+  // non-bonded neighbour grid, m = max(3, int(L / rc))
+  int mnx, mny, mnz, mN;
+  double invdnx, invdny, invdnz;  // m / L
+  // particles and physics
+  int np;
+  int kernel;  // 3 or 4
+  int pair, nonbonded, rfd, bonded;
+  int has_extra;
+  double cutoff, cutoff2, invcut2, soft_eps;
+  double eta, kT, dt, extra_mob, fact1, fact2, fact4;
+  uint64_t seed;
+  uint64_t noise_n;  // 12 nc + 9 np
+};
+
+// ---------------------------------------------------------------- Philox ---
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): multipliers
+// 0xD2511F53 / 0xCD9E8D57, key increments 0x9E3779B9 / 0xBB67AE85.
+__host__ __device__ inline uint32_t mulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * (uint64_t)b) >> 32);
+#endif
+}
+
+__host__ __device__ inline uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0 = mulhi32(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    uint32_t hi1 = mulhi32(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// The four normal deviates with noise indices 4b .. 4b+3 of draw t.  Word w
+// becomes the uniform (2 (w >> 9) + 1) 2^-24 in (0,1), exact in FP32;
+// Box-Muller on the pairs (u0,u1) and (u2,u3).
+__device__ inline float4 philox_normal4(uint64_t seed, uint64_t t, uint64_t b) {
+  uint4 c = make_uint4((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)t, (uint32_t)(t >> 32));
+  uint4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const float s24 = 5.9604644775390625e-08f;  // 2^-24
+  float u0 = (float)(2u * (r.x >> 9) + 1u) * s24;
+  float u1 = (float)(2u * (r.y >> 9) + 1u) * s24;
+  float u2 = (float)(2u * (r.z >> 9) + 1u) * s24;
+  float u3 = (float)(2u * (r.w >> 9) + 1u) * s24;
+  float ra = sqrtf(-2.0f * logf(u0));
+  float rb = sqrtf(-2.0f * logf(u2));
+  float sa, ca, sb, cb;
+  sincospif(2.0f * u1, &sa, &ca);
+  sincospif(2.0f * u3, &sb, &cb);
+  return make_float4(ra * ca, ra * sa, rb * cb, rb * sb);
+}
+
+// --------------------------------------------------- exact cell indices ---
+__device__ __forceinline__ double dsgn(double r) { return (double)((r > 0) - (r < 0)); }
+
+// r - int(r/L + sign(r)/2) L, src/stokesLimitFunctions.cu:41-49
+__device__ __forceinline__ double minimage(double r, double invL, double L) {
+  double t = __dadd_rn(__dmul_rn(r, invL), __dmul_rn(0.5, dsgn(r)));
+  return __dsub_rn(r, __dmul_rn((double)(int)t, L));
+}
+
+// int(r m/L + m/2) % m of a wrapped coordinate.  For finite coordinates
+// within the box this is the reference's formula; any other input (NaN, a
+// coordinate beyond the int range) still lands in [0, m), so no index
+// derived from it can leave its array, and the caller flags the value.
+__device__ __forceinline__ int cellidx(double r, double invd, int m) {
+  int j = ((int)__dadd_rn(__dmul_rn(r, invd), __dmul_rn(0.5, (double)m))) % m;
+  return j < 0 ? j + m : j;
+}
+
+__device__ __forceinline__ int nb_cell(const Params& P, double x, double y, double z) {
+  int jx = cellidx(minimage(x, P.invlx, P.lx), P.invdnx, P.mnx);
+  int jy = cellidx(minimage(y, P.invly, P.ly), P.invdny, P.mny);
+  int jz = cellidx(minimage(z, P.invlz, P.lz), P.invdnz, P.mnz);
+  return jx + jy * P.mnx + jz * P.mnx * P.mny;
+}
+
+// ------------------------------------------------------- Peskin kernels ---
+// 3-point kernel, src/deltaGPU.cu:57-68 (argument = distance / h)
+__device__ __forceinline__ float delta3f(float x) {
+  x = fabsf(x);
+  if (x > 1.5f) return 0.0f;
+  if (x < 0.5f) return (1.0f + sqrtf(1.0f - 3.0f * x * x)) * (1.0f / 3.0f);
+  float y = 1.0f - x;
+  return (5.0f - 3.0f * x - sqrtf(fmaxf(1.0f - 3.0f * y * y, 0.0f))) * (1.0f / 6.0f);
+}
+
+// 4-point kernel (Peskin, Acta Numerica 2002), the 3-D extension of the
+// fractional form of src/deltaGPU.cu:44-53.
+__device__ __forceinline__ float delta4f(float x) {
+  x = fabsf(x);
+  if (x >= 2.0f) return 0.0f;
+  if (x <= 1.0f) return (3.0f - 2.0f * x + sqrtf(1.0f + 4.0f * x - 4.0f * x * x)) * 0.125f;
+  return (5.0f - 2.0f * x - sqrtf(fmaxf(-7.0f + 12.0f * x - 4.0f * x * x, 0.0f))) * 0.125f;
+}
+
+// Stencil of one particle for field component comp: first node index per
+// dimension and the weights.  Nodes of component comp in dimension d sit at
+// (j + 1/2) h - L/2, plus h/2 when d == comp.  posc picks the nodes, posw sets
+// the weights (they differ only in the reference's RFD quirk).
+struct Stencil {
+  int j0[3];
+  float w[3][4];
+};
+
+__device__ __forceinline__ void make_stencil(const Params& P, int comp, const double posc[3],
+                                             const double posw[3], Stencil& st) {
+  const int m[3] = {P.mx, P.my, P.mz};
+  const double h[3] = {P.dx, P.dy, P.dz};
+  const double invd[3] = {P.invdx, P.invdy, P.invdz};
+  const double L[3] = {P.lx, P.ly, P.lz};
+  const double invL[3] = {P.invlx, P.invly, P.invlz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double off = (d == comp) ? __dmul_rn(0.5, h[d]) : 0.0;
+    if (P.kernel == 3) {
+      double r = minimage(__dsub_rn(posc[d], off), invL[d], L[d]);
+      int jc = cellidx(r, invd[d], m[d]);
+      st.j0[d] = (jc - 1 + m[d]) % m[d];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        int j = (st.j0[d] + k) % m[d];
+        double node = ((double)j + 0.5) * h[d] - 0.5 * L[d];
+        double rr = minimage((posw[d] - node) - off, invL[d], L[d]);
+        st.w[d][k] = delta3f((float)(rr * invd[d]));
+      }
+      st.w[d][3] = 0.0f;
+    } else {
+      double r = minimage(__dsub_rn(__dsub_rn(posc[d], off), __dmul_rn(0.5, h[d])), invL[d], L[d]);
+      int jb = cellidx(r, invd[d], m[d]);
+      st.j0[d] = (jb - 1 + m[d]) % m[d];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        int j = (st.j0[d] + k) % m[d];
+        double node = ((double)j + 0.5) * h[d] - 0.5 * L[d] + off;
+        double rr = minimage(posw[d] - node, invL[d], L[d]);
+        st.w[d][k] = delta4f((float)(rr * invd[d]));
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void set_err(int* err, int bit) {
+  atomicOr(&err[ERR_BITS], bit);
+  err[ERR_ANY] = 1;
+}
+
+}  // namespace fsl
+
+// ------------------------------------------------- host-side launchers ---
+// Declared here, defined in the .cu files; all enqueue on `s`.
+namespace fsl {
+
+// Stage timer: mark(name) records an event on the stream; the interval up to
+// the next mark is charged to `name` (nullptr closes the last interval).
+// Off by default; when on, the marks are captured into the step's graph too.
+struct Prof {
+  static constexpr int kMax = 64;
+  bool on = false;
+  cudaEvent_t ev[kMax] = {};
+  const char* name[kMax] = {};
+  int used = 0;
+  int launches = 0;  // kernels of this library enqueued in the current step
+  void mark(cudaStream_t s, const char* n) {
+    if (!on || used >= kMax) return;
+    if (!ev[used]) cudaEventCreate(&ev[used]);
+    // External: under stream capture this becomes an event-record node of
+    // the graph (a plain record would only express a dependency).
+    cudaEventRecordWithFlags(ev[used], s, cudaEventRecordExternal);
+    name[used++] = n;
+  }
+  void count(int k) { launches += k; }
+};
+void launch_noise(const Params& P, const uint64_t* t_dev, float* out, cudaStream_t s);
+void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t count, float* out,
+                        cudaStream_t s);
+void launch_cells(const Params& P, const double* q, int* cell_of, int* cnt, int* start,
+                  int* fill, int* tmp, int* sorted, int* bsum, int* err, cudaStream_t s);
+void launch_forces(const Params& P, const double* q, const int* cell_of, const int* start,
+                   const int* sorted, const int* bpp_cnt, const int* bpp_off, const int* bpp_idx,
+                   const double* bpp_k, const double* bpp_r0, const int* bfp_cnt,
+                   const int* bfp_off, const double* bfp_k, const double* bfp_r0,
+                   const double* bfp_xyz, const float* ljtab, double* F, int* err,
+                   cudaStream_t s);
+void launch_spread_force(const Params& P, const double* q, const double* F,
+                         unsigned long long* grid, int* err, cudaStream_t s);
+void launch_spread_drift(const Params& P, const double* q, const float* noise, int sign,
+                         unsigned long long* grid, int* err, cudaStream_t s);
+void launch_interp_update(const Params& P, int stage, const double* qpos, const double* q0,
+                          const double* F, const float* noise, const float* v, double* qout,
+                          int* err, cudaStream_t s);
+void launch_interp(const Params& P, const double* qpos, const float* v, double* u,
+                   cudaStream_t s);
+void launch_step_counter(uint64_t* t_dev, cudaStream_t s);
+
+struct FftPlan;  // defined in fsl_fft.cu
+FftPlan* fft_plan_create(const Params& P);
+void fft_plan_destroy(FftPlan* fp);
+// W source: the fixed-point spread grid plus the stochastic stress of draw t
+// (nsets = 1 or 2) when wext == nullptr, or a given float field wext.
+void launch_solve(const Params& P, FftPlan* fp, const unsigned long long* grid, const float* noise,
+                  int nsets, const float* wext, float2* spec, float* v, cudaStream_t s,
+                  Prof* prof = nullptr);
+}  // namespace fsl

@@ -1,0 +1,195 @@
+"""Python mirror of the Stokes-limit scheme over the libfluamsl C ABI.
+
+``StokesLimit`` owns one device instance (the state the reference keeps in
+process globals between ``schemeStokesLimit`` and ``runSchemeStokesLimit``,
+src/schemeStokesLimit.cu:27-98).  ``run_data_main`` is the drop-in driver of
+``fluam data.main`` for the stokesLimit scheme.  Arrays are numpy: particle
+arrays have shape (3, np) (x, y and z rows, as rxParticle/ryParticle/
+rzParticle), fields have shape (3, mz, my, mx).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE, check
+
+__all__ = ["StokesLimit", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
+           "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE"]
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair=PAIR_TABLE_LJ,
+                soft_epsilon=1.0, rfd=RFD_REFERENCE, nonbonded=1, extra_mobility=0.0, seed=0,
+                device=-1):
+    c = _lib.Config()
+    _lib.load().fsl_config_defaults(ctypes.byref(c))
+    c.mx, c.my, c.mz = (int(x) for x in cells)
+    c.lx, c.ly, c.lz = (float(x) for x in box)
+    c.shearviscosity, c.temperature, c.dt, c.cutoff = eta, kT, dt, cutoff
+    c.kernel, c.pair, c.soft_epsilon, c.rfd = kernel, pair, soft_epsilon, rfd
+    c.nonbonded, c.extra_mobility, c.seed, c.device = nonbonded, extra_mobility, seed, device
+    return c
+
+
+class StokesLimit:
+    """One Stokes-limit instance on the GPU."""
+
+    def __init__(self, config, q):
+        self.L = _lib.load()
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(3, -1)
+        self.np = q.shape[1]
+        self.cfg = config
+        self.shape = (config.mz, config.my, config.mx)
+        self.nc = config.mx * config.my * config.mz
+        h = ctypes.c_void_p()
+        check(self.L.fsl_create(ctypes.byref(config), self.np, _dp(q), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fsl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- scheme ------------------------------------------------------------
+    def load_bonds(self, bi, bj, k, r0, fi=None, fk=None, fr0=None, fxyz=None):
+        bi = np.ascontiguousarray(bi, dtype=np.int32)
+        bj = np.ascontiguousarray(bj, dtype=np.int32)
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        r0 = np.ascontiguousarray(r0, dtype=np.float64)
+        if fi is None:
+            fi, fk, fr0, fxyz = np.zeros(0, np.int32), np.zeros(0), np.zeros(0), np.zeros((0, 3))
+        fi = np.ascontiguousarray(fi, dtype=np.int32)
+        fk = np.ascontiguousarray(fk, dtype=np.float64)
+        fr0 = np.ascontiguousarray(fr0, dtype=np.float64)
+        fxyz = np.ascontiguousarray(fxyz, dtype=np.float64).reshape(-1, 3)
+        check(self.L.fsl_load_bonds(self.h, len(bi), _ip(bi), _ip(bj), _dp(k), _dp(r0), len(fi),
+                                    _ip(fi), _dp(fk), _dp(fr0), _dp(fxyz)))
+
+    def step(self, n=1):
+        check(self.L.fsl_step(self.h, int(n)))
+
+    def sync(self):
+        check(self.L.fsl_sync(self.h))
+
+    def set_graph(self, enable):
+        check(self.L.fsl_set_graph(self.h, 1 if enable else 0))
+
+    def positions(self):
+        out = np.empty((3, self.np))
+        check(self.L.fsl_get_positions(self.h, _dp(out)))
+        return out
+
+    def set_positions(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(3, self.np)
+        check(self.L.fsl_set_positions(self.h, _dp(q)))
+
+    def forces(self):
+        out = np.empty((3, self.np))
+        check(self.L.fsl_get_forces(self.h, _dp(out)))
+        return out
+
+    def velocity(self):
+        out = np.empty((3,) + self.shape, dtype=np.float32)
+        check(self.L.fsl_get_velocity(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def status(self):
+        st = _lib.Status()
+        check(self.L.fsl_get_status(self.h, ctypes.byref(st)))
+        return {"step": st.step, "error_bits": st.error_bits, "np": st.np, "nc": st.nc,
+                "graph": bool(st.graph), "launches_per_step": st.launches_per_step}
+
+    def profile(self, enable=True):
+        """Per-stage CUDA-event timing of every step (clears the totals)."""
+        check(self.L.fsl_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        n = ctypes.c_int32()
+        check(self.L.fsl_profile_read(self.h, None, 0, ctypes.byref(n)))
+        arr = (_lib.StageTime * max(n.value, 1))()
+        check(self.L.fsl_profile_read(self.h, arr, n.value, ctypes.byref(n)))
+        return {a.name.decode(): {"launches": a.launches, "total_ms": a.total_ms}
+                for a in arr[:n.value]}
+
+    def set_step(self, t):
+        check(self.L.fsl_set_step(self.h, int(t)))
+
+    def clear_errors(self):
+        check(self.L.fsl_clear_errors(self.h))
+
+    # -- components --------------------------------------------------------
+    def neighbor_grid(self):
+        d = np.zeros(3, np.int32)
+        check(self.L.fsl_neighbor_grid(self.h, _ip(d)))
+        return tuple(int(x) for x in d)
+
+    def cell_list(self):
+        m = int(np.prod(self.neighbor_grid()))
+        cell_of = np.empty(self.np, np.int32)
+        start = np.empty(m + 1, np.int32)
+        srt = np.empty(self.np, np.int32)
+        check(self.L.fsl_cell_list(self.h, _ip(cell_of), _ip(start), _ip(srt)))
+        return cell_of, start, srt
+
+    def compute_forces(self):
+        F = np.empty((3, self.np))
+        check(self.L.fsl_compute_forces(self.h, _dp(F)))
+        return F
+
+    def spread(self, F):
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        f = np.empty((3,) + self.shape)
+        check(self.L.fsl_spread(self.h, _dp(F), _dp(f)))
+        return f
+
+    def solve(self, W):
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        v = np.empty((3,) + self.shape)
+        check(self.L.fsl_solve(self.h, _dp(W), _dp(v)))
+        return v
+
+    def interpolate(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        u = np.empty((3, self.np))
+        check(self.L.fsl_interpolate(self.h, _dp(v), _dp(u)))
+        return u
+
+    def noise(self, t, first, count):
+        out = np.empty(count, np.float32)
+        check(self.L.fsl_noise(self.h, int(t), int(first), int(count),
+                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+
+def run_data_main(path):
+    """Run `fluam data.main` for the stokesLimit scheme; raises on failure."""
+    return check(_lib.load().fsl_run_data_main(str(path).encode()))
+
+
+def parse_data_main(path):
+    c = _lib.Config()
+    ns, sf, rx, npart = (ctypes.c_int64() for _ in range(4))
+    check(_lib.load().fsl_parse_data_main(str(path).encode(), ctypes.byref(c), ctypes.byref(ns),
+                                          ctypes.byref(sf), ctypes.byref(rx), ctypes.byref(npart)))
+    return c, {"numsteps": ns.value, "samplefreq": sf.value, "numstepsRelaxation": rx.value,
+               "numberparticles": npart.value}

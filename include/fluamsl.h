@@ -1,0 +1,180 @@
+/* fluamsl.h -- C ABI of libfluamsl, a B200 (sm_100a) implementation of
+ * fluam's Stokes-limit immersed-boundary step ("Brownian dynamics without
+ * Green's functions", the midpoint scheme of Delong et al., JCP 140, 134110,
+ * 2014, Sec. IV.B).
+ *
+ * The reference path this library replaces is a set of process globals and
+ * argument-less functions:
+ *   bool schemeStokesLimit()     src/schemeStokesLimit.cu:27-98
+ *   bool runSchemeStokesLimit()  src/runSchemeStokesLimit.cu:21-298
+ *   main(argc, argv)             src/main.cpp:28-112 (loadDataMain + dispatch)
+ * Here the state lives in an opaque handle.  All functions return 0 on
+ * success and a negative FSL_E* code on failure (no exceptions cross the
+ * boundary); fsl_last_error() gives a one-line message for the calling
+ * thread.  The caller owns every host buffer; the handle owns every device
+ * buffer.  A handle is used by one host thread at a time.
+ *
+ * Array layouts follow the reference: particle arrays are structure-of-arrays
+ * x[0..np) | y[0..np) | z[0..np) in double precision (rxParticle, ...); fields
+ * are component-major [3][nc] with cell index x + y mx + z mx my, and the
+ * x component of cell i lives on the +x face of that cell.
+ */
+#ifndef FLUAMSL_H
+#define FLUAMSL_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+  FSL_OK = 0,
+  FSL_E_ARG = -1,        /* invalid argument or configuration            */
+  FSL_E_CUDA = -2,       /* CUDA runtime error (message has the text)     */
+  FSL_E_NOMEM = -3,      /* device allocation failed                      */
+  FSL_E_KERNEL = -4,     /* a kernel raised its error word (see status)   */
+  FSL_E_IO = -5,         /* file could not be read or written             */
+  FSL_E_INPUT = -6       /* data.main keyword error (ERROR INPUT FILE)    */
+};
+
+/* ---- options that extend the reference ------------------------------- */
+enum { FSL_PAIR_NONE = 0, FSL_PAIR_TABLE_LJ = 1, FSL_PAIR_SOFT = 2 };
+enum { FSL_RFD_REFERENCE = 0, FSL_RFD_PAPER = 1 };
+
+/* Bits of fsl_status.error_bits (device error word, sticky until cleared). */
+enum {
+  FSL_ERRBIT_FIXED_SAT = 1,   /* fixed-point spread value out of range      */
+  FSL_ERRBIT_NONFINITE = 2,   /* non-finite force or position               */
+  FSL_ERRBIT_GRID = 4         /* internal index check failed (access skipped) */
+};
+
+/* Configuration of one instance.  Field names follow data.main keywords
+ * (src/loadDataMain.cu:173-683) where one exists. */
+typedef struct fsl_config {
+  int32_t mx, my, mz;            /* cells                                   */
+  int32_t kernel;                /* Peskin kernel points: 3 (reference) or 4 */
+  double lx, ly, lz;             /* celldimension                           */
+  double shearviscosity;         /* eta                                     */
+  double temperature;            /* kT                                      */
+  double dt;
+  double cutoff;                 /* pair cutoff rc (neighbour grid m=max(3,L/rc)) */
+  double extra_mobility;         /* extraMobility (0 = off)                 */
+  double soft_epsilon;           /* epsilon of U = eps (1 - r/rc)^2         */
+  uint64_t seed;
+  int32_t pair;                  /* FSL_PAIR_*; the reference is TABLE_LJ   */
+  int32_t rfd;                   /* FSL_RFD_*                               */
+  int32_t nonbonded;             /* computeNonBondedForces                  */
+  int32_t device;                /* setDevice; -1 keeps the current device  */
+} fsl_config;
+
+typedef struct fsl_status {
+  uint64_t step;                 /* steps taken since creation              */
+  int32_t error_bits;            /* FSL_ERRBIT_*                            */
+  int32_t np;
+  int64_t nc;
+  int32_t graph;                 /* 1 if steps replay a captured CUDA graph */
+  int32_t launches_per_step;     /* kernels of this library in one step     */
+} fsl_status;
+
+/* Accumulated CUDA-event time of one stage of the step (profiling on). */
+typedef struct fsl_stage_time {
+  char name[32];
+  int64_t launches;
+  double total_ms;
+} fsl_stage_time;
+
+typedef struct fsl_handle fsl_handle;
+
+/* Fill cfg with the reference's defaults (src/loadDataMain.cu:175-299) plus
+ * kernel 3, TABLE_LJ, reference RFD.  Replaces nothing; convenience. */
+void fsl_config_defaults(fsl_config* cfg);
+
+/* Create an instance and upload np positions (SoA, double).  Replaces the
+ * set-up half of schemeStokesLimit (src/schemeStokesLimit.cu:30-58:
+ * createCells, createCellsStokesLimitGPU, createBoundariesRK2GPU). */
+int fsl_create(const fsl_config* cfg, int64_t np, const double* q, fsl_handle** out);
+
+/* Harmonic bonds and fixed-point tethers, in the reference's file order
+ * (src/initializeBondedForces.cpp:31-170, src/createBondedForcesGPU.cu:21-133).
+ * fxyz holds 3 doubles per tether. */
+int fsl_load_bonds(fsl_handle* h, int64_t nbonds, const int32_t* bi, const int32_t* bj,
+                   const double* k, const double* r0, int64_t nfixed, const int32_t* fi,
+                   const double* fk, const double* fr0, const double* fxyz);
+
+/* Advance nsteps midpoint steps (the body of the loop in
+ * src/runSchemeStokesLimit.cu:163-285).  Runs on the handle's stream; returns
+ * after the work is queued unless an error check needs the device. */
+int fsl_step(fsl_handle* h, int64_t nsteps);
+
+/* Block until queued work is done and read the device error word. */
+int fsl_sync(fsl_handle* h);
+
+/* Particle positions q^n (gpuToHostStokesLimit, src/gpuToHostStokesLimit.cu:36-38). */
+int fsl_get_positions(fsl_handle* h, double* out);
+int fsl_set_positions(fsl_handle* h, const double* in);
+/* Particle forces F^{n+1/2} of the last step: what the reference writes to
+ * <out>.velocityParticles (src/gpuToHostStokesLimit.cu:41-43). */
+int fsl_get_forces(fsl_handle* h, double* out);
+/* Fluid velocity of the last solve, float [3][nc] (not written by the
+ * reference on this path; exposed for checks). */
+int fsl_get_velocity(fsl_handle* h, float* out);
+int fsl_get_status(fsl_handle* h, fsl_status* st);
+int fsl_set_step(fsl_handle* h, uint64_t step);
+int fsl_clear_errors(fsl_handle* h);
+/* Capture one step into a CUDA graph and replay it from then on (on by
+ * default once the first step has run; 0 turns it off). */
+int fsl_set_graph(fsl_handle* h, int enable);
+/* The handle's CUDA stream (cudaStream_t), for callers that order work. */
+void* fsl_stream(fsl_handle* h);
+/* Per-stage timing with CUDA events recorded on the handle's stream between
+ * the stages of every step (captured into the graph as well).  While it is
+ * on, fsl_step waits for each step to finish.  fsl_profile(h, 1) also clears
+ * the accumulated times.  The reference only times the whole run
+ * (src/saveTime.cpp:24-45). */
+int fsl_profile(fsl_handle* h, int enable);
+int fsl_profile_read(fsl_handle* h, fsl_stage_time* out, int32_t max, int32_t* n);
+void fsl_destroy(fsl_handle* h);
+const char* fsl_last_error(void);
+
+/* ---- drop-in driver ---------------------------------------------------- */
+/* Run a whole fluam Stokes-limit job from a data.main file: the same
+ * keywords, the same output files (<outputname>.data.main, .cuda, .seed,
+ * .time, .particles, .velocityParticles).  Mirrors main() + schemeStokesLimit()
+ * (src/main.cpp:28-112, src/schemeStokesLimit.cu:27-98).  Returns 0 on
+ * success. */
+int fsl_run_data_main(const char* path);
+/* Parse a data.main into cfg and the run controls without touching a GPU
+ * (src/loadDataMain.cu:173-683).  numsteps/samplefreq/relax may be NULL. */
+int fsl_parse_data_main(const char* path, fsl_config* cfg, int64_t* numsteps,
+                        int64_t* samplefreq, int64_t* relax, int64_t* np);
+
+/* ---- component entry points (one stage of the step each) --------------- */
+/* Non-bonded cell list at the current positions: cell of each particle, the
+ * start offset of every neighbour-grid cell (mN+1 entries) and the particle
+ * indices sorted by cell, ascending inside a cell.  Replaces
+ * findNeighborParticlesStokesLimit_1 (src/stokesLimitFunctions.cu:23-61). */
+int fsl_neighbor_grid(fsl_handle* h, int32_t* dims3);
+int fsl_cell_list(fsl_handle* h, int32_t* cell_of, int32_t* start, int32_t* sorted);
+/* Forces at the current positions (pair + bonded), the force half of
+ * kernelSpreadParticlesForceStokesLimit (src/stokesLimitFunctions.cu:83-657). */
+int fsl_compute_forces(fsl_handle* h, double* F);
+/* f = S(q) F / dV at the current positions for given particle forces F
+ * (spread + addSpreadedForcesStokesLimit, src/stokesLimitFunctions.cu:659-1681). */
+int fsl_spread(fsl_handle* h, const double* F, double* f);
+/* v = (eta L)^-1 P W for a given real field W [3][nc] (FFT, kernelShift,
+ * kernelUpdateVstokesLimit, inverse FFT, normalisation:
+ * src/runSchemeStokesLimit.cu:198-214). */
+int fsl_solve(fsl_handle* h, const double* W, double* v);
+/* u = J(q) v at the current positions for a given field v [3][nc]
+ * (src/stokesLimitFunctions.cu:2616-2642). */
+int fsl_interpolate(fsl_handle* h, const double* v, double* u);
+/* Noise array entries [first, first+count) of draw t, as floats. */
+int fsl_noise(fsl_handle* h, uint64_t t, uint64_t first, int64_t count, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLUAMSL_H */

@@ -1,0 +1,146 @@
+"""The drop-in `fluam data.main` driver on the GPU: same keywords, same output
+files and formats as src/saveParticles.cu, trajectories equal to the oracle's
+within the FP32 tolerance."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import chains, rel_inf
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+FLUAM = os.path.join(ROOT, "fluam_b200", "fluam")
+
+
+def read_particles(path):
+    """Parse a .particles / .velocityParticles file: {time: (3, np)}."""
+    with open(path) as f:
+        head = f.readline()
+        assert head.startswith("#NUMBER PARTICLES ")
+        n = int(head.split()[2])
+        out = {}
+        while True:
+            line = f.readline()
+            if not line:
+                break
+            t = float(line)
+            rows = [f.readline().split() for _ in range(n)]
+            out[t] = np.array(rows, dtype=float).T
+    return n, out
+
+
+def run_fluam(tmp_path, text):
+    p = tmp_path / "data.main"
+    p.write_text(text)
+    r = subprocess.run([FLUAM, str(p)], capture_output=True, text=True, cwd=tmp_path, timeout=600)
+    # the reference's main() returns 1 on success (src/main.cpp:111)
+    assert r.returncode == 1, r.stdout + r.stderr
+    return r
+
+
+def test_reference_style_input(tmp_path, oracle):
+    out = tmp_path / "run"
+    text = f"""# reference keywords only
+stokesLimit
+particles 1
+numberparticles 27
+cutoff 2.2449240966
+maxNumberPartInCellNonBonded 20
+maxNumberPartInCell 20
+densfluid 1
+shearviscosity 1
+temperature 0.1
+cells 32 32 32
+celldimension 64 64 64
+initfluid 1
+backgroundvelocity 0 0 0
+seed 12
+numstepsRelaxation 0
+numsteps 6
+samplefreq 3
+savefreq 0
+dt 0.25
+outputname {out}
+"""
+    r = run_fluam(tmp_path, text)
+    assert "Stokes Limit  3" in r.stdout and "Stokes Limit  6" in r.stdout
+    for ext in (".data.main", ".cuda", ".seed", ".time", ".particles", ".velocityParticles"):
+        assert os.path.exists(str(out) + ext), ext
+    assert open(str(out) + ".seed").read() == "12\n"
+    assert open(str(out) + ".data.main").read().startswith("# reference keywords only\nstokesLimit\n")
+    n, pos = read_particles(str(out) + ".particles")
+    _, frc = read_particles(str(out) + ".velocityParticles")
+    assert n == 27 and sorted(pos) == [0.75, 1.5] and sorted(frc) == [0.75, 1.5]
+    # simple-cubic start (src/simpleCubic.cpp): 3 x 3 x 3 lattice, spacing 64/3
+    g = (np.arange(3) + 0.5) * 64 / 3 - 32
+    q0 = np.stack(np.meshgrid(g, g, g, indexing="ij"))[::-1].reshape(3, -1)
+    o = oracle.Oracle(32, 32, 32, 64.0, 64.0, 64.0, q0, eta=1, kT=0.1, dt=0.25,
+                      cutoff=2.2449240966, kernel=3, pair=oracle.PAIR_TABLE_LJ, seed=12)
+    o.step(3)
+    assert rel_inf(pos[0.75] - q0, o.positions() - q0) < 1e-5
+    o.step(3)
+    assert rel_inf(pos[1.5] - q0, o.positions() - q0) < 1e-5
+    # precision 15 text
+    line = open(str(out) + ".particles").read().splitlines()[2]
+    assert max(len(x.replace("-", "").replace(".", "")) for x in line.split()) <= 15
+
+
+def test_extension_keywords_coordinates_and_bonds(tmp_path, oracle):
+    L = 32.0
+    q, bi, bj = chains(8, 8, (L, L, L), 4)
+    n = q.shape[1]
+    coor = tmp_path / "start.coor"
+    with open(coor, "w") as f:
+        f.write(f"{n}\n")
+        for i in range(n):
+            f.write("%.17g %.17g %.17g\n" % (q[0, i], q[1, i], q[2, i]))
+    bonds = tmp_path / "bonds.dat"
+    with open(bonds, "w") as f:
+        f.write(f"{len(bi)}\n")
+        for a, b in zip(bi, bj):
+            f.write(f"{a} {b} 10 1\n")
+        f.write("1\n0 2.0 0 0.0 0.0 0.0\n")
+    out = tmp_path / "chains"
+    text = f"""stokesLimit
+loadparticles 1
+coordinates {coor}
+bondedForces {bonds}
+cutoff 1.5
+shearviscosity 1
+temperature 0.01
+cells 32 32 32
+celldimension 32 32 32
+seed 5
+numstepsRelaxation 2
+numsteps 4
+samplefreq 2
+dt 0.005
+outputname {out}
+kernelPoints 4
+pairPotential soft
+softEpsilon 1.0
+"""
+    run_fluam(tmp_path, text)
+    _, pos = read_particles(str(out) + ".particles")
+    assert sorted(pos) == [0.01, 0.02]
+    o = oracle.Oracle(32, 32, 32, L, L, L, q, eta=1, kT=0.01, dt=0.005, cutoff=1.5, kernel=4,
+                      pair=oracle.PAIR_SOFT, seed=5)
+    o.set_bonds(bi, bj, np.full(len(bi), 10.0), np.ones(len(bi)), fi=[0], fk=[2.0], fr0=[0.0],
+                fxyz=[[0.0, 0.0, 0.0]])
+    o.step(4)  # 2 relaxation steps + 2
+    assert rel_inf(pos[0.01] - q, o.positions() - q) < 1e-5
+    o.step(2)
+    assert rel_inf(pos[0.02] - q, o.positions() - q) < 1e-5
+
+
+def test_errors_are_reported(tmp_path):
+    p = tmp_path / "data.main"
+    p.write_text("stokesLimit\ncells 8 8 8\nsamplefreq 0\noutputname x\n")
+    r = subprocess.run([FLUAM, str(p)], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 0 and "samplefreq" in r.stdout
+    p.write_text("incompressible\ncells 8 8 8\nsamplefreq 1\noutputname x\n")
+    r = subprocess.run([FLUAM, str(p)], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 0 and "stokesLimit" in r.stdout
