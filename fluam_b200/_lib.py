@@ -24,7 +24,7 @@ EXPORTS = [
     "fsl_profile", "fsl_profile_read",
     "fsl_destroy", "fsl_last_error", "fsl_run_data_main", "fsl_parse_data_main",
     "fsl_neighbor_grid", "fsl_cell_list", "fsl_compute_forces", "fsl_spread", "fsl_solve",
-    "fsl_interpolate", "fsl_noise",
+    "fsl_interpolate", "fsl_noise", "fsl_cell_list_noalloc",
 ]
 
 
@@ -108,6 +108,8 @@ def load(path=None):
     L.fsl_solve.argtypes = [_VP, _D, _D]
     L.fsl_interpolate.argtypes = [_VP, _D, _D]
     L.fsl_noise.argtypes = [_VP, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, _F]
+    L.fsl_cell_list_noalloc.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int64, _VP, _VP, _VP, _VP, _VP]
     if path is None:
         _lib = L
     return L

@@ -32,6 +32,12 @@ int set_error(int code, const char* fmt, ...) {
                        "%s failed: %s", #call, cudaGetErrorString(e_));                  \
   } while (0)
 
+}  // namespace
+
+int fsl::set_last_error(int code, const char* msg) { return set_error(code, "%s", msg); }
+
+namespace {
+
 template <class T>
 cudaError_t dalloc(T** p, size_t n) {
   *p = nullptr;

@@ -189,6 +189,9 @@ __device__ __forceinline__ void set_err(int* err, int bit) {
 // Declared here, defined in the .cu files; all enqueue on `s`.
 namespace fsl {
 
+// Sets the message fsl_last_error() returns on this thread; returns code.
+int set_last_error(int code, const char* msg);
+
 // Stage timer: mark(name) records an event on the stream; the interval up to
 // the next mark is charged to `name` (nullptr closes the last interval).
 // Off by default; when on, the marks are captured into the step's graph too.

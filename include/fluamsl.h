@@ -173,6 +173,29 @@ int fsl_interpolate(fsl_handle* h, const double* v, double* u);
 /* Noise array entries [first, first+count) of draw t, as floats. */
 int fsl_noise(fsl_handle* h, uint64_t t, uint64_t first, int64_t count, float* out);
 
+/* ---- cell list without device allocation -------------------------------
+ * No counterpart in the reference.  The same cell list as fsl_cell_list, for
+ * callers that must not allocate device memory: code recording a CUDA graph
+ * in global capture mode (where cudaMalloc fails), frameworks that own all
+ * device memory through their own pool, and loops that keep other GPU work
+ * in flight (cudaMalloc/cudaFree can synchronise the whole device).  It takes
+ * no handle.  q_dev (np x 3 doubles, SoA), cell_of_dev (np), start_dev (m+1,
+ * m = neighbour-grid cells of max(3, int(L/cutoff)) per direction) and
+ * sorted_dev (np) are device memory owned by the caller; the work is queued
+ * on `stream` (a cudaStream_t, NULL for the default stream).  The sort's
+ * scratch is a fixed array inside the library (about 9 MiB on every GPU that
+ * loads it, held until exit), which limits a call to 262,144 particles and
+ * 1,048,576 neighbour-grid cells; larger sizes are rejected with FSL_E_ARG.
+ * The first call on a device looks up that array's address, so make the first
+ * call on each device before any stream capture.  All calls share the array:
+ * calls whose work overlaps on the GPU (different streams, or different host
+ * threads on one device) race and must be ordered by the caller.  A
+ * non-finite coordinate gives that particle an arbitrary in-range cell and is
+ * not reported here. */
+int fsl_cell_list_noalloc(double lx, double ly, double lz, double cutoff, int64_t np,
+                          const double* q_dev, int32_t* cell_of_dev, int32_t* start_dev,
+                          int32_t* sorted_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
