@@ -1,0 +1,138 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+Each case is a data.main (plus coordinate and bond files) using only the
+reference's own features (LJ force table, 3-point kernel, bonds, tethers,
+extraMobility, the reference RFD).  It is run through oracle/_ref/fluam_ref,
+the reference's stokesLimit sources compiled for the host by
+oracle/ref_cpu/build_ref.py (cuFFT replaced by a direct DFT, cuRAND by the
+Philox normals shared with the oracle and the CUDA path).  The script keeps
+the inputs and the reference's .particles / .velocityParticles / .seed.
+
+Usage (in a container where the reference sources are mounted):
+    python oracle/ref_cpu/build_ref.py && python tests/golden/make_golden.py
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+FLUAM_REF = os.path.join(ROOT, "oracle", "_ref", "fluam_ref")
+
+COMMON = """stokesLimit
+particles 1
+maxNumberPartInCellNonBonded 40
+maxNumberPartInCell 40
+densfluid 1
+initfluid 0
+backgroundvelocity 0 0 0
+outputname out
+"""
+
+
+def lattice(n_per_side, spacing, jitter, seed, origin):
+    g = np.arange(n_per_side) * spacing
+    q = np.stack(np.meshgrid(g, g, g, indexing="ij")).reshape(3, -1) + np.asarray(origin)[:, None]
+    return q + np.random.default_rng(seed).uniform(-jitter, jitter, q.shape)
+
+
+def chains(nch, beads, box, seed):
+    rng = np.random.default_rng(seed)
+    starts = rng.uniform(-0.5, 0.5, (nch, 3)) * np.asarray(box)
+    d = rng.standard_normal((nch, beads - 1, 3))
+    d /= np.linalg.norm(d, axis=2, keepdims=True)
+    pos = np.concatenate([starts[:, None, :], starts[:, None, :] + np.cumsum(d, axis=1)], axis=1)
+    q = pos.reshape(-1, 3).T.copy()
+    idx = np.arange(nch * beads).reshape(nch, beads)
+    return q, list(zip(idx[:, :-1].ravel(), idx[:, 1:].ravel()))
+
+
+def write_coor(path, q):
+    with open(path, "w") as f:
+        f.write(f"{q.shape[1]}\n")
+        for i in range(q.shape[1]):
+            f.write("%.17g %.17g %.17g\n" % tuple(q[:, i]))
+
+
+CASES = {
+    # simple-cubic start of src/simpleCubic.cpp, no particle overlaps
+    "lattice27": dict(text="""numberparticles 27
+cutoff 2.2449240966
+shearviscosity 1
+temperature 0.01
+cells 16 16 16
+celldimension 16 16 16
+seed 3
+numsteps 4
+samplefreq 1
+dt 0.01
+"""),
+    # LJ table forces active: jittered lattice just inside the WCA cutoff
+    # (sigma = 2 dx = 1, rc = 2^(1/6) sigma)
+    "lj_dense": dict(text="""loadparticles 1
+coordinates start.coor
+cutoff 1.12246204830937
+shearviscosity 1.3
+temperature 0.05
+cells 32 32 32
+celldimension 16 16 16
+seed 11
+numsteps 3
+samplefreq 1
+dt 0.001
+""", coor=lambda: lattice(6, 1.05, 0.04, 5, (-2.6, -2.6, -2.6))),
+    # chains + tethers, extraMobility, no pair forces, non-cubic grid and box
+    "bonds_extra": dict(text="""loadparticles 1
+coordinates start.coor
+bondedForces bonds.dat
+computeNonBondedForces 0
+cutoff 1.5
+extraMobility 0.2
+shearviscosity 0.8
+temperature 0.02
+cells 16 24 32
+celldimension 16 24 32
+seed 21
+numstepsRelaxation 2
+numsteps 4
+samplefreq 2
+dt 0.01
+""", chains=(6, 8, (16.0, 24.0, 32.0), 9)),
+}
+
+
+def make_case(name, spec):
+    d = os.path.join(HERE, name)
+    if os.path.isdir(d):
+        shutil.rmtree(d)
+    os.makedirs(d)
+    with open(os.path.join(d, "data.main"), "w") as f:
+        f.write(COMMON + spec["text"])
+    if "coor" in spec:
+        write_coor(os.path.join(d, "start.coor"), spec["coor"]())
+    if "chains" in spec:
+        nch, beads, box, seed = spec["chains"]
+        q, bonds = chains(nch, beads, box, seed)
+        write_coor(os.path.join(d, "start.coor"), q)
+        with open(os.path.join(d, "bonds.dat"), "w") as f:
+            f.write(f"{len(bonds)}\n")
+            for k, (a, b) in enumerate(bonds):
+                f.write(f"{a} {b} {10.0 if k % 2 else 4.0} {1.0 if k % 3 else 0.0}\n")
+            f.write("2\n0 2.0 0.0 0.0 0.0 0.0\n5 1.5 0.5 1.0 -2.0 3.0\n")
+    r = subprocess.run([FLUAM_REF, "data.main"], cwd=d, capture_output=True, text=True,
+                       timeout=600)
+    if "END" not in r.stdout:
+        raise RuntimeError(f"{name}: reference run failed\n{r.stdout[-2000:]}")
+    for ext in (".cuda", ".time", ".data.main"):
+        os.remove(os.path.join(d, "out" + ext))
+
+
+if __name__ == "__main__":
+    if not os.path.exists(FLUAM_REF):
+        sys.exit("build oracle/_ref first (python oracle/ref_cpu/build_ref.py)")
+    for name, spec in CASES.items():
+        make_case(name, spec)
+        print("golden", name)

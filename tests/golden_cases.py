@@ -1,0 +1,95 @@
+"""Loader of the golden fixtures in tests/golden/ (made by make_golden.py from
+the reference's own stokesLimit sources built for the host)."""
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def read_particles(path):
+    """Parse a .particles / .velocityParticles file into {time: (3, np)}."""
+    with open(path) as f:
+        head = f.readline()
+        assert head.startswith("#NUMBER PARTICLES ")
+        n = int(head.split()[2])
+        out = {}
+        while True:
+            line = f.readline()
+            if not line:
+                break
+            t = float(line)
+            rows = [f.readline().split() for _ in range(n)]
+            out[t] = np.array(rows, dtype=float).T
+    return n, out
+
+
+def simple_cubic(np_, lx, ly, lz):
+    """src/simpleCubic.cpp:25-63 (dimension 3)."""
+    sigma = (lx * ly * lz / np_) ** (1.0 / 3.0)
+    nz = int(lz / sigma) or 1
+    nx = int(lx / sigma) or 1
+    ny = int(ly / sigma) or 1
+    while nx * ny * nz < np_:
+        if nx * ny * nz < np_:
+            nx += 1
+        if nx * ny * nz < np_:
+            ny += 1
+        if nx * ny * nz < np_:
+            nz += 1
+    dx, dy, dz = lx / nx, ly / ny, lz / nz
+    q = np.zeros((3, np_))
+    n = 0
+    for i in range(nz):
+        for j in range(ny):
+            for k in range(nx):
+                if n < np_:
+                    q[:, n] = ((k + 0.5) * dx - lx / 2.0, (j + 0.5) * dy - ly / 2.0,
+                               (i + 0.5) * dz - lz / 2.0)
+                    n += 1
+    return q
+
+
+def cases():
+    return sorted(d for d in os.listdir(GOLDEN) if os.path.isdir(os.path.join(GOLDEN, d)))
+
+
+def load(name):
+    """Inputs and reference outputs of one golden case."""
+    from fluam_b200 import parse_data_main
+    d = os.path.join(GOLDEN, name)
+    cfg, run = parse_data_main(os.path.join(d, "data.main"))
+    words = open(os.path.join(d, "data.main")).read().split()
+    if "coordinates" in words:
+        with open(os.path.join(d, "start.coor")) as f:
+            n = int(f.readline())
+            q0 = np.array([f.readline().split() for _ in range(n)], dtype=float).T.copy()
+    else:
+        q0 = simple_cubic(run["numberparticles"], cfg.lx, cfg.ly, cfg.lz)
+    bonds = None
+    if "bondedForces" in words:
+        with open(os.path.join(d, "bonds.dat")) as f:
+            nb = int(f.readline())
+            bb = np.array([f.readline().split() for _ in range(nb)], dtype=float).reshape(nb, 4)
+            nf = int(f.readline())
+            ff = np.array([f.readline().split() for _ in range(nf)], dtype=float).reshape(nf, 6)
+        bonds = dict(bi=bb[:, 0].astype(np.int32), bj=bb[:, 1].astype(np.int32), k=bb[:, 2],
+                     r0=bb[:, 3], fi=ff[:, 0].astype(np.int32), fk=ff[:, 1], fr0=ff[:, 2],
+                     fxyz=ff[:, 3:6])
+    _, pos = read_particles(os.path.join(d, "out.particles"))
+    _, frc = read_particles(os.path.join(d, "out.velocityParticles"))
+    seed = int(open(os.path.join(d, "out.seed")).read())
+    return dict(dir=d, cfg=cfg, run=run, q0=q0, bonds=bonds, pos=pos, frc=frc, seed=seed)
+
+
+def sample_steps(run):
+    """Number of steps taken before each sample (src/runSchemeStokesLimit.cu:83, 280)."""
+    out = []
+    step = -run["numstepsRelaxation"]
+    taken = 0
+    while step < run["numsteps"]:
+        step += 1
+        taken += 1
+        if step % run["samplefreq"] == 0 and step > 0:
+            out.append((step, taken))
+    return out

@@ -136,6 +136,27 @@ softEpsilon 1.0
     assert rel_inf(pos[0.02] - q, o.positions() - q) < 1e-5
 
 
+@pytest.mark.parametrize("name", __import__("golden_cases").cases())
+def test_golden_cases_against_reference_outputs(tmp_path, name):
+    """The drop-in run on the inputs of each golden case reproduces the
+    reference's own outputs (tests/golden) within the FP32 tolerance."""
+    import shutil
+    import golden_cases as G
+    c = G.load(name)
+    for f in os.listdir(c["dir"]):
+        if not f.startswith("out."):
+            shutil.copy(os.path.join(c["dir"], f), tmp_path / f)
+    r = subprocess.run([FLUAM, "data.main"], capture_output=True, text=True, cwd=tmp_path,
+                       timeout=600)
+    assert r.returncode == 1, r.stdout + r.stderr
+    _, pos = G.read_particles(str(tmp_path / "out.particles"))
+    _, frc = G.read_particles(str(tmp_path / "out.velocityParticles"))
+    assert sorted(pos) == sorted(c["pos"])
+    for t in c["pos"]:
+        assert rel_inf(pos[t] - c["q0"], c["pos"][t] - c["q0"]) < 1e-5, (name, t)
+        assert np.abs(frc[t] - c["frc"][t]).max() <= 1e-5 * max(np.abs(c["frc"][t]).max(), 1e-300)
+
+
 def test_errors_are_reported(tmp_path):
     p = tmp_path / "data.main"
     p.write_text("stokesLimit\ncells 8 8 8\nsamplefreq 0\noutputname x\n")

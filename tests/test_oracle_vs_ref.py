@@ -1,0 +1,72 @@
+"""Pin of the FP64 oracle against the reference itself.
+
+tests/golden/ holds outputs of the reference's own stokesLimit sources
+(src/stokesLimitFunctions.cu and the rest of its path) built for the host by
+oracle/ref_cpu/build_ref.py; the oracle, fed the same inputs and the same
+noise, must reproduce them to the precision of the 15-digit text files.
+"""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import golden_cases as G
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+FLUAM_REF = os.path.join(ROOT, "oracle", "_ref", "fluam_ref")
+
+
+def _oracle_for(oracle, c):
+    cfg = c["cfg"]
+    o = oracle.Oracle(cfg.mx, cfg.my, cfg.mz, cfg.lx, cfg.ly, cfg.lz, c["q0"],
+                      eta=cfg.shearviscosity, kT=cfg.temperature, dt=cfg.dt, cutoff=cfg.cutoff,
+                      kernel=cfg.kernel, pair=cfg.pair, soft_epsilon=cfg.soft_epsilon,
+                      rfd=cfg.rfd, nonbonded=cfg.nonbonded, extra_mobility=cfg.extra_mobility,
+                      seed=c["seed"])
+    if c["bonds"] is not None:
+        b = c["bonds"]
+        o.set_bonds(b["bi"], b["bj"], b["k"], b["r0"], b["fi"], b["fk"], b["fr0"], b["fxyz"])
+    return o
+
+
+@pytest.mark.parametrize("name", G.cases())
+def test_oracle_reproduces_reference(oracle, name):
+    c = G.load(name)
+    o = _oracle_for(oracle, c)
+    dt = c["cfg"].dt
+    done = 0
+    samples = G.sample_steps(c["run"])
+    assert len(samples) == len(c["pos"]) > 0
+    for step, taken in samples:
+        o.step(taken - done)
+        done = taken
+        t = step * dt
+        key = min(c["pos"], key=lambda x: abs(x - t))
+        assert abs(key - t) < 1e-12
+        q_ref, f_ref = c["pos"][key], c["frc"][key]
+        dq_ref = q_ref - c["q0"]
+        dq_orc = o.positions() - c["q0"]
+        # 15 significant digits of |q| ~ L/2 bound the text's resolution
+        tol = 1e-14 * np.abs(q_ref).max() * 10
+        assert np.abs(dq_orc - dq_ref).max() <= max(tol, 1e-10 * np.abs(dq_ref).max()), name
+        F = o.forces()
+        assert np.abs(F - f_ref).max() <= 1e-12 + 1e-10 * np.abs(f_ref).max(), name
+
+
+@pytest.mark.parametrize("name", G.cases())
+def test_golden_files_regenerate_identically(tmp_path, name):
+    """Where the reference sources are present, rerun the reference and get
+    the committed fixture back byte for byte."""
+    if not (os.path.exists(FLUAM_REF) and os.path.isdir("/root/reference/src")):
+        pytest.skip("reference host build not available here")
+    src = os.path.join(G.GOLDEN, name)
+    for f in os.listdir(src):
+        if not f.startswith("out."):
+            shutil.copy(os.path.join(src, f), tmp_path / f)
+    r = subprocess.run([FLUAM_REF, "data.main"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600)
+    assert "END" in r.stdout, r.stdout[-1000:]
+    for ext in (".particles", ".velocityParticles", ".seed"):
+        assert open(tmp_path / ("out" + ext)).read() == open(os.path.join(src, "out" + ext)).read()
