@@ -115,9 +115,11 @@ def stage_bytes(name, P):
         "cells": 40 * npart + 12 * P["mN"],
         "forces": 52 * npart + 4 * P["mN"],
         "grid_zero": 24 * nc,
-        "spread_force": 48 * npart + 2 * touched,
-        "spread_drift": 2 * (36 * npart + 2 * touched),
-        "xfwd": 24 * nc + 36 * nc + spec,          # grid + mean noise of the 2 solves + spectrum
+        "spread": 48 * npart + 2 * touched,
+        "spread_rfd": 120 * npart + 2 * 3 * 8 * min(P["nc"], 3 * k ** 3 * npart),
+        "plane_fwd": 24 * nc + 36 * nc + spec,     # grid + mean noise of the 2 solves + spectrum
+        "plane_inv": spec + 12 * nc,
+        "xfwd": 24 * nc + 36 * nc + spec,
         "yfft": 2 * spec,
         "zsolve": 2 * spec,
         "xinv": spec + 12 * nc,
@@ -179,6 +181,22 @@ def run_reference(args, rank, world):
     return 0
 
 
+def aggregate(local_times, dist=None, device=None):
+    """Max over ranks of each local time (ms or s), as floats; the replicas
+    do not exchange data, so this is the only collective of a run."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return [float(x) for x in local_times]
+    import torch
+    t = torch.tensor([float(x) for x in local_times], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def replica_seed(rank, base=1):
+    """Each rank runs its own replica of the workload: same sizes, own seed."""
+    return base + rank
+
+
 def workload_config(name):
     from fluam_b200 import workloads as W
     w = W.WORKLOADS[name]
@@ -211,7 +229,7 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     from fluam_b200 import StokesLimit, workloads
-    cfg, q, bonds = workloads.build(args.workload, seed=1 + rank)
+    cfg, q, bonds = workloads.build(args.workload, seed=replica_seed(rank))
     cfg.device = local
     sim = StokesLimit(cfg, q)
     if bonds is not None:
@@ -268,12 +286,8 @@ def main():
     e2e_s = time.perf_counter() - t0
     sim.sync()
 
-    t_max = total_ms
-    e2e_max = e2e_s
+    t_max, e2e_max = aggregate([total_ms, e2e_s], dist, device="cuda")
     if dist:
-        tt = torch.tensor([total_ms, e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max, e2e_max = float(tt[0]), float(tt[1])
         dist.barrier()
 
     if rank == 0:

@@ -69,6 +69,7 @@ struct fsl_handle {
   float* v = nullptr;
   // scratch for the component entry points (allocated on first use)
   float* wext = nullptr;
+  float* wbuf = nullptr;  // W of the current solve, [3][nc]
   double* u = nullptr;
   float* nbuf = nullptr;
   int64_t nbuf_n = 0;
@@ -93,7 +94,8 @@ void free_all(fsl_handle* h) {
                   h->fill,    h->tmp,     h->sorted,  h->bsum,    h->bpp_cnt, h->bpp_off,
                   h->bpp_idx, h->bpp_k,   h->bpp_r0,  h->bfp_cnt, h->bfp_off, h->bfp_k,
                   h->bfp_r0,  h->bfp_xyz, h->ljtab,   h->noise,   h->grid,    h->spec,
-                  h->v,       h->wext,    h->u,       h->nbuf,    h->err,     h->t_dev};
+                  h->v,       h->wext,    h->u,       h->nbuf,    h->err,     h->t_dev,
+                  h->wbuf};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < fsl::Prof::kMax; ++i)
@@ -147,28 +149,24 @@ void enqueue_step(fsl_handle* h) {
   pr.mark(s, "noise");
   fsl::launch_noise(P, h->t_dev, h->noise, s);
   pr.count(1);
-  // option 0: F^n, f = S(q^n) F^n; solve 1 with sqrt(2) stress 1
+  // option 0: F^n, f = S(q^n) F^n; solve 1 with sqrt(2) stress 1.  The
+  // spread field is all zeros here: it is cleared at creation and by every
+  // W build that reads it.
+  (void)gbytes;
   enqueue_cells_forces(h, h->q);
-  pr.mark(s, "grid_zero");
-  cudaMemsetAsync(h->grid, 0, gbytes, s);
-  pr.mark(s, "spread_force");
-  fsl::launch_spread_force(P, h->q, h->F, h->grid, h->err, s);
+  pr.mark(s, "spread");
+  fsl::launch_spread(P, 0, h->sorted, h->q, h->F, h->q, h->noise, h->grid, h->err, s);
   pr.count(pk);
-  fsl::launch_solve(P, h->fft, h->grid, h->noise, 1, nullptr, h->spec, h->v, s, &pr);
+  fsl::launch_solve(P, h->fft, h->grid, h->noise, 1, nullptr, h->wbuf, h->spec, h->v, s, &pr);
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with sqrt(1/2)(stress 1 + 2)
   pr.mark(s, "interp_update");
   fsl::launch_interp_update(P, 1, h->q, h->q, h->F, h->noise, h->v, h->qp, h->err, s);
   pr.count(pk);
   enqueue_cells_forces(h, h->qp);
-  pr.mark(s, "grid_zero");
-  cudaMemsetAsync(h->grid, 0, gbytes, s);
-  pr.mark(s, "spread_force");
-  fsl::launch_spread_force(P, h->qp, h->F, h->grid, h->err, s);
-  pr.mark(s, "spread_drift");
-  fsl::launch_spread_drift(P, h->q, h->noise, +1, h->grid, h->err, s);
-  fsl::launch_spread_drift(P, h->q, h->noise, -1, h->grid, h->err, s);
-  pr.count(3 * pk);
-  fsl::launch_solve(P, h->fft, h->grid, h->noise, 2, nullptr, h->spec, h->v, s, &pr);
+  pr.mark(s, "spread_rfd");
+  fsl::launch_spread(P, 1, h->sorted, h->qp, h->F, h->q, h->noise, h->grid, h->err, s);
+  pr.count(pk);
+  fsl::launch_solve(P, h->fft, h->grid, h->noise, 2, nullptr, h->wbuf, h->spec, h->v, s, &pr);
   // option 2: corrector
   pr.mark(s, "interp_update");
   fsl::launch_interp_update(P, 2, h->qp, h->q, h->F, h->noise, h->v, h->q, h->err, s);
@@ -363,6 +361,8 @@ int fsl_create(const fsl_config* cfg, int64_t np, const double* q, fsl_handle** 
   TRY(dalloc(&h->grid, n3c));
   TRY(dalloc(&h->spec, 3 * (size_t)P.my * P.mz * P.mxh));
   TRY(dalloc(&h->v, n3c));
+  TRY(dalloc(&h->wbuf, n3c));
+  TRY(cudaMemset(h->grid, 0, sizeof(unsigned long long) * n3c));
   TRY(dalloc(&h->err, 4));
   TRY(dalloc(&h->t_dev, 1));
   if ((int64_t)((P.mN + 4095) / 4096) > 4096) return fail(set_error(FSL_E_ARG, "neighbour grid too large"));
@@ -667,12 +667,14 @@ int fsl_spread(fsl_handle* h, const double* F, double* f) {
   FSL_CUDA(cudaSetDevice(h->device));
   FSL_CUDA(cudaMemcpyAsync(h->F, F, sizeof(double) * 3 * (size_t)P.np, cudaMemcpyHostToDevice, h->stream));
   FSL_CUDA(cudaMemsetAsync(h->grid, 0, sizeof(unsigned long long) * 3 * (size_t)P.nc, h->stream));
-  fsl::launch_spread_force(P, h->q, h->F, h->grid, h->err, h->stream);
+  fsl::launch_spread(P, 0, nullptr, h->q, h->F, h->q, h->noise, h->grid, h->err, h->stream);
   int rc = check_launch();
   if (rc) return rc;
   std::vector<long long> g(3 * (size_t)P.nc);
   FSL_CUDA(cudaMemcpyAsync(g.data(), h->grid, sizeof(long long) * g.size(), cudaMemcpyDeviceToHost,
                            h->stream));
+  // the step expects a cleared spread field
+  FSL_CUDA(cudaMemsetAsync(h->grid, 0, sizeof(unsigned long long) * g.size(), h->stream));
   FSL_CUDA(cudaStreamSynchronize(h->stream));
   const double sc = fsl::kFixedInv / P.dV;
   for (size_t k = 0; k < g.size(); ++k) f[k] = (double)g[k] * sc;
@@ -688,7 +690,7 @@ int fsl_solve(fsl_handle* h, const double* W, double* v) {
   std::vector<float> w(n3);
   for (size_t k = 0; k < n3; ++k) w[k] = (float)W[k];
   FSL_CUDA(cudaMemcpyAsync(h->wext, w.data(), sizeof(float) * n3, cudaMemcpyHostToDevice, h->stream));
-  fsl::launch_solve(P, h->fft, nullptr, nullptr, 1, h->wext, h->spec, h->v, h->stream);
+  fsl::launch_solve(P, h->fft, nullptr, nullptr, 1, h->wext, h->wbuf, h->spec, h->v, h->stream);
   int rc = check_launch();
   if (rc) return rc;
   FSL_CUDA(cudaMemcpyAsync(w.data(), h->v, sizeof(float) * n3, cudaMemcpyDeviceToHost, h->stream));

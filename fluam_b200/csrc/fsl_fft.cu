@@ -35,8 +35,16 @@ struct FftPlan {
   float2 *twx = nullptr, *twy = nullptr, *twz = nullptr;  // exp(-2 pi i t / m)
   float *gx = nullptr, *gy = nullptr, *gz = nullptr;      // 2/h sin(pi j / m)
   float2 *ex = nullptr, *ey = nullptr, *ez = nullptr;     // exp(+i pi j / m)
-  size_t smem_x = 0, smem_y = 0, smem_z = 0;
+  size_t smem_x = 0, smem_y = 0, smem_z = 0, smem_plane = 0;
+  bool use_plane = false;  // whole-plane kernels fit in shared memory
   bool ok = false;
+  // kernel instances: compiled sizes when available, else runtime sizes
+  void (*plane_fwd)(Params, Radices, Radices, const float2*, const float2*, struct WSource,
+                    float2*) = nullptr;
+  void (*plane_inv)(Params, Radices, Radices, const float2*, const float2*, const float2*,
+                    float*) = nullptr;
+  void (*zsolve)(Params, Radices, const float2*, const float*, const float*, const float*,
+                 const float2*, const float2*, const float2*, float2*) = nullptr;
 };
 
 static bool factorize(int n, Radices& R) {
@@ -180,6 +188,76 @@ __device__ float2* fft_lines(float2* A, float2* B, int LS, int nlines, const Rad
   return A;
 }
 
+// Compile-time variant of `stage` / `fft_lines`: with the size, radix
+// schedule, line count and stride known to the compiler, the index
+// arithmetic folds into shifts and multiplies.
+template <int N, int P, int NS, int NL, int LS>
+__device__ __forceinline__ void stage_ct(const float2* __restrict__ A, float2* __restrict__ B,
+                                         const float2* __restrict__ tw, int dir) {
+  constexpr int NBUT = N / P;
+  constexpr int TOT = NBUT * NL;
+  constexpr int TSTRIDE = N / (NS * P);
+  for (int w = threadIdx.x; w < TOT; w += blockDim.x) {
+    const int l = w % NL, j = w / NL;
+    const int k = j % NS;
+    float2 v[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) v[r] = A[(j + r * NBUT) * LS + l];
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < P; ++r) {
+        float2 t = tw[r * k * TSTRIDE];
+        if (dir > 0) t.y = -t.y;
+        v[r] = cmul(v[r], t);
+      }
+    }
+    dft<P>(v, dir);
+    const int base = (j - k) * P + k;
+#pragma unroll
+    for (int r = 0; r < P; ++r) B[(base + r * NS) * LS + l] = v[r];
+  }
+}
+
+template <int N, int NL, int LS, int NS, int... Rs>
+struct FftCT;
+template <int N, int NL, int LS, int NS>
+struct FftCT<N, NL, LS, NS> {
+  __device__ static float2* run(float2* A, float2*, const float2*, int) { return A; }
+};
+template <int N, int NL, int LS, int NS, int P0, int... Rs>
+struct FftCT<N, NL, LS, NS, P0, Rs...> {
+  __device__ static float2* run(float2* A, float2* B, const float2* tw, int dir) {
+    stage_ct<N, P0, NS, NL, LS>(A, B, tw, dir);
+    __syncthreads();
+    return FftCT<N, NL, LS, NS * P0, Rs...>::run(B, A, tw, dir);
+  }
+};
+
+// sizes with a compiled radix schedule; others use the runtime transform
+__host__ __device__ constexpr bool fft_ct_size(int n) {
+  return n == 16 || n == 24 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
+}
+
+template <int N, int NL, int LS>
+__device__ __forceinline__ float2* fft_ct(float2* A, float2* B, const float2* tw, int dir) {
+  if constexpr (N == 256) return FftCT<N, NL, LS, 1, 4, 4, 4, 4>::run(A, B, tw, dir);
+  else if constexpr (N == 128) return FftCT<N, NL, LS, 1, 4, 4, 4, 2>::run(A, B, tw, dir);
+  else if constexpr (N == 96) return FftCT<N, NL, LS, 1, 4, 4, 3, 2>::run(A, B, tw, dir);
+  else if constexpr (N == 64) return FftCT<N, NL, LS, 1, 4, 4, 4>::run(A, B, tw, dir);
+  else if constexpr (N == 48) return FftCT<N, NL, LS, 1, 4, 4, 3>::run(A, B, tw, dir);
+  else if constexpr (N == 32) return FftCT<N, NL, LS, 1, 4, 4, 2>::run(A, B, tw, dir);
+  else if constexpr (N == 24) return FftCT<N, NL, LS, 1, 4, 3, 2>::run(A, B, tw, dir);
+  else return FftCT<N, NL, LS, 1, 4, 4>::run(A, B, tw, dir);  // 16
+}
+
+// N > 0: compiled schedule; N == 0: runtime radices R (any 2,3,5,7,11-smooth n)
+template <int N, int NL, int LS>
+__device__ __forceinline__ float2* fft_any(float2* A, float2* B, const Radices& R,
+                                           const float2* tw, int dir) {
+  if constexpr (N > 0) return fft_ct<N, NL, LS>(A, B, tw, dir);
+  else return fft_lines(A, B, LS, NL, R, tw, dir);
+}
+
 constexpr int kXPairs = 16;  // x pass: row pairs (complex lines) per block
 constexpr int kYTile = 16;   // y pass: kx columns per block
 constexpr int kZTile = 8;    // z pass: kx columns per block (x 3 components)
@@ -306,13 +384,15 @@ __global__ void __launch_bounds__(kFftThreads)
 //   W'_a = W_a e^{-i pi j_a/m_a};  G2 = |g|^2, g_a = 2/h_a sin(pi j_a/m_a)
 //   V'_a = (W'_a - g_a (g.W')/G2) / (eta G2);  v_a = V'_a e^{+i pi j_a/m_a}/nc
 //   and v = 0 for the zero mode.
+template <int MZ>
 __global__ void __launch_bounds__(kFftThreads)
     k_zsolve(Params P, Radices R, const float2* __restrict__ tw, const float* __restrict__ gx,
              const float* __restrict__ gy, const float* __restrict__ gz,
              const float2* __restrict__ ex, const float2* __restrict__ ey,
              const float2* __restrict__ ez, float2* __restrict__ spec) {
   extern __shared__ float2 smem[];
-  const int mz = P.mz, my = P.my, mxh = P.mxh;
+  const int mz = MZ ? MZ : P.mz, my = P.my, mxh = P.mxh;
+  constexpr int NLc = 3 * kZTile;
   const int NL = 3 * kZTile, LS = NL;
   float2* A = smem;
   float2* B = A + mz * LS;
@@ -328,7 +408,7 @@ __global__ void __launch_bounds__(kFftThreads)
         kx < mxh ? spec[comp * cstride + z * zstride + (size_t)ky * mxh + kx] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2* Z = fft_lines(A, B, LS, NL, R, stw, -1);
+  float2* Z = fft_any<MZ, NLc, NLc>(A, B, R, stw, -1);
   const float inv_eta = (float)(1.0 / P.eta);
   const float inv_nc = 1.0f / (float)P.nc;
   for (int e = threadIdx.x; e < mz * kZTile; e += blockDim.x) {
@@ -362,7 +442,7 @@ __global__ void __launch_bounds__(kFftThreads)
   }
   __syncthreads();
   float2* other = (Z == A) ? B : A;
-  float2* Y = fft_lines(Z, other, LS, NL, R, stw, +1);
+  float2* Y = fft_any<MZ, NLc, NLc>(Z, other, R, stw, +1);
   for (int e = threadIdx.x; e < mz * NL; e += blockDim.x) {
     int lx = e % kZTile, r = e / kZTile;
     int z = r % mz, comp = r / mz;
@@ -409,7 +489,217 @@ __global__ void __launch_bounds__(kFftThreads)
   }
 }
 
+// ------------------------------------------------------- whole-plane path ---
+// One block per (z plane, component) does the whole 2-D transform of its
+// plane in shared memory, so a solve is three passes over HBM (plane
+// forward, z pencils with the solve, plane inverse) instead of five.  The
+// plane is kept as its half spectrum P[y][kx] (row pitch kPlanePitch); the
+// 1-D transforms run in batches of kPB lines through two small scratch
+// buffers.
+constexpr int kPB = 16;
+
+__device__ __forceinline__ int plane_pitch(int mxh) { return mxh | 1; }  // odd: fewer conflicts
+
+struct WSource {
+  const unsigned long long* grid;
+  const float* noise;
+  const float* wext;
+  int nsets;
+  float scale, a1x, a1y, a1z, a4x, a4y, a4z;
+  size_t off2;
+};
+
+__device__ __forceinline__ float w_value(const Params& P, const WSource& S, int comp, int x, int y,
+                                         int z) {
+  int i = x + P.mx * (y + P.my * z);
+  if (S.wext) return S.wext[(size_t)comp * P.nc + i];
+  long long g = (long long)S.grid[(size_t)comp * P.nc + i];
+  float w = (float)((double)g * (double)S.scale);
+  w += stress_div(P, S.noise, comp, x, y, z, i, S.a1x, S.a1y, S.a1z, S.a4x, S.a4y, S.a4z);
+  if (S.nsets > 1)
+    w += stress_div(P, S.noise + S.off2, comp, x, y, z, i, S.a1x, S.a1y, S.a1z, S.a4x, S.a4y,
+                    S.a4z);
+  return w;
+}
+
+// W of all three components of every cell (src/stokesLimitFunctions.cu
+// :2281-2378, 3922-4069): the fixed-point spread field times 2^-40/dV plus
+// the stochastic stress divergence.  The spread field is cleared behind the
+// read, ready for the next spread.  One thread per cell, so the loads of a
+// warp are coalesced rows and the kernel runs at full occupancy.
+__global__ void k_wbuild(Params P, WSource S, float* __restrict__ W,
+                         unsigned long long* __restrict__ grid) {
+  const size_t nc = (size_t)P.nc;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc;
+       i += (size_t)gridDim.x * blockDim.x) {
+    int x = (int)(i % P.mx), r = (int)(i / P.mx);
+    int y = r % P.my, z = r / P.my;
+    float w0 = w_value(P, S, 0, x, y, z);
+    float w1 = w_value(P, S, 1, x, y, z);
+    float w2 = w_value(P, S, 2, x, y, z);
+    W[i] = w0;
+    W[nc + i] = w1;
+    W[2 * nc + i] = w2;
+    grid[i] = 0ull;
+    grid[nc + i] = 0ull;
+    grid[2 * nc + i] = 0ull;
+  }
+}
+
+template <int MX, int MY>
+__global__ void __launch_bounds__(kFftThreads)
+    k_plane_fwd(Params P, Radices Rx, Radices Ry, const float2* __restrict__ twx,
+                const float2* __restrict__ twy, WSource S, float2* __restrict__ spec) {
+  extern __shared__ float2 smem[];
+  const int mx = MX ? MX : P.mx, my = MY ? MY : P.my, mxh = mx / 2 + 1;
+  const int LSP = plane_pitch(mxh);
+  constexpr int LS = kPB + 1;
+  const int mmax = mx > my ? mx : my;
+  float2* Pl = smem;                 // [my][LSP]
+  float2* S1 = Pl + my * LSP;        // [mmax][LS]
+  float2* S2 = S1 + mmax * LS;       // [mmax][LS]
+  float2* tx = S2 + mmax * LS;       // [mx]
+  float2* ty = tx + mx;              // [my]
+  const int z = blockIdx.x, comp = blockIdx.y;
+  for (int t = threadIdx.x; t < mx; t += blockDim.x) tx[t] = twx[t];
+  for (int t = threadIdx.x; t < my; t += blockDim.x) ty[t] = twy[t];
+  const int npairs = (my + 1) / 2;
+  // x: real rows (2p, 2p+1) as one complex line, kPB pairs at a time
+  for (int p0 = 0; p0 < npairs; p0 += kPB) {
+    float* S1f = reinterpret_cast<float*>(S1);
+    for (int e = threadIdx.x; e < 2 * kPB * mx; e += blockDim.x) {
+      int rl = e / mx, x = e - rl * mx;
+      int y = 2 * p0 + rl;
+      float w = (y < my && p0 + (rl >> 1) < npairs) ? w_value(P, S, comp, x, y, z) : 0.0f;
+      S1f[2 * (x * LS + (rl >> 1)) + (rl & 1)] = w;
+    }
+    __syncthreads();
+    float2* Z = fft_any<MX, kPB, LS>(S1, S2, Rx, tx, -1);
+    for (int e = threadIdx.x; e < kPB * mxh; e += blockDim.x) {
+      int l = e / mxh, k = e - l * mxh;
+      int y = 2 * (p0 + l);
+      if (y >= my) continue;
+      float2 zk = Z[k * LS + l];
+      float2 zm = Z[((mx - k) % mx) * LS + l];
+      Pl[y * LSP + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      if (y + 1 < my) Pl[(y + 1) * LSP + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    }
+    __syncthreads();
+  }
+  // y: kPB columns at a time, written straight to the spectrum
+  float2* out = spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
+  for (int k0 = 0; k0 < mxh; k0 += kPB) {
+    for (int e = threadIdx.x; e < my * kPB; e += blockDim.x) {
+      int l = e % kPB, y = e / kPB;
+      int k = k0 + l;
+      S1[y * LS + l] = k < mxh ? Pl[y * LSP + k] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* Z = fft_any<MY, kPB, LS>(S1, S2, Ry, ty, -1);
+    for (int e = threadIdx.x; e < my * kPB; e += blockDim.x) {
+      int l = e % kPB, y = e / kPB;
+      int k = k0 + l;
+      if (k < mxh) out[(size_t)y * mxh + k] = Z[y * LS + l];
+    }
+    __syncthreads();
+  }
+}
+
+template <int MX, int MY>
+__global__ void __launch_bounds__(kFftThreads)
+    k_plane_inv(Params P, Radices Rx, Radices Ry, const float2* __restrict__ twx,
+                const float2* __restrict__ twy, const float2* __restrict__ spec,
+                float* __restrict__ v) {
+  extern __shared__ float2 smem[];
+  const int mx = MX ? MX : P.mx, my = MY ? MY : P.my, mxh = mx / 2 + 1;
+  const int LSP = plane_pitch(mxh);
+  constexpr int LS = kPB + 1;
+  const int mmax = mx > my ? mx : my;
+  float2* Pl = smem;
+  float2* S1 = Pl + my * LSP;
+  float2* S2 = S1 + mmax * LS;
+  float2* tx = S2 + mmax * LS;
+  float2* ty = tx + mx;
+  const int z = blockIdx.x, comp = blockIdx.y;
+  for (int t = threadIdx.x; t < mx; t += blockDim.x) tx[t] = twx[t];
+  for (int t = threadIdx.x; t < my; t += blockDim.x) ty[t] = twy[t];
+  const float2* in = spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
+  // y: inverse transform of kPB columns at a time into the plane buffer
+  for (int k0 = 0; k0 < mxh; k0 += kPB) {
+    for (int e = threadIdx.x; e < my * kPB; e += blockDim.x) {
+      int l = e % kPB, y = e / kPB;
+      int k = k0 + l;
+      S1[y * LS + l] = k < mxh ? in[(size_t)y * mxh + k] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* Z = fft_any<MY, kPB, LS>(S1, S2, Ry, ty, +1);
+    for (int e = threadIdx.x; e < my * kPB; e += blockDim.x) {
+      int l = e % kPB, y = e / kPB;
+      int k = k0 + l;
+      if (k < mxh) Pl[y * LSP + k] = Z[y * LS + l];
+    }
+    __syncthreads();
+  }
+  // x: complex-to-real, two rows per complex line
+  const int npairs = (my + 1) / 2;
+  float* out = v + (size_t)comp * P.nc + (size_t)z * my * mx;
+  for (int p0 = 0; p0 < npairs; p0 += kPB) {
+    for (int e = threadIdx.x; e < kPB * mxh; e += blockDim.x) {
+      int l = e / mxh, k = e - l * mxh;
+      int y = 2 * (p0 + l);
+      float2 X = make_float2(0.f, 0.f), Y = make_float2(0.f, 0.f);
+      if (y < my) X = Pl[y * LSP + k];
+      if (y + 1 < my) Y = Pl[(y + 1) * LSP + k];
+      S1[k * LS + l] = make_float2(X.x - Y.y, X.y + Y.x);
+      int km = mx - k;
+      if (k > 0 && km != k && km < mx) S1[km * LS + l] = make_float2(X.x + Y.y, Y.x - X.y);
+    }
+    __syncthreads();
+    float2* Z = fft_any<MX, kPB, LS>(S1, S2, Rx, tx, +1);
+    const float* Zf = reinterpret_cast<const float*>(Z);
+    for (int e = threadIdx.x; e < 2 * kPB * mx; e += blockDim.x) {
+      int rl = e / mx, x = e - rl * mx;
+      int y = 2 * p0 + rl;
+      if (y < my) out[(size_t)y * mx + x] = Zf[2 * (x * LS + (rl >> 1)) + (rl & 1)];
+    }
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------ host side ---
+template <int M>
+static void pick_cubic(FftPlan* fp) {
+  fp->plane_fwd = k_plane_fwd<M, M>;
+  fp->plane_inv = k_plane_inv<M, M>;
+}
+
+static void pick_kernels(const Params& P, FftPlan* fp) {
+  fp->plane_fwd = k_plane_fwd<0, 0>;
+  fp->plane_inv = k_plane_inv<0, 0>;
+  if (P.mx == P.my) {
+    switch (P.mx) {
+      case 16: pick_cubic<16>(fp); break;
+      case 24: pick_cubic<24>(fp); break;
+      case 32: pick_cubic<32>(fp); break;
+      case 48: pick_cubic<48>(fp); break;
+      case 64: pick_cubic<64>(fp); break;
+      case 96: pick_cubic<96>(fp); break;
+      case 128: pick_cubic<128>(fp); break;
+      default: break;
+    }
+  }
+  switch (P.mz) {
+    case 16: fp->zsolve = k_zsolve<16>; break;
+    case 24: fp->zsolve = k_zsolve<24>; break;
+    case 32: fp->zsolve = k_zsolve<32>; break;
+    case 48: fp->zsolve = k_zsolve<48>; break;
+    case 64: fp->zsolve = k_zsolve<64>; break;
+    case 96: fp->zsolve = k_zsolve<96>; break;
+    case 128: fp->zsolve = k_zsolve<128>; break;
+    case 256: fp->zsolve = k_zsolve<256>; break;
+    default: fp->zsolve = k_zsolve<0>; break;
+  }
+}
 static bool upload_table(const std::vector<float2>& h, float2** d) {
   if (cudaMalloc(d, sizeof(float2) * h.size()) != cudaSuccess) return false;
   return cudaMemcpy(*d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -463,10 +753,24 @@ FftPlan* fft_plan_create(const Params& P) {
     fft_plan_destroy(fp);
     return nullptr;
   }
+  {
+    int mmax = P.mx > P.my ? P.mx : P.my;
+    int lsp = P.mxh | 1;
+    fp->smem_plane = sizeof(float2) * ((size_t)P.my * lsp + 2 * (size_t)mmax * (kPB + 1) + P.mx + P.my);
+    fp->use_plane = fp->smem_plane <= lim;
+    pick_kernels(P, fp);
+    if (fp->use_plane) {
+      cudaFuncSetAttribute((const void*)fp->plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)fp->smem_plane);
+      cudaFuncSetAttribute((const void*)fp->plane_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)fp->smem_plane);
+    }
+  }
   cudaFuncSetAttribute(k_xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_x);
   cudaFuncSetAttribute(k_xinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_x);
   cudaFuncSetAttribute(k_yfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_y);
-  cudaFuncSetAttribute(k_zsolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_z);
+  cudaFuncSetAttribute((const void*)fp->zsolve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)fp->smem_z);
   fp->ok = true;
   return fp;
 }
@@ -485,23 +789,65 @@ void fft_plan_destroy(FftPlan* fp) {
   delete fp;
 }
 
-void launch_solve(const Params& P, FftPlan* fp, const unsigned long long* grid, const float* noise,
-                  int nsets, const float* wext, float2* spec, float* v, cudaStream_t s,
-                  Prof* prof) {
+void launch_solve(const Params& P, FftPlan* fp, unsigned long long* grid, const float* noise,
+                  int nsets, const float* wext, float* wbuf, float2* spec, float* v,
+                  cudaStream_t s, Prof* prof) {
   Prof dummy;
   Prof& pr = prof ? *prof : dummy;
   const int nrows = P.my * P.mz;
   const int npairs = (nrows + 1) / 2;
   dim3 gx((npairs + kXPairs - 1) / kXPairs, 3);
   float nfac = nsets > 1 ? (float)sqrt(0.5) : (float)sqrt(2.0);
+  if (!wext) {
+    // W from the spread field and the noise; clears the spread field
+    WSource S;
+    S.grid = grid;
+    S.noise = noise;
+    S.wext = nullptr;
+    S.nsets = nsets;
+    S.scale = (float)(kFixedInv / P.dV);
+    float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
+    S.a1x = (float)P.invdx * f1;
+    S.a1y = (float)P.invdy * f1;
+    S.a1z = (float)P.invdz * f1;
+    S.a4x = (float)P.invdx * f4;
+    S.a4y = (float)P.invdy * f4;
+    S.a4z = (float)P.invdz * f4;
+    S.off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
+    pr.mark(s, "wbuild");
+    int tb = 256;
+    long blocks = ((long)P.nc + tb - 1) / tb;
+    if (blocks > 148L * 64) blocks = 148L * 64;
+    k_wbuild<<<(unsigned)blocks, tb, 0, s>>>(P, S, wbuf, grid);
+    pr.count(1);
+    wext = wbuf;
+  }
+  if (fp->use_plane) {
+    WSource S{};
+    S.wext = wext;
+    dim3 gp(P.mz, 3);
+    pr.mark(s, "plane_fwd");
+    fp->plane_fwd<<<gp, kFftThreads, fp->smem_plane, s>>>(P, fp->rx, fp->ry, fp->twx, fp->twy, S,
+                                                         spec);
+    dim3 gz((P.mxh + kZTile - 1) / kZTile, P.my);
+    pr.mark(s, "zsolve");
+    fp->zsolve<<<gz, kFftThreads, fp->smem_z, s>>>(P, fp->rz, fp->twz, fp->gx, fp->gy, fp->gz, fp->ex,
+                                                 fp->ey, fp->ez, spec);
+    pr.mark(s, "plane_inv");
+    fp->plane_inv<<<gp, kFftThreads, fp->smem_plane, s>>>(P, fp->rx, fp->ry, fp->twx, fp->twy,
+                                                         spec, v);
+    pr.count(3);
+    return;
+  }
   pr.mark(s, "xfwd");
-  k_xfwd<<<gx, kFftThreads, fp->smem_x, s>>>(P, fp->rx, fp->twx, grid, noise, nsets, nfac, wext, spec);
+  k_xfwd<<<gx, kFftThreads, fp->smem_x, s>>>(P, fp->rx, fp->twx, nullptr, noise, nsets, nfac, wext,
+                                             spec);
   dim3 gy((P.mxh + kYTile - 1) / kYTile, P.mz, 3);
   pr.mark(s, "yfft");
   k_yfft<<<gy, kFftThreads, fp->smem_y, s>>>(P, fp->ry, fp->twy, spec, -1);
   dim3 gz((P.mxh + kZTile - 1) / kZTile, P.my);
   pr.mark(s, "zsolve");
-  k_zsolve<<<gz, kFftThreads, fp->smem_z, s>>>(P, fp->rz, fp->twz, fp->gx, fp->gy, fp->gz, fp->ex,
+  fp->zsolve<<<gz, kFftThreads, fp->smem_z, s>>>(P, fp->rz, fp->twz, fp->gx, fp->gy, fp->gz, fp->ex,
                                                fp->ey, fp->ez, spec);
   pr.mark(s, "yfft");
   k_yfft<<<gy, kFftThreads, fp->smem_y, s>>>(P, fp->ry, fp->twy, spec, +1);

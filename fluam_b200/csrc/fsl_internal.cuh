@@ -178,6 +178,79 @@ __device__ __forceinline__ void make_stencil(const Params& P, int comp, const do
   }
 }
 
+// Node k (0..n-1) of the stencil in dimension d alone: grid index j and its
+// weight (the same arithmetic as make_stencil for that dimension).
+__device__ __forceinline__ void stencil_node(const Params& P, int d, int comp, double posc,
+                                             double posw, int k, int& j, float& w) {
+  const int m = d == 0 ? P.mx : (d == 1 ? P.my : P.mz);
+  const double h = d == 0 ? P.dx : (d == 1 ? P.dy : P.dz);
+  const double invd = d == 0 ? P.invdx : (d == 1 ? P.invdy : P.invdz);
+  const double L = d == 0 ? P.lx : (d == 1 ? P.ly : P.lz);
+  const double invL = d == 0 ? P.invlx : (d == 1 ? P.invly : P.invlz);
+  const double off = (d == comp) ? __dmul_rn(0.5, h) : 0.0;
+  if (P.kernel == 3) {
+    double r = minimage(__dsub_rn(posc, off), invL, L);
+    int jc = cellidx(r, invd, m);
+    j = (jc - 1 + k + m) % m;
+    double node = ((double)j + 0.5) * h - 0.5 * L;
+    double rr = minimage((posw - node) - off, invL, L);
+    w = delta3f((float)(rr * invd));
+  } else {
+    double r = minimage(__dsub_rn(__dsub_rn(posc, off), __dmul_rn(0.5, h)), invL, L);
+    int jb = cellidx(r, invd, m);
+    j = (jb - 1 + k + m) % m;
+    double node = ((double)j + 0.5) * h - 0.5 * L + off;
+    double rr = minimage(posw - node, invL, L);
+    w = delta4f((float)(rr * invd));
+  }
+}
+
+// First node index of the stencil in dimension d, for the cell-centre
+// (face == 0) or the face (face == 1) node family; the index arithmetic of
+// stencil_node.
+__device__ __forceinline__ int stencil_base(const Params& P, int d, int face, double posc) {
+  const int m = d == 0 ? P.mx : (d == 1 ? P.my : P.mz);
+  const double h = d == 0 ? P.dx : (d == 1 ? P.dy : P.dz);
+  const double invd = d == 0 ? P.invdx : (d == 1 ? P.invdy : P.invdz);
+  const double L = d == 0 ? P.lx : (d == 1 ? P.ly : P.lz);
+  const double invL = d == 0 ? P.invlx : (d == 1 ? P.invly : P.invlz);
+  const double off = face ? __dmul_rn(0.5, h) : 0.0;
+  double r = P.kernel == 3 ? __dsub_rn(posc, off) : __dsub_rn(__dsub_rn(posc, off), __dmul_rn(0.5, h));
+  return cellidx(minimage(r, invL, L), invd, m);
+}
+
+// Warp-shared stencil of one particle for all three components.  Per
+// dimension d there are two node families: cell centres (components with
+// comp != d) and faces (comp == d); with n nodes each that is 6n values,
+// lane (f * 3 + d) * n + k computing family f, dimension d, node k.  Every
+// lane calls this; the result stays in the computing lane and is read with
+// stencil_get.
+struct WarpStencil {
+  int j;
+  float w;
+};
+
+__device__ __forceinline__ WarpStencil warp_stencil(const Params& P, const double posc[3],
+                                                    const double posw[3], int lane) {
+  WarpStencil s{0, 0.0f};
+  const int n = P.kernel;
+  if (lane < 6 * n) {
+    int k = lane % n, fd = lane / n;
+    int f = fd / 3, d = fd - 3 * f;
+    // family f = 1 is the face family of dimension d: use comp = d
+    stencil_node(P, d, f == 1 ? d : (d + 1) % 3, posc[d], posw[d], k, s.j, s.w);
+  }
+  return s;
+}
+
+// node k of dimension d for component comp, from the lanes of warp_stencil
+__device__ __forceinline__ void stencil_get(const WarpStencil& s, int n, int comp, int d, int k,
+                                            int& j, float& w) {
+  int src = ((comp == d ? 3 : 0) + d) * n + k;
+  j = __shfl_sync(0xffffffffu, s.j, src);
+  w = __shfl_sync(0xffffffffu, s.w, src);
+}
+
 __device__ __forceinline__ void set_err(int* err, int bit) {
   atomicOr(&err[ERR_BITS], bit);
   err[ERR_ANY] = 1;
@@ -223,10 +296,9 @@ void launch_forces(const Params& P, const double* q, const int* cell_of, const i
                    const int* bfp_off, const double* bfp_k, const double* bfp_r0,
                    const double* bfp_xyz, const float* ljtab, double* F, int* err,
                    cudaStream_t s);
-void launch_spread_force(const Params& P, const double* q, const double* F,
-                         unsigned long long* grid, int* err, cudaStream_t s);
-void launch_spread_drift(const Params& P, const double* q, const float* noise, int sign,
-                         unsigned long long* grid, int* err, cudaStream_t s);
+void launch_spread(const Params& P, int drift, const int* order, const double* qf,
+                   const double* F, const double* q0, const float* noise,
+                   unsigned long long* grid, int* err, cudaStream_t s);
 void launch_interp_update(const Params& P, int stage, const double* qpos, const double* q0,
                           const double* F, const float* noise, const float* v, double* qout,
                           int* err, cudaStream_t s);
@@ -239,7 +311,8 @@ FftPlan* fft_plan_create(const Params& P);
 void fft_plan_destroy(FftPlan* fp);
 // W source: the fixed-point spread grid plus the stochastic stress of draw t
 // (nsets = 1 or 2) when wext == nullptr, or a given float field wext.
-void launch_solve(const Params& P, FftPlan* fp, const unsigned long long* grid, const float* noise,
-                  int nsets, const float* wext, float2* spec, float* v, cudaStream_t s,
-                  Prof* prof = nullptr);
+// wbuf: 3 nc floats that receive W; the spread field is cleared on the way.
+void launch_solve(const Params& P, FftPlan* fp, unsigned long long* grid, const float* noise,
+                  int nsets, const float* wext, float* wbuf, float2* spec, float* v,
+                  cudaStream_t s, Prof* prof = nullptr);
 }  // namespace fsl

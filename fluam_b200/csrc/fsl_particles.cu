@@ -247,29 +247,33 @@ __global__ void k_forces(Params P, const double* __restrict__ q, const int* __re
                          const double* __restrict__ bfp_r0, const double* __restrict__ bfp_xyz,
                          const float* __restrict__ ljtab, double* __restrict__ F,
                          int* __restrict__ err) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.np) return;
+  // eight lanes per particle: they share the bonds and the 27 neighbour
+  // cells (cells sub, sub+8, ...), then sum their partial forces
+  const int sub = threadIdx.x & 7;
+  const int ig = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 3);
+  const bool active = ig < P.np;  // inactive lanes still join the shuffles
+  const int i = active ? ig : 0;
   const int np = P.np;
   double rx = q[i], ry = q[np + i], rz = q[2 * np + i];
   double fx = 0.0, fy = 0.0, fz = 0.0;
-  if (P.bonded) {
+  if (P.bonded && active) {
     int nb = bpp_cnt[i], off = bpp_off[i];
-    for (int j = 0; j < nb; ++j) {
+    for (int j = sub; j < nb; j += 8) {
       int idx = bpp_idx[off + j];
       bond_force(rx, ry, rz, q[idx], q[np + idx], q[2 * np + idx], bpp_k[off + j],
                  bpp_r0[off + j], fx, fy, fz);
     }
     nb = bfp_cnt[i];
     off = bfp_off[i];
-    for (int j = 0; j < nb; ++j) {
+    for (int j = sub; j < nb; j += 8) {
       const double* p = bfp_xyz + 3 * (off + j);
       bond_force(rx, ry, rz, p[0], p[1], p[2], bfp_k[off + j], bfp_r0[off + j], fx, fy, fz);
     }
   }
-  if (P.nonbonded && P.pair != 0) {
+  if (P.nonbonded && P.pair != 0 && active) {
     int c = cell_of[i];
     int cx = c % P.mnx, cy = (c / P.mnx) % P.mny, cz = c / (P.mnx * P.mny);
-    for (int nn = 0; nn < 27; ++nn) {
+    for (int nn = sub; nn < 27; nn += 8) {
       int ox = (cx + c_nb_order[nn][0] + P.mnx) % P.mnx;
       int oy = (cy + c_nb_order[nn][1] + P.mny) % P.mny;
       int oz = (cz + c_nb_order[nn][2] + P.mnz) % P.mnz;
@@ -297,6 +301,14 @@ __global__ void k_forces(Params P, const double* __restrict__ q, const int* __re
       }
     }
   }
+  // fixed butterfly order within the eight lanes: the same sum on every run
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (sub != 0 || !active) return;
   if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) set_err(err, 2);
   F[i] = fx;
   F[np + i] = fy;
@@ -310,124 +322,160 @@ void launch_forces(const Params& P, const double* q, const int* cell_of, const i
                    const double* bfp_xyz, const float* ljtab, double* F, int* err,
                    cudaStream_t s) {
   if (P.np == 0) return;
-  int tb = 128;
-  k_forces<<<(P.np + tb - 1) / tb, tb, 0, s>>>(P, q, cell_of, start, sorted, bpp_cnt, bpp_off,
+  const int tb = 256, per_block = tb / 8;
+  k_forces<<<(P.np + per_block - 1) / per_block, tb, 0, s>>>(P, q, cell_of, start, sorted, bpp_cnt, bpp_off,
                                                bpp_idx, bpp_k, bpp_r0, bfp_cnt, bfp_off, bfp_k,
                                                bfp_r0, bfp_xyz, ljtab, F, err);
 }
 
 // ------------------------------------------------------------- spreading ---
-// One thread per (particle, component): n^3 fixed-point atomic adds of
-// w * value onto the staggered field of that component.  Replaces the slot
-// writes of kernelSpreadParticlesForceStokesLimit + the gather of
-// addSpreadedForcesStokesLimit (src/stokesLimitFunctions.cu:659-1681); the
-// 1/dV of the gather is applied when the field is read back.
-__device__ __forceinline__ void spread_one(const Params& P, int comp, const double posc[3],
-                                           const double posw[3], double value,
-                                           unsigned long long* __restrict__ grid,
-                                           int* __restrict__ err) {
-  Stencil st;
-  make_stencil(P, comp, posc, posw, st);
-  unsigned long long* g = grid + (size_t)comp * P.nc;
-  const int n = P.kernel;
-  double vs = value * kFixedScale;
+// One warp per (entry, component); lane l takes stencil nodes l, l+32, ...
+// (x fastest, so a warp's atomics fall on a few 32-byte sectors) and adds
+// w * value in 64-bit fixed point to the staggered field of that component.
+// Replaces the slot writes of kernelSpreadParticlesForceStokesLimit and
+// kernelSpreadParticlesDrift + the gather of addSpreadedForcesStokesLimit
+// (src/stokesLimitFunctions.cu:659-1681, 1705-2255); the 1/dV of the gather
+// is applied when the field is read back.
+//
+// Entries [0, nforce) spread F of particle order[e] at qf; entries
+// [nforce, nforce + 2 np) spread the RFD drift (kT/delta) sign W_p from
+// q + sign (delta/2) W_p, sign + for the first np and - for the second.  In
+// reference mode the drift's nodes come from the displaced position and its
+// weights from q, as the reference does.
+__device__ __forceinline__ void spread_entry(const Params& P, const double posc[3],
+                                             const double posw[3], const double val[3],
+                                             unsigned long long* __restrict__ grid, int lane,
+                                             bool& sat) {
+  const int n = P.kernel, n3 = n * n * n, total = 3 * n3;
+  const WarpStencil st = warp_stencil(P, posc, posw, lane);
+  const int iters = (total + 31) >> 5;
+  for (int it = 0; it < iters; ++it) {
+    const int id = (it << 5) + lane;
+    const bool valid = id < total;
+    const int idc = valid ? id : 0;  // every lane takes part in the shuffles
+    const int comp = idc / n3, r = idc - comp * n3;
+    const int a = r % n, b = (r / n) % n, c = r / (n * n);
+    int x, y, z;
+    float wx, wy, wz;
+    stencil_get(st, n, comp, 0, a, x, wx);
+    stencil_get(st, n, comp, 1, b, y, wy);
+    stencil_get(st, n, comp, 2, c, z, wz);
+    if (!valid) continue;
+    const double vc = comp == 0 ? val[0] : (comp == 1 ? val[1] : val[2]);
+    double v = (double)(wx * (wy * wz)) * (vc * kFixedScale);
+    sat |= !(fabs(v) < kFixedMax);
+    long long iv = sat ? 0ll : __double2ll_rn(v);
+    if (iv != 0)
+      atomicAdd(grid + (size_t)comp * P.nc + x + (size_t)P.mx * (y + (size_t)P.my * z),
+                (unsigned long long)iv);
+  }
+}
+
+// One warp per entry (all three components of one spread of one particle).
+__global__ void k_spread(Params P, int nforce, int drift, const int* __restrict__ order,
+                         const double* __restrict__ qf, const double* __restrict__ F,
+                         const double* __restrict__ q0, const float* __restrict__ noise,
+                         unsigned long long* __restrict__ grid, int* __restrict__ err) {
+  const int lane = threadIdx.x & 31;
+  const long e = (long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int np = P.np;
+  const long nent = (long)nforce + (drift ? (long)np : 0l);
+  if (e >= nent) return;  // uniform per warp
   bool sat = false;
-  for (int c = 0; c < n; ++c) {
-    int z = st.j0[2] + c;
-    z -= (z >= P.mz) ? P.mz : 0;
-    for (int b = 0; b < n; ++b) {
-      int y = st.j0[1] + b;
-      y -= (y >= P.my) ? P.my : 0;
-      float wyz = st.w[1][b] * st.w[2][c];
-      size_t row = (size_t)P.mx * (y + (size_t)P.my * z);
-      for (int a = 0; a < n; ++a) {
-        int x = st.j0[0] + a;
-        x -= (x >= P.mx) ? P.mx : 0;
-        double val = (double)(st.w[0][a] * wyz) * vs;
-        sat |= !(fabs(val) < kFixedMax);
-        long long iv = sat ? 0ll : __double2ll_rn(val);
-        if (iv != 0) atomicAdd(g + row + x, (unsigned long long)iv);
+  if (e < nforce) {
+    int i = order ? order[e] : (int)e;
+    double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
+    double val[3] = {F[i], F[np + i], F[2 * (size_t)np + i]};
+    spread_entry(P, pos, pos, val, grid, lane, sat);
+  } else {
+    // both signs of the drift of one particle
+    int i = (int)(e - nforce);
+    if (order) i = order[i];
+    const size_t wbase = (size_t)6 * P.nc;
+    double W[3] = {(double)noise[wbase + i], (double)noise[wbase + np + i],
+                   (double)noise[wbase + 2 * np + i]};
+    double pos[3] = {q0[i], q0[np + i], q0[2 * np + i]};
+    double pp[3], pm[3], vp[3], vm[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      pp[d] = pos[d] + 0.5 * kRfdDelta * W[d];
+      pm[d] = pos[d] - 0.5 * kRfdDelta * W[d];
+      vp[d] = (P.kT / kRfdDelta) * W[d];
+      vm[d] = (P.kT / kRfdDelta) * -1 * W[d];
+    }
+    if (P.rfd != 1) {
+      // Reference mode weighs both spreads at q: where both displaced
+      // positions pick the same nodes the two fixed-point spreads are exact
+      // negatives of each other (same weights, opposite values, symmetric
+      // rounding), so they are skipped without changing the result.
+      bool same = true;
+      if (lane < 6) {
+        int f = lane / 3, d = lane - 3 * f;
+        same = stencil_base(P, d, f, pp[d]) == stencil_base(P, d, f, pm[d]);
       }
+      if (__all_sync(0xffffffffu, same)) return;
+      spread_entry(P, pp, pos, vp, grid, lane, sat);
+      spread_entry(P, pm, pos, vm, grid, lane, sat);
+    } else {
+      spread_entry(P, pp, pp, vp, grid, lane, sat);
+      spread_entry(P, pm, pm, vm, grid, lane, sat);
     }
   }
   if (sat) set_err(err, 1);
 }
 
-__global__ void k_spread_force(Params P, const double* __restrict__ q,
-                               const double* __restrict__ F, unsigned long long* __restrict__ grid,
-                               int* __restrict__ err) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 3 * P.np) return;
-  int i = t / 3, comp = t - 3 * i;
-  const int np = P.np;
-  double pos[3] = {q[i], q[np + i], q[2 * np + i]};
-  spread_one(P, comp, pos, pos, F[comp * np + i], grid, err);
-}
-
-// RFD drift: (kT/delta) sign W_p spread from q + sign (delta/2) W_p
-// (src/stokesLimitFunctions.cu:1705-2255).  In reference mode the nodes come
-// from the displaced position and the weights from q, as the reference does.
-__global__ void k_spread_drift(Params P, const double* __restrict__ q,
-                               const float* __restrict__ noise, int sign,
-                               unsigned long long* __restrict__ grid, int* __restrict__ err) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 3 * P.np) return;
-  int i = t / 3, comp = t - 3 * i;
-  const int np = P.np;
-  const size_t wbase = (size_t)6 * P.nc;
-  double W[3] = {(double)noise[wbase + i], (double)noise[wbase + np + i],
-                 (double)noise[wbase + 2 * np + i]};
-  double pos[3] = {q[i], q[np + i], q[2 * np + i]};
-  double posd[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) posd[d] = pos[d] + sign * 0.5 * kRfdDelta * W[d];
-  double value = (P.kT / kRfdDelta) * sign * W[comp];
-  if (P.rfd == 1)
-    spread_one(P, comp, posd, posd, value, grid, err);
-  else
-    spread_one(P, comp, posd, pos, value, grid, err);
-}
-
-void launch_spread_force(const Params& P, const double* q, const double* F,
-                         unsigned long long* grid, int* err, cudaStream_t s) {
+// force spread of all particles (at qf, in the order of the cell list when
+// `order` is given) and, with drift != 0, the two RFD spreads at q0
+void launch_spread(const Params& P, int drift, const int* order, const double* qf,
+                   const double* F, const double* q0, const float* noise,
+                   unsigned long long* grid, int* err, cudaStream_t s) {
   if (P.np == 0) return;
-  int n = 3 * P.np, tb = 128;
-  k_spread_force<<<(n + tb - 1) / tb, tb, 0, s>>>(P, q, F, grid, err);
-}
-
-void launch_spread_drift(const Params& P, const double* q, const float* noise, int sign,
-                         unsigned long long* grid, int* err, cudaStream_t s) {
-  if (P.np == 0) return;
-  int n = 3 * P.np, tb = 128;
-  k_spread_drift<<<(n + tb - 1) / tb, tb, 0, s>>>(P, q, noise, sign, grid, err);
+  long nent = (long)P.np * (drift ? 2 : 1);
+  long threads = nent * 32;
+  const int tb = 256;
+  k_spread<<<(unsigned)((threads + tb - 1) / tb), tb, 0, s>>>(P, P.np, drift, order, qf, F, q0,
+                                                             noise, grid, err);
 }
 
 // -------------------------------------------------------- interpolation ---
-__device__ __forceinline__ float interp_one(const Params& P, int comp, const double pos[3],
-                                            const float* __restrict__ v) {
-  Stencil st;
-  make_stencil(P, comp, pos, pos, st);
-  const float* vc = v + (size_t)comp * P.nc;
-  const int n = P.kernel;
-  float sum = 0.0f;
-  for (int c = 0; c < n; ++c) {
-    int z = st.j0[2] + c;
-    z -= (z >= P.mz) ? P.mz : 0;
-    for (int b = 0; b < n; ++b) {
-      int y = st.j0[1] + b;
-      y -= (y >= P.my) ? P.my : 0;
-      float wyz = st.w[1][b] * st.w[2][c];
-      const float* row = vc + (size_t)P.mx * (y + (size_t)P.my * z);
-      float s = 0.0f;
-      for (int a = 0; a < n; ++a) {
-        int x = st.j0[0] + a;
-        x -= (x >= P.mx) ? P.mx : 0;
-        s = fmaf(st.w[0][a], __ldg(row + x), s);
-      }
-      sum = fmaf(wyz, s, sum);
-    }
+// One warp per particle: lane l reads nodes l, l+32, ... of the three
+// components' stencils and the warp sums w v per component in a fixed
+// butterfly order (src/stokesLimitFunctions.cu:2616-2642).  Every lane gets
+// the three sums.
+__device__ __forceinline__ void interp_particle(const Params& P, const double pos[3],
+                                                const float* __restrict__ v, int lane,
+                                                float u[3]) {
+  const int n = P.kernel, n3 = n * n * n, total = 3 * n3;
+  const WarpStencil st = warp_stencil(P, pos, pos, lane);
+  float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+  const int iters = (total + 31) >> 5;
+  for (int it = 0; it < iters; ++it) {
+    const int id = (it << 5) + lane;
+    const bool valid = id < total;
+    const int idc = valid ? id : 0;
+    const int comp = idc / n3, r = idc - comp * n3;
+    const int a = r % n, b = (r / n) % n, c = r / (n * n);
+    int x, y, z;
+    float wx, wy, wz;
+    stencil_get(st, n, comp, 0, a, x, wx);
+    stencil_get(st, n, comp, 1, b, y, wy);
+    stencil_get(st, n, comp, 2, c, z, wz);
+    if (!valid) continue;
+    float t = wx * (wy * wz) *
+              __ldg(v + (size_t)comp * P.nc + x + (size_t)P.mx * (y + (size_t)P.my * z));
+    if (comp == 0) s0 += t;
+    else if (comp == 1) s1 += t;
+    else s2 += t;
   }
-  return sum;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  u[0] = s0;
+  u[1] = s1;
+  u[2] = s2;
 }
 
 // stage 1: q^{n+1/2} = q^n + dt/2 J(q^n) v (+ extraMobility terms),
@@ -438,12 +486,17 @@ __global__ void k_interp_update(Params P, int stage, const double* __restrict__ 
                                 const double* __restrict__ q0, const double* __restrict__ F,
                                 const float* __restrict__ noise, const float* __restrict__ v,
                                 double* __restrict__ qout, int* __restrict__ err) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 3 * P.np) return;
-  int i = t / 3, comp = t - 3 * i;
+  const int lane = threadIdx.x & 31;
+  const long t = (long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  if (t >= P.np) return;  // uniform per warp
+  const int i = (int)t;
   const int np = P.np;
   double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
-  double u = (double)interp_one(P, comp, pos, v);
+  float us[3];
+  interp_particle(P, pos, v, lane, us);
+  if (lane >= 3) return;
+  const int comp = lane;  // lanes 0, 1, 2 update x, y, z
+  const double u = (double)(comp == 0 ? us[0] : (comp == 1 ? us[1] : us[2]));
   size_t k = (size_t)comp * np + i;
   double h = stage == 1 ? 0.5 * P.dt : P.dt;
   double r = q0[k] + h * u;
@@ -459,27 +512,35 @@ __global__ void k_interp_update(Params P, int stage, const double* __restrict__ 
 
 __global__ void k_interp(Params P, const double* __restrict__ qpos, const float* __restrict__ v,
                          double* __restrict__ u) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 3 * P.np) return;
-  int i = t / 3, comp = t - 3 * i;
+  const int lane = threadIdx.x & 31;
+  const long t = (long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  if (t >= P.np) return;  // uniform per warp
+  const int i = (int)t;
   const int np = P.np;
   double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
-  u[(size_t)comp * np + i] = (double)interp_one(P, comp, pos, v);
+  float us[3];
+  interp_particle(P, pos, v, lane, us);
+  if (lane < 3) u[(size_t)lane * np + i] = (double)(lane == 0 ? us[0] : (lane == 1 ? us[1] : us[2]));
+}
+
+static unsigned warp_blocks(long warps, int tb) {
+  return (unsigned)((warps * 32 + tb - 1) / tb);
 }
 
 void launch_interp_update(const Params& P, int stage, const double* qpos, const double* q0,
                           const double* F, const float* noise, const float* v, double* qout,
                           int* err, cudaStream_t s) {
   if (P.np == 0) return;
-  int n = 3 * P.np, tb = 128;
-  k_interp_update<<<(n + tb - 1) / tb, tb, 0, s>>>(P, stage, qpos, q0, F, noise, v, qout, err);
+  const int tb = 256;
+  k_interp_update<<<warp_blocks(P.np, tb), tb, 0, s>>>(P, stage, qpos, q0, F, noise, v, qout,
+                                                           err);
 }
 
 void launch_interp(const Params& P, const double* qpos, const float* v, double* u,
                    cudaStream_t s) {
   if (P.np == 0) return;
-  int n = 3 * P.np, tb = 128;
-  k_interp<<<(n + tb - 1) / tb, tb, 0, s>>>(P, qpos, v, u);
+  const int tb = 256;
+  k_interp<<<warp_blocks(P.np, tb), tb, 0, s>>>(P, qpos, v, u);
 }
 
 __global__ void k_step_counter(uint64_t* t_dev) { *t_dev += 1; }
