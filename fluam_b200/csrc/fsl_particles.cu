@@ -272,11 +272,15 @@ __global__ void k_forces(Params P, const double* __restrict__ q, const int* __re
   }
   if (P.nonbonded && P.pair != 0 && active) {
     int c = cell_of[i];
-    int cx = c % P.mnx, cy = (c / P.mnx) % P.mny, cz = c / (P.mnx * P.mny);
+    int cxy = c % (P.mnx * P.mny);
+    int cz = c / (P.mnx * P.mny), cy = cxy / P.mnx, cx = cxy - cy * P.mnx;
     for (int nn = sub; nn < 27; nn += 8) {
-      int ox = (cx + c_nb_order[nn][0] + P.mnx) % P.mnx;
-      int oy = (cy + c_nb_order[nn][1] + P.mny) % P.mny;
-      int oz = (cz + c_nb_order[nn][2] + P.mnz) % P.mnz;
+      // the 27 cells in z-major order; the summation order only moves the
+      // result at the FP64 rounding level
+      int ox = cx + nn % 3 - 1, oy = cy + (nn / 3) % 3 - 1, oz = cz + nn / 9 - 1;
+      ox += ox < 0 ? P.mnx : (ox >= P.mnx ? -P.mnx : 0);
+      oy += oy < 0 ? P.mny : (oy >= P.mny ? -P.mny : 0);
+      oz += oz < 0 ? P.mnz : (oz >= P.mnz ? -P.mnz : 0);
       int cc = ox + oy * P.mnx + oz * P.mnx * P.mny;
       int e = start[cc + 1];
       for (int jj = start[cc]; jj < e; ++jj) {
@@ -342,13 +346,15 @@ void launch_forces(const Params& P, const double* q, const int* cell_of, const i
 // q + sign (delta/2) W_p, sign + for the first np and - for the second.  In
 // reference mode the drift's nodes come from the displaced position and its
 // weights from q, as the reference does.
+template <int KN>  // kernel width 3 or 4
 __device__ __forceinline__ void spread_entry(const Params& P, const double posc[3],
                                              const double posw[3], const double val[3],
                                              unsigned long long* __restrict__ grid, int lane,
                                              bool& sat) {
-  const int n = P.kernel, n3 = n * n * n, total = 3 * n3;
+  constexpr int n = KN, n3 = n * n * n, total = 3 * n3;
   const WarpStencil st = warp_stencil(P, posc, posw, lane);
-  const int iters = (total + 31) >> 5;
+  constexpr int iters = (total + 31) >> 5;
+#pragma unroll
   for (int it = 0; it < iters; ++it) {
     const int id = (it << 5) + lane;
     const bool valid = id < total;
@@ -372,6 +378,7 @@ __device__ __forceinline__ void spread_entry(const Params& P, const double posc[
 }
 
 // One warp per entry (all three components of one spread of one particle).
+template <int KN>
 __global__ void k_spread(Params P, int nforce, int drift, const int* __restrict__ order,
                          const double* __restrict__ qf, const double* __restrict__ F,
                          const double* __restrict__ q0, const float* __restrict__ noise,
@@ -386,7 +393,7 @@ __global__ void k_spread(Params P, int nforce, int drift, const int* __restrict_
     int i = order ? order[e] : (int)e;
     double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
     double val[3] = {F[i], F[np + i], F[2 * (size_t)np + i]};
-    spread_entry(P, pos, pos, val, grid, lane, sat);
+    spread_entry<KN>(P, pos, pos, val, grid, lane, sat);
   } else {
     // both signs of the drift of one particle
     int i = (int)(e - nforce);
@@ -414,11 +421,11 @@ __global__ void k_spread(Params P, int nforce, int drift, const int* __restrict_
         same = stencil_base(P, d, f, pp[d]) == stencil_base(P, d, f, pm[d]);
       }
       if (__all_sync(0xffffffffu, same)) return;
-      spread_entry(P, pp, pos, vp, grid, lane, sat);
-      spread_entry(P, pm, pos, vm, grid, lane, sat);
+      spread_entry<KN>(P, pp, pos, vp, grid, lane, sat);
+      spread_entry<KN>(P, pm, pos, vm, grid, lane, sat);
     } else {
-      spread_entry(P, pp, pp, vp, grid, lane, sat);
-      spread_entry(P, pm, pm, vm, grid, lane, sat);
+      spread_entry<KN>(P, pp, pp, vp, grid, lane, sat);
+      spread_entry<KN>(P, pm, pm, vm, grid, lane, sat);
     }
   }
   if (sat) set_err(err, 1);
@@ -433,8 +440,11 @@ void launch_spread(const Params& P, int drift, const int* order, const double* q
   long nent = (long)P.np * (drift ? 2 : 1);
   long threads = nent * 32;
   const int tb = 256;
-  k_spread<<<(unsigned)((threads + tb - 1) / tb), tb, 0, s>>>(P, P.np, drift, order, qf, F, q0,
-                                                             noise, grid, err);
+  unsigned nb = (unsigned)((threads + tb - 1) / tb);
+  if (P.kernel == 4)
+    k_spread<4><<<nb, tb, 0, s>>>(P, P.np, drift, order, qf, F, q0, noise, grid, err);
+  else
+    k_spread<3><<<nb, tb, 0, s>>>(P, P.np, drift, order, qf, F, q0, noise, grid, err);
 }
 
 // -------------------------------------------------------- interpolation ---
@@ -442,13 +452,17 @@ void launch_spread(const Params& P, int drift, const int* order, const double* q
 // components' stencils and the warp sums w v per component in a fixed
 // butterfly order (src/stokesLimitFunctions.cu:2616-2642).  Every lane gets
 // the three sums.
+template <int KN>
 __device__ __forceinline__ void interp_particle(const Params& P, const double pos[3],
                                                 const float* __restrict__ v, int lane,
                                                 float u[3]) {
-  const int n = P.kernel, n3 = n * n * n, total = 3 * n3;
+  constexpr int n = KN, n3 = n * n * n, total = 3 * n3;
+  constexpr int iters = (total + 31) >> 5;
   const WarpStencil st = warp_stencil(P, pos, pos, lane);
-  float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
-  const int iters = (total + 31) >> 5;
+  // gather every node's address and weight first, then all loads at once
+  float wt[iters];
+  const float* ad[iters];
+#pragma unroll
   for (int it = 0; it < iters; ++it) {
     const int id = (it << 5) + lane;
     const bool valid = id < total;
@@ -460,9 +474,18 @@ __device__ __forceinline__ void interp_particle(const Params& P, const double po
     stencil_get(st, n, comp, 0, a, x, wx);
     stencil_get(st, n, comp, 1, b, y, wy);
     stencil_get(st, n, comp, 2, c, z, wz);
-    if (!valid) continue;
-    float t = wx * (wy * wz) *
-              __ldg(v + (size_t)comp * P.nc + x + (size_t)P.mx * (y + (size_t)P.my * z));
+    wt[it] = valid ? wx * (wy * wz) : 0.0f;
+    ad[it] = v + (size_t)comp * P.nc + x + (size_t)P.mx * (y + (size_t)P.my * z);
+  }
+  float val[iters];
+#pragma unroll
+  for (int it = 0; it < iters; ++it) val[it] = __ldg(ad[it]);
+  float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+  for (int it = 0; it < iters; ++it) {
+    const int id = (it << 5) + lane;
+    const int comp = (id < total ? id : 0) / n3;
+    float t = wt[it] * val[it];
     if (comp == 0) s0 += t;
     else if (comp == 1) s1 += t;
     else s2 += t;
@@ -482,6 +505,7 @@ __device__ __forceinline__ void interp_particle(const Params& P, const double po
 //          src/stokesLimitFunctions.cu:2646-2650
 // stage 2: q^{n+1}   = q^n + dt J(q^{n+1/2}) v (+ extraMobility terms),
 //          src/stokesLimitFunctions.cu:3676-3681
+template <int KN>
 __global__ void k_interp_update(Params P, int stage, const double* __restrict__ qpos,
                                 const double* __restrict__ q0, const double* __restrict__ F,
                                 const float* __restrict__ noise, const float* __restrict__ v,
@@ -493,7 +517,7 @@ __global__ void k_interp_update(Params P, int stage, const double* __restrict__ 
   const int np = P.np;
   double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
   float us[3];
-  interp_particle(P, pos, v, lane, us);
+  interp_particle<KN>(P, pos, v, lane, us);
   if (lane >= 3) return;
   const int comp = lane;  // lanes 0, 1, 2 update x, y, z
   const double u = (double)(comp == 0 ? us[0] : (comp == 1 ? us[1] : us[2]));
@@ -510,6 +534,7 @@ __global__ void k_interp_update(Params P, int stage, const double* __restrict__ 
   qout[k] = r;
 }
 
+template <int KN>
 __global__ void k_interp(Params P, const double* __restrict__ qpos, const float* __restrict__ v,
                          double* __restrict__ u) {
   const int lane = threadIdx.x & 31;
@@ -519,7 +544,7 @@ __global__ void k_interp(Params P, const double* __restrict__ qpos, const float*
   const int np = P.np;
   double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
   float us[3];
-  interp_particle(P, pos, v, lane, us);
+  interp_particle<KN>(P, pos, v, lane, us);
   if (lane < 3) u[(size_t)lane * np + i] = (double)(lane == 0 ? us[0] : (lane == 1 ? us[1] : us[2]));
 }
 
@@ -532,15 +557,22 @@ void launch_interp_update(const Params& P, int stage, const double* qpos, const 
                           int* err, cudaStream_t s) {
   if (P.np == 0) return;
   const int tb = 256;
-  k_interp_update<<<warp_blocks(P.np, tb), tb, 0, s>>>(P, stage, qpos, q0, F, noise, v, qout,
-                                                           err);
+  if (P.kernel == 4)
+    k_interp_update<4><<<warp_blocks(P.np, tb), tb, 0, s>>>(P, stage, qpos, q0, F, noise, v, qout,
+                                                            err);
+  else
+    k_interp_update<3><<<warp_blocks(P.np, tb), tb, 0, s>>>(P, stage, qpos, q0, F, noise, v, qout,
+                                                            err);
 }
 
 void launch_interp(const Params& P, const double* qpos, const float* v, double* u,
                    cudaStream_t s) {
   if (P.np == 0) return;
   const int tb = 256;
-  k_interp<<<warp_blocks(P.np, tb), tb, 0, s>>>(P, qpos, v, u);
+  if (P.kernel == 4)
+    k_interp<4><<<warp_blocks(P.np, tb), tb, 0, s>>>(P, qpos, v, u);
+  else
+    k_interp<3><<<warp_blocks(P.np, tb), tb, 0, s>>>(P, qpos, v, u);
 }
 
 __global__ void k_step_counter(uint64_t* t_dev) { *t_dev += 1; }
