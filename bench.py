@@ -116,8 +116,12 @@ def stage_bytes(name, P):
         "forces": 52 * npart + 4 * P["mN"],
         "grid_zero": 24 * nc,
         "spread": 48 * npart + 2 * touched,
-        "spread_rfd": 120 * npart + 2 * 3 * 8 * min(P["nc"], 3 * k ** 3 * npart),
-        "plane_fwd": 24 * nc + 36 * nc + spec,     # grid + mean noise of the 2 solves + spectrum
+        # force spread + the drift test (reference mode: the drift spreads
+        # cancel and are skipped except at stencil changes)
+        "spread_rfd": 48 * npart + 2 * touched + 36 * npart,
+        # int64 field read + cleared, mean noise of the two solves, W written
+        "wbuild": 24 * nc + 24 * nc + 36 * nc + 12 * nc,
+        "plane_fwd": 12 * nc + spec,               # W read, half spectrum written
         "plane_inv": spec + 12 * nc,
         "xfwd": 24 * nc + 36 * nc + spec,
         "yfft": 2 * spec,
@@ -300,6 +304,14 @@ def main():
         avg_ms = dv["total_ms"] / max(dv["launches"], 1)
         abytes = stage_bytes(dname, P)
         achieved = abytes / (avg_ms * 1e-3) / 1e9
+        traffic = None  # DRAM bytes of one launch from the committed ncu capture
+        try:
+            with open(os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload.replace("plain_", "plain"))) as f:
+                tr = json.load(f)
+            if dname in tr["stages"]:
+                traffic = tr["stages"][dname]["dram_bytes"]
+        except (OSError, KeyError, ValueError):
+            traffic = None
         cpu = None
         if not args.no_cpu_baseline:
             try:
@@ -320,7 +332,7 @@ def main():
                     "h2d_bytes_per_step": 24 * npart, "d2h_bytes_per_step": 24 * npart},
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": None, "algorithmic_bytes_per_launch": abytes,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": abytes,
                          "avg_launch_ms": avg_ms},
             "stages_ms_per_step": {k: v["total_ms"] / args.steps for k, v in sorted(stages.items())},
             "profiled_ms_per_step": prof_ms / args.steps,
