@@ -6,13 +6,15 @@
 // doubleComplexToDoubleNormalized).  The reference runs 3 + 3 cuFFT Z2Z
 // transforms and 5 elementwise passes per solve in FP64; here the transform is
 // a hand-written FP32 mixed-radix Stockham FFT in shared memory, done as
-// three passes over the half spectrum:
-//   k_xfwd   builds W in registers from the fixed-point spread field and the
-//            noise, and transforms two real x-lines as one complex line;
-//   k_yfft   transforms along y (forward and inverse);
-//   k_zsolve transforms along z, applies the spectral multiplier to all three
-//            components of each mode, and transforms back along z;
-//   k_xinv   rebuilds two real x-lines from their half spectra.
+// passes over the half spectrum:
+//   k_wbuild    builds W from the fixed-point spread field and the noise;
+//   k_plane_fwd 2-D real-to-complex transform of one xy plane per block;
+//   k_zsolve    transforms along z, applies the spectral multiplier to all
+//               three components of each mode, and transforms back along z;
+//   k_plane_inv 2-D complex-to-real transform of one xy plane per block.
+// Planes too large for shared memory take five passes instead (k_xfwd,
+// k_yfft, k_zsolve, k_yfft, k_xinv).  Every kernel serves a batch of
+// instances of one size class; the grid's last dimension picks the instance.
 // The multiplier keeps Hermitian symmetry (the sign of sin(pi j/m) for
 // j > m/2 cancels between gradient and shift), so the real-to-complex form
 // equals the reference's Re(IFFT(...)) up to rounding.
@@ -33,18 +35,19 @@ struct Radices {
 struct FftPlan {
   Radices rx, ry, rz;
   float2 *twx = nullptr, *twy = nullptr, *twz = nullptr;  // exp(-2 pi i t / m)
-  float *gx = nullptr, *gy = nullptr, *gz = nullptr;      // 2/h sin(pi j / m)
-  float2 *ex = nullptr, *ey = nullptr, *ez = nullptr;     // exp(+i pi j / m)
+  // sin(pi j / m); the kernel multiplies by the instance's 2/h, so one table
+  // serves every instance of a size class whatever its box
+  float *sx = nullptr, *sy = nullptr, *sz = nullptr;
+  float2 *ex = nullptr, *ey = nullptr, *ez = nullptr;  // exp(+i pi j / m)
   size_t smem_x = 0, smem_y = 0, smem_z = 0, smem_plane = 0;
   bool use_plane = false;  // whole-plane kernels fit in shared memory
   bool ok = false;
-  // kernel instances: compiled sizes when available, else runtime sizes
-  void (*plane_fwd)(Params, Radices, Radices, const float2*, const float2*, struct WSource,
-                    float2*) = nullptr;
-  void (*plane_inv)(Params, Radices, Radices, const float2*, const float2*, const float2*,
-                    float*) = nullptr;
-  void (*zsolve)(Params, Radices, const float2*, const float*, const float*, const float*,
-                 const float2*, const float2*, const float2*, float2*) = nullptr;
+  // kernel instances: compiled sizes when available, else runtime sizes;
+  // [0] batched, [1] single instance
+  void (*plane_fwd[2])(RepSrc, Rep, Radices, Radices, const float2*, const float2*) = {};
+  void (*plane_inv[2])(RepSrc, Rep, Radices, Radices, const float2*, const float2*) = {};
+  void (*zsolve[2])(RepSrc, Rep, Radices, const float2*, const float*, const float*, const float*,
+                    const float2*, const float2*, const float2*) = {};
 };
 
 static bool factorize(int n, Radices& R) {
@@ -292,13 +295,46 @@ __device__ __forceinline__ float stress_div(const Params& P, const float* __rest
   }
 }
 
-// W build + real-to-complex transform along x.  Block (bx, comp) handles the
-// row pairs [bx*kXPairs, ...); row R = y + my z; the pair (2p, 2p+1) is
-// transformed as the complex line row_2p + i row_2p+1.
+// W = f + c div(Sigma) of all three components of every cell
+// (src/stokesLimitFunctions.cu:2281-2378, 3922-4069): the fixed-point spread
+// field times 2^-40/dV plus the stochastic stress divergence, with
+// c = sqrt(2) (one stress sample) or sqrt(1/2) (two samples).  The spread
+// field is cleared behind the read, ready for the next spread.  One thread
+// per cell: the loads of a warp are coalesced rows, full occupancy.
+template <bool ONE>
+__global__ void k_wbuild(FSL_KARGS, int nsets) {
+  FSL_REP_AT(blockIdx.y);
+  const double nfac = nsets > 1 ? 0.70710678118654752440 : 1.41421356237309504880;
+  const float scale = (float)(kFixedInv / P.dV);
+  const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
+  const float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
+  const float a4x = (float)P.invdx * f4, a4y = (float)P.invdy * f4, a4z = (float)P.invdz * f4;
+  const float* n1 = R.noise;
+  const float* n2 = R.noise + (size_t)6 * P.nc + (size_t)9 * P.np;
+  const size_t nc = (size_t)P.nc;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc;
+       i += (size_t)gridDim.x * blockDim.x) {
+    int x = (int)(i % P.mx), r = (int)(i / P.mx);
+    int y = r % P.my, z = r / P.my;
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      long long g = (long long)R.grid[comp * nc + i];
+      float w = (float)((double)g * (double)scale);
+      w += stress_div(P, n1, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
+      if (nsets > 1) w += stress_div(P, n2, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
+      R.wbuf[comp * nc + i] = w;
+      R.grid[comp * nc + i] = 0ull;
+    }
+  }
+}
+
+// Real-to-complex transform along x of W.  Block (bx, comp, instance)
+// handles the row pairs [bx*kXPairs, ...); row R = y + my z; the pair
+// (2p, 2p+1) is transformed as the complex line row_2p + i row_2p+1.
+template <bool ONE>
 __global__ void __launch_bounds__(kFftThreads)
-    k_xfwd(Params P, Radices R, const float2* __restrict__ tw,
-           const unsigned long long* __restrict__ grid, const float* __restrict__ noise,
-           int nsets, float nfac, const float* __restrict__ wext, float2* __restrict__ spec) {
+    k_xfwd(FSL_KARGS, Radices Rx, const float2* __restrict__ tw) {
+  FSL_REP_AT(blockIdx.z);
   extern __shared__ float2 smem[];
   const int mx = P.mx, mxh = P.mxh;
   const int LS = kXPairs + 1;
@@ -309,35 +345,18 @@ __global__ void __launch_bounds__(kFftThreads)
   const int nrows = P.my * P.mz;
   const int row0 = blockIdx.x * 2 * kXPairs;
   for (int t = threadIdx.x; t < mx; t += blockDim.x) stw[t] = tw[t];
-
-  const float scale = (float)(kFixedInv / P.dV);
-  float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
-  float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
-  float a4x = (float)P.invdx * f4, a4y = (float)P.invdy * f4, a4z = (float)P.invdz * f4;
-  const size_t off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
+  const float* W = R.wbuf + (size_t)comp * P.nc;
   float* Af = reinterpret_cast<float*>(A);
   for (int e = threadIdx.x; e < 2 * kXPairs * mx; e += blockDim.x) {
     int rl = e / mx, x = e - rl * mx;
     int Rw = row0 + rl;
-    float w = 0.0f;
-    if (Rw < nrows) {
-      int i = x + mx * Rw;
-      if (wext) {
-        w = wext[(size_t)comp * P.nc + i];
-      } else {
-        int y = Rw % P.my, z = Rw / P.my;
-        long long g = (long long)grid[(size_t)comp * P.nc + i];
-        w = (float)((double)g * (double)scale);
-        w += stress_div(P, noise, comp, x, y, z, i, a1x, a1y, a1z, a4x, a4y, a4z);
-        if (nsets > 1)
-          w += stress_div(P, noise + off2, comp, x, y, z, i, a1x, a1y, a1z, a4x, a4y, a4z);
-      }
-    }
+    float w = Rw < nrows ? W[x + (size_t)mx * Rw] : 0.0f;
     Af[2 * (x * LS + (rl >> 1)) + (rl & 1)] = w;
   }
   __syncthreads();
-  float2* Z = fft_lines(A, B, LS, kXPairs, R, stw, -1);
+  float2* Z = fft_lines(A, B, LS, kXPairs, Rx, stw, -1);
   // split the two spectra: X_k = (Z_k + conj Z_-k)/2, Y_k = -i (Z_k - conj Z_-k)/2
+  float2* out = R.spec + (size_t)comp * nrows * mxh;
   for (int e = threadIdx.x; e < kXPairs * mxh; e += blockDim.x) {
     int l = e / mxh, k = e - l * mxh;
     int Rw = row0 + 2 * l;
@@ -346,31 +365,33 @@ __global__ void __launch_bounds__(kFftThreads)
     float2 zm = Z[((mx - k) % mx) * LS + l];
     float2 X = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
     float2 Y = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
-    float2* out = spec + (size_t)comp * nrows * mxh;
     out[(size_t)Rw * mxh + k] = X;
     if (Rw + 1 < nrows) out[(size_t)(Rw + 1) * mxh + k] = Y;
   }
 }
 
 // Complex transform along y of the half spectrum, in place.
+// blockIdx.z = 3 * instance + component.
+template <bool ONE>
 __global__ void __launch_bounds__(kFftThreads)
-    k_yfft(Params P, Radices R, const float2* __restrict__ tw, float2* __restrict__ spec, int dir) {
+    k_yfft(FSL_KARGS, Radices Ry, const float2* __restrict__ tw, int dir) {
+  FSL_REP_AT(blockIdx.z / 3);
   extern __shared__ float2 smem[];
   const int my = P.my, mxh = P.mxh;
   const int LS = kYTile;
   float2* A = smem;
   float2* B = A + my * LS;
   float2* stw = B + my * LS;
-  const int kx0 = blockIdx.x * kYTile, z = blockIdx.y, comp = blockIdx.z;
+  const int kx0 = blockIdx.x * kYTile, z = blockIdx.y, comp = blockIdx.z % 3;
   for (int t = threadIdx.x; t < my; t += blockDim.x) stw[t] = tw[t];
-  float2* base = spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
+  float2* base = R.spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
   for (int e = threadIdx.x; e < my * kYTile; e += blockDim.x) {
     int l = e % kYTile, y = e / kYTile;
     int kx = kx0 + l;
     A[y * LS + l] = kx < mxh ? base[(size_t)y * mxh + kx] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2* Z = fft_lines(A, B, LS, kYTile, R, stw, dir);
+  float2* Z = fft_lines(A, B, LS, kYTile, Ry, stw, dir);
   for (int e = threadIdx.x; e < my * kYTile; e += blockDim.x) {
     int l = e % kYTile, y = e / kYTile;
     int kx = kx0 + l;
@@ -383,22 +404,24 @@ __global__ void __launch_bounds__(kFftThreads)
 // src/realToComplex.cu:263-303 and the 1/ncells of :40-59):
 //   W'_a = W_a e^{-i pi j_a/m_a};  G2 = |g|^2, g_a = 2/h_a sin(pi j_a/m_a)
 //   V'_a = (W'_a - g_a (g.W')/G2) / (eta G2);  v_a = V'_a e^{+i pi j_a/m_a}/nc
-//   and v = 0 for the zero mode.
-template <int MZ>
+//   and v = 0 for the zero mode.  blockIdx.z = instance.
+template <bool ONE, int MZ>
 __global__ void __launch_bounds__(kFftThreads)
-    k_zsolve(Params P, Radices R, const float2* __restrict__ tw, const float* __restrict__ gx,
-             const float* __restrict__ gy, const float* __restrict__ gz,
+    k_zsolve(FSL_KARGS, Radices Rz, const float2* __restrict__ tw, const float* __restrict__ sx,
+             const float* __restrict__ sy, const float* __restrict__ sz,
              const float2* __restrict__ ex, const float2* __restrict__ ey,
-             const float2* __restrict__ ez, float2* __restrict__ spec) {
+             const float2* __restrict__ ez) {
+  FSL_REP_AT(blockIdx.z);
   extern __shared__ float2 smem[];
   const int mz = MZ ? MZ : P.mz, my = P.my, mxh = P.mxh;
   constexpr int NLc = 3 * kZTile;
-  const int NL = 3 * kZTile, LS = NL;
+  const int NL = NLc, LS = NL;
   float2* A = smem;
   float2* B = A + mz * LS;
   float2* stw = B + mz * LS;
   const int kx0 = blockIdx.x * kZTile, ky = blockIdx.y;
   for (int t = threadIdx.x; t < mz; t += blockDim.x) stw[t] = tw[t];
+  float2* spec = R.spec;
   const size_t cstride = (size_t)mz * my * mxh, zstride = (size_t)my * mxh;
   for (int e = threadIdx.x; e < mz * NL; e += blockDim.x) {
     int lx = e % kZTile, r = e / kZTile;
@@ -408,16 +431,18 @@ __global__ void __launch_bounds__(kFftThreads)
         kx < mxh ? spec[comp * cstride + z * zstride + (size_t)ky * mxh + kx] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2* Z = fft_any<MZ, NLc, NLc>(A, B, R, stw, -1);
+  float2* Z = fft_any<MZ, NLc, NLc>(A, B, Rz, stw, -1);
   const float inv_eta = (float)(1.0 / P.eta);
   const float inv_nc = 1.0f / (float)P.nc;
+  const float tdx = (float)(2.0 * P.invdx), tdy = (float)(2.0 * P.invdy), tdz = (float)(2.0 * P.invdz);
   for (int e = threadIdx.x; e < mz * kZTile; e += blockDim.x) {
     int lx = e % kZTile, kz = e / kZTile;
     int kx = kx0 + lx;
     if (kx >= mxh) continue;
     float2* p = Z + kz * LS + lx;
     float2 E[3] = {__ldg(ex + kx), __ldg(ey + ky), __ldg(ez + kz)};
-    float g[3] = {__ldg(gx + kx), __ldg(gy + ky), __ldg(gz + kz)};
+    // src/initializePrefactorFourierSpace.cu:48-66: g = 2/h sin(pi j/m)
+    float g[3] = {tdx * __ldg(sx + kx), tdy * __ldg(sy + ky), tdz * __ldg(sz + kz)};
     float2 W[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -442,7 +467,7 @@ __global__ void __launch_bounds__(kFftThreads)
   }
   __syncthreads();
   float2* other = (Z == A) ? B : A;
-  float2* Y = fft_any<MZ, NLc, NLc>(Z, other, R, stw, +1);
+  float2* Y = fft_any<MZ, NLc, NLc>(Z, other, Rz, stw, +1);
   for (int e = threadIdx.x; e < mz * NL; e += blockDim.x) {
     int lx = e % kZTile, r = e / kZTile;
     int z = r % mz, comp = r / mz;
@@ -453,10 +478,11 @@ __global__ void __launch_bounds__(kFftThreads)
 
 // Complex-to-real along x: Z_k = X_k + i Y_k (k <= mx/2) and its Hermitian
 // completion conj X_{m-k} + i conj Y_{m-k}; the inverse transform gives the
-// two real rows as real and imaginary parts.
+// two real rows as real and imaginary parts.  blockIdx.z = instance.
+template <bool ONE>
 __global__ void __launch_bounds__(kFftThreads)
-    k_xinv(Params P, Radices R, const float2* __restrict__ tw, const float2* __restrict__ spec,
-           float* __restrict__ v) {
+    k_xinv(FSL_KARGS, Radices Rx, const float2* __restrict__ tw) {
+  FSL_REP_AT(blockIdx.z);
   extern __shared__ float2 smem[];
   const int mx = P.mx, mxh = P.mxh;
   const int LS = kXPairs + 1;
@@ -467,7 +493,7 @@ __global__ void __launch_bounds__(kFftThreads)
   const int nrows = P.my * P.mz;
   const int row0 = blockIdx.x * 2 * kXPairs;
   for (int t = threadIdx.x; t < mx; t += blockDim.x) stw[t] = tw[t];
-  const float2* in = spec + (size_t)comp * nrows * mxh;
+  const float2* in = R.spec + (size_t)comp * nrows * mxh;
   for (int e = threadIdx.x; e < kXPairs * mxh; e += blockDim.x) {
     int l = e / mxh, k = e - l * mxh;
     int Rw = row0 + 2 * l;
@@ -479,9 +505,9 @@ __global__ void __launch_bounds__(kFftThreads)
     if (k > 0 && km != k && km < mx) A[km * LS + l] = make_float2(X.x + Y.y, Y.x - X.y);
   }
   __syncthreads();
-  float2* Z = fft_lines(A, B, LS, kXPairs, R, stw, +1);
+  float2* Z = fft_lines(A, B, LS, kXPairs, Rx, stw, +1);
   const float* Zf = reinterpret_cast<const float*>(Z);
-  float* out = v + (size_t)comp * P.nc;
+  float* out = R.v + (size_t)comp * P.nc;
   for (int e = threadIdx.x; e < 2 * kXPairs * mx; e += blockDim.x) {
     int rl = e / mx, x = e - rl * mx;
     int Rw = row0 + rl;
@@ -490,66 +516,20 @@ __global__ void __launch_bounds__(kFftThreads)
 }
 
 // ------------------------------------------------------- whole-plane path ---
-// One block per (z plane, component) does the whole 2-D transform of its
-// plane in shared memory, so a solve is three passes over HBM (plane
-// forward, z pencils with the solve, plane inverse) instead of five.  The
-// plane is kept as its half spectrum P[y][kx] (row pitch kPlanePitch); the
-// 1-D transforms run in batches of kPB lines through two small scratch
-// buffers.
+// One block per (z plane, component, instance) does the whole 2-D transform
+// of its plane in shared memory, so a solve is three passes over the fields
+// (plane forward, z pencils with the solve, plane inverse) instead of five.
+// The plane is kept as its half spectrum P[y][kx]; the 1-D transforms run in
+// batches of kPB lines through two small scratch buffers.
 constexpr int kPB = 16;
 
 __device__ __forceinline__ int plane_pitch(int mxh) { return mxh | 1; }  // odd: fewer conflicts
 
-struct WSource {
-  const unsigned long long* grid;
-  const float* noise;
-  const float* wext;
-  int nsets;
-  float scale, a1x, a1y, a1z, a4x, a4y, a4z;
-  size_t off2;
-};
-
-__device__ __forceinline__ float w_value(const Params& P, const WSource& S, int comp, int x, int y,
-                                         int z) {
-  int i = x + P.mx * (y + P.my * z);
-  if (S.wext) return S.wext[(size_t)comp * P.nc + i];
-  long long g = (long long)S.grid[(size_t)comp * P.nc + i];
-  float w = (float)((double)g * (double)S.scale);
-  w += stress_div(P, S.noise, comp, x, y, z, i, S.a1x, S.a1y, S.a1z, S.a4x, S.a4y, S.a4z);
-  if (S.nsets > 1)
-    w += stress_div(P, S.noise + S.off2, comp, x, y, z, i, S.a1x, S.a1y, S.a1z, S.a4x, S.a4y,
-                    S.a4z);
-  return w;
-}
-
-// W of all three components of every cell (src/stokesLimitFunctions.cu
-// :2281-2378, 3922-4069): the fixed-point spread field times 2^-40/dV plus
-// the stochastic stress divergence.  The spread field is cleared behind the
-// read, ready for the next spread.  One thread per cell, so the loads of a
-// warp are coalesced rows and the kernel runs at full occupancy.
-__global__ void k_wbuild(Params P, WSource S, float* __restrict__ W,
-                         unsigned long long* __restrict__ grid) {
-  const size_t nc = (size_t)P.nc;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc;
-       i += (size_t)gridDim.x * blockDim.x) {
-    int x = (int)(i % P.mx), r = (int)(i / P.mx);
-    int y = r % P.my, z = r / P.my;
-    float w0 = w_value(P, S, 0, x, y, z);
-    float w1 = w_value(P, S, 1, x, y, z);
-    float w2 = w_value(P, S, 2, x, y, z);
-    W[i] = w0;
-    W[nc + i] = w1;
-    W[2 * nc + i] = w2;
-    grid[i] = 0ull;
-    grid[nc + i] = 0ull;
-    grid[2 * nc + i] = 0ull;
-  }
-}
-
-template <int MX, int MY>
+template <bool ONE, int MX, int MY>
 __global__ void __launch_bounds__(kFftThreads)
-    k_plane_fwd(Params P, Radices Rx, Radices Ry, const float2* __restrict__ twx,
-                const float2* __restrict__ twy, WSource S, float2* __restrict__ spec) {
+    k_plane_fwd(FSL_KARGS, Radices Rx, Radices Ry, const float2* __restrict__ twx,
+                const float2* __restrict__ twy) {
+  FSL_REP_AT(blockIdx.z);
   extern __shared__ float2 smem[];
   const int mx = MX ? MX : P.mx, my = MY ? MY : P.my, mxh = mx / 2 + 1;
   const int LSP = plane_pitch(mxh);
@@ -563,6 +543,7 @@ __global__ void __launch_bounds__(kFftThreads)
   const int z = blockIdx.x, comp = blockIdx.y;
   for (int t = threadIdx.x; t < mx; t += blockDim.x) tx[t] = twx[t];
   for (int t = threadIdx.x; t < my; t += blockDim.x) ty[t] = twy[t];
+  const float* W = R.wbuf + (size_t)comp * P.nc + (size_t)z * my * mx;
   const int npairs = (my + 1) / 2;
   // x: real rows (2p, 2p+1) as one complex line, kPB pairs at a time
   for (int p0 = 0; p0 < npairs; p0 += kPB) {
@@ -570,7 +551,7 @@ __global__ void __launch_bounds__(kFftThreads)
     for (int e = threadIdx.x; e < 2 * kPB * mx; e += blockDim.x) {
       int rl = e / mx, x = e - rl * mx;
       int y = 2 * p0 + rl;
-      float w = (y < my && p0 + (rl >> 1) < npairs) ? w_value(P, S, comp, x, y, z) : 0.0f;
+      float w = (y < my && p0 + (rl >> 1) < npairs) ? W[(size_t)y * mx + x] : 0.0f;
       S1f[2 * (x * LS + (rl >> 1)) + (rl & 1)] = w;
     }
     __syncthreads();
@@ -587,7 +568,7 @@ __global__ void __launch_bounds__(kFftThreads)
     __syncthreads();
   }
   // y: kPB columns at a time, written straight to the spectrum
-  float2* out = spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
+  float2* out = R.spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
   for (int k0 = 0; k0 < mxh; k0 += kPB) {
     for (int e = threadIdx.x; e < my * kPB; e += blockDim.x) {
       int l = e % kPB, y = e / kPB;
@@ -605,11 +586,11 @@ __global__ void __launch_bounds__(kFftThreads)
   }
 }
 
-template <int MX, int MY>
+template <bool ONE, int MX, int MY>
 __global__ void __launch_bounds__(kFftThreads)
-    k_plane_inv(Params P, Radices Rx, Radices Ry, const float2* __restrict__ twx,
-                const float2* __restrict__ twy, const float2* __restrict__ spec,
-                float* __restrict__ v) {
+    k_plane_inv(FSL_KARGS, Radices Rx, Radices Ry, const float2* __restrict__ twx,
+                const float2* __restrict__ twy) {
+  FSL_REP_AT(blockIdx.z);
   extern __shared__ float2 smem[];
   const int mx = MX ? MX : P.mx, my = MY ? MY : P.my, mxh = mx / 2 + 1;
   const int LSP = plane_pitch(mxh);
@@ -623,7 +604,7 @@ __global__ void __launch_bounds__(kFftThreads)
   const int z = blockIdx.x, comp = blockIdx.y;
   for (int t = threadIdx.x; t < mx; t += blockDim.x) tx[t] = twx[t];
   for (int t = threadIdx.x; t < my; t += blockDim.x) ty[t] = twy[t];
-  const float2* in = spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
+  const float2* in = R.spec + ((size_t)comp * P.mz + z) * (size_t)my * mxh;
   // y: inverse transform of kPB columns at a time into the plane buffer
   for (int k0 = 0; k0 < mxh; k0 += kPB) {
     for (int e = threadIdx.x; e < my * kPB; e += blockDim.x) {
@@ -642,7 +623,7 @@ __global__ void __launch_bounds__(kFftThreads)
   }
   // x: complex-to-real, two rows per complex line
   const int npairs = (my + 1) / 2;
-  float* out = v + (size_t)comp * P.nc + (size_t)z * my * mx;
+  float* out = R.v + (size_t)comp * P.nc + (size_t)z * my * mx;
   for (int p0 = 0; p0 < npairs; p0 += kPB) {
     for (int e = threadIdx.x; e < kPB * mxh; e += blockDim.x) {
       int l = e / mxh, k = e - l * mxh;
@@ -669,13 +650,20 @@ __global__ void __launch_bounds__(kFftThreads)
 // ------------------------------------------------------------ host side ---
 template <int M>
 static void pick_cubic(FftPlan* fp) {
-  fp->plane_fwd = k_plane_fwd<M, M>;
-  fp->plane_inv = k_plane_inv<M, M>;
+  fp->plane_fwd[0] = k_plane_fwd<false, M, M>;
+  fp->plane_fwd[1] = k_plane_fwd<true, M, M>;
+  fp->plane_inv[0] = k_plane_inv<false, M, M>;
+  fp->plane_inv[1] = k_plane_inv<true, M, M>;
+}
+
+template <int M>
+static void pick_z(FftPlan* fp) {
+  fp->zsolve[0] = k_zsolve<false, M>;
+  fp->zsolve[1] = k_zsolve<true, M>;
 }
 
 static void pick_kernels(const Params& P, FftPlan* fp) {
-  fp->plane_fwd = k_plane_fwd<0, 0>;
-  fp->plane_inv = k_plane_inv<0, 0>;
+  pick_cubic<0>(fp);
   if (P.mx == P.my) {
     switch (P.mx) {
       case 16: pick_cubic<16>(fp); break;
@@ -689,17 +677,18 @@ static void pick_kernels(const Params& P, FftPlan* fp) {
     }
   }
   switch (P.mz) {
-    case 16: fp->zsolve = k_zsolve<16>; break;
-    case 24: fp->zsolve = k_zsolve<24>; break;
-    case 32: fp->zsolve = k_zsolve<32>; break;
-    case 48: fp->zsolve = k_zsolve<48>; break;
-    case 64: fp->zsolve = k_zsolve<64>; break;
-    case 96: fp->zsolve = k_zsolve<96>; break;
-    case 128: fp->zsolve = k_zsolve<128>; break;
-    case 256: fp->zsolve = k_zsolve<256>; break;
-    default: fp->zsolve = k_zsolve<0>; break;
+    case 16: pick_z<16>(fp); break;
+    case 24: pick_z<24>(fp); break;
+    case 32: pick_z<32>(fp); break;
+    case 48: pick_z<48>(fp); break;
+    case 64: pick_z<64>(fp); break;
+    case 96: pick_z<96>(fp); break;
+    case 128: pick_z<128>(fp); break;
+    case 256: pick_z<256>(fp); break;
+    default: pick_z<0>(fp); break;
   }
 }
+
 static bool upload_table(const std::vector<float2>& h, float2** d) {
   if (cudaMalloc(d, sizeof(float2) * h.size()) != cudaSuccess) return false;
   return cudaMemcpy(*d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -725,22 +714,21 @@ FftPlan* fft_plan_create(const Params& P) {
   cudaMemcpyToSymbol(c_w11, w11, sizeof(w11));
 
   const int m[3] = {P.mx, P.my, P.mz};
-  const double invd[3] = {P.invdx, P.invdy, P.invdz};
   float2** tws[3] = {&fp->twx, &fp->twy, &fp->twz};
-  float** gs[3] = {&fp->gx, &fp->gy, &fp->gz};
+  float** ss[3] = {&fp->sx, &fp->sy, &fp->sz};
   float2** es[3] = {&fp->ex, &fp->ey, &fp->ez};
   double pi = 4. * atan(1.);
   for (int a = 0; a < 3; ++a) {
     std::vector<float2> tw(m[a]), e(m[a]);
-    std::vector<float> g(m[a]);
+    std::vector<float> sn(m[a]);
     for (int t = 0; t < m[a]; ++t) {
       double ang = 2.0 * pi * (double)t / (double)m[a];
       tw[t] = make_float2((float)cos(ang), (float)-sin(ang));
-      // src/initializePrefactorFourierSpace.cu:48-66
-      g[t] = (float)(2 * invd[a] * sin(pi * t / double(m[a])));
+      // src/initializePrefactorFourierSpace.cu:48-66 (times 2/h in the kernel)
+      sn[t] = (float)sin(pi * t / double(m[a]));
       e[t] = make_float2((float)cos(pi * t / double(m[a])), (float)sin(pi * t / double(m[a])));
     }
-    if (!upload_table(tw, tws[a]) || !upload_table(g, gs[a]) || !upload_table(e, es[a])) {
+    if (!upload_table(tw, tws[a]) || !upload_table(sn, ss[a]) || !upload_table(e, es[a])) {
       fft_plan_destroy(fp);
       return nullptr;
     }
@@ -748,29 +736,37 @@ FftPlan* fft_plan_create(const Params& P) {
   fp->smem_x = sizeof(float2) * (2 * (size_t)P.mx * (kXPairs + 1) + P.mx);
   fp->smem_y = sizeof(float2) * (2 * (size_t)P.my * kYTile + P.my);
   fp->smem_z = sizeof(float2) * (2 * (size_t)P.mz * 3 * kZTile + P.mz);
-  size_t lim = 227 * 1024;
+  // The opt-in limit of the device.  Every kernel's attribute is set to it,
+  // not to this plan's need: kernels with runtime sizes are shared by plans
+  // of different sizes, and a larger attribute costs nothing.
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      optin <= 0)
+    optin = 227 * 1024;
+  const size_t lim = (size_t)optin;
   if (fp->smem_x > lim || fp->smem_y > lim || fp->smem_z > lim) {
     fft_plan_destroy(fp);
     return nullptr;
   }
+  pick_kernels(P, fp);
   {
     int mmax = P.mx > P.my ? P.mx : P.my;
     int lsp = P.mxh | 1;
     fp->smem_plane = sizeof(float2) * ((size_t)P.my * lsp + 2 * (size_t)mmax * (kPB + 1) + P.mx + P.my);
     fp->use_plane = fp->smem_plane <= lim;
-    pick_kernels(P, fp);
-    if (fp->use_plane) {
-      cudaFuncSetAttribute((const void*)fp->plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)fp->smem_plane);
-      cudaFuncSetAttribute((const void*)fp->plane_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)fp->smem_plane);
+    for (int v = 0; v < 2 && fp->use_plane; ++v) {
+      cudaFuncSetAttribute((const void*)fp->plane_fwd[v], cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+      cudaFuncSetAttribute((const void*)fp->plane_inv[v], cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     }
   }
-  cudaFuncSetAttribute(k_xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_x);
-  cudaFuncSetAttribute(k_xinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_x);
-  cudaFuncSetAttribute(k_yfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp->smem_y);
-  cudaFuncSetAttribute((const void*)fp->zsolve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)fp->smem_z);
+  const void* fixed[6] = {(const void*)k_xfwd<false>, (const void*)k_xfwd<true>,
+                          (const void*)k_xinv<false>, (const void*)k_xinv<true>,
+                          (const void*)k_yfft<false>, (const void*)k_yfft<true>};
+  for (const void* f : fixed) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  for (int v = 0; v < 2; ++v)
+    cudaFuncSetAttribute((const void*)fp->zsolve[v], cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  cudaGetLastError();
   fp->ok = true;
   return fp;
 }
@@ -780,79 +776,72 @@ void fft_plan_destroy(FftPlan* fp) {
   cudaFree(fp->twx);
   cudaFree(fp->twy);
   cudaFree(fp->twz);
-  cudaFree(fp->gx);
-  cudaFree(fp->gy);
-  cudaFree(fp->gz);
+  cudaFree(fp->sx);
+  cudaFree(fp->sy);
+  cudaFree(fp->sz);
   cudaFree(fp->ex);
   cudaFree(fp->ey);
   cudaFree(fp->ez);
   delete fp;
 }
 
-void launch_solve(const Params& P, FftPlan* fp, unsigned long long* grid, const float* noise,
-                  int nsets, const float* wext, float* wbuf, float2* spec, float* v,
-                  cudaStream_t s, Prof* prof) {
+static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
+  if (B.one)
+    fp->zsolve[1]<<<gz, kFftThreads, fp->smem_z, s>>>(RepSrc{}, *B.one, fp->rz, fp->twz, fp->sx, fp->sy,
+                                                     fp->sz, fp->ex, fp->ey, fp->ez);
+  else
+    fp->zsolve[0]<<<gz, kFftThreads, fp->smem_z, s>>>(B.src(), Rep{}, fp->rz, fp->twz, fp->sx, fp->sy,
+                                                     fp->sz, fp->ex, fp->ey, fp->ez);
+}
+
+void launch_solve(const Batch& B, FftPlan* fp, int nsets, int w_given, cudaStream_t s,
+                  Prof* prof) {
   Prof dummy;
   Prof& pr = prof ? *prof : dummy;
-  const int nrows = P.my * P.mz;
-  const int npairs = (nrows + 1) / 2;
-  dim3 gx((npairs + kXPairs - 1) / kXPairs, 3);
-  float nfac = nsets > 1 ? (float)sqrt(0.5) : (float)sqrt(2.0);
-  if (!wext) {
+  const int nrep = B.nrep;
+  if (!w_given) {
     // W from the spread field and the noise; clears the spread field
-    WSource S;
-    S.grid = grid;
-    S.noise = noise;
-    S.wext = nullptr;
-    S.nsets = nsets;
-    S.scale = (float)(kFixedInv / P.dV);
-    float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
-    S.a1x = (float)P.invdx * f1;
-    S.a1y = (float)P.invdy * f1;
-    S.a1z = (float)P.invdz * f1;
-    S.a4x = (float)P.invdx * f4;
-    S.a4y = (float)P.invdy * f4;
-    S.a4z = (float)P.invdz * f4;
-    S.off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
     pr.mark(s, "wbuild");
     int tb = 256;
-    long blocks = ((long)P.nc + tb - 1) / tb;
-    if (blocks > 148L * 64) blocks = 148L * 64;
-    k_wbuild<<<(unsigned)blocks, tb, 0, s>>>(P, S, wbuf, grid);
+    long blocks = ((long)B.nc + tb - 1) / tb;
+    long cap = (148L * 64 + nrep - 1) / nrep;
+    if (blocks > cap) blocks = cap < 1 ? 1 : cap;
+    FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets);
     pr.count(1);
-    wext = wbuf;
   }
   if (fp->use_plane) {
-    WSource S{};
-    S.wext = wext;
-    dim3 gp(P.mz, 3);
+    dim3 gp(B.mz, 3, nrep);
     pr.mark(s, "plane_fwd");
-    fp->plane_fwd<<<gp, kFftThreads, fp->smem_plane, s>>>(P, fp->rx, fp->ry, fp->twx, fp->twy, S,
-                                                         spec);
-    dim3 gz((P.mxh + kZTile - 1) / kZTile, P.my);
+    if (B.one)
+      fp->plane_fwd[1]<<<gp, kFftThreads, fp->smem_plane, s>>>(RepSrc{}, *B.one, fp->rx, fp->ry, fp->twx, fp->twy);
+    else
+      fp->plane_fwd[0]<<<gp, kFftThreads, fp->smem_plane, s>>>(B.src(), Rep{}, fp->rx, fp->ry, fp->twx, fp->twy);
+    dim3 gz((B.mxh + kZTile - 1) / kZTile, B.my, nrep);
     pr.mark(s, "zsolve");
-    fp->zsolve<<<gz, kFftThreads, fp->smem_z, s>>>(P, fp->rz, fp->twz, fp->gx, fp->gy, fp->gz, fp->ex,
-                                                 fp->ey, fp->ez, spec);
+    zsolve(B, fp, gz, s);
     pr.mark(s, "plane_inv");
-    fp->plane_inv<<<gp, kFftThreads, fp->smem_plane, s>>>(P, fp->rx, fp->ry, fp->twx, fp->twy,
-                                                         spec, v);
+    if (B.one)
+      fp->plane_inv[1]<<<gp, kFftThreads, fp->smem_plane, s>>>(RepSrc{}, *B.one, fp->rx, fp->ry, fp->twx, fp->twy);
+    else
+      fp->plane_inv[0]<<<gp, kFftThreads, fp->smem_plane, s>>>(B.src(), Rep{}, fp->rx, fp->ry, fp->twx, fp->twy);
     pr.count(3);
     return;
   }
+  const int nrows = B.my * B.mz;
+  const int npairs = (nrows + 1) / 2;
+  dim3 gx((npairs + kXPairs - 1) / kXPairs, 3, nrep);
   pr.mark(s, "xfwd");
-  k_xfwd<<<gx, kFftThreads, fp->smem_x, s>>>(P, fp->rx, fp->twx, nullptr, noise, nsets, nfac, wext,
-                                             spec);
-  dim3 gy((P.mxh + kYTile - 1) / kYTile, P.mz, 3);
+  FSL_GO(k_xfwd, gx, kFftThreads, fp->smem_x, s, B, fp->rx, fp->twx);
+  dim3 gy((B.mxh + kYTile - 1) / kYTile, B.mz, 3 * nrep);
   pr.mark(s, "yfft");
-  k_yfft<<<gy, kFftThreads, fp->smem_y, s>>>(P, fp->ry, fp->twy, spec, -1);
-  dim3 gz((P.mxh + kZTile - 1) / kZTile, P.my);
+  FSL_GO(k_yfft, gy, kFftThreads, fp->smem_y, s, B, fp->ry, fp->twy, -1);
+  dim3 gz((B.mxh + kZTile - 1) / kZTile, B.my, nrep);
   pr.mark(s, "zsolve");
-  fp->zsolve<<<gz, kFftThreads, fp->smem_z, s>>>(P, fp->rz, fp->twz, fp->gx, fp->gy, fp->gz, fp->ex,
-                                               fp->ey, fp->ez, spec);
+  zsolve(B, fp, gz, s);
   pr.mark(s, "yfft");
-  k_yfft<<<gy, kFftThreads, fp->smem_y, s>>>(P, fp->ry, fp->twy, spec, +1);
+  FSL_GO(k_yfft, gy, kFftThreads, fp->smem_y, s, B, fp->ry, fp->twy, +1);
   pr.mark(s, "xinv");
-  k_xinv<<<gx, kFftThreads, fp->smem_x, s>>>(P, fp->rx, fp->twx, spec, v);
+  FSL_GO(k_xinv, gx, kFftThreads, fp->smem_x, s, B, fp->rx, fp->twx);
   pr.count(5);
 }
 

@@ -1,0 +1,657 @@
+// fsl_group.cu -- slots, size-class groups and the graph-captured step of
+// any number of groups (declared in fsl_group.cuh).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "fsl_group.cuh"
+
+namespace fsl {
+
+namespace {
+thread_local char g_msg[512] = "";
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
+
+// Byte offsets of one slot's buffers inside its arena.
+struct SlotLayout {
+  size_t q, qp, F, u, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
+      bsum, ljtab, noise, grid, spec, v, wbuf, err, t, total;
+};
+
+SlotLayout layout(const Params& P, int np_cap) {
+  SlotLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += align_up(std::max<size_t>(bytes, 1));
+    return o;
+  };
+  const size_t np = (size_t)np_cap, nc = (size_t)P.nc;
+  const size_t mN = (size_t)P.mN;
+  const uint64_t noise = ((uint64_t)12 * nc + (uint64_t)9 * np + 3) / 4 * 4;
+  L.q = take(sizeof(double) * 3 * np);
+  L.qp = take(sizeof(double) * 3 * np);
+  L.F = take(sizeof(double) * 3 * np);
+  L.u = take(sizeof(double) * 3 * np);
+  L.cell_of = take(sizeof(int) * np);
+  L.tmp = take(sizeof(int) * np);
+  L.sorted = take(sizeof(int) * np);
+  L.bpp_cnt = take(sizeof(int) * np);
+  L.bpp_off = take(sizeof(int) * np);
+  L.bfp_cnt = take(sizeof(int) * np);
+  L.bfp_off = take(sizeof(int) * np);
+  L.cnt = take(sizeof(int) * mN);
+  L.fill = take(sizeof(int) * mN);
+  L.start = take(sizeof(int) * (mN + 1));
+  L.bsum = take(sizeof(int) * ((mN + 4095) / 4096 + 1));
+  L.ljtab = take(sizeof(float) * kLjTableSize);
+  L.noise = take(sizeof(float) * noise);
+  L.grid = take(sizeof(unsigned long long) * 3 * nc);
+  L.spec = take(sizeof(float2) * 3 * (size_t)P.my * P.mz * P.mxh);
+  L.v = take(sizeof(float) * 3 * nc);
+  L.wbuf = take(sizeof(float) * 3 * nc);
+  L.err = take(sizeof(int) * 4);
+  L.t = take(sizeof(uint64_t));
+  L.total = off;
+  return L;
+}
+
+bool factor_ok(int n) {
+  if (n < 3) return false;
+  const int ps[5] = {2, 3, 5, 7, 11};
+  for (int p : ps)
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+}  // namespace
+
+int errorf(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+const char* last_error() { return g_msg; }
+
+int set_last_error(int code, const char* msg) { return errorf(code, "%s", msg); }
+
+int cuda_fail(cudaError_t e, const char* what) {
+  cudaGetLastError();
+  return errorf(e == cudaErrorMemoryAllocation ? FSL_E_NOMEM : FSL_E_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+}
+
+bool ClassKey::operator<(const ClassKey& o) const {
+  const int a[7] = {mx, my, mz, mnx, mny, mnz, kernel};
+  const int b[7] = {o.mx, o.my, o.mz, o.mnx, o.mny, o.mnz, o.kernel};
+  return std::lexicographical_compare(a, a + 7, b, b + 7);
+}
+bool ClassKey::operator==(const ClassKey& o) const { return !(*this < o) && !(o < *this); }
+
+ClassKey class_of(const Params& P) { return ClassKey{P.mx, P.my, P.mz, P.mnx, P.mny, P.mnz, P.kernel}; }
+
+int make_params(const fsl_config& c, int64_t np, Params& P) {
+  if (c.mx < 3 || c.my < 3 || c.mz < 3)
+    return errorf(FSL_E_ARG, "cells must be >= 3 in every direction");
+  if (!factor_ok(c.mx) || !factor_ok(c.my) || !factor_ok(c.mz))
+    return errorf(FSL_E_ARG, "cells %d %d %d: every extent must factor into 2,3,5,7,11", c.mx, c.my,
+                  c.mz);
+  if (c.mx > 1024 || c.my > 1024 || c.mz > 1024)
+    return errorf(FSL_E_ARG, "cells per direction limited to 1024");
+  if (!(c.lx > 0 && c.ly > 0 && c.lz > 0)) return errorf(FSL_E_ARG, "celldimension must be > 0");
+  if (!(c.dt > 0)) return errorf(FSL_E_ARG, "dt must be > 0");
+  if (!(c.shearviscosity > 0)) return errorf(FSL_E_ARG, "shearviscosity must be > 0");
+  if (!(c.temperature >= 0)) return errorf(FSL_E_ARG, "temperature must be >= 0");
+  if (c.kernel != 3 && c.kernel != 4) return errorf(FSL_E_ARG, "kernel must be 3 or 4");
+  if (c.pair < 0 || c.pair > 2) return errorf(FSL_E_ARG, "unknown pair potential %d", c.pair);
+  if (c.rfd < 0 || c.rfd > 1) return errorf(FSL_E_ARG, "unknown rfd mode %d", c.rfd);
+  if (c.extra_mobility < 0) return errorf(FSL_E_ARG, "extraMobility must be >= 0");
+  if (np < 0 || np > (int64_t)1 << 28) return errorf(FSL_E_ARG, "bad particle count");
+  bool pairs = c.nonbonded && c.pair != FSL_PAIR_NONE && np > 0;
+  if (pairs && !(c.cutoff > 0)) return errorf(FSL_E_ARG, "cutoff must be > 0 with pair forces");
+  int64_t nc64 = (int64_t)c.mx * c.my * c.mz;
+  if (nc64 > ((int64_t)1 << 30)) return errorf(FSL_E_ARG, "grid too large");
+
+  std::memset(&P, 0, sizeof(P));
+  P.mx = c.mx;
+  P.my = c.my;
+  P.mz = c.mz;
+  P.mxh = c.mx / 2 + 1;
+  P.nc = (int)nc64;
+  P.lx = c.lx;
+  P.ly = c.ly;
+  P.lz = c.lz;
+  // src/createCellsStokesLimitGPU.cu:71-91
+  P.dx = c.lx / double(c.mx);
+  P.dy = c.ly / double(c.my);
+  P.dz = c.lz / double(c.mz);
+  P.invdx = double(c.mx) / c.lx;
+  P.invdy = double(c.my) / c.ly;
+  P.invdz = double(c.mz) / c.lz;
+  P.invlx = 1. / c.lx;
+  P.invly = 1. / c.ly;
+  P.invlz = 1. / c.lz;
+  P.dV = P.dx * P.dy * P.dz;
+  // src/createBoundariesRK2GPU.cu:134-141
+  if (c.cutoff > 0) {
+    P.mnx = std::max(3, (int)(c.lx / c.cutoff));
+    P.mny = std::max(3, (int)(c.ly / c.cutoff));
+    P.mnz = std::max(3, (int)(c.lz / c.cutoff));
+  } else {
+    P.mnx = P.mny = P.mnz = 3;
+  }
+  if ((int64_t)P.mnx * P.mny * P.mnz > ((int64_t)1 << 28))
+    return errorf(FSL_E_ARG, "cutoff too small for the box (neighbour grid too large)");
+  P.mN = P.mnx * P.mny * P.mnz;
+  if ((int64_t)((P.mN + 4095) / 4096) > 4096) return errorf(FSL_E_ARG, "neighbour grid too large");
+  P.invdnx = double(P.mnx) / c.lx;
+  P.invdny = double(P.mny) / c.ly;
+  P.invdnz = double(P.mnz) / c.lz;
+  P.np = (int)np;
+  P.kernel = c.kernel;
+  P.pair = c.pair;
+  P.nonbonded = c.nonbonded ? 1 : 0;
+  P.rfd = c.rfd;
+  P.bonded = 0;
+  P.has_extra = c.extra_mobility != 0.0;
+  P.cutoff = c.cutoff;
+  P.cutoff2 = c.cutoff * c.cutoff;
+  P.invcut2 = c.cutoff > 0 ? 1. / (c.cutoff * c.cutoff) : 0.0;
+  P.soft_eps = c.soft_epsilon;
+  P.eta = c.shearviscosity;
+  P.kT = c.temperature;
+  P.dt = c.dt;
+  P.extra_mob = c.extra_mobility;
+  // src/createCellsStokesLimitGPU.cu:58-61
+  P.fact1 = std::sqrt((4. * c.temperature * c.shearviscosity) / (P.dV * c.dt));
+  P.fact4 = std::sqrt((2. * c.temperature * c.shearviscosity) / (P.dV * c.dt));
+  P.fact2 = std::sqrt(c.temperature * c.extra_mobility * c.dt);
+  P.seed = c.seed;
+  P.noise_n = (uint64_t)12 * P.nc + (uint64_t)9 * P.np;
+  return FSL_OK;
+}
+
+void build_ljtable(const Params& P, double temperature, double cutoff, std::vector<float>& t) {
+  const int size = kLjTableSize;
+  t.assign(size, 0.0f);
+  float sigma = (float)(2.0 * P.lx / (double)P.mx);
+  float epsilon = (float)temperature;
+  float cutoff2 = (float)(cutoff * cutoff);
+  float dr = cutoff2 / (float)size;
+  float r = 0.5f * dr;
+  for (int i = 0; i < size; ++i) {
+    double rr = (double)sqrtf(r);
+    float fr = (float)(48. * epsilon * (std::pow(sigma / rr, 12) - 0.5 * std::pow(sigma / rr, 6)) / rr);
+    t[i] = fr / sqrtf(r);
+    r += dr;
+  }
+  t[size - 1] = 0.0f;
+  t[0] = 0.0f;
+}
+
+// ------------------------------------------------------------------ slots --
+size_t slot_bytes(const Params& P, int np_cap) { return layout(P, np_cap).total; }
+
+int slot_alloc(Slot& s, const Params& P, int np_cap) {
+  slot_free(s);
+  const SlotLayout L = layout(P, np_cap);
+  char* base = nullptr;
+  FSL_TRY(cudaMalloc((void**)&base, L.total));
+  s.arena = base;
+  s.bytes = L.total;
+  s.np_cap = np_cap;
+  cudaError_t e = cudaMemset(base, 0, L.total);
+  if (e != cudaSuccess) {
+    slot_free(s);
+    return cuda_fail(e, "cudaMemset(slot)");
+  }
+  Rep& r = s.r;
+  std::memset(&r, 0, sizeof(r));
+  r.P = P;
+  r.active = 0;
+  r.q = (double*)(base + L.q);
+  r.qp = (double*)(base + L.qp);
+  r.F = (double*)(base + L.F);
+  r.u = (double*)(base + L.u);
+  r.cell_of = (int*)(base + L.cell_of);
+  r.tmp = (int*)(base + L.tmp);
+  r.sorted = (int*)(base + L.sorted);
+  r.bpp_cnt = (int*)(base + L.bpp_cnt);
+  r.bpp_off = (int*)(base + L.bpp_off);
+  r.bfp_cnt = (int*)(base + L.bfp_cnt);
+  r.bfp_off = (int*)(base + L.bfp_off);
+  r.cnt = (int*)(base + L.cnt);
+  r.fill = (int*)(base + L.fill);
+  r.start = (int*)(base + L.start);
+  r.bsum = (int*)(base + L.bsum);
+  r.ljtab = (float*)(base + L.ljtab);
+  r.noise = (float*)(base + L.noise);
+  r.grid = (unsigned long long*)(base + L.grid);
+  r.spec = (float2*)(base + L.spec);
+  r.v = (float*)(base + L.v);
+  r.wbuf = (float*)(base + L.wbuf);
+  r.err = (int*)(base + L.err);
+  r.t = (uint64_t*)(base + L.t);
+  return FSL_OK;
+}
+
+void slot_free(Slot& s) {
+  if (s.arena) cudaFree(s.arena);
+  if (s.bonds) cudaFree(s.bonds);
+  s.arena = s.bonds = nullptr;
+  s.bytes = 0;
+  s.np_cap = 0;
+  std::memset(&s.r, 0, sizeof(s.r));
+}
+
+int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, cudaStream_t st) {
+  if (!s.arena) return errorf(FSL_E_ARG, "slot not allocated");
+  if (P.np > s.np_cap) return errorf(FSL_E_ARG, "%d particles exceed the slot's %d", P.np, s.np_cap);
+  if (!(class_of(P) == class_of(s.r.P))) return errorf(FSL_E_ARG, "instance is not of the slot's size class");
+  if (P.np > 0 && !q) return errorf(FSL_E_ARG, "null positions");
+  Rep& r = s.r;
+  r.P = P;
+  r.P.bonded = 0;
+  r.bpp_idx = nullptr;
+  r.bpp_k = r.bpp_r0 = nullptr;
+  r.bfp_k = r.bfp_r0 = r.bfp_xyz = nullptr;
+  const size_t n3p = 3 * (size_t)P.np, cap = (size_t)std::max(s.np_cap, 1);
+  if (P.np > 0) {
+    FSL_TRY(cudaMemcpyAsync(r.q, q, sizeof(double) * n3p, cudaMemcpyHostToDevice, st));
+    FSL_TRY(cudaMemcpyAsync(r.qp, q, sizeof(double) * n3p, cudaMemcpyHostToDevice, st));
+  }
+  std::vector<float> tab;
+  build_ljtable(P, c.temperature, c.cutoff, tab);
+  // pageable source: the copy is staged before the call returns
+  FSL_TRY(cudaMemcpyAsync(r.ljtab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, st));
+  FSL_TRY(cudaMemsetAsync(r.F, 0, sizeof(double) * 3 * cap, st));
+  FSL_TRY(cudaMemsetAsync(r.bpp_cnt, 0, sizeof(int) * cap, st));
+  FSL_TRY(cudaMemsetAsync(r.bpp_off, 0, sizeof(int) * cap, st));
+  FSL_TRY(cudaMemsetAsync(r.bfp_cnt, 0, sizeof(int) * cap, st));
+  FSL_TRY(cudaMemsetAsync(r.bfp_off, 0, sizeof(int) * cap, st));
+  FSL_TRY(cudaMemsetAsync(r.grid, 0, sizeof(unsigned long long) * 3 * (size_t)P.nc, st));
+  FSL_TRY(cudaMemsetAsync(r.v, 0, sizeof(float) * 3 * (size_t)P.nc, st));
+  FSL_TRY(cudaMemsetAsync(r.err, 0, sizeof(int) * 4, st));
+  FSL_TRY(cudaMemsetAsync(r.t, 0, sizeof(uint64_t), st));
+  r.active = 1;
+  return FSL_OK;
+}
+
+int slot_bonds(Slot& s, int64_t nbonds, const int32_t* bi, const int32_t* bj, const double* k,
+               const double* r0, int64_t nfixed, const int32_t* fi, const double* fk,
+               const double* fr0, const double* fxyz, cudaStream_t st) {
+  Rep& r = s.r;
+  const int np = r.P.np;
+  if (nbonds < 0 || nfixed < 0) return errorf(FSL_E_ARG, "negative bond count");
+  if (nbonds > 0 && (!bi || !bj || !k || !r0)) return errorf(FSL_E_ARG, "null bond array");
+  if (nfixed > 0 && (!fi || !fk || !fr0 || !fxyz)) return errorf(FSL_E_ARG, "null tether array");
+  for (int64_t b = 0; b < nbonds; ++b)
+    if (bi[b] < 0 || bi[b] >= np || bj[b] < 0 || bj[b] >= np)
+      return errorf(FSL_E_ARG, "bond %lld: particle index out of range", (long long)b);
+  for (int64_t b = 0; b < nfixed; ++b)
+    if (fi[b] < 0 || fi[b] >= np)
+      return errorf(FSL_E_ARG, "tether %lld: particle index out of range", (long long)b);
+  // both endpoints store each particle-particle bond, in file order
+  std::vector<int> pc(np, 0), po(np, 0), fc(np, 0), fo(np, 0), tmp(np, 0);
+  for (int64_t b = 0; b < nbonds; ++b) {
+    pc[bi[b]]++;
+    pc[bj[b]]++;
+  }
+  for (int64_t b = 0; b < nfixed; ++b) fc[fi[b]]++;
+  for (int i = 1; i < np; ++i) {
+    po[i] = po[i - 1] + pc[i - 1];
+    fo[i] = fo[i - 1] + fc[i - 1];
+  }
+  std::vector<int> idx(2 * nbonds);
+  std::vector<double> kk(2 * nbonds), rr(2 * nbonds);
+  for (int64_t b = 0; b < nbonds; ++b) {
+    int i1 = bi[b], i2 = bj[b];
+    int p1 = po[i1] + tmp[i1]++, p2 = po[i2] + tmp[i2]++;
+    idx[p1] = i2;
+    kk[p1] = k[b];
+    rr[p1] = r0[b];
+    idx[p2] = i1;
+    kk[p2] = k[b];
+    rr[p2] = r0[b];
+  }
+  std::fill(tmp.begin(), tmp.end(), 0);
+  std::vector<double> fkk(nfixed), frr(nfixed), fxx(3 * nfixed);
+  for (int64_t b = 0; b < nfixed; ++b) {
+    int i1 = fi[b];
+    int p = fo[i1] + tmp[i1]++;
+    fkk[p] = fk[b];
+    frr[p] = fr0[b];
+    fxx[3 * p] = fxyz[3 * b];
+    fxx[3 * p + 1] = fxyz[3 * b + 1];
+    fxx[3 * p + 2] = fxyz[3 * b + 2];
+  }
+  // one allocation for the tables: idx | k | r0 | fk | fr0 | fxyz
+  const size_t nb2 = (size_t)2 * nbonds, nf = (size_t)nfixed;
+  const size_t o_idx = 0, o_k = align_up(sizeof(int) * nb2), o_r0 = o_k + align_up(sizeof(double) * nb2),
+               o_fk = o_r0 + align_up(sizeof(double) * nb2), o_fr0 = o_fk + align_up(sizeof(double) * nf),
+               o_fx = o_fr0 + align_up(sizeof(double) * nf), total = o_fx + align_up(sizeof(double) * 3 * nf);
+  FSL_TRY(cudaStreamSynchronize(st));  // the old tables may still be read
+  if (s.bonds) cudaFree(s.bonds);
+  s.bonds = nullptr;
+  char* base = nullptr;
+  FSL_TRY(cudaMalloc((void**)&base, std::max<size_t>(total, kAlign)));
+  s.bonds = base;
+  r.bpp_idx = (int*)(base + o_idx);
+  r.bpp_k = (double*)(base + o_k);
+  r.bpp_r0 = (double*)(base + o_r0);
+  r.bfp_k = (double*)(base + o_fk);
+  r.bfp_r0 = (double*)(base + o_fr0);
+  r.bfp_xyz = (double*)(base + o_fx);
+  if (np > 0) {
+    FSL_TRY(cudaMemcpy(r.bpp_cnt, pc.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpy(r.bpp_off, po.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpy(r.bfp_cnt, fc.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpy(r.bfp_off, fo.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+  }
+  if (nbonds > 0) {
+    FSL_TRY(cudaMemcpy(r.bpp_idx, idx.data(), sizeof(int) * nb2, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpy(r.bpp_k, kk.data(), sizeof(double) * nb2, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpy(r.bpp_r0, rr.data(), sizeof(double) * nb2, cudaMemcpyHostToDevice));
+  }
+  if (nfixed > 0) {
+    FSL_TRY(cudaMemcpy(r.bfp_k, fkk.data(), sizeof(double) * nf, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpy(r.bfp_r0, frr.data(), sizeof(double) * nf, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpy(r.bfp_xyz, fxx.data(), sizeof(double) * 3 * nf, cudaMemcpyHostToDevice));
+  }
+  r.P.bonded = (nbonds + nfixed) > 0;
+  return FSL_OK;
+}
+
+// ----------------------------------------------------------------- groups --
+int group_init(Group& g, const Params& P0) {
+  g.key = class_of(P0);
+  g.P0 = P0;
+  g.fft = fft_plan_create(P0);
+  if (!g.fft) return errorf(FSL_E_ARG, "FFT plan creation failed (sizes or shared memory)");
+  return FSL_OK;
+}
+
+void group_destroy(Group& g) {
+  fft_plan_destroy(g.fft);
+  g.fft = nullptr;
+  if (g.d_reps) cudaFree(g.d_reps);
+  if (g.d_boff) cudaFree(g.d_boff);
+  g.d_reps = nullptr;
+  g.d_boff = nullptr;
+  g.d_cap = 0;
+  for (int i = 0; i < Prof::kMax; ++i)
+    if (g.prof.ev[i]) cudaEventDestroy(g.prof.ev[i]);
+  std::memset(g.prof.ev, 0, sizeof(g.prof.ev));
+}
+
+int group_upload(Group& g) {
+  const int n = (int)g.slots.size();
+  Batch& B = g.B;
+  B.nrep = n;
+  B.mx = g.P0.mx;
+  B.my = g.P0.my;
+  B.mz = g.P0.mz;
+  B.mxh = g.P0.mxh;
+  B.nc = g.P0.nc;
+  B.mN = g.P0.mN;
+  B.kernel = g.P0.kernel;
+  B.max_np = 0;
+  B.max_noise_n = 0;
+  for (const Slot* s : g.slots) {
+    B.max_np = std::max(B.max_np, s->np_cap);
+    B.max_noise_n = std::max<uint64_t>(B.max_noise_n, (uint64_t)12 * B.nc + (uint64_t)9 * s->np_cap);
+  }
+  if (n > g.d_cap) {
+    if (g.d_reps || g.d_boff) {
+      FSL_TRY(cudaStreamSynchronize(g.stream));
+      cudaFree(g.d_reps);
+      cudaFree(g.d_boff);
+      g.d_reps = nullptr;
+      g.d_boff = nullptr;
+      g.d_cap = 0;
+    }
+    int cap = std::max(n, 1);
+    FSL_TRY(cudaMalloc((void**)&g.d_reps, sizeof(Rep) * cap));
+    FSL_TRY(cudaMalloc((void**)&g.d_boff, sizeof(int) * NKIND * (cap + 1)));
+    g.d_cap = cap;
+    g.dirty = true;
+  }
+  B.reps = g.d_reps;
+  B.boff = g.d_boff;
+  if (!g.dirty) return FSL_OK;
+  g.h_reps.resize(n);
+  for (int i = 0; i < n; ++i) g.h_reps[i] = g.slots[i]->r;
+  // first block of every instance per particle launch kind, from the
+  // capacities (fixed while the slots are), so the launch shapes stay put
+  g.h_boff.assign((size_t)NKIND * (n + 1), 0);
+  for (int k = 0; k < NKIND; ++k) {
+    int* off = g.h_boff.data() + (size_t)k * (n + 1);
+    long acc = 0;
+    for (int i = 0; i < n; ++i) {
+      off[i] = (int)acc;
+      acc += ((long)g.slots[i]->np_cap + kind_ppb(k) - 1) / kind_ppb(k);
+    }
+    off[n] = (int)acc;
+    if (acc > (long)INT_MAX / 2) return errorf(FSL_E_ARG, "batch too large for one launch");
+    B.nblk[k] = (int)acc;
+  }
+  B.one = n == 1 ? &g.h_reps[0] : nullptr;
+  if (n > 0) {
+    FSL_TRY(cudaMemcpyAsync(g.d_reps, g.h_reps.data(), sizeof(Rep) * n, cudaMemcpyHostToDevice,
+                            g.stream));
+    FSL_TRY(cudaMemcpyAsync(g.d_boff, g.h_boff.data(), sizeof(int) * g.h_boff.size(),
+                            cudaMemcpyHostToDevice, g.stream));
+  }
+  g.dirty = false;
+  return FSL_OK;
+}
+
+// One midpoint step (src/runSchemeStokesLimit.cu:163-275) of every active
+// instance of the group.
+void group_enqueue_step(Group& g) {
+  const Batch& B = g.B;
+  cudaStream_t s = g.stream;
+  Prof& pr = g.prof;
+  pr.used = 0;
+  pr.launches = 0;
+  if (B.nrep == 0) {
+    g.launches = 0;
+    return;
+  }
+  const int pk = B.max_np > 0 ? 1 : 0;
+  auto cells_forces = [&](int which) {
+    pr.mark(s, "cells");
+    launch_cells(B, which, s);
+    pr.mark(s, "forces");
+    launch_forces(B, which, s);
+    pr.count(pk ? 8 : 1);
+  };
+  pr.mark(s, "noise");
+  launch_noise(B, s);
+  pr.count(1);
+  // option 0: F^n, f = S(q^n) F^n; solve 1 with sqrt(2) stress 1.  The
+  // spread field is all zeros here: it starts cleared and every W build
+  // clears what it reads.
+  cells_forces(0);
+  pr.mark(s, "spread");
+  launch_spread(B, 0, 1, s);
+  pr.count(pk);
+  launch_solve(B, g.fft, 1, 0, s, &pr);
+  // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
+  // sqrt(1/2) (stress 1 + stress 2)
+  pr.mark(s, "interp_update");
+  launch_interp_update(B, 1, s);
+  pr.count(pk);
+  cells_forces(1);
+  pr.mark(s, "spread_rfd");
+  launch_spread(B, 1, 1, s);
+  pr.count(pk);
+  launch_solve(B, g.fft, 2, 0, s, &pr);
+  // option 2: corrector
+  pr.mark(s, "interp_update");
+  launch_interp_update(B, 2, s);
+  pr.count(pk);
+  pr.mark(s, "counter");
+  launch_step_counter(B, s);
+  pr.count(1);
+  pr.mark(s, nullptr);
+  g.launches = pr.launches;
+}
+
+int group_prof_collect(Group& g) {
+  Prof& pr = g.prof;
+  if (!pr.on || pr.used < 2) return FSL_OK;
+  cudaError_t e = cudaEventSynchronize(pr.ev[pr.used - 1]);
+  if (e != cudaSuccess) return errorf(FSL_E_CUDA, "profile sync: %s", cudaGetErrorString(e));
+  for (int i = 0; i + 1 < pr.used; ++i) {
+    if (!pr.name[i]) continue;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, pr.ev[i], pr.ev[i + 1]);
+    auto& a = g.stage_acc[pr.name[i]];
+    a.first += 1;
+    a.second += ms;
+  }
+  return FSL_OK;
+}
+
+// ------------------------------------------------------------------- exec --
+int exec_init(Exec& e, int device) {
+  e.device = device;
+  FSL_TRY(cudaSetDevice(device));
+  FSL_TRY(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
+  return FSL_OK;
+}
+
+void exec_drop_graph(Exec& e) {
+  if (e.gexec) cudaGraphExecDestroy(e.gexec);
+  if (e.graph) cudaGraphDestroy(e.graph);
+  e.gexec = nullptr;
+  e.graph = nullptr;
+  e.shape.clear();
+}
+
+void exec_destroy(Exec& e) {
+  if (e.stream) cudaStreamSynchronize(e.stream);
+  exec_drop_graph(e);
+  for (cudaStream_t s : e.side) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  e.side.clear();
+  for (cudaEvent_t ev : e.ev) cudaEventDestroy(ev);
+  e.ev.clear();
+  if (e.stream) cudaStreamDestroy(e.stream);
+  e.stream = nullptr;
+}
+
+namespace {
+
+int exec_prepare(Exec& e) {
+  const size_t ng = e.groups.size();
+  while (e.side.size() + 1 < ng) {
+    cudaStream_t s;
+    FSL_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    e.side.push_back(s);
+  }
+  while (e.ev.size() < ng + 1) {
+    cudaEvent_t ev;
+    FSL_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    e.ev.push_back(ev);
+  }
+  std::vector<long long> shape;
+  for (size_t i = 0; i < ng; ++i) {
+    Group& g = *e.groups[i];
+    g.stream = i == 0 ? e.stream : e.side[i - 1];
+    int rc = group_upload(g);
+    if (rc) return rc;
+    shape.push_back((long long)(uintptr_t)g.B.reps);
+    shape.push_back(g.B.nrep);
+    shape.push_back(g.B.max_np);
+    shape.push_back((long long)g.B.max_noise_n);
+    shape.push_back(g.prof.on ? 1 : 0);
+    for (int k = 0; k < NKIND; ++k) shape.push_back(g.B.nblk[k]);
+    // a single instance is a by-value kernel argument: any change to it
+    // needs a new capture
+    if (g.B.one) {
+      long long w[(sizeof(Rep) + 7) / 8] = {};
+      std::memcpy(w, g.B.one, sizeof(Rep));
+      shape.insert(shape.end(), w, w + (sizeof(Rep) + 7) / 8);
+    }
+  }
+  if (shape != e.shape) {
+    exec_drop_graph(e);
+    e.shape = shape;
+  }
+  // the uploads on the side streams must land before the step
+  for (size_t i = 1; i < ng; ++i) {
+    FSL_TRY(cudaEventRecord(e.ev[i], e.side[i - 1]));
+    FSL_TRY(cudaStreamWaitEvent(e.stream, e.ev[i], 0));
+  }
+  return FSL_OK;
+}
+
+void exec_enqueue(Exec& e) {
+  const size_t ng = e.groups.size();
+  if (ng == 1) {
+    group_enqueue_step(*e.groups[0]);
+    e.launches_per_step = e.groups[0]->launches;
+    return;
+  }
+  // fork: every group on its own stream, joined back into the main one
+  cudaEventRecord(e.ev[0], e.stream);
+  for (size_t i = 1; i < ng; ++i) cudaStreamWaitEvent(e.side[i - 1], e.ev[0], 0);
+  int total = 0;
+  for (size_t i = 0; i < ng; ++i) {
+    group_enqueue_step(*e.groups[i]);
+    total += e.groups[i]->launches;
+  }
+  for (size_t i = 1; i < ng; ++i) {
+    cudaEventRecord(e.ev[i], e.side[i - 1]);
+    cudaStreamWaitEvent(e.stream, e.ev[i], 0);
+  }
+  e.launches_per_step = total;
+}
+
+}  // namespace
+
+int exec_step(Exec& e, int64_t nsteps) {
+  if (nsteps < 0) return errorf(FSL_E_ARG, "negative step count");
+  FSL_TRY(cudaSetDevice(e.device));
+  if (nsteps == 0) return FSL_OK;
+  int rc = exec_prepare(e);
+  if (rc) return rc;
+  if (e.groups.empty()) return FSL_OK;
+  for (int64_t k = 0; k < nsteps; ++k) {
+    if (e.use_graph && e.steps > 0) {
+      if (!e.gexec) {
+        FSL_TRY(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+        exec_enqueue(e);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(e.stream, &g);
+        if (ce != cudaSuccess) return cuda_fail(ce, "graph capture");
+        e.graph = g;
+        FSL_TRY(cudaGraphInstantiate(&e.gexec, g, 0));
+      }
+      FSL_TRY(cudaGraphLaunch(e.gexec, e.stream));
+    } else {
+      exec_enqueue(e);
+      cudaError_t le = cudaGetLastError();
+      if (le != cudaSuccess) return cuda_fail(le, "kernel launch");
+    }
+    e.steps++;
+    for (Group* g : e.groups) {
+      rc = group_prof_collect(*g);
+      if (rc) return rc;
+    }
+  }
+  return FSL_OK;
+}
+
+}  // namespace fsl

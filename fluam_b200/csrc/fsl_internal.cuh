@@ -285,34 +285,165 @@ struct Prof {
   }
   void count(int k) { launches += k; }
 };
-void launch_noise(const Params& P, const uint64_t* t_dev, float* out, cudaStream_t s);
+// One instance of the step: its parameters and device buffers.  A kernel
+// launch serves a batch of instances of one size class (same grid and
+// neighbour-grid extents, same kernel width).  A single instance is a batch
+// of one and is passed to its kernels by value.
+struct Rep {
+  Params P;
+  int active;  // 0: unused slot, every kernel returns at once
+  double *q, *qp, *F;
+  int *cell_of, *cnt, *start, *fill, *tmp, *sorted, *bsum;
+  int *bpp_cnt, *bpp_off, *bpp_idx;
+  double *bpp_k, *bpp_r0;
+  int *bfp_cnt, *bfp_off;
+  double *bfp_k, *bfp_r0, *bfp_xyz;
+  float* ljtab;
+  float* noise;
+  unsigned long long* grid;
+  float2* spec;
+  float* v;
+  float* wbuf;
+  double* u;  // interpolated velocities of the component entry point
+  int* err;
+  uint64_t* t;
+};
+
+// Launch kinds of the particle kernels (256-thread blocks): threads per
+// particle 1 (cell list), 8 (forces), 32 (one spread or interpolation per
+// particle), 64 (force spread plus drift spread per particle).
+enum { KIND_T1 = 0, KIND_T8 = 1, KIND_T32 = 2, KIND_T64 = 3, NKIND = 4 };
+constexpr int kPartThreads = 256;
+__host__ __device__ constexpr int kind_threads(int k) { return k == 0 ? 1 : k == 1 ? 8 : k == 2 ? 32 : 64; }
+__host__ __device__ constexpr int kind_ppb(int k) { return kPartThreads / kind_threads(k); }
+
+// Where a batched kernel finds its instance: the device table, and for the
+// particle kernels the first block of every instance per launch kind,
+// boff[kind * (nrep + 1) + r] (a flat grid with no idle blocks for small
+// instances).
+struct RepSrc {
+  const Rep* reps;
+  const int* boff;
+  int nrep;
+};
+
+// Launch shape of a batch: sizes shared by the class and the largest
+// per-instance ones.
+struct Batch {
+  const Rep* reps;  // device table
+  const int* boff;  // device block offsets, [NKIND][nrep + 1]
+  int nrep;
+  int mx, my, mz, mxh, nc, mN, kernel;
+  int max_np;
+  uint64_t max_noise_n;
+  int nblk[NKIND];  // total blocks of each particle launch kind
+  const Rep* one;   // host copy of the single instance (nrep == 1), else null
+  RepSrc src() const { return RepSrc{reps, boff, nrep}; }
+};
+
+// Instance of a block.  ONE: the launch serves a single instance passed by
+// value as a __grid_constant__ parameter, read in place from the parameter
+// bank.  Otherwise the block copies its table entry into shared memory.
+template <bool ONE>
+__device__ __forceinline__ const Rep& rep_copy(const RepSrc& src, const Rep& one, int idx, Rep& sh) {
+  if constexpr (ONE) {
+    return one;
+  } else {
+    const int* from = reinterpret_cast<const int*>(src.reps + idx);
+    int* to = reinterpret_cast<int*>(&sh);
+    for (int k = threadIdx.x; k < (int)(sizeof(Rep) / sizeof(int)); k += blockDim.x) to[k] = __ldg(from + k);
+    __syncthreads();
+    return sh;
+  }
+}
+
+// Particle kernels: the instance of this block of the flat grid and the
+// block's index within that instance (blk).
+template <bool ONE>
+__device__ __forceinline__ const Rep& rep_flat(const RepSrc& src, const Rep& one, int kind, int& blk,
+                                               Rep& sh) {
+  if constexpr (ONE) {
+    blk = blockIdx.x;
+    return one;
+  } else {
+    __shared__ int s_r;
+    const int* off = src.boff + kind * (src.nrep + 1);
+    if (threadIdx.x == 0) {
+      // largest r with off[r] <= blockIdx.x (instances without blocks are
+      // skipped because their successor starts at the same offset)
+      int lo = 0, hi = src.nrep - 1;
+      const int b = (int)blockIdx.x;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= b) lo = mid;
+        else hi = mid - 1;
+      }
+      s_r = lo;
+    }
+    __syncthreads();
+    const int r = s_r;
+    blk = (int)blockIdx.x - __ldg(off + r);
+    return rep_copy<false>(src, one, r, sh);
+  }
+}
+
+#define FSL_KARGS const RepSrc src, const __grid_constant__ Rep one
+
+#define FSL_REP_AT(IDX)                                            \
+  __shared__ Rep fsl_sh_rep_;                                      \
+  const Rep& R = rep_copy<ONE>(src, one, (int)(IDX), fsl_sh_rep_); \
+  if (!R.active) return;                                           \
+  const Params& P = R.P
+
+#define FSL_REP_FLAT(KIND)                                         \
+  __shared__ Rep fsl_sh_rep_;                                      \
+  int blk;                                                         \
+  const Rep& R = rep_flat<ONE>(src, one, (KIND), blk, fsl_sh_rep_); \
+  if (!R.active) return;                                           \
+  const Params& P = R.P
+
+// Launch of a kernel template whose first template argument is ONE.
+#define FSL_GO(KERN, GRID, BLOCK, SMEM, S, B, ...)                                     \
+  do {                                                                                 \
+    if ((B).one)                                                                       \
+      KERN<true><<<(GRID), (BLOCK), (SMEM), (S)>>>(RepSrc{}, *(B).one, ##__VA_ARGS__); \
+    else                                                                               \
+      KERN<false><<<(GRID), (BLOCK), (SMEM), (S)>>>((B).src(), Rep{}, ##__VA_ARGS__);  \
+  } while (0)
+// ... with a second template argument T
+#define FSL_GO_T(KERN, T, GRID, BLOCK, SMEM, S, B, ...)                                   \
+  do {                                                                                    \
+    if ((B).one)                                                                          \
+      KERN<true, T><<<(GRID), (BLOCK), (SMEM), (S)>>>(RepSrc{}, *(B).one, ##__VA_ARGS__); \
+    else                                                                                  \
+      KERN<false, T><<<(GRID), (BLOCK), (SMEM), (S)>>>((B).src(), Rep{}, ##__VA_ARGS__);  \
+  } while (0)
+
+// Blocks of a particle launch of kind k.
+inline unsigned part_blocks(const Batch& B, int k) {
+  if (B.one) return (unsigned)(((long)B.max_np * kind_threads(k) + kPartThreads - 1) / kPartThreads);
+  return (unsigned)B.nblk[k];
+}
+
+void launch_noise(const Batch& B, cudaStream_t s);
 void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t count, float* out,
                         cudaStream_t s);
-void launch_cells(const Params& P, const double* q, int* cell_of, int* cnt, int* start,
-                  int* fill, int* tmp, int* sorted, int* bsum, int* err, cudaStream_t s);
-void launch_forces(const Params& P, const double* q, const int* cell_of, const int* start,
-                   const int* sorted, const int* bpp_cnt, const int* bpp_off, const int* bpp_idx,
-                   const double* bpp_k, const double* bpp_r0, const int* bfp_cnt,
-                   const int* bfp_off, const double* bfp_k, const double* bfp_r0,
-                   const double* bfp_xyz, const float* ljtab, double* F, int* err,
-                   cudaStream_t s);
-void launch_spread(const Params& P, int drift, const int* order, const double* qf,
-                   const double* F, const double* q0, const float* noise,
-                   unsigned long long* grid, int* err, cudaStream_t s);
-void launch_interp_update(const Params& P, int stage, const double* qpos, const double* q0,
-                          const double* F, const float* noise, const float* v, double* qout,
-                          int* err, cudaStream_t s);
-void launch_interp(const Params& P, const double* qpos, const float* v, double* u,
-                   cudaStream_t s);
-void launch_step_counter(uint64_t* t_dev, cudaStream_t s);
+// which = 0: cell list / forces at q, 1: at q^{n+1/2}
+void launch_cells(const Batch& B, int which, cudaStream_t s);
+void launch_forces(const Batch& B, int which, cudaStream_t s);
+// drift = 0: spread F at q (cell-list order when ordered != 0);
+// drift = 1: spread F at q^{n+1/2} and the RFD drift at q
+void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s);
+void launch_interp_update(const Batch& B, int stage, cudaStream_t s);
+void launch_interp(const Batch& B, cudaStream_t s);  // u = J(q) v
+void launch_step_counter(const Batch& B, cudaStream_t s);
 
 struct FftPlan;  // defined in fsl_fft.cu
 FftPlan* fft_plan_create(const Params& P);
 void fft_plan_destroy(FftPlan* fp);
-// W source: the fixed-point spread grid plus the stochastic stress of draw t
-// (nsets = 1 or 2) when wext == nullptr, or a given float field wext.
-// wbuf: 3 nc floats that receive W; the spread field is cleared on the way.
-void launch_solve(const Params& P, FftPlan* fp, unsigned long long* grid, const float* noise,
-                  int nsets, const float* wext, float* wbuf, float2* spec, float* v,
-                  cudaStream_t s, Prof* prof = nullptr);
+// v = solve(W).  nsets = 1 or 2 stress samples; W is built from the spread
+// field (which is cleared on the way) and the noise into Rep::wbuf, unless
+// w_given, in which case Rep::wbuf already holds W.
+void launch_solve(const Batch& B, FftPlan* fp, int nsets, int w_given, cudaStream_t s,
+                  Prof* prof = nullptr);
 }  // namespace fsl

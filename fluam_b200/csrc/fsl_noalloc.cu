@@ -103,9 +103,26 @@ extern "C" int fsl_cell_list_noalloc(double lx, double ly, double lz, double cut
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   // the counters start at zero; the unordered buckets and block totals are
-  // fully rewritten before they are read
-  fsl::launch_cells(P, q_dev, cell_of_dev, s->cnt, start_dev, s->fill, s->tmp, sorted_dev, s->bsum,
-                    s->err, st);
+  // fully rewritten before they are read.  A single instance travels to the
+  // kernels as a by-value argument: nothing to allocate or copy first.
+  fsl::Rep r{};
+  r.P = P;
+  r.active = 1;
+  r.q = const_cast<double*>(q_dev);
+  r.cell_of = cell_of_dev;
+  r.start = start_dev;
+  r.sorted = sorted_dev;
+  r.cnt = s->cnt;
+  r.fill = s->fill;
+  r.tmp = s->tmp;
+  r.bsum = s->bsum;
+  r.err = s->err;
+  fsl::Batch B{};
+  B.one = &r;
+  B.nrep = 1;
+  B.mN = P.mN;
+  B.max_np = P.np;
+  fsl::launch_cells(B, 0, st);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(FSL_E_CUDA, cudaGetErrorString(e));
   return FSL_OK;

@@ -1,23 +1,31 @@
 // fsl_particles.cu -- particle-side kernels of the Stokes-limit step:
 // noise, counting-sort cell list, pair/bonded forces, fixed-point spreading
 // (forces and random-finite-difference drift), interpolation + midpoint
-// updates.
+// updates.  Every kernel serves a batch of instances (see Rep / Batch in
+// fsl_internal.cuh): kernels over cells take the instance from blockIdx.y,
+// kernels over particles run a flat grid whose blocks map to instances
+// through the block-offset table.  ONE = true compiles the single-instance
+// form, whose instance is a by-value parameter.
 #include "fsl_internal.cuh"
 
 namespace fsl {
+
+static unsigned blocks_for(long work, int tb) { return (unsigned)((work + tb - 1) / tb); }
 
 // ------------------------------------------------------------------ noise ---
 // The noise array of one draw, in the reference's layout
 // (src/runSchemeStokesLimit.cu:86-90, src/randomNumbers.cu:37-40):
 // [0,6nc) stress 1 (XX,XY,XZ,YY,YZ,ZZ), [6nc,6nc+3np) RFD vector,
 // [6nc+3np,6nc+9np) extra-mobility noises, [6nc+9np,12nc+9np) stress 2.
-__global__ void k_noise(uint64_t seed, const uint64_t* __restrict__ t_dev, uint64_t n,
-                        float4* __restrict__ out) {
-  uint64_t t = *t_dev;
-  uint64_t nb = (n + 3) >> 2;
+template <bool ONE>
+__global__ void k_noise(FSL_KARGS) {
+  FSL_REP_AT(blockIdx.y);
+  const uint64_t t = *R.t;
+  const uint64_t nb = (P.noise_n + 3) >> 2;
+  float4* out = reinterpret_cast<float4*>(R.noise);
   for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < nb;
        b += (uint64_t)gridDim.x * blockDim.x)
-    out[b] = philox_normal4(seed, t, b);
+    out[b] = philox_normal4(P.seed, t, b);
 }
 
 __global__ void k_noise_range(uint64_t seed, uint64_t t, uint64_t first, int64_t count,
@@ -30,12 +38,13 @@ __global__ void k_noise_range(uint64_t seed, uint64_t t, uint64_t first, int64_t
   out[k] = lane == 0 ? v.x : lane == 1 ? v.y : lane == 2 ? v.z : v.w;
 }
 
-void launch_noise(const Params& P, const uint64_t* t_dev, float* out, cudaStream_t s) {
-  uint64_t nb = (P.noise_n + 3) / 4;
-  int threads = 256;
-  int blocks = (int)((nb + threads - 1) / threads);
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  k_noise<<<blocks, threads, 0, s>>>(P.seed, t_dev, P.noise_n, reinterpret_cast<float4*>(out));
+void launch_noise(const Batch& B, cudaStream_t s) {
+  const int tb = 256;
+  uint64_t nb = (B.max_noise_n + 3) / 4;
+  unsigned bx = blocks_for((long)nb, tb);
+  unsigned cap = (unsigned)((148 * 16 + B.nrep - 1) / B.nrep);
+  if (bx > cap) bx = cap < 1 ? 1 : cap;
+  FSL_GO(k_noise, dim3(bx, B.nrep), tb, 0, s, B);
 }
 
 void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t count, float* out,
@@ -49,36 +58,41 @@ void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t cou
 // scatter, then order each cell's particles by index so that the list is
 // deterministic (the reference appends with atomics, in arbitrary order:
 // src/stokesLimitFunctions.cu:52-57).
-__global__ void k_cell_count(Params P, const double* __restrict__ q, int* __restrict__ cell_of,
-                             int* __restrict__ cnt, int* __restrict__ err) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+template <bool ONE>
+__global__ void k_zero_cells(FSL_KARGS) {
+  FSL_REP_AT(blockIdx.y);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < P.mN; c += gridDim.x * blockDim.x) {
+    R.cnt[c] = 0;
+    R.fill[c] = 0;
+    if (P.np == 0) R.start[c] = 0;  // no scan follows for an empty instance
+  }
+  if (P.np == 0 && blockIdx.x == 0 && threadIdx.x == 0) R.start[P.mN] = 0;
+}
+
+template <bool ONE>
+__global__ void k_cell_count(FSL_KARGS, int which) {
+  FSL_REP_FLAT(KIND_T1);
+  int i = blk * blockDim.x + threadIdx.x;
   if (i >= P.np) return;
+  const double* q = which ? R.qp : R.q;
   double x = q[i], y = q[P.np + i], z = q[2 * P.np + i];
   // a coordinate this large or non-finite means the run has blown up
   const double lim = 1e15;
-  if (!(fabs(x) < lim && fabs(y) < lim && fabs(z) < lim)) set_err(err, 2);
+  if (!(fabs(x) < lim && fabs(y) < lim && fabs(z) < lim)) set_err(R.err, 2);
   int c = nb_cell(P, x, y, z);
-  cell_of[i] = c;
-  atomicAdd(&cnt[c], 1);
+  R.cell_of[i] = c;
+  atomicAdd(&R.cnt[c], 1);
 }
 
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-// Block-local exclusive scan of cnt into start, block totals into bsum.
-__global__ void __launch_bounds__(kScanThreads) k_scan_local(const int* __restrict__ cnt, int n,
-                                                             int* __restrict__ start,
-                                                             int* __restrict__ bsum) {
-  __shared__ int warp_tot[kScanThreads / 32];
-  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-  int v[kScanItems];
+__device__ __forceinline__ void block_scan(const int (&v)[kScanItems], int& incl_out, int& sum_out,
+                                           int* warp_tot, int& total) {
   int sum = 0;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    v[k] = (base + k < n) ? cnt[base + k] : 0;
-    sum += v[k];
-  }
+  for (int k = 0; k < kScanItems; ++k) sum += v[k];
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int incl = sum;
 #pragma unroll
@@ -97,104 +111,100 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_local(const int* __restri
       if (lane >= o) wi += y;
     }
     warp_tot[lane] = wi - wt;  // exclusive
-    if (lane == 31) bsum[blockIdx.x] = wi;
+    if (lane == 31) warp_tot[32] = wi;
   }
   __syncthreads();
-  int run = warp_tot[warp] + incl - sum;
+  incl_out = warp_tot[warp] + incl - sum;  // exclusive prefix of this thread
+  sum_out = sum;
+  total = warp_tot[32];
+}
+
+// Block-local exclusive scan of cnt into start, block totals into bsum.
+template <bool ONE>
+__global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS) {
+  FSL_REP_AT(blockIdx.y);
+  __shared__ int warp_tot[33];
+  const int n = P.mN;
+  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < n) ? R.cnt[base + k] : 0;
+  int run, sum, total;
+  block_scan(v, run, sum, warp_tot, total);
+  if (threadIdx.x == 0) R.bsum[blockIdx.x] = total;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < n) start[base + k] = run;
+    if (base + k < n) R.start[base + k] = run;
     run += v[k];
   }
 }
 
 // Exclusive scan of the block totals (at most kScanTile of them), in place;
-// also writes the grand total to start[n].
-__global__ void __launch_bounds__(kScanThreads) k_scan_top(int* __restrict__ bsum, int nb,
-                                                           int* __restrict__ start, int n) {
-  __shared__ int warp_tot[kScanThreads / 32];
+// also writes the grand total to start[mN].
+template <bool ONE>
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(FSL_KARGS) {
+  FSL_REP_AT(blockIdx.y);
+  __shared__ int warp_tot[33];
+  const int nb = (P.mN + kScanTile - 1) / kScanTile;
   int base = threadIdx.x * kScanItems;
   int v[kScanItems];
-  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < nb) ? R.bsum[base + k] : 0;
+  int run, sum, total;
+  block_scan(v, run, sum, warp_tot, total);
+  if (threadIdx.x == 0) R.start[P.mN] = total;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    v[k] = (base + k < nb) ? bsum[base + k] : 0;
-    sum += v[k];
-  }
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int incl = sum;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  if (lane == 31) warp_tot[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    int wt = warp_tot[lane];
-    int wi = wt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += y;
-    }
-    warp_tot[lane] = wi - wt;
-    if (lane == 31) start[n] = wi;
-  }
-  __syncthreads();
-  int run = warp_tot[warp] + incl - sum;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < nb) bsum[base + k] = run;
+    if (base + k < nb) R.bsum[base + k] = run;
     run += v[k];
   }
 }
 
-__global__ void k_scan_add(int* __restrict__ start, int n, const int* __restrict__ bsum) {
+template <bool ONE>
+__global__ void k_scan_add(FSL_KARGS) {
+  FSL_REP_AT(blockIdx.y);
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  start[i] += bsum[i / kScanTile];
+  if (i >= P.mN) return;
+  R.start[i] += R.bsum[i / kScanTile];
 }
 
-__global__ void k_cell_scatter(Params P, const int* __restrict__ cell_of,
-                               const int* __restrict__ start, int* __restrict__ fill,
-                               int* __restrict__ tmp) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+template <bool ONE>
+__global__ void k_cell_scatter(FSL_KARGS) {
+  FSL_REP_FLAT(KIND_T1);
+  int i = blk * blockDim.x + threadIdx.x;
   if (i >= P.np) return;
-  int c = cell_of[i];
-  tmp[start[c] + atomicAdd(&fill[c], 1)] = i;
+  int c = R.cell_of[i];
+  R.tmp[R.start[c] + atomicAdd(&R.fill[c], 1)] = i;
 }
 
 // Rank of particle i among the particles of its cell = number of smaller
 // indices in the (unordered) bucket; gives the ascending order.
-__global__ void k_cell_rank(Params P, const int* __restrict__ cell_of,
-                            const int* __restrict__ start, const int* __restrict__ tmp,
-                            int* __restrict__ sorted) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+template <bool ONE>
+__global__ void k_cell_rank(FSL_KARGS) {
+  FSL_REP_FLAT(KIND_T1);
+  int i = blk * blockDim.x + threadIdx.x;
   if (i >= P.np) return;
-  int c = cell_of[i];
-  int s = start[c], e = start[c + 1];
+  int c = R.cell_of[i];
+  int s = R.start[c], e = R.start[c + 1];
   int rank = 0;
-  for (int k = s; k < e; ++k) rank += tmp[k] < i;
-  sorted[s + rank] = i;
+  for (int k = s; k < e; ++k) rank += R.tmp[k] < i;
+  R.sorted[s + rank] = i;
 }
 
-void launch_cells(const Params& P, const double* q, int* cell_of, int* cnt, int* start,
-                  int* fill, int* tmp, int* sorted, int* bsum, int* err, cudaStream_t s) {
-  cudaMemsetAsync(cnt, 0, sizeof(int) * P.mN, s);
-  cudaMemsetAsync(fill, 0, sizeof(int) * P.mN, s);
-  if (P.np == 0) {
-    cudaMemsetAsync(start, 0, sizeof(int) * (P.mN + 1), s);
-    return;
-  }
-  int tb = 256, nbp = (P.np + tb - 1) / tb;
-  k_cell_count<<<nbp, tb, 0, s>>>(P, q, cell_of, cnt, err);
-  int nblk = (P.mN + kScanTile - 1) / kScanTile;
-  k_scan_local<<<nblk, kScanThreads, 0, s>>>(cnt, P.mN, start, bsum);
-  k_scan_top<<<1, kScanThreads, 0, s>>>(bsum, nblk, start, P.mN);
-  k_scan_add<<<(P.mN + 255) / 256, 256, 0, s>>>(start, P.mN, bsum);
-  k_cell_scatter<<<nbp, tb, 0, s>>>(P, cell_of, start, fill, tmp);
-  k_cell_rank<<<nbp, tb, 0, s>>>(P, cell_of, start, tmp, sorted);
+void launch_cells(const Batch& B, int which, cudaStream_t s) {
+  const int tb = kPartThreads;
+  unsigned zb = blocks_for(B.mN, tb);
+  if (zb > 1024) zb = 1024;
+  FSL_GO(k_zero_cells, dim3(zb, B.nrep), tb, 0, s, B);
+  if (B.max_np == 0) return;
+  const unsigned pb = part_blocks(B, KIND_T1);
+  FSL_GO(k_cell_count, pb, tb, 0, s, B, which);
+  unsigned nblk = blocks_for(B.mN, kScanTile);
+  FSL_GO(k_scan_local, dim3(nblk, B.nrep), kScanThreads, 0, s, B);
+  FSL_GO(k_scan_top, dim3(1, B.nrep), kScanThreads, 0, s, B);
+  FSL_GO(k_scan_add, dim3(blocks_for(B.mN, 256), B.nrep), 256, 0, s, B);
+  FSL_GO(k_cell_scatter, pb, tb, 0, s, B);
+  FSL_GO(k_cell_rank, pb, tb, 0, s, B);
 }
 
 // ----------------------------------------------------------------- forces ---
@@ -209,15 +219,6 @@ __device__ __forceinline__ float tex_linear(const float* __restrict__ T, int N, 
   int i1 = min(max(i + 1, 0), N - 1);
   return __fadd_rn(__fmul_rn(1.0f - a, __ldg(T + i0)), __fmul_rn(a, __ldg(T + i1)));
 }
-
-// Neighbour-cell order of the reference's pair loop
-// (src/stokesLimitFunctions.cu:191-653).
-__constant__ signed char c_nb_order[27][3] = {
-    {0, 0, 0},   {0, 0, -1},  {0, -1, 0},  {-1, 0, 0},  {1, 0, 0},   {0, 1, 0},
-    {0, 0, 1},   {1, 1, 0},   {1, -1, 0},  {1, 0, 1},   {1, 0, -1},  {-1, 1, 0},
-    {-1, -1, 0}, {-1, 0, 1},  {-1, 0, -1}, {0, 1, 1},   {0, 1, -1},  {0, -1, 1},
-    {0, -1, -1}, {1, 1, 1},   {1, 1, -1},  {1, -1, 1},  {1, -1, -1}, {-1, 1, 1},
-    {-1, 1, -1}, {-1, -1, 1}, {-1, -1, -1}};
 
 __device__ __forceinline__ void bond_force(double rx, double ry, double rz, double x, double y,
                                            double z, double k, double r0, double& fx,
@@ -238,40 +239,39 @@ __device__ __forceinline__ void bond_force(double rx, double ry, double rz, doub
   }
 }
 
-__global__ void k_forces(Params P, const double* __restrict__ q, const int* __restrict__ cell_of,
-                         const int* __restrict__ start, const int* __restrict__ sorted,
-                         const int* __restrict__ bpp_cnt, const int* __restrict__ bpp_off,
-                         const int* __restrict__ bpp_idx, const double* __restrict__ bpp_k,
-                         const double* __restrict__ bpp_r0, const int* __restrict__ bfp_cnt,
-                         const int* __restrict__ bfp_off, const double* __restrict__ bfp_k,
-                         const double* __restrict__ bfp_r0, const double* __restrict__ bfp_xyz,
-                         const float* __restrict__ ljtab, double* __restrict__ F,
-                         int* __restrict__ err) {
-  // eight lanes per particle: they share the bonds and the 27 neighbour
-  // cells (cells sub, sub+8, ...), then sum their partial forces
+// Pair (src/stokesLimitFunctions.cu:191-653 with the table of
+// src/initForcesNonBonded.cu:21-66, or soft repulsion) and bonded
+// (src/forceBondedGPU.cu:21-121) force on every particle.  Eight lanes per
+// particle share its bonds and its 27 neighbour cells (cells sub, sub+8, ...),
+// then sum their partial forces in a fixed butterfly order.
+template <bool ONE>
+__global__ void k_forces(FSL_KARGS, int which) {
+  FSL_REP_FLAT(KIND_T8);
   const int sub = threadIdx.x & 7;
-  const int ig = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 3);
+  const int ig = (int)((blk * (size_t)blockDim.x + threadIdx.x) >> 3);
+  if ((ig & ~3) >= P.np) return;  // uniform per warp (4 particles per warp)
   const bool active = ig < P.np;  // inactive lanes still join the shuffles
   const int i = active ? ig : 0;
   const int np = P.np;
+  const double* __restrict__ q = which ? R.qp : R.q;
   double rx = q[i], ry = q[np + i], rz = q[2 * np + i];
   double fx = 0.0, fy = 0.0, fz = 0.0;
   if (P.bonded && active) {
-    int nb = bpp_cnt[i], off = bpp_off[i];
+    int nb = R.bpp_cnt[i], off = R.bpp_off[i];
     for (int j = sub; j < nb; j += 8) {
-      int idx = bpp_idx[off + j];
-      bond_force(rx, ry, rz, q[idx], q[np + idx], q[2 * np + idx], bpp_k[off + j],
-                 bpp_r0[off + j], fx, fy, fz);
+      int idx = R.bpp_idx[off + j];
+      bond_force(rx, ry, rz, q[idx], q[np + idx], q[2 * np + idx], R.bpp_k[off + j],
+                 R.bpp_r0[off + j], fx, fy, fz);
     }
-    nb = bfp_cnt[i];
-    off = bfp_off[i];
+    nb = R.bfp_cnt[i];
+    off = R.bfp_off[i];
     for (int j = sub; j < nb; j += 8) {
-      const double* p = bfp_xyz + 3 * (off + j);
-      bond_force(rx, ry, rz, p[0], p[1], p[2], bfp_k[off + j], bfp_r0[off + j], fx, fy, fz);
+      const double* p = R.bfp_xyz + 3 * (off + j);
+      bond_force(rx, ry, rz, p[0], p[1], p[2], R.bfp_k[off + j], R.bfp_r0[off + j], fx, fy, fz);
     }
   }
   if (P.nonbonded && P.pair != 0 && active) {
-    int c = cell_of[i];
+    int c = R.cell_of[i];
     int cxy = c % (P.mnx * P.mny);
     int cz = c / (P.mnx * P.mny), cy = cxy / P.mnx, cx = cxy - cy * P.mnx;
     for (int nn = sub; nn < 27; nn += 8) {
@@ -282,9 +282,9 @@ __global__ void k_forces(Params P, const double* __restrict__ q, const int* __re
       oy += oy < 0 ? P.mny : (oy >= P.mny ? -P.mny : 0);
       oz += oz < 0 ? P.mnz : (oz >= P.mnz ? -P.mnz : 0);
       int cc = ox + oy * P.mnx + oz * P.mnx * P.mny;
-      int e = start[cc + 1];
-      for (int jj = start[cc]; jj < e; ++jj) {
-        int j = sorted[jj];
+      int e = R.start[cc + 1];
+      for (int jj = R.start[cc]; jj < e; ++jj) {
+        int j = R.sorted[jj];
         double rxij = minimage(rx - q[j], P.invlx, P.lx);
         double ryij = minimage(ry - q[np + j], P.invly, P.ly);
         double rzij = minimage(rz - q[2 * np + j], P.invlz, P.lz);
@@ -293,7 +293,7 @@ __global__ void k_forces(Params P, const double* __restrict__ q, const int* __re
                               __dmul_rn(rzij, rzij));
         double f;
         if (P.pair == 1) {
-          f = (double)tex_linear(ljtab, kLjTableSize, (float)(r2 * P.invcut2));
+          f = (double)tex_linear(R.ljtab, kLjTableSize, (float)(r2 * P.invcut2));
         } else {
           if (j == i || r2 >= P.cutoff2 || r2 == 0.0) continue;
           double r = sqrt(r2);
@@ -305,7 +305,6 @@ __global__ void k_forces(Params P, const double* __restrict__ q, const int* __re
       }
     }
   }
-  // fixed butterfly order within the eight lanes: the same sum on every run
 #pragma unroll
   for (int o = 4; o > 0; o >>= 1) {
     fx += __shfl_xor_sync(0xffffffffu, fx, o);
@@ -313,39 +312,25 @@ __global__ void k_forces(Params P, const double* __restrict__ q, const int* __re
     fz += __shfl_xor_sync(0xffffffffu, fz, o);
   }
   if (sub != 0 || !active) return;
-  if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) set_err(err, 2);
-  F[i] = fx;
-  F[np + i] = fy;
-  F[2 * np + i] = fz;
+  if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) set_err(R.err, 2);
+  R.F[i] = fx;
+  R.F[np + i] = fy;
+  R.F[2 * np + i] = fz;
 }
 
-void launch_forces(const Params& P, const double* q, const int* cell_of, const int* start,
-                   const int* sorted, const int* bpp_cnt, const int* bpp_off, const int* bpp_idx,
-                   const double* bpp_k, const double* bpp_r0, const int* bfp_cnt,
-                   const int* bfp_off, const double* bfp_k, const double* bfp_r0,
-                   const double* bfp_xyz, const float* ljtab, double* F, int* err,
-                   cudaStream_t s) {
-  if (P.np == 0) return;
-  const int tb = 256, per_block = tb / 8;
-  k_forces<<<(P.np + per_block - 1) / per_block, tb, 0, s>>>(P, q, cell_of, start, sorted, bpp_cnt, bpp_off,
-                                               bpp_idx, bpp_k, bpp_r0, bfp_cnt, bfp_off, bfp_k,
-                                               bfp_r0, bfp_xyz, ljtab, F, err);
+void launch_forces(const Batch& B, int which, cudaStream_t s) {
+  if (B.max_np == 0) return;
+  FSL_GO(k_forces, part_blocks(B, KIND_T8), kPartThreads, 0, s, B, which);
 }
 
 // ------------------------------------------------------------- spreading ---
-// One warp per (entry, component); lane l takes stencil nodes l, l+32, ...
-// (x fastest, so a warp's atomics fall on a few 32-byte sectors) and adds
-// w * value in 64-bit fixed point to the staggered field of that component.
+// One warp per entry (all three components of one spread of one particle);
+// lane l takes stencil nodes l, l+32, ... (x fastest, so a warp's atomics
+// fall on a few 32-byte sectors) and adds w * value in 64-bit fixed point.
 // Replaces the slot writes of kernelSpreadParticlesForceStokesLimit and
 // kernelSpreadParticlesDrift + the gather of addSpreadedForcesStokesLimit
 // (src/stokesLimitFunctions.cu:659-1681, 1705-2255); the 1/dV of the gather
 // is applied when the field is read back.
-//
-// Entries [0, nforce) spread F of particle order[e] at qf; entries
-// [nforce, nforce + 2 np) spread the RFD drift (kT/delta) sign W_p from
-// q + sign (delta/2) W_p, sign + for the first np and - for the second.  In
-// reference mode the drift's nodes come from the displaced position and its
-// weights from q, as the reference does.
 template <int KN>  // kernel width 3 or 4
 __device__ __forceinline__ void spread_entry(const Params& P, const double posc[3],
                                              const double posw[3], const double val[3],
@@ -377,31 +362,34 @@ __device__ __forceinline__ void spread_entry(const Params& P, const double posc[
   }
 }
 
-// One warp per entry (all three components of one spread of one particle).
-template <int KN>
-__global__ void k_spread(Params P, int nforce, int drift, const int* __restrict__ order,
-                         const double* __restrict__ qf, const double* __restrict__ F,
-                         const double* __restrict__ q0, const float* __restrict__ noise,
-                         unsigned long long* __restrict__ grid, int* __restrict__ err) {
+// drift = 0: entries [0, np) spread F at q; drift = 1: entries [0, np) spread
+// F at q^{n+1/2}, entries [np, 2np) the RFD drift of one particle each:
+// (kT/delta) sign W_p from q + sign (delta/2) W_p for both signs.  In
+// reference mode the drift's nodes come from the displaced position and its
+// weights from q, as the reference does.
+template <bool ONE, int KN>
+__global__ void k_spread(FSL_KARGS, int drift, int ordered) {
+  FSL_REP_FLAT(drift ? KIND_T64 : KIND_T32);
   const int lane = threadIdx.x & 31;
-  const long e = (long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const long e = (long)((blk * (size_t)blockDim.x + threadIdx.x) >> 5);
   const int np = P.np;
-  const long nent = (long)nforce + (drift ? (long)np : 0l);
+  const long nent = (long)np * (drift ? 2 : 1);
   if (e >= nent) return;  // uniform per warp
+  const int* order = ordered ? R.sorted : nullptr;
   bool sat = false;
-  if (e < nforce) {
+  if (e < np) {
+    const double* qf = drift ? R.qp : R.q;
     int i = order ? order[e] : (int)e;
     double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
-    double val[3] = {F[i], F[np + i], F[2 * (size_t)np + i]};
-    spread_entry<KN>(P, pos, pos, val, grid, lane, sat);
+    double val[3] = {R.F[i], R.F[np + i], R.F[2 * (size_t)np + i]};
+    spread_entry<KN>(P, pos, pos, val, R.grid, lane, sat);
   } else {
-    // both signs of the drift of one particle
-    int i = (int)(e - nforce);
+    int i = (int)(e - np);
     if (order) i = order[i];
     const size_t wbase = (size_t)6 * P.nc;
-    double W[3] = {(double)noise[wbase + i], (double)noise[wbase + np + i],
-                   (double)noise[wbase + 2 * np + i]};
-    double pos[3] = {q0[i], q0[np + i], q0[2 * np + i]};
+    double W[3] = {(double)R.noise[wbase + i], (double)R.noise[wbase + np + i],
+                   (double)R.noise[wbase + 2 * np + i]};
+    double pos[3] = {R.q[i], R.q[np + i], R.q[2 * np + i]};
     double pp[3], pm[3], vp[3], vm[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -421,30 +409,23 @@ __global__ void k_spread(Params P, int nforce, int drift, const int* __restrict_
         same = stencil_base(P, d, f, pp[d]) == stencil_base(P, d, f, pm[d]);
       }
       if (__all_sync(0xffffffffu, same)) return;
-      spread_entry<KN>(P, pp, pos, vp, grid, lane, sat);
-      spread_entry<KN>(P, pm, pos, vm, grid, lane, sat);
+      spread_entry<KN>(P, pp, pos, vp, R.grid, lane, sat);
+      spread_entry<KN>(P, pm, pos, vm, R.grid, lane, sat);
     } else {
-      spread_entry<KN>(P, pp, pp, vp, grid, lane, sat);
-      spread_entry<KN>(P, pm, pm, vm, grid, lane, sat);
+      spread_entry<KN>(P, pp, pp, vp, R.grid, lane, sat);
+      spread_entry<KN>(P, pm, pm, vm, R.grid, lane, sat);
     }
   }
-  if (sat) set_err(err, 1);
+  if (sat) set_err(R.err, 1);
 }
 
-// force spread of all particles (at qf, in the order of the cell list when
-// `order` is given) and, with drift != 0, the two RFD spreads at q0
-void launch_spread(const Params& P, int drift, const int* order, const double* qf,
-                   const double* F, const double* q0, const float* noise,
-                   unsigned long long* grid, int* err, cudaStream_t s) {
-  if (P.np == 0) return;
-  long nent = (long)P.np * (drift ? 2 : 1);
-  long threads = nent * 32;
-  const int tb = 256;
-  unsigned nb = (unsigned)((threads + tb - 1) / tb);
-  if (P.kernel == 4)
-    k_spread<4><<<nb, tb, 0, s>>>(P, P.np, drift, order, qf, F, q0, noise, grid, err);
+void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s) {
+  if (B.max_np == 0) return;
+  const unsigned g = part_blocks(B, drift ? KIND_T64 : KIND_T32);
+  if (B.kernel == 4)
+    FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered);
   else
-    k_spread<3><<<nb, tb, 0, s>>>(P, P.np, drift, order, qf, F, q0, noise, grid, err);
+    FSL_GO_T(k_spread, 3, g, kPartThreads, 0, s, B, drift, ordered);
 }
 
 // -------------------------------------------------------- interpolation ---
@@ -459,7 +440,7 @@ __device__ __forceinline__ void interp_particle(const Params& P, const double po
   constexpr int n = KN, n3 = n * n * n, total = 3 * n3;
   constexpr int iters = (total + 31) >> 5;
   const WarpStencil st = warp_stencil(P, pos, pos, lane);
-  // gather every node's address and weight first, then all loads at once
+  // every node's address and weight first, then all loads at once
   float wt[iters];
   const float* ad[iters];
 #pragma unroll
@@ -505,78 +486,76 @@ __device__ __forceinline__ void interp_particle(const Params& P, const double po
 //          src/stokesLimitFunctions.cu:2646-2650
 // stage 2: q^{n+1}   = q^n + dt J(q^{n+1/2}) v (+ extraMobility terms),
 //          src/stokesLimitFunctions.cu:3676-3681
-template <int KN>
-__global__ void k_interp_update(Params P, int stage, const double* __restrict__ qpos,
-                                const double* __restrict__ q0, const double* __restrict__ F,
-                                const float* __restrict__ noise, const float* __restrict__ v,
-                                double* __restrict__ qout, int* __restrict__ err) {
+template <bool ONE, int KN>
+__global__ void k_interp_update(FSL_KARGS, int stage) {
+  FSL_REP_FLAT(KIND_T32);
   const int lane = threadIdx.x & 31;
-  const long t = (long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const long t = (long)((blk * (size_t)blockDim.x + threadIdx.x) >> 5);
   if (t >= P.np) return;  // uniform per warp
   const int i = (int)t;
   const int np = P.np;
+  const double* qpos = stage == 1 ? R.q : R.qp;
+  double* qout = stage == 1 ? R.qp : R.q;
   double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
   float us[3];
-  interp_particle<KN>(P, pos, v, lane, us);
+  interp_particle<KN>(P, pos, R.v, lane, us);
   if (lane >= 3) return;
   const int comp = lane;  // lanes 0, 1, 2 update x, y, z
   const double u = (double)(comp == 0 ? us[0] : (comp == 1 ? us[1] : us[2]));
   size_t k = (size_t)comp * np + i;
   double h = stage == 1 ? 0.5 * P.dt : P.dt;
-  double r = q0[k] + h * u;
+  double r = R.q[k] + h * u;
   if (P.has_extra) {
     size_t nb = (size_t)6 * P.nc + (size_t)(3 + comp) * np + i;
-    double xi = (double)noise[nb];
-    if (stage == 2) xi += (double)noise[nb + (size_t)3 * np];
-    r += h * P.extra_mob * F[k] + P.fact2 * xi;
+    double xi = (double)R.noise[nb];
+    if (stage == 2) xi += (double)R.noise[nb + (size_t)3 * np];
+    r += h * P.extra_mob * R.F[k] + P.fact2 * xi;
   }
-  if (!isfinite(r)) set_err(err, 2);
+  if (!isfinite(r)) set_err(R.err, 2);
   qout[k] = r;
 }
 
-template <int KN>
-__global__ void k_interp(Params P, const double* __restrict__ qpos, const float* __restrict__ v,
-                         double* __restrict__ u) {
+template <bool ONE, int KN>
+__global__ void k_interp(FSL_KARGS) {
+  FSL_REP_FLAT(KIND_T32);
   const int lane = threadIdx.x & 31;
-  const long t = (long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const long t = (long)((blk * (size_t)blockDim.x + threadIdx.x) >> 5);
   if (t >= P.np) return;  // uniform per warp
   const int i = (int)t;
   const int np = P.np;
-  double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
+  double pos[3] = {R.q[i], R.q[np + i], R.q[2 * np + i]};
   float us[3];
-  interp_particle<KN>(P, pos, v, lane, us);
-  if (lane < 3) u[(size_t)lane * np + i] = (double)(lane == 0 ? us[0] : (lane == 1 ? us[1] : us[2]));
+  interp_particle<KN>(P, pos, R.v, lane, us);
+  if (lane < 3) R.u[(size_t)lane * np + i] = (double)(lane == 0 ? us[0] : (lane == 1 ? us[1] : us[2]));
 }
 
-static unsigned warp_blocks(long warps, int tb) {
-  return (unsigned)((warps * 32 + tb - 1) / tb);
-}
-
-void launch_interp_update(const Params& P, int stage, const double* qpos, const double* q0,
-                          const double* F, const float* noise, const float* v, double* qout,
-                          int* err, cudaStream_t s) {
-  if (P.np == 0) return;
-  const int tb = 256;
-  if (P.kernel == 4)
-    k_interp_update<4><<<warp_blocks(P.np, tb), tb, 0, s>>>(P, stage, qpos, q0, F, noise, v, qout,
-                                                            err);
+void launch_interp_update(const Batch& B, int stage, cudaStream_t s) {
+  if (B.max_np == 0) return;
+  const unsigned g = part_blocks(B, KIND_T32);
+  if (B.kernel == 4)
+    FSL_GO_T(k_interp_update, 4, g, kPartThreads, 0, s, B, stage);
   else
-    k_interp_update<3><<<warp_blocks(P.np, tb), tb, 0, s>>>(P, stage, qpos, q0, F, noise, v, qout,
-                                                            err);
+    FSL_GO_T(k_interp_update, 3, g, kPartThreads, 0, s, B, stage);
 }
 
-void launch_interp(const Params& P, const double* qpos, const float* v, double* u,
-                   cudaStream_t s) {
-  if (P.np == 0) return;
-  const int tb = 256;
-  if (P.kernel == 4)
-    k_interp<4><<<warp_blocks(P.np, tb), tb, 0, s>>>(P, qpos, v, u);
+void launch_interp(const Batch& B, cudaStream_t s) {
+  if (B.max_np == 0) return;
+  const unsigned g = part_blocks(B, KIND_T32);
+  if (B.kernel == 4)
+    FSL_GO_T(k_interp, 4, g, kPartThreads, 0, s, B);
   else
-    k_interp<3><<<warp_blocks(P.np, tb), tb, 0, s>>>(P, qpos, v, u);
+    FSL_GO_T(k_interp, 3, g, kPartThreads, 0, s, B);
 }
 
-__global__ void k_step_counter(uint64_t* t_dev) { *t_dev += 1; }
+template <bool ONE>
+__global__ void k_step_counter(FSL_KARGS) {
+  FSL_REP_AT(blockIdx.y);
+  (void)P;
+  if (threadIdx.x == 0) *R.t += 1;
+}
 
-void launch_step_counter(uint64_t* t_dev, cudaStream_t s) { k_step_counter<<<1, 1, 0, s>>>(t_dev); }
+void launch_step_counter(const Batch& B, cudaStream_t s) {
+  FSL_GO(k_step_counter, dim3(1, B.nrep), 32, 0, s, B);
+}
 
 }  // namespace fsl
