@@ -25,6 +25,11 @@ EXPORTS = [
     "fsl_destroy", "fsl_last_error", "fsl_run_data_main", "fsl_parse_data_main",
     "fsl_neighbor_grid", "fsl_cell_list", "fsl_compute_forces", "fsl_spread", "fsl_solve",
     "fsl_interpolate", "fsl_noise", "fsl_cell_list_noalloc",
+    "fsl_batch_create", "fsl_batch_load_bonds", "fsl_batch_step", "fsl_batch_sync",
+    "fsl_batch_get_positions", "fsl_batch_get_forces", "fsl_batch_get_status",
+    "fsl_batch_get_positions_packed", "fsl_batch_set_positions_packed",
+    "fsl_batch_get_positions_packed_async", "fsl_batch_set_positions_packed_async",
+    "fsl_batch_set_graph", "fsl_batch_get_info", "fsl_batch_stream", "fsl_batch_destroy",
 ]
 
 
@@ -52,6 +57,14 @@ class Status(ctypes.Structure):
 class StageTime(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_int64),
                 ("total_ms", ctypes.c_double)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32), ("classes", ctypes.c_int32), ("graph", ctypes.c_int32),
+        ("launches_per_step", ctypes.c_int32), ("np_total", ctypes.c_int64),
+        ("nc_total", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
+    ]
 
 
 class FslError(RuntimeError):
@@ -110,6 +123,26 @@ def load(path=None):
     L.fsl_noise.argtypes = [_VP, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, _F]
     L.fsl_cell_list_noalloc.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, ctypes.c_int64, _VP, _VP, _VP, _VP, _VP]
+    L.fsl_batch_create.argtypes = [ctypes.c_int32, ctypes.POINTER(Config),
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(_D),
+                                   ctypes.POINTER(_VP)]
+    L.fsl_batch_load_bonds.argtypes = [_VP, ctypes.c_int32, ctypes.c_int64, _I, _I, _D, _D,
+                                       ctypes.c_int64, _I, _D, _D, _D]
+    L.fsl_batch_step.argtypes = [_VP, ctypes.c_int64]
+    L.fsl_batch_sync.argtypes = [_VP]
+    L.fsl_batch_get_positions.argtypes = [_VP, ctypes.c_int32, _D]
+    L.fsl_batch_get_forces.argtypes = [_VP, ctypes.c_int32, _D]
+    L.fsl_batch_get_status.argtypes = [_VP, ctypes.c_int32, ctypes.POINTER(Status)]
+    L.fsl_batch_get_positions_packed.argtypes = [_VP, _D]
+    L.fsl_batch_set_positions_packed.argtypes = [_VP, _D]
+    L.fsl_batch_get_positions_packed_async.argtypes = [_VP, _VP]
+    L.fsl_batch_set_positions_packed_async.argtypes = [_VP, _VP]
+    L.fsl_batch_set_graph.argtypes = [_VP, ctypes.c_int]
+    L.fsl_batch_get_info.argtypes = [_VP, ctypes.POINTER(BatchInfo)]
+    L.fsl_batch_stream.argtypes = [_VP]
+    L.fsl_batch_stream.restype = _VP
+    L.fsl_batch_destroy.argtypes = [_VP]
+    L.fsl_batch_destroy.restype = None
     if path is None:
         _lib = L
     return L

@@ -14,7 +14,7 @@ import numpy as np
 from . import _lib
 from ._lib import PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE, check
 
-__all__ = ["StokesLimit", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
+__all__ = ["StokesLimit", "Batch", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
            "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE"]
 
 
@@ -179,6 +179,112 @@ class StokesLimit:
         check(self.L.fsl_noise(self.h, int(t), int(first), int(count),
                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
+
+
+class Batch:
+    """Independent Stokes-limit instances stepped together (fsl_batch_*).
+
+    ``configs`` is a sequence of Config, ``positions`` a sequence of (3, np_i)
+    arrays.  Instances of the same size class share every kernel launch; each
+    instance's results equal those of the same instance run alone.
+    """
+
+    def __init__(self, configs, positions):
+        self.L = _lib.load()
+        n = len(configs)
+        if len(positions) != n:
+            raise ValueError("one position array per configuration")
+        qs = [np.ascontiguousarray(q, dtype=np.float64).reshape(3, -1) for q in positions]
+        self.nps = np.array([q.shape[1] for q in qs], dtype=np.int64)
+        cfgs = (_lib.Config * max(n, 1))(*configs)
+        qp = (ctypes.POINTER(ctypes.c_double) * max(n, 1))(*[_dp(q) for q in qs])
+        h = ctypes.c_void_p()
+        check(self.L.fsl_batch_create(n, cfgs, self.nps.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                      qp, ctypes.byref(h)))
+        self.h = h
+        self.n = n
+        self.offsets = np.concatenate([[0], np.cumsum(3 * self.nps)]).astype(np.int64)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fsl_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def load_bonds(self, i, bi, bj, k, r0):
+        bi = np.ascontiguousarray(bi, dtype=np.int32)
+        bj = np.ascontiguousarray(bj, dtype=np.int32)
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        r0 = np.ascontiguousarray(r0, dtype=np.float64)
+        z, zi = np.zeros(1), np.zeros(1, np.int32)
+        check(self.L.fsl_batch_load_bonds(self.h, int(i), len(bi), _ip(bi), _ip(bj), _dp(k), _dp(r0),
+                                          0, _ip(zi), _dp(z), _dp(z), _dp(z)))
+
+    def step(self, n=1):
+        check(self.L.fsl_batch_step(self.h, int(n)))
+
+    def sync(self):
+        check(self.L.fsl_batch_sync(self.h))
+
+    def set_graph(self, enable):
+        check(self.L.fsl_batch_set_graph(self.h, 1 if enable else 0))
+
+    def positions(self, i):
+        out = np.empty((3, int(self.nps[i])))
+        check(self.L.fsl_batch_get_positions(self.h, int(i), _dp(out)))
+        return out
+
+    def forces(self, i):
+        out = np.empty((3, int(self.nps[i])))
+        check(self.L.fsl_batch_get_forces(self.h, int(i), _dp(out)))
+        return out
+
+    def status(self, i):
+        st = _lib.Status()
+        check(self.L.fsl_batch_get_status(self.h, int(i), ctypes.byref(st)))
+        return {"step": st.step, "error_bits": st.error_bits, "np": st.np, "nc": st.nc,
+                "graph": bool(st.graph), "launches_per_step": st.launches_per_step}
+
+    def positions_packed(self, out=None):
+        if out is None:
+            out = np.empty(int(self.offsets[-1]))
+        check(self.L.fsl_batch_get_positions_packed(self.h, _dp(out)))
+        return out
+
+    def set_positions_packed(self, packed):
+        packed = np.ascontiguousarray(packed, dtype=np.float64).reshape(-1)
+        if packed.size != self.offsets[-1]:
+            raise ValueError("packed array has the wrong size")
+        check(self.L.fsl_batch_set_positions_packed(self.h, _dp(packed)))
+
+    def positions_packed_async(self, host_ptr):
+        """Queue the packed positions into host memory at host_ptr (an int)."""
+        check(self.L.fsl_batch_get_positions_packed_async(self.h, ctypes.c_void_p(host_ptr)))
+
+    def set_positions_packed_async(self, host_ptr):
+        check(self.L.fsl_batch_set_positions_packed_async(self.h, ctypes.c_void_p(host_ptr)))
+
+    def unpack(self, packed, i):
+        return packed[self.offsets[i]:self.offsets[i + 1]].reshape(3, -1)
+
+    def info(self):
+        b = _lib.BatchInfo()
+        check(self.L.fsl_batch_get_info(self.h, ctypes.byref(b)))
+        return {f: getattr(b, f) for f, _ in _lib.BatchInfo._fields_}
+
+    def stream(self):
+        return self.L.fsl_batch_stream(self.h)
 
 
 def run_data_main(path):

@@ -9,6 +9,10 @@ bead-spring chains) and the noise is drawn on the device from the seed.
              65,536 particles = 4,096 chains x 16 beads, harmonic bonds k 10,
              r0 1 (chain starts seeded uniform, each bond a seeded random unit
              vector), soft repulsion eps 1, rc 1.5
+  mixed_1024 1,024 independent periodic cubic replicas, dx = 1: edge uniform
+             over {16, 24, 32, 48, 64}, np = round(exp(U[ln 8, ln 2048])) seeded
+             uniform positions, eta ~ U[0.5, 2], kT 0.01, dt 0.01, 3-pt kernel,
+             soft repulsion eps 1, rc 1.5, one seed per replica
 """
 import numpy as np
 
@@ -53,3 +57,20 @@ def build(name, seed=1):
     else:
         q, bonds = uniform(w["n"], L, seed), None
     return cfg, q, bonds
+
+
+MIXED_EDGES = (16, 24, 32, 48, 64)
+
+
+def mixed(n=1024, seed=7, edges=MIXED_EDGES, np_range=(8, 2048)):
+    """Replica set of the batched workload: a list of (config, positions)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        m = int(rng.choice(edges))
+        npart = int(round(np.exp(rng.uniform(np.log(np_range[0]), np.log(np_range[1])))))
+        eta = float(rng.uniform(0.5, 2.0))
+        cfg = make_config((m, m, m), (float(m),) * 3, eta=eta, kT=0.01, dt=0.01, cutoff=1.5,
+                          kernel=3, pair=PAIR_SOFT, soft_epsilon=1.0, seed=seed * 100003 + i)
+        out.append((cfg, uniform(npart, m, seed * 7919 + i)))
+    return out

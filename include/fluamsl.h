@@ -173,6 +173,60 @@ int fsl_interpolate(fsl_handle* h, const double* v, double* u);
 /* Noise array entries [first, first+count) of draw t, as floats. */
 int fsl_noise(fsl_handle* h, uint64_t t, uint64_t first, int64_t count, float* out);
 
+/* ---- batched instances --------------------------------------------------
+ * No counterpart in the reference, which runs one instance per process
+ * (process globals, src/schemeStokesLimit.cu:27-98).  A batch holds n
+ * independent instances, each with its own configuration, particles, seed
+ * and step counter.  Instances with the same cells, neighbour-grid extents
+ * (max(3, int(L/cutoff)) per direction) and kernel width form a size class:
+ * one kernel launch per stage serves a whole class, the classes run on
+ * separate streams, and from the second step on a step of the batch is one
+ * CUDA graph launch.  Each instance's results are bit-identical to the same
+ * instance run alone through fsl_create/fsl_step.  Instance i is addressed
+ * by its index in the arrays given to fsl_batch_create.  Packed particle
+ * arrays concatenate the instances' SoA blocks (3 np_i doubles each) in
+ * index order. */
+typedef struct fsl_batch fsl_batch;
+
+typedef struct fsl_batch_info {
+  int32_t n;                     /* instances                                 */
+  int32_t classes;               /* size classes (launch groups)              */
+  int32_t graph;                 /* 1 if steps replay a captured CUDA graph   */
+  int32_t launches_per_step;     /* kernels of this library in one step       */
+  int64_t np_total;              /* particles over all instances              */
+  int64_t nc_total;              /* cells over all instances                  */
+  int64_t device_bytes;          /* device memory held by the batch           */
+} fsl_batch_info;
+
+/* cfgs[i], np[i] and q[i] (SoA, 3 np[i] doubles) describe instance i; all
+ * instances live on one device (the first cfgs[i].device >= 0, else the
+ * current one). */
+int fsl_batch_create(int32_t n, const fsl_config* cfgs, const int64_t* np, const double* const* q,
+                     fsl_batch** out);
+int fsl_batch_load_bonds(fsl_batch* b, int32_t i, int64_t nbonds, const int32_t* bi,
+                         const int32_t* bj, const double* k, const double* r0, int64_t nfixed,
+                         const int32_t* fi, const double* fk, const double* fr0, const double* fxyz);
+int fsl_batch_step(fsl_batch* b, int64_t nsteps);
+/* Block until queued work is done; FSL_E_KERNEL if any instance's error word
+ * is set (the message names the first such instance). */
+int fsl_batch_sync(fsl_batch* b);
+int fsl_batch_get_positions(fsl_batch* b, int32_t i, double* out);
+int fsl_batch_get_forces(fsl_batch* b, int32_t i, double* out);
+int fsl_batch_get_status(fsl_batch* b, int32_t i, fsl_status* st);
+/* All instances' positions in one packed array (one copy each way plus one
+ * gather/scatter kernel). */
+int fsl_batch_get_positions_packed(fsl_batch* b, double* out);
+int fsl_batch_set_positions_packed(fsl_batch* b, const double* in);
+/* The same, asynchronous on the batch's stream: `host` must stay valid (and,
+ * for a copy that overlaps other work, be page-locked) until the stream
+ * reaches the copy. */
+int fsl_batch_get_positions_packed_async(fsl_batch* b, double* host);
+int fsl_batch_set_positions_packed_async(fsl_batch* b, const double* host);
+int fsl_batch_set_graph(fsl_batch* b, int enable);
+int fsl_batch_get_info(fsl_batch* b, fsl_batch_info* info);
+void* fsl_batch_stream(fsl_batch* b);
+void fsl_batch_destroy(fsl_batch* b);
+
 /* ---- cell list without device allocation -------------------------------
  * No counterpart in the reference.  The same cell list as fsl_cell_list, for
  * callers that must not allocate device memory: code recording a CUDA graph
