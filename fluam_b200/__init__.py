@@ -7,7 +7,7 @@ ABI and the data.main driver), ``build.py`` (nvcc recipe), ``_lib.py``
 (ctypes binding) and ``stokes.py`` (the Python interface).
 """
 from .stokes import (PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE, Batch,
-                     StokesLimit, make_config, parse_data_main, run_data_main)
+                     Server, StokesLimit, make_config, parse_data_main, run_data_main)
 
-__all__ = ["StokesLimit", "Batch", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
+__all__ = ["StokesLimit", "Batch", "Server", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
            "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE"]

@@ -30,7 +30,10 @@ EXPORTS = [
     "fsl_batch_get_positions_packed", "fsl_batch_set_positions_packed",
     "fsl_batch_get_positions_packed_async", "fsl_batch_set_positions_packed_async",
     "fsl_batch_set_graph", "fsl_batch_get_info", "fsl_batch_stream", "fsl_batch_destroy",
+    "fsl_server_config_defaults", "fsl_server_create", "fsl_server_submit", "fsl_server_poll",
+    "fsl_server_wait", "fsl_server_result", "fsl_server_get_stats", "fsl_server_destroy",
 ]
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 
 class Config(ctypes.Structure):
@@ -65,6 +68,26 @@ class BatchInfo(ctypes.Structure):
         ("launches_per_step", ctypes.c_int32), ("np_total", ctypes.c_int64),
         ("nc_total", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
     ]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_int64), ("device", ctypes.c_int32),
+                ("max_round_steps", ctypes.c_int32)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [
+        ("state", ctypes.c_int32), ("error_bits", ctypes.c_int32), ("np", ctypes.c_int64),
+        ("steps", ctypes.c_int64), ("steps_done", ctypes.c_int64), ("submit_s", ctypes.c_double),
+        ("start_s", ctypes.c_double), ("done_s", ctypes.c_double),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int64) for f in (
+        "submitted", "completed", "failed", "queued", "running", "rounds", "steps",
+        "particle_steps", "bytes_held", "slots", "groups", "captures")] + [
+        ("busy_s", ctypes.c_double), ("now_s", ctypes.c_double)]
 
 
 class FslError(RuntimeError):
@@ -143,6 +166,17 @@ def load(path=None):
     L.fsl_batch_stream.restype = _VP
     L.fsl_batch_destroy.argtypes = [_VP]
     L.fsl_batch_destroy.restype = None
+    L.fsl_server_config_defaults.argtypes = [ctypes.POINTER(ServerConfig)]
+    L.fsl_server_config_defaults.restype = None
+    L.fsl_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]
+    L.fsl_server_submit.argtypes = [_VP, ctypes.POINTER(Config), ctypes.c_int64, _D, ctypes.c_int64,
+                                    ctypes.POINTER(ctypes.c_int64)]
+    L.fsl_server_poll.argtypes = [_VP, ctypes.c_int64, ctypes.POINTER(RequestInfo)]
+    L.fsl_server_wait.argtypes = [_VP, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(RequestInfo)]
+    L.fsl_server_result.argtypes = [_VP, ctypes.c_int64, _D, _D]
+    L.fsl_server_get_stats.argtypes = [_VP, ctypes.POINTER(ServerStats)]
+    L.fsl_server_destroy.argtypes = [_VP]
+    L.fsl_server_destroy.restype = None
     if path is None:
         _lib = L
     return L

@@ -17,7 +17,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfluamsl.so")
 EXE = os.path.join(HERE, "fluam")
 
-CU_SOURCES = ["fsl_particles.cu", "fsl_fft.cu", "fsl_group.cu", "fsl_api.cu", "fsl_batch.cu", "fsl_noalloc.cu"]
+CU_SOURCES = ["fsl_particles.cu", "fsl_fft.cu", "fsl_group.cu", "fsl_api.cu", "fsl_batch.cu", "fsl_server.cu", "fsl_noalloc.cu"]
 CPP_SOURCES = ["fsl_datamain.cpp"]
 HEADERS = ["fsl_internal.cuh", "fsl_group.cuh"]
 

@@ -442,7 +442,7 @@ int group_upload(Group& g) {
     if (acc > (long)INT_MAX / 2) return errorf(FSL_E_ARG, "batch too large for one launch");
     B.nblk[k] = (int)acc;
   }
-  B.one = n == 1 ? &g.h_reps[0] : nullptr;
+  B.one = (n == 1 && g.allow_one) ? &g.h_reps[0] : nullptr;
   if (n > 0) {
     FSL_TRY(cudaMemcpyAsync(g.d_reps, g.h_reps.data(), sizeof(Rep) * n, cudaMemcpyHostToDevice,
                             g.stream));
@@ -638,6 +638,7 @@ int exec_step(Exec& e, int64_t nsteps) {
         if (ce != cudaSuccess) return cuda_fail(ce, "graph capture");
         e.graph = g;
         FSL_TRY(cudaGraphInstantiate(&e.gexec, g, 0));
+        e.captures++;
       }
       FSL_TRY(cudaGraphLaunch(e.gexec, e.stream));
     } else {

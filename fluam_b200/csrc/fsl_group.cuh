@@ -81,6 +81,8 @@ struct Group {
   std::vector<int> h_boff;
   Batch B{};
   bool dirty = true;            // host table changed since the last upload
+  bool allow_one = true;        // a lone instance may travel by value (its
+                                // changes then need a new graph capture)
   cudaStream_t stream = nullptr;
   Prof prof;
   std::map<std::string, std::pair<int64_t, double>> stage_acc;
@@ -107,6 +109,7 @@ struct Exec {
   std::vector<long long> shape;       // what the graph was captured for
   uint64_t steps = 0;
   int launches_per_step = 0;
+  int64_t captures = 0;               // graphs captured so far
 };
 
 int exec_init(Exec& e, int device);

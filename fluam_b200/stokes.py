@@ -14,7 +14,7 @@ import numpy as np
 from . import _lib
 from ._lib import PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE, check
 
-__all__ = ["StokesLimit", "Batch", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
+__all__ = ["StokesLimit", "Batch", "Server", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
            "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE"]
 
 
@@ -285,6 +285,74 @@ class Batch:
 
     def stream(self):
         return self.L.fsl_batch_stream(self.h)
+
+
+class Server:
+    """The serving loop (fsl_server_*): submit requests from any thread, wait
+    for them, fetch their results.  The scheduler runs in the library."""
+
+    def __init__(self, hbm_budget=None, device=-1, max_round_steps=8):
+        self.L = _lib.load()
+        c = _lib.ServerConfig()
+        self.L.fsl_server_config_defaults(ctypes.byref(c))
+        if hbm_budget is not None:
+            c.hbm_budget = int(hbm_budget)
+        c.device, c.max_round_steps = device, max_round_steps
+        h = ctypes.c_void_p()
+        check(self.L.fsl_server_create(ctypes.byref(c), ctypes.byref(h)))
+        self.h = h
+        self._np = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fsl_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, config, q, nsteps):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(3, -1)
+        rid = ctypes.c_int64()
+        check(self.L.fsl_server_submit(self.h, ctypes.byref(config), q.shape[1], _dp(q), int(nsteps),
+                                       ctypes.byref(rid)))
+        self._np[rid.value] = q.shape[1]
+        return rid.value
+
+    @staticmethod
+    def _info(i):
+        return {f: getattr(i, f) for f, _ in _lib.RequestInfo._fields_}
+
+    def poll(self, rid):
+        i = _lib.RequestInfo()
+        check(self.L.fsl_server_poll(self.h, int(rid), ctypes.byref(i)))
+        return self._info(i)
+
+    def wait(self, rid, timeout=-1.0):
+        i = _lib.RequestInfo()
+        check(self.L.fsl_server_wait(self.h, int(rid), float(timeout), ctypes.byref(i)))
+        return self._info(i)
+
+    def result(self, rid):
+        n = self._np.pop(rid)
+        q = np.empty((3, n))
+        F = np.empty((3, n))
+        check(self.L.fsl_server_result(self.h, int(rid), _dp(q), _dp(F)))
+        return q, F
+
+    def stats(self):
+        st = _lib.ServerStats()
+        check(self.L.fsl_server_get_stats(self.h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _lib.ServerStats._fields_}
 
 
 def run_data_main(path):

@@ -227,6 +227,65 @@ int fsl_batch_get_info(fsl_batch* b, fsl_batch_info* info);
 void* fsl_batch_stream(fsl_batch* b);
 void fsl_batch_destroy(fsl_batch* b);
 
+/* ---- serving loop ---------------------------------------------------------
+ * No counterpart in the reference (one instance per process run to
+ * completion).  A server owns one device and a scheduler thread.  Requests
+ * (a configuration, positions and a step count) are queued by
+ * fsl_server_submit from any thread.  The scheduler admits queued requests
+ * in arrival order into slots of their size class while the device memory of
+ * all slots stays within the budget, and advances every admitted request
+ * together: one launch per stage and size class, the whole step one CUDA
+ * graph.  Requests that arrive while others run join at the next round; a
+ * round lasts as many steps as the nearest completion (at most
+ * max_round_steps), so every request takes exactly its own step count and
+ * its results are bit-identical to the same instance run alone through
+ * fsl_create/fsl_step.  Instance state stays on the device from admission to
+ * completion; the slot of a finished request is reused by the next one of
+ * its class.  All fsl_server_* calls are thread-safe. */
+typedef struct fsl_server fsl_server;
+
+typedef struct fsl_server_config {
+  int64_t hbm_budget;            /* device bytes for instance state          */
+  int32_t device;                /* -1 keeps the current device              */
+  int32_t max_round_steps;       /* longest stretch between admissions       */
+} fsl_server_config;
+
+enum { FSL_REQ_QUEUED = 0, FSL_REQ_RUNNING = 1, FSL_REQ_DONE = 2, FSL_REQ_FAILED = 3 };
+
+typedef struct fsl_request_info {
+  int32_t state;                 /* FSL_REQ_*                                 */
+  int32_t error_bits;            /* FSL_ERRBIT_* of the instance              */
+  int64_t np;
+  int64_t steps;                 /* requested                                 */
+  int64_t steps_done;
+  double submit_s, start_s, done_s;  /* on the server's clock (seconds)       */
+} fsl_request_info;
+
+typedef struct fsl_server_stats {
+  int64_t submitted, completed, failed, queued, running;
+  int64_t rounds, steps, particle_steps;  /* steps: sum over requests        */
+  int64_t bytes_held, slots;
+  int64_t groups, captures;
+  double busy_s;                 /* time the scheduler spent in rounds        */
+  double now_s;                  /* the server's clock                        */
+} fsl_server_stats;
+
+void fsl_server_config_defaults(fsl_server_config* cfg);
+int fsl_server_create(const fsl_server_config* cfg, fsl_server** out);
+/* Copies q (SoA, 3 np doubles); *id identifies the request. */
+int fsl_server_submit(fsl_server* s, const fsl_config* cfg, int64_t np, const double* q,
+                      int64_t nsteps, int64_t* id);
+int fsl_server_poll(fsl_server* s, int64_t id, fsl_request_info* info);
+/* Blocks until the request is done or failed, or timeout_s elapses
+ * (negative: no limit); returns FSL_OK either way, with the state in info. */
+int fsl_server_wait(fsl_server* s, int64_t id, double timeout_s, fsl_request_info* info);
+/* Final positions and forces (F^{n+1/2} of the last step) of a finished
+ * request, then forgets it.  Either output may be NULL. */
+int fsl_server_result(fsl_server* s, int64_t id, double* q_out, double* F_out);
+int fsl_server_get_stats(fsl_server* s, fsl_server_stats* st);
+/* Stops the scheduler after its current round; unfinished requests fail. */
+void fsl_server_destroy(fsl_server* s);
+
 /* ---- cell list without device allocation -------------------------------
  * No counterpart in the reference.  The same cell list as fsl_cell_list, for
  * callers that must not allocate device memory: code recording a CUDA graph

@@ -130,3 +130,29 @@ def test_create_validates_before_touching_the_device():
         with pytest.raises(_lib.FslError) as e:
             StokesLimit(c, np.zeros((3, 4)))
         assert e.value.code == -1
+
+
+def test_batch_and_server_fail_loudly_without_device():
+    """The batched and serving entry points have no CPU path either."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from fluam_b200 import Batch, Server, make_config
+    import numpy as np
+    c = make_config((8, 8, 8), (8, 8, 8), kT=0.01, dt=0.01, cutoff=1.5)
+    with pytest.raises(_lib.FslError) as e:
+        Batch([c, c], [np.zeros((3, 4)), np.zeros((3, 2))])
+    assert e.value.code in (-2, -3)
+    with pytest.raises(_lib.FslError) as e:
+        Server(hbm_budget=1 << 30)
+    assert e.value.code in (-2, -3)
+
+
+def test_batch_validates_every_instance():
+    from fluam_b200 import Batch, make_config
+    import numpy as np
+    good = make_config((8, 8, 8), (8, 8, 8), kT=0.01, dt=0.01, cutoff=1.5)
+    bad = make_config((13, 8, 8), (8, 8, 8), kT=0.01, dt=0.01, cutoff=1.5)
+    with pytest.raises(_lib.FslError) as e:
+        Batch([good, bad], [np.zeros((3, 4)), np.zeros((3, 4))])
+    assert e.value.code == -1 and "instance 1" in str(e.value)
