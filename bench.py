@@ -44,6 +44,7 @@ def parse_args():
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched and served lines")
     return p.parse_args()
 
 
@@ -215,6 +216,155 @@ def workload_config(name):
 
 
 # -------------------------------------------------------------- GPU side ---
+def step_bytes(nc, npart):
+    """Algorithmic HBM bytes of one midpoint step: 144 nc + 384 np (FP32
+    fields written and read once per pass, FP64 particle state, noise kept
+    in registers)."""
+    return 144 * nc + 384 * npart
+
+
+def run_batched(torch, steps=20, warmup=3, plain_sample=128):
+    """The mixed 1,024-replica workload as one batch (one launch per stage and
+    size class, one graph per step), next to the same replicas stepped one at
+    a time on the plain single-instance path (a seeded sample of them)."""
+    import ctypes
+    from fluam_b200 import Batch, StokesLimit, workloads
+    inst = workloads.mixed(1024)
+    b = Batch([c for c, _ in inst], [q for _, q in inst])
+    info = b.info()
+    stream = torch.cuda.ExternalStream(b.stream())
+    b.step(warmup)
+    b.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(steps)
+    e1.record(stream)
+    b.sync()
+    ms = e0.elapsed_time(e1) / steps
+    npt, nct = info["np_total"], info["nc_total"]
+    # end to end: every step's positions in from and out to pinned host memory
+    hq = torch.empty(int(b.offsets[-1]), dtype=torch.float64).pin_memory()
+    b.positions_packed(hq.numpy())
+    ke = max(5, steps // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        b.set_positions_packed_async(hq.data_ptr())
+        b.step(1)
+        b.positions_packed_async(hq.data_ptr())
+    b.sync()
+    e2e_s = time.perf_counter() - t0
+    launches = b.info()["launches_per_step"]
+    b.close()
+    # plain path, one replica at a time: device time of its own steps
+    tot_p, tot_ms = 0, 0.0
+    for c, q in inst[:plain_sample]:
+        g = StokesLimit(c, q)
+        s = torch.cuda.ExternalStream(g.L.fsl_stream(g.h))
+        g.step(3)
+        g.sync()
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        g.step(5)
+        z.record(s)
+        g.sync()
+        tot_ms += a.elapsed_time(z)
+        tot_p += 5 * q.shape[1]
+        g.close()
+    plain = tot_p / (tot_ms * 1e-3)
+    value = npt / (ms * 1e-3)
+    return {
+        "workload": "mixed_1024: 1,024 cubic replicas, edge U{16,24,32,48,64}, np log-U[8,2048], "
+                    "eta U[0.5,2], kT 0.01, dt 0.01, 3-pt kernel, soft repulsion eps 1 rc 1.5",
+        "replicas": info["n"], "classes": info["classes"], "np_total": npt, "nc_total": nct,
+        "value": value, "unit": "particle-steps/s", "ms_per_step": ms, "steps": steps,
+        "grid_cell_updates_per_s": nct / (ms * 1e-3),
+        "step_bytes": step_bytes(nct, npt),
+        "achieved_GBs": step_bytes(nct, npt) / (ms * 1e-3) / 1e9,
+        "e2e": {"value": npt * ke / e2e_s, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": 24 * npt, "d2h_bytes_per_step": 24 * npt},
+        "plain_one_at_a_time": {"value": plain, "unit": "particle-steps/s",
+                                "sample": f"first {plain_sample} replicas, 5 graph-replayed steps "
+                                          "each, device time"},
+        "speedup_vs_plain": value / plain,
+        "gpu_launches_per_step": launches,
+        "l2": "inputs (device state of all replicas) far larger than L2",
+    }
+
+
+def serve_requests(n_per_s, duration, seed, steps_range):
+    """A seeded open-loop Poisson request stream: (arrival s, config, q, steps)."""
+    from fluam_b200 import PAIR_SOFT, make_config, workloads
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / n_per_s)
+        if t > duration:
+            return out
+        m = int(rng.choice(np.arange(16, 97, 8)))
+        npart = int(round(np.exp(rng.uniform(np.log(16), np.log(16384)))))
+        nst = int(round(np.exp(rng.uniform(np.log(steps_range[0]), np.log(steps_range[1])))))
+        cfg = make_config((m, m, m), (float(m),) * 3, eta=float(rng.uniform(0.5, 2.0)), kT=0.01,
+                          dt=0.01, cutoff=1.5, kernel=int(rng.choice((3, 4))), pair=PAIR_SOFT,
+                          seed=int(rng.integers(1, 1 << 40)))
+        out.append((t, cfg, workloads.uniform(npart, m, int(rng.integers(1 << 30))), nst))
+
+
+def run_served(rate=100.0, duration=3.0, steps_range=(10, 500), seed=11, plain_sample=24):
+    """The serving loop under a Poisson stream; completion latency and
+    aggregate throughput, next to a sample of the same requests run one at a
+    time on the plain path (wall time of create + steps + read-back)."""
+    from fluam_b200 import Server, StokesLimit
+    reqs = serve_requests(rate, duration, seed, steps_range)
+    srv = Server(hbm_budget=150 * 10 ** 9)
+    # warm-up: one short request per size class builds the FFT plans
+    warm = {}
+    for _, c, q, _ in reqs:
+        warm.setdefault((c.mx, c.kernel), (c, q[:, :16]))
+    for rid in [srv.submit(c, q, 2) for c, q in warm.values()]:
+        srv.wait(rid)
+        srv.result(rid)
+    ids = []
+    t0 = time.perf_counter()
+    for t, c, q, n in reqs:
+        d = t0 + t - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ids.append(srv.submit(c, q, n))
+    infos = [srv.wait(i) for i in ids]
+    for i in ids:
+        srv.result(i)
+    st = srv.stats()
+    srv.close()
+    lat = np.array([x["done_s"] - x["submit_s"] for x in infos])
+    span = max(x["done_s"] for x in infos) - min(x["submit_s"] for x in infos)
+    work = sum(q.shape[1] * n for _, _, q, n in reqs)
+    ok = sum(x["state"] == 2 for x in infos)
+    # plain path, one request at a time
+    p_work, p_s = 0, 0.0
+    for _, c, q, n in reqs[:plain_sample]:
+        a = time.perf_counter()
+        g = StokesLimit(c, q)
+        g.step(n)
+        g.positions()
+        g.close()
+        p_s += time.perf_counter() - a
+        p_work += q.shape[1] * n
+    plain = p_work / p_s
+    return {
+        "workload": f"Poisson {rate:g} req/s for {duration:g} s: edge U{{16,24,...,96}}, np "
+                    f"log-U[16,16384], steps log-U[{steps_range[0]},{steps_range[1]}], eta "
+                    "U[0.5,2], 3/4-pt kernel 50/50, soft repulsion, 150 GB budget",
+        "requests": len(reqs), "completed": ok, "value": work / span,
+        "unit": "particle-steps/s", "latency_p50_s": float(np.percentile(lat, 50)),
+        "latency_p99_s": float(np.percentile(lat, 99)), "span_s": span,
+        "rounds": st["rounds"], "captures": st["captures"], "slots": st["slots"],
+        "plain_one_at_a_time": {"value": plain, "unit": "particle-steps/s",
+                                "sample": f"first {plain_sample} requests, wall time"},
+        "speedup_vs_plain": (work / span) / plain,
+    }
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -339,7 +489,18 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": st["launches_per_step"] * args.steps,
+            "step_roofline": {"bytes_per_step": step_bytes(P["nc"], npart),
+                              "achieved": step_bytes(P["nc"], npart) / (t_max / args.steps * 1e-3) / 1e9,
+                              "peak": hbm, "unit": "GB/s",
+                              "frac": step_bytes(P["nc"], npart) / (t_max / args.steps * 1e-3) / 1e9 / hbm},
         }
+        if world == 1 and not args.no_batched:
+            sim.close()
+            for key, fn in (("batched", run_batched), ("served", run_served)):
+                try:
+                    line[key] = fn(torch) if key == "batched" else fn()
+                except Exception as e:  # reported, not fatal
+                    line[key] = {"error": repr(e)}
         print(json.dumps(line), flush=True)
     sim.close()
     if dist:
