@@ -736,36 +736,45 @@ FftPlan* fft_plan_create(const Params& P) {
   fp->smem_x = sizeof(float2) * (2 * (size_t)P.mx * (kXPairs + 1) + P.mx);
   fp->smem_y = sizeof(float2) * (2 * (size_t)P.my * kYTile + P.my);
   fp->smem_z = sizeof(float2) * (2 * (size_t)P.mz * 3 * kZTile + P.mz);
-  // The opt-in limit of the device.  Every kernel's attribute is set to it,
-  // not to this plan's need: kernels with runtime sizes are shared by plans
-  // of different sizes, and a larger attribute costs nothing.
+  // Every kernel's dynamic limit is raised to the most the device allows
+  // beside the kernel's own static shared memory (the batched forms hold a
+  // copy of their instance there), not to this plan's need: kernels with
+  // runtime sizes are shared by plans of different sizes, and a larger limit
+  // costs nothing.  A kernel whose need exceeds its limit is not used.
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
       optin <= 0)
     optin = 227 * 1024;
-  const size_t lim = (size_t)optin;
-  if (fp->smem_x > lim || fp->smem_y > lim || fp->smem_z > lim) {
+  auto allow = [&](const void* f, size_t need) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, f) != cudaSuccess) return false;
+    const int most = optin - (int)a.sharedSizeBytes;
+    if (most <= 0 || need > (size_t)most) return false;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, most) == cudaSuccess;
+  };
+  pick_kernels(P, fp);
+  bool ok = true;
+  for (int v = 0; v < 2; ++v) {
+    ok = ok && allow((const void*)(v ? k_xfwd<true> : k_xfwd<false>), fp->smem_x);
+    ok = ok && allow((const void*)(v ? k_xinv<true> : k_xinv<false>), fp->smem_x);
+    ok = ok && allow((const void*)(v ? k_yfft<true> : k_yfft<false>), fp->smem_y);
+    ok = ok && allow((const void*)fp->zsolve[v], fp->smem_z);
+  }
+  if (!ok) {
+    cudaGetLastError();
     fft_plan_destroy(fp);
     return nullptr;
   }
-  pick_kernels(P, fp);
   {
     int mmax = P.mx > P.my ? P.mx : P.my;
     int lsp = P.mxh | 1;
     fp->smem_plane = sizeof(float2) * ((size_t)P.my * lsp + 2 * (size_t)mmax * (kPB + 1) + P.mx + P.my);
-    fp->use_plane = fp->smem_plane <= lim;
-    for (int v = 0; v < 2 && fp->use_plane; ++v) {
-      cudaFuncSetAttribute((const void*)fp->plane_fwd[v], cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-      cudaFuncSetAttribute((const void*)fp->plane_inv[v], cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    }
+    fp->use_plane = true;
+    for (int v = 0; v < 2; ++v)
+      fp->use_plane = fp->use_plane && allow((const void*)fp->plane_fwd[v], fp->smem_plane) &&
+                      allow((const void*)fp->plane_inv[v], fp->smem_plane);
   }
-  const void* fixed[6] = {(const void*)k_xfwd<false>, (const void*)k_xfwd<true>,
-                          (const void*)k_xinv<false>, (const void*)k_xinv<true>,
-                          (const void*)k_yfft<false>, (const void*)k_yfft<true>};
-  for (const void* f : fixed) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-  for (int v = 0; v < 2; ++v)
-    cudaFuncSetAttribute((const void*)fp->zsolve[v], cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   cudaGetLastError();
   fp->ok = true;
   return fp;

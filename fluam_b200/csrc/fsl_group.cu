@@ -466,15 +466,24 @@ void group_enqueue_step(Group& g) {
     return;
   }
   const int pk = B.max_np > 0 ? 1 : 0;
+  // remembers the first stage whose launch was refused, for the message
+  auto chk = [&](const char* stage) {
+    if (!g.fail_stage && cudaPeekAtLastError() != cudaSuccess) g.fail_stage = stage;
+  };
   auto cells_forces = [&](int which) {
     pr.mark(s, "cells");
     launch_cells(B, which, s);
+    chk("cells");
     pr.mark(s, "forces");
     launch_forces(B, which, s);
+    chk("forces");
     pr.count(pk ? 8 : 1);
   };
+  g.fail_stage = nullptr;
+  chk("before the step");
   pr.mark(s, "noise");
   launch_noise(B, s);
+  chk("noise");
   pr.count(1);
   // option 0: F^n, f = S(q^n) F^n; solve 1 with sqrt(2) stress 1.  The
   // spread field is all zeros here: it starts cleared and every W build
@@ -482,24 +491,31 @@ void group_enqueue_step(Group& g) {
   cells_forces(0);
   pr.mark(s, "spread");
   launch_spread(B, 0, 1, s);
+  chk("spread");
   pr.count(pk);
   launch_solve(B, g.fft, 1, 0, s, &pr);
+  chk("solve");
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
   // sqrt(1/2) (stress 1 + stress 2)
   pr.mark(s, "interp_update");
   launch_interp_update(B, 1, s);
+  chk("interp_update");
   pr.count(pk);
   cells_forces(1);
   pr.mark(s, "spread_rfd");
   launch_spread(B, 1, 1, s);
+  chk("spread_rfd");
   pr.count(pk);
   launch_solve(B, g.fft, 2, 0, s, &pr);
+  chk("solve");
   // option 2: corrector
   pr.mark(s, "interp_update");
   launch_interp_update(B, 2, s);
+  chk("interp_update");
   pr.count(pk);
   pr.mark(s, "counter");
   launch_step_counter(B, s);
+  chk("counter");
   pr.count(1);
   pr.mark(s, nullptr);
   g.launches = pr.launches;
@@ -644,7 +660,14 @@ int exec_step(Exec& e, int64_t nsteps) {
     } else {
       exec_enqueue(e);
       cudaError_t le = cudaGetLastError();
-      if (le != cudaSuccess) return cuda_fail(le, "kernel launch");
+      if (le != cudaSuccess) {
+        for (Group* g : e.groups)
+          if (g->fail_stage)
+            return errorf(FSL_E_CUDA, "kernel launch (stage %s, cells %d %d %d, kernel %d, %d instances): %s",
+                          g->fail_stage, g->key.mx, g->key.my, g->key.mz, g->key.kernel, g->B.nrep,
+                          cudaGetErrorString(le));
+        return cuda_fail(le, "kernel launch");
+      }
     }
     e.steps++;
     for (Group* g : e.groups) {

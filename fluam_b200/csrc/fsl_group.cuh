@@ -87,6 +87,7 @@ struct Group {
   Prof prof;
   std::map<std::string, std::pair<int64_t, double>> stage_acc;
   int launches = 0;             // kernels of this group in one step
+  const char* fail_stage = nullptr;  // first stage whose launch failed
 };
 
 int group_init(Group& g, const Params& P0);

@@ -143,3 +143,20 @@ def test_batch_instance_tracks_oracle(fsl, oracle):
     b.sync()
     assert rel_inf(b.positions(1) - q, o.positions() - q) < 1e-4
     b.close()
+
+
+def test_batch_large_planes_equal_alone(fsl):
+    """Classes whose whole-plane transforms need more than 48 KB of shared
+    memory (edges 72..128), two instances each, and a 5-7-11 edge."""
+    inst = []
+    for i, (m, k) in enumerate([(96, 3), (96, 3), (80, 4), (80, 4), (88, 3), (88, 3), (128, 4)]):
+        cfg = fsl.make_config((m, m, m), (float(m),) * 3, eta=1.0 + 0.1 * i, kT=0.01, dt=0.01,
+                              cutoff=1.5, kernel=k, pair=fsl.PAIR_SOFT, seed=500 + i)
+        inst.append((cfg, uniform_positions(64 + 16 * i, (m, m, m), 70 + i)))
+    b = fsl.Batch([c for c, _ in inst], [q for _, q in inst])
+    b.step(2)
+    b.sync()
+    for i, (cfg, q) in enumerate(inst):
+        qa, Fa, _ = run_alone(fsl, cfg, q, 2)
+        np.testing.assert_array_equal(b.positions(i), qa)
+    b.close()
