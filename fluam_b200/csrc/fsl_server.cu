@@ -4,7 +4,7 @@
 // batching).  The slot of a finished request is switched off in its group's
 // instance table and handed to the next request of the class, so the
 // captured step graph stays valid; only a group whose slot list grows or
-// shrinks, or a change in the set of busy groups, needs a new capture.
+// shrinks needs a new capture.
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -234,10 +234,13 @@ void scheduler(fsl_server* s) {
       }
     }
     if (running.empty()) continue;
-    // one round: every busy class, as many steps as the nearest completion
+    // one round: every class that holds slots (an idle class's kernels
+    // return at once, which costs far less than capturing a new graph each
+    // time the set of busy classes changes), as many steps as the nearest
+    // completion
     std::vector<fsl::Group*> gl;
     for (auto& kv : s->groups)
-      if (kv.second->busy > 0) gl.push_back(&kv.second->g);
+      if (!kv.second->slots.empty()) gl.push_back(&kv.second->g);
     if (gl != s->exec.groups) s->exec.groups = gl;
     int64_t n = s->cfg.max_round_steps;
     for (Request* r : running) n = std::min(n, r->remaining);
