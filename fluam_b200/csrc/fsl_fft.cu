@@ -48,6 +48,14 @@ struct FftPlan {
   void (*plane_inv[2])(RepSrc, Rep, Radices, Radices, const float2*, const float2*) = {};
   void (*zsolve[2])(RepSrc, Rep, Radices, const float2*, const float*, const float*, const float*,
                     const float2*, const float2*, const float2*) = {};
+  // register-resident passes for compiled edges (null: not available)
+  void (*plane_fwd_r[2])(RepSrc, Rep, const float2*) = {};
+  void (*plane_inv_r[2])(RepSrc, Rep, const float2*) = {};
+  void (*zsolve_r[2])(RepSrc, Rep, const float2*, const float*, const float*, const float*,
+                      const float2*, const float2*, const float2*) = {};
+  int plane_pb = 0, plane_threads = 0;      // planes per block, threads per block
+  int z_kx = 0, z_ky = 0, z_threads = 0;    // zsolve tile and threads per block
+  size_t smem_plane_r = 0, smem_z_r = 0;
 };
 
 static bool factorize(int n, Radices& R) {
@@ -647,7 +655,56 @@ __global__ void __launch_bounds__(kFftThreads)
   }
 }
 
+#include "fsl_fft_reg.cuh"
+
 // ------------------------------------------------------------ host side ---
+template <int N, int R, int T, int PB>
+static void pick_plane_r(FftPlan* fp) {
+  fp->plane_fwd_r[0] = k_plane_fwd_r<false, N, R, T, PB>;
+  fp->plane_fwd_r[1] = k_plane_fwd_r<true, N, R, T, PB>;
+  fp->plane_inv_r[0] = k_plane_inv_r<false, N, R, T, PB>;
+  fp->plane_inv_r[1] = k_plane_inv_r<true, N, R, T, PB>;
+  fp->plane_pb = PB;
+  fp->plane_threads = PB * (N / 2) * T;
+  fp->smem_plane_r = sizeof(float2) * (N + (size_t)PB * plane_buf<N, R, T>());
+}
+
+template <int MZ, int R, int T, int KX, int KY>
+static void pick_z_r(FftPlan* fp) {
+  fp->zsolve_r[0] = k_zsolve_r<false, MZ, R, T, KX, KY>;
+  fp->zsolve_r[1] = k_zsolve_r<true, MZ, R, T, KX, KY>;
+  fp->z_kx = KX;
+  fp->z_ky = KY;
+  fp->z_threads = 3 * KX * KY * T;
+  fp->smem_z_r = sizeof(float2) * (MZ + (size_t)3 * KX * KY * LineGeom<R, T>::LS);
+}
+
+// Register-pass shapes per edge: N = R x T; planes per block; z tiles.
+static void pick_register_kernels(const Params& P, FftPlan* fp) {
+  if (P.mx == P.my) {
+    switch (P.mx) {
+      case 16: pick_plane_r<16, 16, 1, 16>(fp); break;
+      case 24: pick_plane_r<24, 24, 1, 16>(fp); break;
+      case 32: pick_plane_r<32, 16, 2, 4>(fp); break;
+      case 48: pick_plane_r<48, 12, 4, 2>(fp); break;
+      case 64: pick_plane_r<64, 16, 4, 2>(fp); break;
+      case 96: pick_plane_r<96, 24, 4, 1>(fp); break;
+      case 128: pick_plane_r<128, 16, 8, 1>(fp); break;
+      default: break;
+    }
+  }
+  switch (P.mz) {
+    case 16: pick_z_r<16, 16, 1, 9, 8>(fp); break;
+    case 24: pick_z_r<24, 24, 1, 13, 8>(fp); break;
+    case 32: pick_z_r<32, 16, 2, 17, 4>(fp); break;
+    case 48: pick_z_r<48, 12, 4, 25, 1>(fp); break;
+    case 64: pick_z_r<64, 16, 4, 33, 1>(fp); break;
+    case 96: pick_z_r<96, 24, 4, 25, 1>(fp); break;
+    case 128: pick_z_r<128, 16, 8, 13, 1>(fp); break;
+    case 256: pick_z_r<256, 16, 16, 8, 1>(fp); break;
+    default: break;
+  }
+}
 template <int M>
 static void pick_cubic(FftPlan* fp) {
   fp->plane_fwd[0] = k_plane_fwd<false, M, M>;
@@ -712,6 +769,13 @@ FftPlan* fft_plan_create(const Params& P) {
   cudaMemcpyToSymbol(c_w5, w5, sizeof(w5));
   cudaMemcpyToSymbol(c_w7, w7, sizeof(w7));
   cudaMemcpyToSymbol(c_w11, w11, sizeof(w11));
+  {
+    static float2 rwt[33][32];
+    for (int R = 1; R <= 32; ++R)
+      for (int j = 0; j < 32; ++j)
+        rwt[R][j] = make_float2((float)cos(2 * M_PI * j / R), (float)-sin(2 * M_PI * j / R));
+    cudaMemcpyToSymbol(c_rw, rwt, sizeof(rwt));
+  }
 
   const int m[3] = {P.mx, P.my, P.mz};
   float2** tws[3] = {&fp->twx, &fp->twy, &fp->twz};
@@ -775,6 +839,15 @@ FftPlan* fft_plan_create(const Params& P) {
       fp->use_plane = fp->use_plane && allow((const void*)fp->plane_fwd[v], fp->smem_plane) &&
                       allow((const void*)fp->plane_inv[v], fp->smem_plane);
   }
+  pick_register_kernels(P, fp);
+  for (int v = 0; v < 2; ++v) {
+    if (fp->plane_fwd_r[0] &&
+        !(allow((const void*)fp->plane_fwd_r[v], fp->smem_plane_r) &&
+          allow((const void*)fp->plane_inv_r[v], fp->smem_plane_r)))
+      fp->plane_fwd_r[0] = fp->plane_fwd_r[1] = fp->plane_inv_r[0] = fp->plane_inv_r[1] = nullptr;
+    if (fp->zsolve_r[0] && !allow((const void*)fp->zsolve_r[v], fp->smem_z_r))
+      fp->zsolve_r[0] = fp->zsolve_r[1] = nullptr;
+  }
   cudaGetLastError();
   fp->ok = true;
   return fp;
@@ -795,6 +868,16 @@ void fft_plan_destroy(FftPlan* fp) {
 }
 
 static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
+  if (fp->zsolve_r[0]) {
+    dim3 g((B.mxh + fp->z_kx - 1) / fp->z_kx, (B.my + fp->z_ky - 1) / fp->z_ky, B.nrep);
+    if (B.one)
+      fp->zsolve_r[1]<<<g, fp->z_threads, fp->smem_z_r, s>>>(RepSrc{}, *B.one, fp->twz, fp->sx, fp->sy,
+                                                             fp->sz, fp->ex, fp->ey, fp->ez);
+    else
+      fp->zsolve_r[0]<<<g, fp->z_threads, fp->smem_z_r, s>>>(B.src(), Rep{}, fp->twz, fp->sx, fp->sy,
+                                                             fp->sz, fp->ex, fp->ey, fp->ez);
+    return;
+  }
   if (B.one)
     fp->zsolve[1]<<<gz, kFftThreads, fp->smem_z, s>>>(RepSrc{}, *B.one, fp->rz, fp->twz, fp->sx, fp->sy,
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
@@ -817,6 +900,24 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, int w_given, cudaStrea
     if (blocks > cap) blocks = cap < 1 ? 1 : cap;
     FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets);
     pr.count(1);
+  }
+  if (fp->plane_fwd_r[0]) {
+    dim3 gp((3 * B.mz + fp->plane_pb - 1) / fp->plane_pb, 1, nrep);
+    const int tb = fp->plane_threads;
+    pr.mark(s, "plane_fwd");
+    if (B.one)
+      fp->plane_fwd_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
+    else
+      fp->plane_fwd_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
+    pr.mark(s, "zsolve");
+    zsolve(B, fp, dim3((B.mxh + kZTile - 1) / kZTile, B.my, nrep), s);
+    pr.mark(s, "plane_inv");
+    if (B.one)
+      fp->plane_inv_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
+    else
+      fp->plane_inv_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
+    pr.count(3);
+    return;
   }
   if (fp->use_plane) {
     dim3 gp(B.mz, 3, nrep);
