@@ -113,6 +113,15 @@ __device__ __forceinline__ int nb_cell(const Params& P, double x, double y, doub
   return jx + jy * P.mnx + jz * P.mnx * P.mny;
 }
 
+// minimage for |r| < 1.5 L (a difference of two wrapped coordinates): the
+// same n = int(r/L + sign(r)/2) in {-1, 0, 1}, found by comparisons instead
+// of float-to-integer conversions.
+__device__ __forceinline__ double minimage_near(double r, double invL, double L) {
+  const double t = __dadd_rn(__dmul_rn(r, invL), copysign(0.5, r));
+  const double n = t >= 1.0 ? 1.0 : (t <= -1.0 ? -1.0 : 0.0);
+  return __dsub_rn(r, __dmul_rn(n, L));
+}
+
 // ------------------------------------------------------- Peskin kernels ---
 // 3-point kernel, src/deltaGPU.cu:57-68 (argument = distance / h)
 __device__ __forceinline__ float delta3f(float x) {
@@ -305,6 +314,7 @@ struct Rep {
   float* v;
   float* wbuf;
   double* u;  // interpolated velocities of the component entry point
+  double* qw;  // positions wrapped into the box by the last cell-list build
   int* err;
   uint64_t* t;
 };

@@ -79,8 +79,16 @@ __global__ void k_cell_count(FSL_KARGS, int which) {
   // a coordinate this large or non-finite means the run has blown up
   const double lim = 1e15;
   if (!(fabs(x) < lim && fabs(y) < lim && fabs(z) < lim)) set_err(R.err, 2);
-  int c = nb_cell(P, x, y, z);
+  const double wx = minimage(x, P.invlx, P.lx), wy = minimage(y, P.invly, P.ly),
+               wz = minimage(z, P.invlz, P.lz);
+  int c = cellidx(wx, P.invdnx, P.mnx) + cellidx(wy, P.invdny, P.mny) * P.mnx +
+          cellidx(wz, P.invdnz, P.mnz) * P.mnx * P.mny;
   R.cell_of[i] = c;
+  if (R.qw) {  // the pair loop works on wrapped positions
+    R.qw[i] = wx;
+    R.qw[P.np + i] = wy;
+    R.qw[2 * P.np + i] = wz;
+  }
   atomicAdd(&R.cnt[c], 1);
 }
 
@@ -271,6 +279,10 @@ __global__ void k_forces(FSL_KARGS, int which) {
     }
   }
   if (P.nonbonded && P.pair != 0 && active) {
+    // wrapped positions: every difference is within (-L, L)
+    const double* __restrict__ w = R.qw;
+    const double wx = w[i], wy = w[np + i], wz = w[2 * np + i];
+    const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
     int c = R.cell_of[i];
     int cxy = c % (P.mnx * P.mny);
     int cz = c / (P.mnx * P.mny), cy = cxy / P.mnx, cx = cxy - cy * P.mnx;
@@ -285,9 +297,9 @@ __global__ void k_forces(FSL_KARGS, int which) {
       int e = R.start[cc + 1];
       for (int jj = R.start[cc]; jj < e; ++jj) {
         int j = R.sorted[jj];
-        double rxij = minimage(rx - q[j], P.invlx, P.lx);
-        double ryij = minimage(ry - q[np + j], P.invly, P.ly);
-        double rzij = minimage(rz - q[2 * np + j], P.invlz, P.lz);
+        double rxij = minimage_near(wx - w[j], P.invlx, P.lx);
+        double ryij = minimage_near(wy - w[np + j], P.invly, P.ly);
+        double rzij = minimage_near(wz - w[2 * np + j], P.invlz, P.lz);
         // no fused multiply-add: r^2 selects the table entry bit-exactly
         double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rxij, rxij), __dmul_rn(ryij, ryij)),
                               __dmul_rn(rzij, rzij));
@@ -296,8 +308,8 @@ __global__ void k_forces(FSL_KARGS, int which) {
           f = (double)tex_linear(R.ljtab, kLjTableSize, (float)(r2 * P.invcut2));
         } else {
           if (j == i || r2 >= P.cutoff2 || r2 == 0.0) continue;
-          double r = sqrt(r2);
-          f = (2.0 * P.soft_eps / P.cutoff) * (1.0 - r / P.cutoff) / r;
+          // (2 eps / rc) (1 - r / rc) / r = c1 (1/r - 1/rc)
+          f = c1 * (rsqrt(r2) - c2);
         }
         fx += f * rxij;
         fy += f * ryij;
