@@ -19,7 +19,7 @@ size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 
 // Byte offsets of one slot's buffers inside its arena.
 struct SlotLayout {
-  size_t q, qp, F, u, qw, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
+  size_t q, qp, F, u, qw, ws, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
       bsum, ljtab, noise, grid, spec, v, wbuf, err, t, total;
 };
 
@@ -39,6 +39,7 @@ SlotLayout layout(const Params& P, int np_cap) {
   L.F = take(sizeof(double) * 3 * np);
   L.u = take(sizeof(double) * 3 * np);
   L.qw = take(sizeof(double) * 3 * np);
+  L.ws = take(sizeof(double) * 3 * np);
   L.cell_of = take(sizeof(int) * np);
   L.tmp = take(sizeof(int) * np);
   L.sorted = take(sizeof(int) * np);
@@ -222,6 +223,7 @@ int slot_alloc(Slot& s, const Params& P, int np_cap) {
   r.F = (double*)(base + L.F);
   r.u = (double*)(base + L.u);
   r.qw = (double*)(base + L.qw);
+  r.ws = (double*)(base + L.ws);
   r.cell_of = (int*)(base + L.cell_of);
   r.tmp = (int*)(base + L.tmp);
   r.sorted = (int*)(base + L.sorted);

@@ -315,6 +315,7 @@ struct Rep {
   float* wbuf;
   double* u;  // interpolated velocities of the component entry point
   double* qw;  // positions wrapped into the box by the last cell-list build
+  double* ws;  // the same in cell-list order
   int* err;
   uint64_t* t;
 };

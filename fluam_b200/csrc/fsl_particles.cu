@@ -197,6 +197,11 @@ __global__ void k_cell_rank(FSL_KARGS) {
   int rank = 0;
   for (int k = s; k < e; ++k) rank += R.tmp[k] < i;
   R.sorted[s + rank] = i;
+  if (R.ws) {  // wrapped positions in cell order for the pair loop
+    R.ws[s + rank] = R.qw[i];
+    R.ws[P.np + s + rank] = R.qw[P.np + i];
+    R.ws[2 * P.np + s + rank] = R.qw[2 * P.np + i];
+  }
 }
 
 void launch_cells(const Batch& B, int which, cudaStream_t s) {
@@ -250,21 +255,27 @@ __device__ __forceinline__ void bond_force(double rx, double ry, double rz, doub
 // Pair (src/stokesLimitFunctions.cu:191-653 with the table of
 // src/initForcesNonBonded.cu:21-66, or soft repulsion) and bonded
 // (src/forceBondedGPU.cu:21-121) force on every particle.  Eight lanes per
-// particle share its bonds and its 27 neighbour cells (cells sub, sub+8, ...),
-// then sum their partial forces in a fixed butterfly order.
+// particle, particles taken in cell order.  The lanes concatenate the
+// candidate lists of the 27 neighbour cells (an exclusive scan of the cell
+// counts in shared memory) and take candidates sub, sub+8, ... of the whole
+// list, so the work is split evenly whatever the cell occupancy; candidates
+// are read from the positions wrapped and stored in cell order by the cell
+// list build.  The partial forces are summed in a fixed butterfly order.
 template <bool ONE>
-__global__ void k_forces(FSL_KARGS, int which) {
+__global__ void __launch_bounds__(kPartThreads) k_forces(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T8);
-  const int sub = threadIdx.x & 7;
-  const int ig = (int)((blk * (size_t)blockDim.x + threadIdx.x) >> 3);
+  __shared__ int s_pre[kPartThreads / 8][28];
+  __shared__ int s_st[kPartThreads / 8][27];
+  const int sub = threadIdx.x & 7, grp = threadIdx.x >> 3;
+  const int ig = (int)((blk * (size_t)blockDim.x + threadIdx.x) >> 3);  // rank in cell order
   if ((ig & ~3) >= P.np) return;  // uniform per warp (4 particles per warp)
   const bool active = ig < P.np;  // inactive lanes still join the shuffles
-  const int i = active ? ig : 0;
   const int np = P.np;
+  const int i = active ? R.sorted[ig] : 0;
   const double* __restrict__ q = which ? R.qp : R.q;
-  double rx = q[i], ry = q[np + i], rz = q[2 * np + i];
   double fx = 0.0, fy = 0.0, fz = 0.0;
   if (P.bonded && active) {
+    const double rx = q[i], ry = q[np + i], rz = q[2 * np + i];
     int nb = R.bpp_cnt[i], off = R.bpp_off[i];
     for (int j = sub; j < nb; j += 8) {
       int idx = R.bpp_idx[off + j];
@@ -278,43 +289,71 @@ __global__ void k_forces(FSL_KARGS, int which) {
       bond_force(rx, ry, rz, p[0], p[1], p[2], R.bfp_k[off + j], R.bfp_r0[off + j], fx, fy, fz);
     }
   }
-  if (P.nonbonded && P.pair != 0 && active) {
-    // wrapped positions: every difference is within (-L, L)
-    const double* __restrict__ w = R.qw;
-    const double wx = w[i], wy = w[np + i], wz = w[2 * np + i];
-    const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
-    int c = R.cell_of[i];
-    int cxy = c % (P.mnx * P.mny);
-    int cz = c / (P.mnx * P.mny), cy = cxy / P.mnx, cx = cxy - cy * P.mnx;
-    for (int nn = sub; nn < 27; nn += 8) {
-      // the 27 cells in z-major order; the summation order only moves the
-      // result at the FP64 rounding level
-      int ox = cx + nn % 3 - 1, oy = cy + (nn / 3) % 3 - 1, oz = cz + nn / 9 - 1;
-      ox += ox < 0 ? P.mnx : (ox >= P.mnx ? -P.mnx : 0);
-      oy += oy < 0 ? P.mny : (oy >= P.mny ? -P.mny : 0);
-      oz += oz < 0 ? P.mnz : (oz >= P.mnz ? -P.mnz : 0);
-      int cc = ox + oy * P.mnx + oz * P.mnx * P.mny;
-      int e = R.start[cc + 1];
-      for (int jj = R.start[cc]; jj < e; ++jj) {
-        int j = R.sorted[jj];
-        double rxij = minimage_near(wx - w[j], P.invlx, P.lx);
-        double ryij = minimage_near(wy - w[np + j], P.invly, P.ly);
-        double rzij = minimage_near(wz - w[2 * np + j], P.invlz, P.lz);
-        // no fused multiply-add: r^2 selects the table entry bit-exactly
-        double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rxij, rxij), __dmul_rn(ryij, ryij)),
-                              __dmul_rn(rzij, rzij));
-        double f;
-        if (P.pair == 1) {
-          f = (double)tex_linear(R.ljtab, kLjTableSize, (float)(r2 * P.invcut2));
-        } else {
-          if (j == i || r2 >= P.cutoff2 || r2 == 0.0) continue;
-          // (2 eps / rc) (1 - r / rc) / r = c1 (1/r - 1/rc)
-          f = c1 * (rsqrt(r2) - c2);
-        }
-        fx += f * rxij;
-        fy += f * ryij;
-        fz += f * rzij;
+  if (P.nonbonded && P.pair != 0) {
+    const double* __restrict__ ws = R.ws;  // wrapped, cell order
+    const double wx = active ? ws[ig] : 0.0, wy = active ? ws[np + ig] : 0.0,
+                 wz = active ? ws[2 * np + ig] : 0.0;
+    const int c = active ? R.cell_of[i] : 0;
+    const int cxy = c % (P.mnx * P.mny);
+    const int cz = c / (P.mnx * P.mny), cy = cxy / P.mnx, cx = cxy - cy * P.mnx;
+    // this lane's cells nn = sub + 8 m, in z-major order
+    int st[4], cnt[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int nn = sub + 8 * m;
+      st[m] = 0;
+      cnt[m] = 0;
+      if (active && nn < 27) {
+        int ox = cx + nn % 3 - 1, oy = cy + (nn / 3) % 3 - 1, oz = cz + nn / 9 - 1;
+        ox += ox < 0 ? P.mnx : (ox >= P.mnx ? -P.mnx : 0);
+        oy += oy < 0 ? P.mny : (oy >= P.mny ? -P.mny : 0);
+        oz += oz < 0 ? P.mnz : (oz >= P.mnz ? -P.mnz : 0);
+        const int cc = ox + oy * P.mnx + oz * P.mnx * P.mny;
+        st[m] = R.start[cc];
+        cnt[m] = R.start[cc + 1] - st[m];
       }
+    }
+    // exclusive scan of the 27 counts in cell order, within the 8 lanes
+    int carry = 0;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      int incl = cnt[m];
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o, 8);
+        if (sub >= o) incl += y;
+      }
+      if (sub + 8 * m < 27) {
+        s_pre[grp][sub + 8 * m] = carry + incl - cnt[m];
+        s_st[grp][sub + 8 * m] = st[m];
+      }
+      carry += __shfl_sync(0xffffffffu, incl, 7, 8);
+    }
+    const int K = carry;
+    if (sub == 0) s_pre[grp][27] = K;
+    __syncwarp();
+    const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
+    int cp = 0;
+    for (int kk = sub; kk < K; kk += 8) {
+      while (s_pre[grp][cp + 1] <= kk) ++cp;
+      const int jj = s_st[grp][cp] + (kk - s_pre[grp][cp]);
+      const double rxij = minimage_near(wx - ws[jj], P.invlx, P.lx);
+      const double ryij = minimage_near(wy - ws[np + jj], P.invly, P.ly);
+      const double rzij = minimage_near(wz - ws[2 * np + jj], P.invlz, P.lz);
+      // no fused multiply-add: r^2 selects the table entry bit-exactly
+      const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rxij, rxij), __dmul_rn(ryij, ryij)),
+                                  __dmul_rn(rzij, rzij));
+      double f;
+      if (P.pair == 1) {
+        f = (double)tex_linear(R.ljtab, kLjTableSize, (float)(r2 * P.invcut2));
+      } else {
+        if (jj == ig || r2 >= P.cutoff2 || r2 == 0.0) continue;
+        // (2 eps / rc) (1 - r / rc) / r = c1 (1/r - 1/rc)
+        f = c1 * (rsqrt(r2) - c2);
+      }
+      fx += f * rxij;
+      fy += f * ryij;
+      fz += f * rzij;
     }
   }
 #pragma unroll
