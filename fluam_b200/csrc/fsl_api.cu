@@ -87,7 +87,7 @@ int fsl_create(const fsl_config* cfg, int64_t np, const double* q, fsl_handle** 
     return code;
   };
   if ((rc = fsl::exec_init(h->exec, dev))) return fail(rc);
-  if ((rc = fsl::slot_alloc(h->slot, P, (int)np))) return fail(rc);
+  if ((rc = fsl::slot_alloc(h->slot, P, (int)np, h->exec.stream))) return fail(rc);
   if ((rc = fsl::slot_reset(h->slot, P, q, *cfg, h->exec.stream))) return fail(rc);
   if ((rc = fsl::group_init(h->group, P))) return fail(rc);
   h->group.slots.push_back(&h->slot);

@@ -127,7 +127,7 @@ int fsl_batch_create(int32_t n, const fsl_config* cfgs, const int64_t* np, const
   for (int32_t i = 0; i < n; ++i) {
     b->slots.emplace_back(new fsl::Slot());
     fsl::Slot& s = *b->slots.back();
-    if ((rc = fsl::slot_alloc(s, P[i], (int)np[i]))) return fail(instance_error(rc, i));
+    if ((rc = fsl::slot_alloc(s, P[i], (int)np[i], st))) return fail(instance_error(rc, i));
     if ((rc = fsl::slot_reset(s, P[i], q[i], cfgs[i], st))) return fail(rc);
     fsl::ClassKey key = fsl::class_of(P[i]);
     auto it = b->groups.find(key);
@@ -155,7 +155,7 @@ int fsl_batch_create(int32_t n, const fsl_config* cfgs, const int64_t* np, const
       (e = cudaMalloc((void**)&b->d_packed, sizeof(double) * std::max<long long>(off, 1))) != cudaSuccess ||
       (e = cudaMalloc((void**)&b->d_errs, sizeof(int) * std::max(n, 1))) != cudaSuccess)
     return fail(fsl::cuda_fail(e, "batch tables"));
-  if (n > 0 && (e = cudaMemcpy(b->d_ents, ents.data(), sizeof(PackEnt) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+  if (n > 0 && (e = cudaMemcpyAsync(b->d_ents, ents.data(), sizeof(PackEnt) * n, cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return fail(fsl::cuda_fail(e, "batch tables"));
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(fsl::cuda_fail(e, "create"));
   *out = b;

@@ -849,6 +849,12 @@ FftPlan* fft_plan_create(const Params& P) {
       fp->zsolve_r[0] = fp->zsolve_r[1] = nullptr;
   }
   cudaGetLastError();
+  // the tables went up with plain copies on the default stream; the step
+  // runs on other streams
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    fft_plan_destroy(fp);
+    return nullptr;
+  }
   fp->ok = true;
   return fp;
 }

@@ -201,7 +201,7 @@ void build_ljtable(const Params& P, double temperature, double cutoff, std::vect
 // ------------------------------------------------------------------ slots --
 size_t slot_bytes(const Params& P, int np_cap) { return layout(P, np_cap).total; }
 
-int slot_alloc(Slot& s, const Params& P, int np_cap) {
+int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st) {
   slot_free(s);
   const SlotLayout L = layout(P, np_cap);
   char* base = nullptr;
@@ -209,7 +209,9 @@ int slot_alloc(Slot& s, const Params& P, int np_cap) {
   s.arena = base;
   s.bytes = L.total;
   s.np_cap = np_cap;
-  cudaError_t e = cudaMemset(base, 0, L.total);
+  // on the stream of the uploads that follow: a memset on the legacy default
+  // stream is not ordered with a non-blocking stream and could land after them
+  cudaError_t e = cudaMemsetAsync(base, 0, L.total, st);
   if (e != cudaSuccess) {
     slot_free(s);
     return cuda_fail(e, "cudaMemset(slot)");
@@ -354,21 +356,23 @@ int slot_bonds(Slot& s, int64_t nbonds, const int32_t* bi, const int32_t* bj, co
   r.bfp_r0 = (double*)(base + o_fr0);
   r.bfp_xyz = (double*)(base + o_fx);
   if (np > 0) {
-    FSL_TRY(cudaMemcpy(r.bpp_cnt, pc.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
-    FSL_TRY(cudaMemcpy(r.bpp_off, po.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
-    FSL_TRY(cudaMemcpy(r.bfp_cnt, fc.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
-    FSL_TRY(cudaMemcpy(r.bfp_off, fo.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpyAsync(r.bpp_cnt, pc.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+    FSL_TRY(cudaMemcpyAsync(r.bpp_off, po.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+    FSL_TRY(cudaMemcpyAsync(r.bfp_cnt, fc.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+    FSL_TRY(cudaMemcpyAsync(r.bfp_off, fo.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
   }
   if (nbonds > 0) {
-    FSL_TRY(cudaMemcpy(r.bpp_idx, idx.data(), sizeof(int) * nb2, cudaMemcpyHostToDevice));
-    FSL_TRY(cudaMemcpy(r.bpp_k, kk.data(), sizeof(double) * nb2, cudaMemcpyHostToDevice));
-    FSL_TRY(cudaMemcpy(r.bpp_r0, rr.data(), sizeof(double) * nb2, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpyAsync(r.bpp_idx, idx.data(), sizeof(int) * nb2, cudaMemcpyHostToDevice, st));
+    FSL_TRY(cudaMemcpyAsync(r.bpp_k, kk.data(), sizeof(double) * nb2, cudaMemcpyHostToDevice, st));
+    FSL_TRY(cudaMemcpyAsync(r.bpp_r0, rr.data(), sizeof(double) * nb2, cudaMemcpyHostToDevice, st));
   }
   if (nfixed > 0) {
-    FSL_TRY(cudaMemcpy(r.bfp_k, fkk.data(), sizeof(double) * nf, cudaMemcpyHostToDevice));
-    FSL_TRY(cudaMemcpy(r.bfp_r0, frr.data(), sizeof(double) * nf, cudaMemcpyHostToDevice));
-    FSL_TRY(cudaMemcpy(r.bfp_xyz, fxx.data(), sizeof(double) * 3 * nf, cudaMemcpyHostToDevice));
+    FSL_TRY(cudaMemcpyAsync(r.bfp_k, fkk.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    FSL_TRY(cudaMemcpyAsync(r.bfp_r0, frr.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    FSL_TRY(cudaMemcpyAsync(r.bfp_xyz, fxx.data(), sizeof(double) * 3 * nf, cudaMemcpyHostToDevice, st));
   }
+  // staged copies of host vectors that end here: wait for them
+  FSL_TRY(cudaStreamSynchronize(st));
   r.P.bonded = (nbonds + nfixed) > 0;
   return FSL_OK;
 }

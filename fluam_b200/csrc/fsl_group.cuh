@@ -56,9 +56,9 @@ struct Slot {
 };
 
 // Allocates the slot's buffers for class P with room for np_cap particles
-// and zeroes them (the spread field must start cleared).  The slot stays
-// inactive until slot_reset.
-int slot_alloc(Slot& s, const Params& P, int np_cap);
+// and zeroes them on st (the spread field must start cleared).  The slot
+// stays inactive until slot_reset.
+int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st);
 void slot_free(Slot& s);
 // Puts a new instance (parameters P, positions q on the host) into an
 // allocated slot of its class: positions, LJ table, cleared forces, error

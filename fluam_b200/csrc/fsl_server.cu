@@ -149,7 +149,7 @@ int admit(fsl_server* s, Request* r) {
     }
     if (!make_room(s, need)) return 0;
     std::unique_ptr<fsl::Slot> sl(new fsl::Slot());
-    if (fsl::slot_alloc(*sl, r->P, cap)) {
+    if (fsl::slot_alloc(*sl, r->P, cap, s->exec.stream)) {
       r->msg = fsl::last_error();
       return -1;
     }
