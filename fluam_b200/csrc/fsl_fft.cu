@@ -336,6 +336,100 @@ __global__ void k_wbuild(FSL_KARGS, int nsets) {
   }
 }
 
+// Four consecutive x cells of a row for one stress sample d: the x, y, z
+// neighbours as 16-byte rows (aligned: the sample's base is a multiple of 4
+// floats; otherwise four scalar loads) plus the two x-edge scalars.
+__device__ __forceinline__ float4 ld_row4(const float* __restrict__ p, bool aligned) {
+  if (aligned) return __ldg(reinterpret_cast<const float4*>(p));
+  return make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3));
+}
+
+// w[comp][c] += the stress divergence of cells x0 .. x0+3 (the arithmetic of
+// stress_div, four cells at a time).
+__device__ __forceinline__ void stress_div4(const Params& P, const float* __restrict__ d,
+                                            bool aligned, int x0, int y, int z, size_t i0,
+                                            float a1x, float a1y, float a1z, float a4x,
+                                            float a4y, float a4z, float (&w)[3][4]) {
+  const size_t nc = (size_t)P.nc;
+  const int mx = P.mx, my = P.my, mz = P.mz;
+  const size_t row = i0 - x0;  // first cell of the row
+  const long dym = (y == 0 ? (long)(my - 1) * mx : -(long)mx);
+  const long dyp = (y == my - 1 ? -(long)(my - 1) * mx : (long)mx);
+  const long dzm = (z == 0 ? (long)(mz - 1) * my * mx : -(long)my * mx);
+  const long dzp = (z == mz - 1 ? -(long)(mz - 1) * my * mx : (long)my * mx);
+  const int xl = x0 == 0 ? mx - 1 : x0 - 1, xr = x0 + 4 == mx ? 0 : x0 + 4;
+  const float4 r0 = ld_row4(d + i0, aligned);
+  const float e0 = __ldg(d + row + xr);
+  const float4 r1 = ld_row4(d + nc + i0, aligned), r1ym = ld_row4(d + nc + i0 + dym, aligned);
+  const float e1 = __ldg(d + nc + row + xl);
+  const float4 r2 = ld_row4(d + 2 * nc + i0, aligned), r2zm = ld_row4(d + 2 * nc + i0 + dzm, aligned);
+  const float e2 = __ldg(d + 2 * nc + row + xl);
+  const float4 r3 = ld_row4(d + 3 * nc + i0, aligned), r3yp = ld_row4(d + 3 * nc + i0 + dyp, aligned);
+  const float4 r4 = ld_row4(d + 4 * nc + i0, aligned), r4zm = ld_row4(d + 4 * nc + i0 + dzm, aligned),
+               r4ym = ld_row4(d + 4 * nc + i0 + dym, aligned);
+  const float4 r5 = ld_row4(d + 5 * nc + i0, aligned), r5zp = ld_row4(d + 5 * nc + i0 + dzp, aligned);
+  const float d0[5] = {r0.x, r0.y, r0.z, r0.w, e0};          // d0[x .. x+4]
+  const float d1[5] = {e1, r1.x, r1.y, r1.z, r1.w};          // d1[x-1 .. x+3]
+  const float d2[5] = {e2, r2.x, r2.y, r2.z, r2.w};          // d2[x-1 .. x+3]
+  const float d1ym[4] = {r1ym.x, r1ym.y, r1ym.z, r1ym.w}, d2zm[4] = {r2zm.x, r2zm.y, r2zm.z, r2zm.w};
+  const float d3[4] = {r3.x, r3.y, r3.z, r3.w}, d3yp[4] = {r3yp.x, r3yp.y, r3yp.z, r3yp.w};
+  const float d4[4] = {r4.x, r4.y, r4.z, r4.w}, d4zm[4] = {r4zm.x, r4zm.y, r4zm.z, r4zm.w},
+              d4ym[4] = {r4ym.x, r4ym.y, r4ym.z, r4ym.w};
+  const float d5[4] = {r5.x, r5.y, r5.z, r5.w}, d5zp[4] = {r5zp.x, r5zp.y, r5zp.z, r5zp.w};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    w[0][c] += a1x * (d0[c + 1] - d0[c]) + a4y * (d1[c + 1] - d1ym[c]) + a4z * (d2[c + 1] - d2zm[c]);
+    w[1][c] += a1y * (d3yp[c] - d3[c]) + a4x * (d1[c + 1] - d1[c]) + a4z * (d4[c] - d4zm[c]);
+    w[2][c] += a1z * (d5zp[c] - d5[c]) + a4x * (d2[c + 1] - d2[c]) + a4y * (d4[c] - d4ym[c]);
+  }
+}
+
+// k_wbuild for mx a multiple of 4: one thread per four x cells, 16-byte loads
+// of the fixed-point field, the noise rows and W, and 16-byte clears.
+template <bool ONE>
+__global__ void k_wbuild4(FSL_KARGS, int nsets) {
+  FSL_REP_AT(blockIdx.y);
+  const double nfac = nsets > 1 ? 0.70710678118654752440 : 1.41421356237309504880;
+  const float scale = (float)(kFixedInv / P.dV);
+  const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
+  const float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
+  const float a4x = (float)P.invdx * f4, a4y = (float)P.invdy * f4, a4z = (float)P.invdz * f4;
+  const float* n1 = R.noise;
+  const size_t off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
+  const float* n2 = R.noise + off2;
+  const bool al2 = (off2 & 3) == 0;
+  const size_t nc = (size_t)P.nc;
+  const int gx = P.mx >> 2;
+  const size_t ng = nc >> 2;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < ng;
+       g += (size_t)gridDim.x * blockDim.x) {
+    const int x0 = (int)(g % gx) << 2;
+    const int r = (int)(g / gx);
+    const int y = r % P.my, z = r / P.my;
+    const size_t i0 = g << 2;
+    float w[3][4];
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      const longlong2* gp = reinterpret_cast<const longlong2*>(R.grid + comp * nc + i0);
+      const longlong2 ga = gp[0], gb = gp[1];
+      w[comp][0] = (float)((double)ga.x * (double)scale);
+      w[comp][1] = (float)((double)ga.y * (double)scale);
+      w[comp][2] = (float)((double)gb.x * (double)scale);
+      w[comp][3] = (float)((double)gb.y * (double)scale);
+    }
+    stress_div4(P, n1, true, x0, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
+    if (nsets > 1) stress_div4(P, n2, al2, x0, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      *reinterpret_cast<float4*>(R.wbuf + comp * nc + i0) =
+          make_float4(w[comp][0], w[comp][1], w[comp][2], w[comp][3]);
+      longlong2* gq = reinterpret_cast<longlong2*>(R.grid + comp * nc + i0);
+      gq[0] = make_longlong2(0, 0);
+      gq[1] = make_longlong2(0, 0);
+    }
+  }
+}
+
 // Real-to-complex transform along x of W.  Block (bx, comp, instance)
 // handles the row pairs [bx*kXPairs, ...); row R = y + my z; the pair
 // (2p, 2p+1) is transformed as the complex line row_2p + i row_2p+1.
@@ -904,7 +998,13 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, int w_given, cudaStrea
     long blocks = ((long)B.nc + tb - 1) / tb;
     long cap = (148L * 64 + nrep - 1) / nrep;
     if (blocks > cap) blocks = cap < 1 ? 1 : cap;
-    FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets);
+    if ((B.mx & 3) == 0) {
+      long b4 = ((long)B.nc / 4 + tb - 1) / tb;
+      if (b4 > cap) b4 = cap < 1 ? 1 : cap;
+      FSL_GO(k_wbuild4, dim3((unsigned)b4, nrep), tb, 0, s, B, nsets);
+    } else {
+      FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets);
+    }
     pr.count(1);
   }
   if (fp->plane_fwd_r[0]) {

@@ -82,10 +82,13 @@ __device__ inline float4 philox_normal4(uint64_t seed, uint64_t t, uint64_t b) {
   float u3 = (float)(2u * (r.w >> 9) + 1u) * s24;
   float ra = sqrtf(-2.0f * logf(u0));
   float rb = sqrtf(-2.0f * logf(u2));
+  // the angle 2 pi u taken as 2 pi (u - 1/2) + pi, within [-pi, pi] where the
+  // hardware sine and cosine are accurate to about 2^-21 (u - 1/2 is exact);
+  // the radius keeps the accurate logarithm
   float sa, ca, sb, cb;
-  sincospif(2.0f * u1, &sa, &ca);
-  sincospif(2.0f * u3, &sb, &cb);
-  return make_float4(ra * ca, ra * sa, rb * cb, rb * sb);
+  __sincosf(6.28318530717958647692f * (u1 - 0.5f), &sa, &ca);
+  __sincosf(6.28318530717958647692f * (u3 - 0.5f), &sb, &cb);
+  return make_float4(-ra * ca, -ra * sa, -rb * cb, -rb * sb);
 }
 
 // --------------------------------------------------- exact cell indices ---
