@@ -15,6 +15,7 @@ ERRORS = {-1: "FSL_E_ARG", -2: "FSL_E_CUDA", -3: "FSL_E_NOMEM", -4: "FSL_E_KERNE
           -5: "FSL_E_IO", -6: "FSL_E_INPUT"}
 PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
 RFD_REFERENCE, RFD_PAPER = 0, 1
+SCHEME_MIDPOINT, SCHEME_FIRST_ORDER = 0, 1
 
 # Every symbol include/fluamsl.h declares.
 EXPORTS = [
@@ -47,6 +48,7 @@ class Config(ctypes.Structure):
         ("seed", ctypes.c_uint64),
         ("pair", ctypes.c_int32), ("rfd", ctypes.c_int32),
         ("nonbonded", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("scheme", ctypes.c_int32),
     ]
 
 

@@ -302,7 +302,7 @@ int fsl_solve(fsl_handle* h, const double* W, double* v) {
   std::vector<float> w(n3);
   for (size_t k = 0; k < n3; ++k) w[k] = (float)W[k];
   FSL_TRY(cudaMemcpyAsync(R.wbuf, w.data(), sizeof(float) * n3, cudaMemcpyHostToDevice, s));
-  fsl::launch_solve(h->group.B, h->group.fft, 1, 1, s);
+  fsl::launch_solve(h->group.B, h->group.fft, 1, 1.0, 1, s);
   if ((rc = check_launch())) return rc;
   FSL_TRY(cudaMemcpyAsync(w.data(), R.v, sizeof(float) * n3, cudaMemcpyDeviceToHost, s));
   FSL_TRY(cudaStreamSynchronize(s));

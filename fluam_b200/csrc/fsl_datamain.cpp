@@ -38,7 +38,7 @@ struct Run {
   std::string coordinates, outputname, bondfile;
   bool bonded = false;
   // scheme flags that select another fluam scheme (src/main.cpp:36-105)
-  bool stokesLimit = false;
+  bool stokesLimit = false, first_order = false;
   std::vector<std::string> other_schemes;
   std::string wordfile;
 };
@@ -180,6 +180,8 @@ int parse(const char* path, Run& r, std::string& err) {
         c.device = (int)I(0);
       } else if (word == "stokesLimit") {
         r.stokesLimit = true;
+      } else if (word == "stokesLimitFirstOrder") {
+        r.first_order = true;
       } else if (word == "thermostat") {
         thermostat = 1;
       } else if (word == "pairPotential") {
@@ -209,7 +211,7 @@ int parse(const char* path, Run& r, std::string& err) {
                  word == "incompressibleBinaryMixtureMidPoint" ||
                  word == "quasiNeutrallyBuoyant" || word == "quasiNeutrallyBuoyant2D" ||
                  word == "quasiNeutrallyBuoyant4pt2D" || word == "quasi2D" ||
-                 word == "stokesLimit2D" || word == "stokesLimitFirstOrder") {
+                 word == "stokesLimit2D") {
         r.other_schemes.push_back(word);
       }
     }
@@ -219,6 +221,13 @@ int parse(const char* path, Run& r, std::string& err) {
   // the reference's scheme precedence (src/main.cpp:36-99): all of these come
   // before stokesLimit in its if-chain
   if (thermostat) r.other_schemes.push_back("thermostat");
+  // stokesLimitFirstOrder precedes stokesLimit (src/main.cpp:94-99).  With
+  // stokesLimitFirstOrder alone the reference never uploads the cell-centre
+  // coordinates (src/initializeFluidIncompressibleGPU.cu:27 tests stokesLimit
+  // only) and its kernels read uninitialised device memory; this build uses
+  // the cell centres in both cases, which is what the reference computes when
+  // the file holds both keywords.
+  if (r.first_order) r.cfg.scheme = FSL_SCHEME_FIRST_ORDER;
   return FSL_OK;
 }
 
@@ -382,8 +391,8 @@ extern "C" int fsl_run_data_main(const char* path) {
     fo << r.wordfile << std::endl;
   }
   std::cout << "READ " << (path ? path : "data.main") << " :                DONE" << std::endl;
-  if (!r.other_schemes.empty() || !r.stokesLimit) {
-    std::cout << "ERROR: this build runs the stokesLimit scheme only"
+  if (!r.other_schemes.empty() || !(r.stokesLimit || r.first_order)) {
+    std::cout << "ERROR: this build runs the stokesLimit and stokesLimitFirstOrder schemes only"
               << (r.other_schemes.empty() ? std::string(" (keyword stokesLimit missing)")
                                           : " (found " + r.other_schemes[0] + ")")
               << std::endl;
@@ -446,11 +455,14 @@ extern "C" int fsl_run_data_main(const char* path) {
     fs << r.cfg.seed << std::endl;
   }
   time_t t0 = time(NULL);
-  std::ofstream fp(r.outputname + ".particles"), fv(r.outputname + ".velocityParticles");
+  // the first-order scheme writes no .velocityParticles (src/saveParticles.cu:43-46)
+  const bool write_forces = r.cfg.scheme != FSL_SCHEME_FIRST_ORDER;
+  std::ofstream fp(r.outputname + ".particles"), fv;
+  if (write_forces) fv.open(r.outputname + ".velocityParticles");
   fp.precision(15);
   fv.precision(15);
   fp << "#NUMBER PARTICLES " << np << std::endl;
-  fv << "#NUMBER PARTICLES " << np << std::endl;
+  if (write_forces) fv << "#NUMBER PARTICLES " << np << std::endl;
   std::vector<double> pos(3 * np), frc(3 * np);
   // src/runSchemeStokesLimit.cu:83, 163-285
   int64_t step = -r.relax;
@@ -473,7 +485,7 @@ extern "C" int fsl_run_data_main(const char* path) {
       }
       if ((rc = fsl_get_positions(h, pos.data())) || (rc = fsl_get_forces(h, frc.data()))) break;
       write_sample(fp, np, pos, step * r.cfg.dt);
-      write_sample(fv, np, frc, step * r.cfg.dt);
+      if (write_forces) write_sample(fv, np, frc, step * r.cfg.dt);
     }
   }
   if (rc) std::cout << "ERROR: " << fsl_last_error() << std::endl;

@@ -306,13 +306,13 @@ __device__ __forceinline__ float stress_div(const Params& P, const float* __rest
 // W = f + c div(Sigma) of all three components of every cell
 // (src/stokesLimitFunctions.cu:2281-2378, 3922-4069): the fixed-point spread
 // field times 2^-40/dV plus the stochastic stress divergence, with
-// c = sqrt(2) (one stress sample) or sqrt(1/2) (two samples).  The spread
+// c = sqrt(2) (midpoint, one stress sample), sqrt(1/2) (two samples) or 1
+// (first-order scheme, src/runSchemeStokesLimitFirstOrder.cu:181-190).  The spread
 // field is cleared behind the read, ready for the next spread.  One thread
 // per cell: the loads of a warp are coalesced rows, full occupancy.
 template <bool ONE>
-__global__ void k_wbuild(FSL_KARGS, int nsets) {
+__global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
   FSL_REP_AT(blockIdx.y);
-  const double nfac = nsets > 1 ? 0.70710678118654752440 : 1.41421356237309504880;
   const float scale = (float)(kFixedInv / P.dV);
   const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
   const float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
@@ -387,9 +387,8 @@ __device__ __forceinline__ void stress_div4(const Params& P, const float* __rest
 // k_wbuild for mx a multiple of 4: one thread per four x cells, 16-byte loads
 // of the fixed-point field, the noise rows and W, and 16-byte clears.
 template <bool ONE>
-__global__ void k_wbuild4(FSL_KARGS, int nsets) {
+__global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
   FSL_REP_AT(blockIdx.y);
-  const double nfac = nsets > 1 ? 0.70710678118654752440 : 1.41421356237309504880;
   const float scale = (float)(kFixedInv / P.dV);
   const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
   const float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
@@ -986,7 +985,7 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
 }
 
-void launch_solve(const Batch& B, FftPlan* fp, int nsets, int w_given, cudaStream_t s,
+void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof) {
   Prof dummy;
   Prof& pr = prof ? *prof : dummy;
@@ -1001,9 +1000,9 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, int w_given, cudaStrea
     if ((B.mx & 3) == 0) {
       long b4 = ((long)B.nc / 4 + tb - 1) / tb;
       if (b4 > cap) b4 = cap < 1 ? 1 : cap;
-      FSL_GO(k_wbuild4, dim3((unsigned)b4, nrep), tb, 0, s, B, nsets);
+      FSL_GO(k_wbuild4, dim3((unsigned)b4, nrep), tb, 0, s, B, nsets, nfac);
     } else {
-      FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets);
+      FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets, nfac);
     }
     pr.count(1);
   }

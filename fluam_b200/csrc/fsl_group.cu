@@ -91,13 +91,15 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 bool ClassKey::operator<(const ClassKey& o) const {
-  const int a[7] = {mx, my, mz, mnx, mny, mnz, kernel};
-  const int b[7] = {o.mx, o.my, o.mz, o.mnx, o.mny, o.mnz, o.kernel};
-  return std::lexicographical_compare(a, a + 7, b, b + 7);
+  const int a[8] = {mx, my, mz, mnx, mny, mnz, kernel, scheme};
+  const int b[8] = {o.mx, o.my, o.mz, o.mnx, o.mny, o.mnz, o.kernel, o.scheme};
+  return std::lexicographical_compare(a, a + 8, b, b + 8);
 }
 bool ClassKey::operator==(const ClassKey& o) const { return !(*this < o) && !(o < *this); }
 
-ClassKey class_of(const Params& P) { return ClassKey{P.mx, P.my, P.mz, P.mnx, P.mny, P.mnz, P.kernel}; }
+ClassKey class_of(const Params& P) {
+  return ClassKey{P.mx, P.my, P.mz, P.mnx, P.mny, P.mnz, P.kernel, P.scheme};
+}
 
 int make_params(const fsl_config& c, int64_t np, Params& P) {
   if (c.mx < 3 || c.my < 3 || c.mz < 3)
@@ -114,6 +116,7 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   if (c.kernel != 3 && c.kernel != 4) return errorf(FSL_E_ARG, "kernel must be 3 or 4");
   if (c.pair < 0 || c.pair > 2) return errorf(FSL_E_ARG, "unknown pair potential %d", c.pair);
   if (c.rfd < 0 || c.rfd > 1) return errorf(FSL_E_ARG, "unknown rfd mode %d", c.rfd);
+  if (c.scheme < 0 || c.scheme > 1) return errorf(FSL_E_ARG, "unknown scheme %d", c.scheme);
   if (c.extra_mobility < 0) return errorf(FSL_E_ARG, "extraMobility must be >= 0");
   if (np < 0 || np > (int64_t)1 << 28) return errorf(FSL_E_ARG, "bad particle count");
   bool pairs = c.nonbonded && c.pair != FSL_PAIR_NONE && np > 0;
@@ -161,6 +164,7 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   P.pair = c.pair;
   P.nonbonded = c.nonbonded ? 1 : 0;
   P.rfd = c.rfd;
+  P.scheme = c.scheme;
   P.bonded = 0;
   P.has_extra = c.extra_mobility != 0.0;
   P.cutoff = c.cutoff;
@@ -493,6 +497,34 @@ void group_enqueue_step(Group& g) {
   launch_noise(B, s);
   chk("noise");
   pr.count(1);
+  if (g.key.scheme == FSL_SCHEME_FIRST_ORDER) {
+    // src/runSchemeStokesLimitFirstOrder.cu:163-241: f = S(q^n) F^n + RFD
+    // drift, one solve with noise factor 1, predictor, forces at q^{n+1/2}
+    // only with extraMobility (k_forces returns at once otherwise), corrector
+    cells_forces(0);
+    pr.mark(s, "spread_rfd");
+    launch_spread(B, 2, 1, s);
+    chk("spread_rfd");
+    pr.count(pk);
+    launch_solve(B, g.fft, 1, 1.0, 0, s, &pr);
+    chk("solve");
+    pr.mark(s, "interp_update");
+    launch_interp_update(B, 1, s);
+    chk("interp_update");
+    pr.count(pk);
+    cells_forces(1);
+    pr.mark(s, "interp_update");
+    launch_interp_update(B, 2, s);
+    chk("interp_update");
+    pr.count(pk);
+    pr.mark(s, "counter");
+    launch_step_counter(B, s);
+    chk("counter");
+    pr.count(1);
+    pr.mark(s, nullptr);
+    g.launches = pr.launches;
+    return;
+  }
   // option 0: F^n, f = S(q^n) F^n; solve 1 with sqrt(2) stress 1.  The
   // spread field is all zeros here: it starts cleared and every W build
   // clears what it reads.
@@ -501,7 +533,7 @@ void group_enqueue_step(Group& g) {
   launch_spread(B, 0, 1, s);
   chk("spread");
   pr.count(pk);
-  launch_solve(B, g.fft, 1, 0, s, &pr);
+  launch_solve(B, g.fft, 1, 1.41421356237309504880, 0, s, &pr);
   chk("solve");
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
   // sqrt(1/2) (stress 1 + stress 2)
@@ -514,7 +546,7 @@ void group_enqueue_step(Group& g) {
   launch_spread(B, 1, 1, s);
   chk("spread_rfd");
   pr.count(pk);
-  launch_solve(B, g.fft, 2, 0, s, &pr);
+  launch_solve(B, g.fft, 2, 0.70710678118654752440, 0, s, &pr);
   chk("solve");
   // option 2: corrector
   pr.mark(s, "interp_update");

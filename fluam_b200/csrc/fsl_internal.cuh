@@ -40,6 +40,7 @@ struct Params {
   int np;
   int kernel;  // 3 or 4
   int pair, nonbonded, rfd, bonded;
+  int scheme;  // FSL_SCHEME_* (0 midpoint, 1 first order)
   int has_extra;
   double cutoff, cutoff2, invcut2, soft_eps;
   double eta, kT, dt, extra_mob, fact1, fact2, fact4;
@@ -446,7 +447,8 @@ void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t cou
 void launch_cells(const Batch& B, int which, cudaStream_t s);
 void launch_forces(const Batch& B, int which, cudaStream_t s);
 // drift = 0: spread F at q (cell-list order when ordered != 0);
-// drift = 1: spread F at q^{n+1/2} and the RFD drift at q
+// drift = 1: spread F at q^{n+1/2} and the RFD drift at q;
+// drift = 2: spread F at q and the RFD drift at q (first-order scheme)
 void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s);
 void launch_interp_update(const Batch& B, int stage, cudaStream_t s);
 void launch_interp(const Batch& B, cudaStream_t s);  // u = J(q) v
@@ -455,9 +457,9 @@ void launch_step_counter(const Batch& B, cudaStream_t s);
 struct FftPlan;  // defined in fsl_fft.cu
 FftPlan* fft_plan_create(const Params& P);
 void fft_plan_destroy(FftPlan* fp);
-// v = solve(W).  nsets = 1 or 2 stress samples; W is built from the spread
-// field (which is cleared on the way) and the noise into Rep::wbuf, unless
-// w_given, in which case Rep::wbuf already holds W.
-void launch_solve(const Batch& B, FftPlan* fp, int nsets, int w_given, cudaStream_t s,
+// v = solve(W).  W = f + nfac div(stress 1 [+ stress 2 when nsets == 2]) is
+// built from the spread field (which is cleared on the way) and the noise
+// into Rep::wbuf, unless w_given, in which case Rep::wbuf already holds W.
+void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof = nullptr);
 }  // namespace fsl

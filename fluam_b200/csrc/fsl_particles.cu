@@ -271,6 +271,9 @@ __global__ void __launch_bounds__(kPartThreads) k_forces(FSL_KARGS, int which) {
   if ((ig & ~3) >= P.np) return;  // uniform per warp (4 particles per warp)
   const bool active = ig < P.np;  // inactive lanes still join the shuffles
   const int np = P.np;
+  // first-order scheme: forces at q^{n+1/2} only with extraMobility
+  // (src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:170-180)
+  if (which == 1 && P.scheme == 1 && !P.has_extra) return;
   const int i = active ? R.sorted[ig] : 0;
   const double* __restrict__ q = which ? R.qp : R.q;
   double fx = 0.0, fy = 0.0, fz = 0.0;
@@ -429,7 +432,7 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
   const int* order = ordered ? R.sorted : nullptr;
   bool sat = false;
   if (e < np) {
-    const double* qf = drift ? R.qp : R.q;
+    const double* qf = drift == 1 ? R.qp : R.q;
     int i = order ? order[e] : (int)e;
     double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
     double val[3] = {R.F[i], R.F[np + i], R.F[2 * (size_t)np + i]};

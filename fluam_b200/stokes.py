@@ -12,10 +12,12 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE, check
+from ._lib import (PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE, SCHEME_FIRST_ORDER,
+                   SCHEME_MIDPOINT, check)
 
 __all__ = ["StokesLimit", "Batch", "Server", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
-           "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE"]
+           "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE", "SCHEME_MIDPOINT",
+           "SCHEME_FIRST_ORDER"]
 
 
 def _dp(a):
@@ -28,7 +30,7 @@ def _ip(a):
 
 def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair=PAIR_TABLE_LJ,
                 soft_epsilon=1.0, rfd=RFD_REFERENCE, nonbonded=1, extra_mobility=0.0, seed=0,
-                device=-1):
+                device=-1, scheme=0):
     c = _lib.Config()
     _lib.load().fsl_config_defaults(ctypes.byref(c))
     c.mx, c.my, c.mz = (int(x) for x in cells)
@@ -36,6 +38,7 @@ def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair
     c.shearviscosity, c.temperature, c.dt, c.cutoff = eta, kT, dt, cutoff
     c.kernel, c.pair, c.soft_epsilon, c.rfd = kernel, pair, soft_epsilon, rfd
     c.nonbonded, c.extra_mobility, c.seed, c.device = nonbonded, extra_mobility, seed, device
+    c.scheme = scheme
     return c
 
 

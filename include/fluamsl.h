@@ -42,6 +42,11 @@ enum {
 /* ---- options that extend the reference ------------------------------- */
 enum { FSL_PAIR_NONE = 0, FSL_PAIR_TABLE_LJ = 1, FSL_PAIR_SOFT = 2 };
 enum { FSL_RFD_REFERENCE = 0, FSL_RFD_PAPER = 1 };
+/* The integrator: the midpoint scheme of keyword stokesLimit
+ * (src/runSchemeStokesLimit.cu:163-285) or the first-order scheme of keyword
+ * stokesLimitFirstOrder (src/runSchemeStokesLimitFirstOrder.cu:163-241: one
+ * solve per step with the RFD drift, the same predictor and corrector). */
+enum { FSL_SCHEME_MIDPOINT = 0, FSL_SCHEME_FIRST_ORDER = 1 };
 
 /* Bits of fsl_status.error_bits (device error word, sticky until cleared). */
 enum {
@@ -67,6 +72,7 @@ typedef struct fsl_config {
   int32_t rfd;                   /* FSL_RFD_*                               */
   int32_t nonbonded;             /* computeNonBondedForces                  */
   int32_t device;                /* setDevice; -1 keeps the current device  */
+  int32_t scheme;                /* FSL_SCHEME_*                            */
 } fsl_config;
 
 typedef struct fsl_status {

@@ -659,7 +659,58 @@ void spread_drift(orc_state* s, int sign) {
     spread_add(s, qd.data(), s->q.data(), val.data());
 }
 
+// One step of the first-order scheme, src/runSchemeStokesLimitFirstOrder.cu
+// :163-241 with src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:32-214:
+// one solve with f = S(q^n) F^n + RFD drift and noise factor 1, then the
+// predictor and corrector of the midpoint step with the same velocity field;
+// forces at q^{n+1/2} only with extraMobility (particlesForceStokesLimit).
+void one_step_first_order(orc_state* s) {
+  const int np = s->np, nc = s->nc;
+  const double dt = s->c.dt;
+  draw_noise(s);
+  std::vector<double> u(3 * (size_t)np);
+  std::fill(s->f.begin(), s->f.end(), 0.0);
+  if (np > 0) {
+    build_cells(s, s->q.data());
+    compute_forces(s, s->q.data(), s->F.data());
+    spread_add(s, s->q.data(), s->q.data(), s->F.data());
+    spread_drift(s, +1);
+    spread_drift(s, -1);
+  }
+  construct_W(s, 1.0, false);
+  solve(s);
+  if (np > 0) {
+    interpolate(s, s->q.data(), s->v.data(), u.data());
+    for (int d = 0; d < 3; ++d)
+      for (int i = 0; i < np; ++i) {
+        size_t k = (size_t)d * np + i;
+        double rnew = s->q[k] + 0.5 * dt * u[k];
+        if (s->c.extra_mobility != 0.0)
+          rnew += 0.5 * dt * s->c.extra_mobility * s->F[k] +
+                  s->fact2 * s->noise[(size_t)6 * nc + (size_t)(3 + d) * np + i];
+        s->qp[k] = rnew;
+      }
+    if (s->c.extra_mobility != 0.0) {
+      build_cells(s, s->qp.data());
+      compute_forces(s, s->qp.data(), s->F.data());
+    }
+    interpolate(s, s->qp.data(), s->v.data(), u.data());
+    for (int d = 0; d < 3; ++d)
+      for (int i = 0; i < np; ++i) {
+        size_t k = (size_t)d * np + i;
+        double rnew = s->q[k] + dt * u[k];
+        if (s->c.extra_mobility != 0.0)
+          rnew += dt * s->c.extra_mobility * s->F[k] +
+                  s->fact2 * (s->noise[(size_t)6 * nc + (size_t)(3 + d) * np + i] +
+                              s->noise[(size_t)6 * nc + (size_t)(6 + d) * np + i]);
+        s->q[k] = rnew;
+      }
+  }
+  s->t++;
+}
+
 void one_step(orc_state* s) {
+  if (s->c.scheme == ORC_SCHEME_FIRST_ORDER) return one_step_first_order(s);
   const int np = s->np, nc = s->nc;
   const double dt = s->c.dt;
   draw_noise(s);

@@ -29,6 +29,10 @@ extern "C" {
 
 enum { ORC_PAIR_NONE = 0, ORC_PAIR_TABLE_LJ = 1, ORC_PAIR_SOFT = 2 };
 enum { ORC_RFD_REFERENCE = 0, ORC_RFD_PAPER = 1 };
+/* ORC_SCHEME_MIDPOINT: stokesLimit (src/runSchemeStokesLimit.cu:163-285);
+ * ORC_SCHEME_FIRST_ORDER: stokesLimitFirstOrder
+ * (src/runSchemeStokesLimitFirstOrder.cu:163-241). */
+enum { ORC_SCHEME_MIDPOINT = 0, ORC_SCHEME_FIRST_ORDER = 1 };
 
 typedef struct orc_config {
   int32_t mx, my, mz;
@@ -44,7 +48,7 @@ typedef struct orc_config {
   int32_t pair;           /* ORC_PAIR_*                                  */
   int32_t rfd;            /* ORC_RFD_*                                   */
   int32_t nonbonded;      /* computeNonBondedForces                      */
-  int32_t pad_;
+  int32_t scheme;         /* ORC_SCHEME_*                                */
 } orc_config;
 
 typedef struct orc_state orc_state;

@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
 RFD_REFERENCE, RFD_PAPER = 0, 1
+SCHEME_MIDPOINT, SCHEME_FIRST_ORDER = 0, 1
 
 
 class OrcConfig(ctypes.Structure):
@@ -25,7 +26,7 @@ class OrcConfig(ctypes.Structure):
         ("extra_mobility", ctypes.c_double), ("soft_epsilon", ctypes.c_double),
         ("seed", ctypes.c_uint64),
         ("pair", ctypes.c_int32), ("rfd", ctypes.c_int32),
-        ("nonbonded", ctypes.c_int32), ("pad_", ctypes.c_int32),
+        ("nonbonded", ctypes.c_int32), ("scheme", ctypes.c_int32),
     ]
 
 
@@ -120,7 +121,7 @@ class Oracle:
 
     def __init__(self, mx, my, mz, lx, ly, lz, q, eta=1.0, kT=0.01, dt=0.01, cutoff=1.5,
                  kernel=3, pair=PAIR_SOFT, soft_epsilon=1.0, rfd=RFD_REFERENCE,
-                 nonbonded=1, extra_mobility=0.0, seed=1):
+                 nonbonded=1, extra_mobility=0.0, seed=1, scheme=0):
         self.L = _load()
         q = np.ascontiguousarray(q, dtype=np.float64).reshape(3, -1)
         self.np = q.shape[1]
@@ -129,7 +130,7 @@ class Oracle:
         c = OrcConfig(mx=mx, my=my, mz=mz, kernel=kernel, lx=lx, ly=ly, lz=lz,
                       shearviscosity=eta, temperature=kT, dt=dt, cutoff=cutoff,
                       extra_mobility=extra_mobility, soft_epsilon=soft_epsilon,
-                      seed=seed, pair=pair, rfd=rfd, nonbonded=nonbonded, pad_=0)
+                      seed=seed, pair=pair, rfd=rfd, nonbonded=nonbonded, scheme=scheme)
         self.cfg = c
         self.h = self.L.orc_create(ctypes.byref(c), self.np, _dp(q))
         if not self.h:

@@ -40,6 +40,7 @@ GPU_FILES = [
     "freeBoundariesRK2GPU.cu", "createCellsStokesLimitGPU.cu", "freeCellsStokesLimitGPU.cu",
     "stokesLimitFunctions.cu", "boundaryParticlesFunctionStokesLimit.cu",
     "saveFunctionsSchemeStokesLimit.cu", "gpuToHostStokesLimit.cu", "runSchemeStokesLimit.cu",
+    "boundaryParticlesFunctionStokesLimitFirstOrder.cu", "runSchemeStokesLimitFirstOrder.cu",
 ]
 GPU_HEADERS = ["header.h", "cells.h", "fluid.h", "boundary.h", "headerOtherFluidVariables.h",
                "particles.h", "hydroAnalysis.h"]
@@ -47,7 +48,7 @@ GPU_HEADERS = ["header.h", "cells.h", "fluid.h", "boundary.h", "headerOtherFluid
 # reference's Makefile does).
 HOST_FILES = [
     "main.cpp", "loadDataMain.cu", "cudaDevice.cu", "initializeRandomNumber.cpp", "rantest.cu",
-    "gauss.cu", "schemeStokesLimit.cu", "createCells.cpp", "createParticles.cpp",
+    "gauss.cu", "schemeStokesLimit.cu", "schemeStokesLimitFirstOrder.cu", "createCells.cpp", "createParticles.cpp",
     "simpleCubic.cpp", "initializeBondedForces.cpp", "initializeFluid.cpp", "modu.cu",
     "saveSeed.cpp", "saveTime.cpp", "saveParticles.cu", "freeParticles.cu", "random_frenk.cu",
 ]

@@ -62,5 +62,4 @@ FLUAM_SCHEME_STUB(schemeQuasiNeutrallyBuoyant4pt2D)
 FLUAM_SCHEME_STUB(schemeRK3)
 FLUAM_SCHEME_STUB(schemeRK3Ghost)
 FLUAM_SCHEME_STUB(schemeSemiImplicitCompressibleParticles)
-FLUAM_SCHEME_STUB(schemeStokesLimitFirstOrder)
 FLUAM_SCHEME_STUB(schemeThermostat)

@@ -22,6 +22,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 FLUAM_REF = os.path.join(ROOT, "oracle", "_ref", "fluam_ref")
 
+FIRST_ORDER = "stokesLimitFirstOrder\nstokesLimit"
+
 COMMON = """stokesLimit
 particles 1
 maxNumberPartInCellNonBonded 40
@@ -101,6 +103,42 @@ numsteps 4
 samplefreq 2
 dt 0.01
 """, chains=(6, 8, (16.0, 24.0, 32.0), 9)),
+    # the first-order scheme (keyword stokesLimitFirstOrder, which takes
+    # precedence over stokesLimit, src/main.cpp:94-99) with LJ forces.  The
+    # stokesLimit keyword stays in the file: without it the reference never
+    # copies the cell-centre coordinates to the device
+    # (src/initializeFluidIncompressibleGPU.cu:27 tests stokesLimit only) and
+    # its first-order kernels read uninitialised memory
+    "first_order_lj": dict(scheme=FIRST_ORDER, text="""loadparticles 1
+coordinates start.coor
+cutoff 1.12246204830937
+shearviscosity 0.9
+temperature 0.05
+cells 24 24 24
+celldimension 12 12 12
+seed 13
+numsteps 3
+samplefreq 1
+dt 0.001
+""", coor=lambda: lattice(5, 1.05, 0.04, 7, (-2.1, -2.1, -2.1))),
+    # first order with chains, tethers and extraMobility (forces at the
+    # midpoint) on a non-cubic grid
+    "first_order_extra": dict(scheme=FIRST_ORDER, text="""loadparticles 1
+coordinates start.coor
+bondedForces bonds.dat
+computeNonBondedForces 0
+cutoff 1.5
+extraMobility 0.3
+shearviscosity 1.1
+temperature 0.02
+cells 20 16 24
+celldimension 20 16 24
+seed 29
+numstepsRelaxation 1
+numsteps 4
+samplefreq 2
+dt 0.01
+""", chains=(5, 7, (20.0, 16.0, 24.0), 12)),
 }
 
 
@@ -110,7 +148,10 @@ def make_case(name, spec):
         shutil.rmtree(d)
     os.makedirs(d)
     with open(os.path.join(d, "data.main"), "w") as f:
-        f.write(COMMON + spec["text"])
+        common = COMMON
+        if "scheme" in spec:
+            common = common.replace("stokesLimit\n", spec["scheme"] + "\n", 1)
+        f.write(common + spec["text"])
     if "coor" in spec:
         write_coor(os.path.join(d, "start.coor"), spec["coor"]())
     if "chains" in spec:
@@ -133,6 +174,9 @@ def make_case(name, spec):
 if __name__ == "__main__":
     if not os.path.exists(FLUAM_REF):
         sys.exit("build oracle/_ref first (python oracle/ref_cpu/build_ref.py)")
+    only = sys.argv[1:]  # case names; all cases when none are given
     for name, spec in CASES.items():
+        if only and name not in only:
+            continue
         make_case(name, spec)
         print("golden", name)

@@ -77,7 +77,9 @@ def load(name):
                      r0=bb[:, 3], fi=ff[:, 0].astype(np.int32), fk=ff[:, 1], fr0=ff[:, 2],
                      fxyz=ff[:, 3:6])
     _, pos = read_particles(os.path.join(d, "out.particles"))
-    _, frc = read_particles(os.path.join(d, "out.velocityParticles"))
+    # the first-order scheme writes no .velocityParticles (src/saveParticles.cu:43-46)
+    fv = os.path.join(d, "out.velocityParticles")
+    frc = read_particles(fv)[1] if os.path.exists(fv) else None
     seed = int(open(os.path.join(d, "out.seed")).read())
     return dict(dir=d, cfg=cfg, run=run, q0=q0, bonds=bonds, pos=pos, frc=frc, seed=seed)
 

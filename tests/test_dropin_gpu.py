@@ -150,11 +150,14 @@ def test_golden_cases_against_reference_outputs(tmp_path, name):
                        timeout=600)
     assert r.returncode == 1, r.stdout + r.stderr
     _, pos = G.read_particles(str(tmp_path / "out.particles"))
-    _, frc = G.read_particles(str(tmp_path / "out.velocityParticles"))
+    fv = tmp_path / "out.velocityParticles"
+    assert fv.exists() == (c["frc"] is not None)
+    frc = G.read_particles(str(fv))[1] if fv.exists() else None
     assert sorted(pos) == sorted(c["pos"])
     for t in c["pos"]:
         assert rel_inf(pos[t] - c["q0"], c["pos"][t] - c["q0"]) < 1e-5, (name, t)
-        assert np.abs(frc[t] - c["frc"][t]).max() <= 1e-5 * max(np.abs(c["frc"][t]).max(), 1e-300)
+        if frc is not None:
+            assert np.abs(frc[t] - c["frc"][t]).max() <= 1e-5 * max(np.abs(c["frc"][t]).max(), 1e-300)
 
 
 def test_errors_are_reported(tmp_path):

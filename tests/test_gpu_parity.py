@@ -15,18 +15,21 @@ TOL = 1e-5
 
 
 def make_pair(fsl, oracle, m, L, q, *, eta=1.0, kT=0.01, dt=0.01, cutoff=1.5, kernel=3,
-              pair="soft", eps=1.0, rfd="reference", nonbonded=1, extra=0.0, seed=7):
+              pair="soft", eps=1.0, rfd="reference", nonbonded=1, extra=0.0, seed=7,
+              scheme="midpoint"):
     pg = {"none": fsl.PAIR_NONE, "lj": fsl.PAIR_TABLE_LJ, "soft": fsl.PAIR_SOFT}[pair]
     po = {"none": oracle.PAIR_NONE, "lj": oracle.PAIR_TABLE_LJ, "soft": oracle.PAIR_SOFT}[pair]
     rg = fsl.RFD_REFERENCE if rfd == "reference" else fsl.RFD_PAPER
     ro = oracle.RFD_REFERENCE if rfd == "reference" else oracle.RFD_PAPER
     cfg = fsl.make_config(m, L, eta=eta, kT=kT, dt=dt, cutoff=cutoff, kernel=kernel, pair=pg,
                           soft_epsilon=eps, rfd=rg, nonbonded=nonbonded, extra_mobility=extra,
-                          seed=seed)
+                          seed=seed,
+                          scheme=fsl.SCHEME_FIRST_ORDER if scheme == "first" else fsl.SCHEME_MIDPOINT)
     g = fsl.StokesLimit(cfg, q)
     o = oracle.Oracle(m[0], m[1], m[2], L[0], L[1], L[2], q, eta=eta, kT=kT, dt=dt, cutoff=cutoff,
                       kernel=kernel, pair=po, soft_epsilon=eps, rfd=ro, nonbonded=nonbonded,
-                      extra_mobility=extra, seed=seed)
+                      extra_mobility=extra, seed=seed,
+                      scheme=oracle.SCHEME_FIRST_ORDER if scheme == "first" else oracle.SCHEME_MIDPOINT)
     return g, o
 
 
@@ -142,6 +145,15 @@ STEP_CASES = {
     "4pt_paper_rfd_extra": dict(m=(20, 24, 28), L=(20.0, 24.0, 28.0), n=150, kernel=4, pair="soft",
                                 rfd="paper", extra=0.3),
     "3pt_no_pairs": dict(m=(16, 16, 16), L=(16.0,) * 3, n=64, kernel=3, pair="none"),
+    # the first-order integrator (keyword stokesLimitFirstOrder)
+    "first_3pt_soft": dict(m=(32, 32, 32), L=(32.0,) * 3, n=256, kernel=3, pair="soft",
+                           scheme="first"),
+    "first_3pt_lj": dict(m=(32, 32, 32), L=(16.0,) * 3, n=300, kernel=3, pair="lj",
+                         cutoff=2 ** (1 / 6), kT=0.05, scheme="first"),
+    "first_4pt_chains_extra": dict(m=(32, 32, 32), L=(32.0,) * 3, n=None, kernel=4, pair="soft",
+                                   dt=0.005, extra=0.3, scheme="first"),
+    "first_4pt_paper_rfd": dict(m=(20, 24, 28), L=(20.0, 24.0, 28.0), n=150, kernel=4,
+                                pair="soft", rfd="paper", scheme="first"),
 }
 
 

@@ -24,7 +24,7 @@ def _oracle_for(oracle, c):
                       eta=cfg.shearviscosity, kT=cfg.temperature, dt=cfg.dt, cutoff=cfg.cutoff,
                       kernel=cfg.kernel, pair=cfg.pair, soft_epsilon=cfg.soft_epsilon,
                       rfd=cfg.rfd, nonbonded=cfg.nonbonded, extra_mobility=cfg.extra_mobility,
-                      seed=c["seed"])
+                      seed=c["seed"], scheme=cfg.scheme)
     if c["bonds"] is not None:
         b = c["bonds"]
         o.set_bonds(b["bi"], b["bj"], b["k"], b["r0"], b["fi"], b["fk"], b["fr0"], b["fxyz"])
@@ -45,14 +45,16 @@ def test_oracle_reproduces_reference(oracle, name):
         t = step * dt
         key = min(c["pos"], key=lambda x: abs(x - t))
         assert abs(key - t) < 1e-12
-        q_ref, f_ref = c["pos"][key], c["frc"][key]
+        q_ref = c["pos"][key]
         dq_ref = q_ref - c["q0"]
         dq_orc = o.positions() - c["q0"]
         # 15 significant digits of |q| ~ L/2 bound the text's resolution
         tol = 1e-14 * np.abs(q_ref).max() * 10
         assert np.abs(dq_orc - dq_ref).max() <= max(tol, 1e-10 * np.abs(dq_ref).max()), name
-        F = o.forces()
-        assert np.abs(F - f_ref).max() <= 1e-12 + 1e-10 * np.abs(f_ref).max(), name
+        if c["frc"] is not None:
+            f_ref = c["frc"][key]
+            F = o.forces()
+            assert np.abs(F - f_ref).max() <= 1e-12 + 1e-10 * np.abs(f_ref).max(), name
 
 
 @pytest.mark.parametrize("name", G.cases())
@@ -69,4 +71,7 @@ def test_golden_files_regenerate_identically(tmp_path, name):
                        timeout=600)
     assert "END" in r.stdout, r.stdout[-1000:]
     for ext in (".particles", ".velocityParticles", ".seed"):
-        assert open(tmp_path / ("out" + ext)).read() == open(os.path.join(src, "out" + ext)).read()
+        mine, ref = tmp_path / ("out" + ext), os.path.join(src, "out" + ext)
+        assert os.path.exists(mine) == os.path.exists(ref), ext
+        if os.path.exists(ref):
+            assert open(mine).read() == open(ref).read()
