@@ -16,11 +16,13 @@ ERRORS = {-1: "FSL_E_ARG", -2: "FSL_E_CUDA", -3: "FSL_E_NOMEM", -4: "FSL_E_KERNE
 PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
 RFD_REFERENCE, RFD_PAPER = 0, 1
 SCHEME_MIDPOINT, SCHEME_FIRST_ORDER = 0, 1
+PRECISION_FIXED64, PRECISION_FLOAT_ATOMIC, PRECISION_FP64 = 0, 1, 2
 
 # Every symbol include/fluamsl.h declares.
 EXPORTS = [
     "fsl_config_defaults", "fsl_create", "fsl_load_bonds", "fsl_step", "fsl_sync",
     "fsl_get_positions", "fsl_set_positions", "fsl_get_forces", "fsl_get_velocity",
+    "fsl_get_velocity_f64",
     "fsl_get_status", "fsl_set_step", "fsl_clear_errors", "fsl_set_graph", "fsl_stream",
     "fsl_profile", "fsl_profile_read",
     "fsl_destroy", "fsl_last_error", "fsl_run_data_main", "fsl_parse_data_main",
@@ -49,6 +51,7 @@ class Config(ctypes.Structure):
         ("pair", ctypes.c_int32), ("rfd", ctypes.c_int32),
         ("nonbonded", ctypes.c_int32), ("device", ctypes.c_int32),
         ("scheme", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
     ]
 
 
@@ -123,6 +126,7 @@ def load(path=None):
     L.fsl_set_positions.argtypes = [_VP, _D]
     L.fsl_get_forces.argtypes = [_VP, _D]
     L.fsl_get_velocity.argtypes = [_VP, _F]
+    L.fsl_get_velocity_f64.argtypes = [_VP, _D]
     L.fsl_get_status.argtypes = [_VP, ctypes.POINTER(Status)]
     L.fsl_set_step.argtypes = [_VP, ctypes.c_uint64]
     L.fsl_clear_errors.argtypes = [_VP]

@@ -17,9 +17,10 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfluamsl.so")
 EXE = os.path.join(HERE, "fluam")
 
-CU_SOURCES = ["fsl_particles.cu", "fsl_fft.cu", "fsl_group.cu", "fsl_api.cu", "fsl_batch.cu", "fsl_server.cu", "fsl_noalloc.cu"]
+CU_SOURCES = ["fsl_particles.cu", "fsl_fft.cu", "fsl_group.cu", "fsl_api.cu", "fsl_batch.cu", "fsl_server.cu", "fsl_noalloc.cu",
+              "fsl_fp64.cu"]
 CPP_SOURCES = ["fsl_datamain.cpp"]
-HEADERS = ["fsl_internal.cuh", "fsl_group.cuh"]
+HEADERS = ["fsl_internal.cuh", "fsl_group.cuh", "fsl_fft_reg.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

@@ -47,6 +47,12 @@ int check_launch() {
 const fsl::Params& params(const fsl_handle* h) { return h->slot.r.P; }
 const fsl::Rep& rep(const fsl_handle* h) { return h->slot.r; }
 
+// The stage entry points exchange the FP32 fields of the default form.
+int fixed_form_only(const fsl_handle* h, const char* what) {
+  if (params(h).prec == fsl::PREC_FIXED) return FSL_OK;
+  return errorf(FSL_E_ARG, "%s: available in the FIXED64 precision form only", what);
+}
+
 }  // namespace
 
 extern "C" {
@@ -194,9 +200,27 @@ int fsl_get_forces(fsl_handle* h, double* out) {
 
 int fsl_get_velocity(fsl_handle* h, float* out) {
   if (!h || !out) return errorf(FSL_E_ARG, "null argument");
+  if (params(h).prec == fsl::PREC_F64)
+    return errorf(FSL_E_ARG, "fsl_get_velocity: the FP64 form's field is read by fsl_get_velocity_f64");
   FSL_TRY(cudaSetDevice(h->exec.device));
   FSL_TRY(cudaMemcpyAsync(out, rep(h).v, sizeof(float) * 3 * (size_t)params(h).nc,
                           cudaMemcpyDeviceToHost, h->exec.stream));
+  FSL_TRY(cudaStreamSynchronize(h->exec.stream));
+  return FSL_OK;
+}
+
+int fsl_get_velocity_f64(fsl_handle* h, double* out) {
+  if (!h || !out) return errorf(FSL_E_ARG, "null argument");
+  const size_t n3 = 3 * (size_t)params(h).nc;
+  if (params(h).prec != fsl::PREC_F64) {
+    std::vector<float> v(n3);
+    int rc = fsl_get_velocity(h, v.data());
+    if (rc) return rc;
+    for (size_t k = 0; k < n3; ++k) out[k] = (double)v[k];
+    return FSL_OK;
+  }
+  FSL_TRY(cudaSetDevice(h->exec.device));
+  FSL_TRY(cudaMemcpyAsync(out, rep(h).v64, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->exec.stream));
   FSL_TRY(cudaStreamSynchronize(h->exec.stream));
   return FSL_OK;
 }
@@ -272,7 +296,9 @@ int fsl_compute_forces(fsl_handle* h, double* F) {
 
 int fsl_spread(fsl_handle* h, const double* F, double* f) {
   if (!h || !F || !f) return errorf(FSL_E_ARG, "null argument");
-  int rc = prepare(h);
+  int rc = fixed_form_only(h, "fsl_spread");
+  if (rc) return rc;
+  rc = prepare(h);
   if (rc) return rc;
   const fsl::Params& P = params(h);
   const fsl::Rep& R = rep(h);
@@ -293,7 +319,9 @@ int fsl_spread(fsl_handle* h, const double* F, double* f) {
 
 int fsl_solve(fsl_handle* h, const double* W, double* v) {
   if (!h || !W || !v) return errorf(FSL_E_ARG, "null argument");
-  int rc = prepare(h);
+  int rc = fixed_form_only(h, "fsl_solve");
+  if (rc) return rc;
+  rc = prepare(h);
   if (rc) return rc;
   const fsl::Params& P = params(h);
   const fsl::Rep& R = rep(h);
@@ -312,7 +340,9 @@ int fsl_solve(fsl_handle* h, const double* W, double* v) {
 
 int fsl_interpolate(fsl_handle* h, const double* vin, double* u) {
   if (!h || !vin || !u) return errorf(FSL_E_ARG, "null argument");
-  int rc = prepare(h);
+  int rc = fixed_form_only(h, "fsl_interpolate");
+  if (rc) return rc;
+  rc = prepare(h);
   if (rc) return rc;
   const fsl::Params& P = params(h);
   const fsl::Rep& R = rep(h);

@@ -5,9 +5,10 @@
 //   followed by a fixed number of values; '#' starts a comment to end of line;
 //   an unknown keyword is an error ("ERROR INPUT FILE").  Every keyword of the
 //   reference parser is accepted and consumes the same tokens; the ones that
-//   the Stokes-limit path does not read are ignored.  Four keywords are new
+//   the Stokes-limit path does not read are ignored.  Five keywords are new
 //   (the reference parser would reject them): pairPotential lj|soft|none,
-//   softEpsilon <eps>, kernelPoints 3|4, rfdMode reference|paper.
+//   softEpsilon <eps>, kernelPoints 3|4, rfdMode reference|paper,
+//   precision fixed64|float_atomic|fp64.
 // Output (src/saveFunctionsSchemeStokesLimit.cu, src/saveParticles.cu:32-82,
 //   src/saveSeed.cpp, src/saveTime.cpp, src/cudaDevice.cu):
 //   <out>.data.main echo, <out>.cuda, <out>.seed, <out>.time,
@@ -75,7 +76,7 @@ const std::map<std::string, int>& keyword_arity() {
       {"stokesLimitFirstOrder", 0}, {"stokesLimit", 0}, {"extraMobility", 1},
       // extensions of this build
       {"pairPotential", 1}, {"softEpsilon", 1}, {"kernelPoints", 1}, {"rfdMode", 1},
-      {"savedensity", -1}};
+      {"precision", 1}, {"savedensity", -1}};
   return m;
 }
 
@@ -201,6 +202,14 @@ int parse(const char* path, Run& r, std::string& err) {
         else if (vals[0] == "paper") c.rfd = FSL_RFD_PAPER;
         else {
           err = "rfdMode must be reference or paper";
+          return FSL_E_INPUT;
+        }
+      } else if (word == "precision") {
+        if (vals[0] == "fixed64") c.precision = FSL_PRECISION_FIXED64;
+        else if (vals[0] == "float_atomic") c.precision = FSL_PRECISION_FLOAT_ATOMIC;
+        else if (vals[0] == "fp64") c.precision = FSL_PRECISION_FP64;
+        else {
+          err = "precision must be fixed64, float_atomic or fp64";
           return FSL_E_INPUT;
         }
       } else if (word == "continuousGradient" || word == "giantFluctuations" ||

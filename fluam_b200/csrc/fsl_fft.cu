@@ -320,18 +320,28 @@ __global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
   const float* n1 = R.noise;
   const float* n2 = R.noise + (size_t)6 * P.nc + (size_t)9 * P.np;
   const size_t nc = (size_t)P.nc;
+  // float-atomic form: FP32 sums in the first 3 nc floats of the buffer
+  const bool fatom = P.prec == PREC_FLOAT;
+  float* gf = reinterpret_cast<float*>(R.grid);
+  const float fscale = (float)(1.0 / P.dV);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc;
        i += (size_t)gridDim.x * blockDim.x) {
     int x = (int)(i % P.mx), r = (int)(i / P.mx);
     int y = r % P.my, z = r / P.my;
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
-      long long g = (long long)R.grid[comp * nc + i];
-      float w = (float)((double)g * (double)scale);
+      float w;
+      if (fatom) {
+        w = gf[comp * nc + i] * fscale;
+        gf[comp * nc + i] = 0.0f;
+      } else {
+        long long g = (long long)R.grid[comp * nc + i];
+        w = (float)((double)g * (double)scale);
+        R.grid[comp * nc + i] = 0ull;
+      }
       w += stress_div(P, n1, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
       if (nsets > 1) w += stress_div(P, n2, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
       R.wbuf[comp * nc + i] = w;
-      R.grid[comp * nc + i] = 0ull;
     }
   }
 }
@@ -400,6 +410,9 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
   const size_t nc = (size_t)P.nc;
   const int gx = P.mx >> 2;
   const size_t ng = nc >> 2;
+  const bool fatom = P.prec == PREC_FLOAT;
+  float* gf = reinterpret_cast<float*>(R.grid);
+  const float fscale = (float)(1.0 / P.dV);
   for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < ng;
        g += (size_t)gridDim.x * blockDim.x) {
     const int x0 = (int)(g % gx) << 2;
@@ -409,6 +422,16 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
     float w[3][4];
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
+      if (fatom) {
+        float4* fp = reinterpret_cast<float4*>(gf + comp * nc + i0);
+        const float4 ga = *fp;
+        w[comp][0] = ga.x * fscale;
+        w[comp][1] = ga.y * fscale;
+        w[comp][2] = ga.z * fscale;
+        w[comp][3] = ga.w * fscale;
+        *fp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        continue;
+      }
       const longlong2* gp = reinterpret_cast<const longlong2*>(R.grid + comp * nc + i0);
       const longlong2 ga = gp[0], gb = gp[1];
       w[comp][0] = (float)((double)ga.x * (double)scale);
@@ -422,6 +445,7 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
     for (int comp = 0; comp < 3; ++comp) {
       *reinterpret_cast<float4*>(R.wbuf + comp * nc + i0) =
           make_float4(w[comp][0], w[comp][1], w[comp][2], w[comp][3]);
+      if (fatom) continue;  // cleared at the read
       longlong2* gq = reinterpret_cast<longlong2*>(R.grid + comp * nc + i0);
       gq[0] = make_longlong2(0, 0);
       gq[1] = make_longlong2(0, 0);
@@ -987,6 +1011,7 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
 
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof) {
+  if (B.prec == PREC_F64) return launch_solve64(B, nsets, nfac, s, prof);
   Prof dummy;
   Prof& pr = prof ? *prof : dummy;
   const int nrep = B.nrep;

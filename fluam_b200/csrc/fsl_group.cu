@@ -11,6 +11,11 @@
 
 namespace fsl {
 
+static_assert((int)PREC_FIXED == (int)FSL_PRECISION_FIXED64 &&
+                  (int)PREC_FLOAT == (int)FSL_PRECISION_FLOAT_ATOMIC &&
+                  (int)PREC_F64 == (int)FSL_PRECISION_FP64,
+              "precision codes");
+
 namespace {
 thread_local char g_msg[512] = "";
 
@@ -20,7 +25,7 @@ size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 // Byte offsets of one slot's buffers inside its arena.
 struct SlotLayout {
   size_t q, qp, F, u, qw, ws, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
-      bsum, ljtab, noise, grid, spec, v, wbuf, err, t, total;
+      bsum, ljtab, noise, grid, spec, v, wbuf, noise64, v64, z64, err, t, total;
 };
 
 SlotLayout layout(const Params& P, int np_cap) {
@@ -52,11 +57,18 @@ SlotLayout layout(const Params& P, int np_cap) {
   L.start = take(sizeof(int) * (mN + 1));
   L.bsum = take(sizeof(int) * ((mN + 4095) / 4096 + 1));
   L.ljtab = take(sizeof(float) * kLjTableSize);
-  L.noise = take(sizeof(float) * noise);
+  // the FP32 field buffers, or their FP64 counterparts (the spread field has
+  // 8-byte entries in every form: fixed point, or FP64; the float-atomic
+  // form uses its first 3 nc floats)
+  const bool f64 = P.prec == FSL_PRECISION_FP64;
+  L.noise = take(f64 ? 0 : sizeof(float) * noise);
   L.grid = take(sizeof(unsigned long long) * 3 * nc);
-  L.spec = take(sizeof(float2) * 3 * (size_t)P.my * P.mz * P.mxh);
-  L.v = take(sizeof(float) * 3 * nc);
-  L.wbuf = take(sizeof(float) * 3 * nc);
+  L.spec = take(f64 ? 0 : sizeof(float2) * 3 * (size_t)P.my * P.mz * P.mxh);
+  L.v = take(f64 ? 0 : sizeof(float) * 3 * nc);
+  L.wbuf = take(f64 ? 0 : sizeof(float) * 3 * nc);
+  L.noise64 = take(f64 ? sizeof(double) * noise : 0);
+  L.v64 = take(f64 ? sizeof(double) * 3 * nc : 0);
+  L.z64 = take(f64 ? sizeof(double2) * 3 * nc : 0);
   L.err = take(sizeof(int) * 4);
   L.t = take(sizeof(uint64_t));
   L.total = off;
@@ -91,14 +103,14 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 bool ClassKey::operator<(const ClassKey& o) const {
-  const int a[8] = {mx, my, mz, mnx, mny, mnz, kernel, scheme};
-  const int b[8] = {o.mx, o.my, o.mz, o.mnx, o.mny, o.mnz, o.kernel, o.scheme};
-  return std::lexicographical_compare(a, a + 8, b, b + 8);
+  const int a[9] = {mx, my, mz, mnx, mny, mnz, kernel, scheme, prec};
+  const int b[9] = {o.mx, o.my, o.mz, o.mnx, o.mny, o.mnz, o.kernel, o.scheme, o.prec};
+  return std::lexicographical_compare(a, a + 9, b, b + 9);
 }
 bool ClassKey::operator==(const ClassKey& o) const { return !(*this < o) && !(o < *this); }
 
 ClassKey class_of(const Params& P) {
-  return ClassKey{P.mx, P.my, P.mz, P.mnx, P.mny, P.mnz, P.kernel, P.scheme};
+  return ClassKey{P.mx, P.my, P.mz, P.mnx, P.mny, P.mnz, P.kernel, P.scheme, P.prec};
 }
 
 int make_params(const fsl_config& c, int64_t np, Params& P) {
@@ -117,6 +129,8 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   if (c.pair < 0 || c.pair > 2) return errorf(FSL_E_ARG, "unknown pair potential %d", c.pair);
   if (c.rfd < 0 || c.rfd > 1) return errorf(FSL_E_ARG, "unknown rfd mode %d", c.rfd);
   if (c.scheme < 0 || c.scheme > 1) return errorf(FSL_E_ARG, "unknown scheme %d", c.scheme);
+  if (c.precision < 0 || c.precision > 2)
+    return errorf(FSL_E_ARG, "unknown precision form %d", c.precision);
   if (c.extra_mobility < 0) return errorf(FSL_E_ARG, "extraMobility must be >= 0");
   if (np < 0 || np > (int64_t)1 << 28) return errorf(FSL_E_ARG, "bad particle count");
   bool pairs = c.nonbonded && c.pair != FSL_PAIR_NONE && np > 0;
@@ -165,6 +179,7 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   P.nonbonded = c.nonbonded ? 1 : 0;
   P.rfd = c.rfd;
   P.scheme = c.scheme;
+  P.prec = c.precision;
   P.bonded = 0;
   P.has_extra = c.extra_mobility != 0.0;
   P.cutoff = c.cutoff;
@@ -247,6 +262,10 @@ int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st) {
   r.spec = (float2*)(base + L.spec);
   r.v = (float*)(base + L.v);
   r.wbuf = (float*)(base + L.wbuf);
+  const bool f64 = P.prec == FSL_PRECISION_FP64;
+  r.noise64 = f64 ? (double*)(base + L.noise64) : nullptr;
+  r.v64 = f64 ? (double*)(base + L.v64) : nullptr;
+  r.z64 = f64 ? (double2*)(base + L.z64) : nullptr;
   r.err = (int*)(base + L.err);
   r.t = (uint64_t*)(base + L.t);
   return FSL_OK;
@@ -287,7 +306,10 @@ int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, c
   FSL_TRY(cudaMemsetAsync(r.bfp_cnt, 0, sizeof(int) * cap, st));
   FSL_TRY(cudaMemsetAsync(r.bfp_off, 0, sizeof(int) * cap, st));
   FSL_TRY(cudaMemsetAsync(r.grid, 0, sizeof(unsigned long long) * 3 * (size_t)P.nc, st));
-  FSL_TRY(cudaMemsetAsync(r.v, 0, sizeof(float) * 3 * (size_t)P.nc, st));
+  if (P.prec == PREC_F64)
+    FSL_TRY(cudaMemsetAsync(r.v64, 0, sizeof(double) * 3 * (size_t)P.nc, st));
+  else
+    FSL_TRY(cudaMemsetAsync(r.v, 0, sizeof(float) * 3 * (size_t)P.nc, st));
   FSL_TRY(cudaMemsetAsync(r.err, 0, sizeof(int) * 4, st));
   FSL_TRY(cudaMemsetAsync(r.t, 0, sizeof(uint64_t), st));
   r.active = 1;
@@ -414,6 +436,7 @@ int group_upload(Group& g) {
   B.nc = g.P0.nc;
   B.mN = g.P0.mN;
   B.kernel = g.P0.kernel;
+  B.prec = g.P0.prec;
   B.max_np = 0;
   B.max_noise_n = 0;
   for (const Slot* s : g.slots) {

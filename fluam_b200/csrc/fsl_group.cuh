@@ -38,7 +38,7 @@ int make_params(const fsl_config& c, int64_t np, Params& P);
 
 // Size-class key: instances that can share every launch of a step.
 struct ClassKey {
-  int mx, my, mz, mnx, mny, mnz, kernel, scheme;
+  int mx, my, mz, mnx, mny, mnz, kernel, scheme, prec;
   bool operator<(const ClassKey& o) const;
   bool operator==(const ClassKey& o) const;
 };

@@ -11,6 +11,9 @@
 //     whole step is bit-reproducible run to run;
 //   * kernel weights, the noise, the fields, the FFTs and the spectral
 //     multiplier are FP32.
+// Two other forms of the fluid side exist for the precision study
+// (Params::prec): float atomics instead of the fixed point, and FP64
+// everywhere (fsl_fp64.cu).
 #pragma once
 
 #include <cstdint>
@@ -25,6 +28,8 @@ constexpr double kRfdDelta = 0.001;  // src/stokesLimitFunctions.cu:1719
 constexpr int kLjTableSize = 4096;   // src/initForcesNonBonded.cu:36
 
 enum { ERR_ANY = 0, ERR_BITS = 1 };
+// Params::prec, the values of FSL_PRECISION_* (include/fluamsl.h)
+enum { PREC_FIXED = 0, PREC_FLOAT = 1, PREC_F64 = 2 };
 
 // Everything a kernel needs about one instance, passed by value.
 struct Params {
@@ -41,6 +46,7 @@ struct Params {
   int kernel;  // 3 or 4
   int pair, nonbonded, rfd, bonded;
   int scheme;  // FSL_SCHEME_* (0 midpoint, 1 first order)
+  int prec;    // FSL_PRECISION_* (0 fixed point, 1 float atomics, 2 FP64)
   int has_extra;
   double cutoff, cutoff2, invcut2, soft_eps;
   double eta, kT, dt, extra_mob, fact1, fact2, fact4;
@@ -320,6 +326,10 @@ struct Rep {
   double* u;  // interpolated velocities of the component entry point
   double* qw;  // positions wrapped into the box by the last cell-list build
   double* ws;  // the same in cell-list order
+  // FP64 form only (null otherwise): noise, field, complex spectrum
+  double* noise64;
+  double* v64;
+  double2* z64;
   int* err;
   uint64_t* t;
 };
@@ -349,6 +359,7 @@ struct Batch {
   const int* boff;  // device block offsets, [NKIND][nrep + 1]
   int nrep;
   int mx, my, mz, mxh, nc, mN, kernel;
+  int prec;  // FSL_PRECISION_* of the class
   int max_np;
   uint64_t max_noise_n;
   int nblk[NKIND];  // total blocks of each particle launch kind
@@ -453,6 +464,12 @@ void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s);
 void launch_interp_update(const Batch& B, int stage, cudaStream_t s);
 void launch_interp(const Batch& B, cudaStream_t s);  // u = J(q) v
 void launch_step_counter(const Batch& B, cudaStream_t s);
+// The FP64 form (fsl_fp64.cu); the launchers above hand a class of that
+// form to these.
+void launch_noise64(const Batch& B, cudaStream_t s);
+void launch_spread64(const Batch& B, int drift, cudaStream_t s);
+void launch_interp_update64(const Batch& B, int stage, cudaStream_t s);
+void launch_solve64(const Batch& B, int nsets, double nfac, cudaStream_t s, Prof* prof);
 
 struct FftPlan;  // defined in fsl_fft.cu
 FftPlan* fft_plan_create(const Params& P);

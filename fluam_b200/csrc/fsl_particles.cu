@@ -39,6 +39,7 @@ __global__ void k_noise_range(uint64_t seed, uint64_t t, uint64_t first, int64_t
 }
 
 void launch_noise(const Batch& B, cudaStream_t s) {
+  if (B.prec == PREC_F64) return launch_noise64(B, s);
   const int tb = 256;
   uint64_t nb = (B.max_noise_n + 3) / 4;
   unsigned bx = blocks_for((long)nb, tb);
@@ -380,7 +381,8 @@ void launch_forces(const Batch& B, int which, cudaStream_t s) {
 // ------------------------------------------------------------- spreading ---
 // One warp per entry (all three components of one spread of one particle);
 // lane l takes stencil nodes l, l+32, ... (x fastest, so a warp's atomics
-// fall on a few 32-byte sectors) and adds w * value in 64-bit fixed point.
+// fall on a few 32-byte sectors) and adds w * value in 64-bit fixed point
+// (in the float-atomic form: w * value as an FP32 atomic).
 // Replaces the slot writes of kernelSpreadParticlesForceStokesLimit and
 // kernelSpreadParticlesDrift + the gather of addSpreadedForcesStokesLimit
 // (src/stokesLimitFunctions.cu:659-1681, 1705-2255); the 1/dV of the gather
@@ -407,12 +409,17 @@ __device__ __forceinline__ void spread_entry(const Params& P, const double posc[
     stencil_get(st, n, comp, 2, c, z, wz);
     if (!valid) continue;
     const double vc = comp == 0 ? val[0] : (comp == 1 ? val[1] : val[2]);
+    const size_t at = (size_t)comp * P.nc + x + (size_t)P.mx * (y + (size_t)P.my * z);
+    if (P.prec == PREC_FLOAT) {
+      // float-atomic form: the first 3 nc floats of the spread buffer
+      const float fv = (float)((double)(wx * (wy * wz)) * vc);
+      if (fv != 0.0f) atomicAdd(reinterpret_cast<float*>(grid) + at, fv);
+      continue;
+    }
     double v = (double)(wx * (wy * wz)) * (vc * kFixedScale);
     sat |= !(fabs(v) < kFixedMax);
     long long iv = sat ? 0ll : __double2ll_rn(v);
-    if (iv != 0)
-      atomicAdd(grid + (size_t)comp * P.nc + x + (size_t)P.mx * (y + (size_t)P.my * z),
-                (unsigned long long)iv);
+    if (iv != 0) atomicAdd(grid + at, (unsigned long long)iv);
   }
 }
 
@@ -475,6 +482,7 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
 
 void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s) {
   if (B.max_np == 0) return;
+  if (B.prec == PREC_F64) return launch_spread64(B, drift, s);
   const unsigned g = part_blocks(B, drift ? KIND_T64 : KIND_T32);
   if (B.kernel == 4)
     FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered);
@@ -585,6 +593,7 @@ __global__ void k_interp(FSL_KARGS) {
 
 void launch_interp_update(const Batch& B, int stage, cudaStream_t s) {
   if (B.max_np == 0) return;
+  if (B.prec == PREC_F64) return launch_interp_update64(B, stage, s);
   const unsigned g = part_blocks(B, KIND_T32);
   if (B.kernel == 4)
     FSL_GO_T(k_interp_update, 4, g, kPartThreads, 0, s, B, stage);

@@ -30,7 +30,7 @@ def _ip(a):
 
 def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair=PAIR_TABLE_LJ,
                 soft_epsilon=1.0, rfd=RFD_REFERENCE, nonbonded=1, extra_mobility=0.0, seed=0,
-                device=-1, scheme=0):
+                device=-1, scheme=0, precision=0):
     c = _lib.Config()
     _lib.load().fsl_config_defaults(ctypes.byref(c))
     c.mx, c.my, c.mz = (int(x) for x in cells)
@@ -39,6 +39,7 @@ def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair
     c.kernel, c.pair, c.soft_epsilon, c.rfd = kernel, pair, soft_epsilon, rfd
     c.nonbonded, c.extra_mobility, c.seed, c.device = nonbonded, extra_mobility, seed, device
     c.scheme = scheme
+    c.precision = precision
     return c
 
 
@@ -109,6 +110,12 @@ class StokesLimit:
     def forces(self):
         out = np.empty((3, self.np))
         check(self.L.fsl_get_forces(self.h, _dp(out)))
+        return out
+
+    def velocity64(self):
+        """The fluid velocity of the last solve as float64, in every precision form."""
+        out = np.empty((3,) + self.shape, dtype=np.float64)
+        check(self.L.fsl_get_velocity_f64(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
     def velocity(self):

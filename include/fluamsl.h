@@ -47,6 +47,17 @@ enum { FSL_RFD_REFERENCE = 0, FSL_RFD_PAPER = 1 };
  * stokesLimitFirstOrder (src/runSchemeStokesLimitFirstOrder.cu:163-241: one
  * solve per step with the RFD drift, the same predictor and corrector). */
 enum { FSL_SCHEME_MIDPOINT = 0, FSL_SCHEME_FIRST_ORDER = 1 };
+/* Arithmetic of the fluid side (no counterpart in the reference, which is
+ * FP64 throughout).  Particle positions, forces and the cell lists are FP64
+ * in every form.
+ *   FIXED64:      FP32 fields, noise and FFTs; spreading accumulated in 64-bit
+ *                 fixed point (2^-40) with integer atomics: order-independent,
+ *                 bit-reproducible run to run (the default);
+ *   FLOAT_ATOMIC: the same with spreading accumulated by FP32 atomics (the
+ *                 sum depends on the order the atomics land in);
+ *   FP64:         noise, spreading (FP64 atomics), fields, FFTs and
+ *                 interpolation all in FP64. */
+enum { FSL_PRECISION_FIXED64 = 0, FSL_PRECISION_FLOAT_ATOMIC = 1, FSL_PRECISION_FP64 = 2 };
 
 /* Bits of fsl_status.error_bits (device error word, sticky until cleared). */
 enum {
@@ -73,6 +84,7 @@ typedef struct fsl_config {
   int32_t nonbonded;             /* computeNonBondedForces                  */
   int32_t device;                /* setDevice; -1 keeps the current device  */
   int32_t scheme;                /* FSL_SCHEME_*                            */
+  int32_t precision;             /* FSL_PRECISION_*                         */
 } fsl_config;
 
 typedef struct fsl_status {
@@ -126,6 +138,9 @@ int fsl_get_forces(fsl_handle* h, double* out);
 /* Fluid velocity of the last solve, float [3][nc] (not written by the
  * reference on this path; exposed for checks). */
 int fsl_get_velocity(fsl_handle* h, float* out);
+/* The same as double [3][nc], in every precision form (the only full-precision
+ * read of the FP64 form's field). */
+int fsl_get_velocity_f64(fsl_handle* h, double* out);
 int fsl_get_status(fsl_handle* h, fsl_status* st);
 int fsl_set_step(fsl_handle* h, uint64_t step);
 int fsl_clear_errors(fsl_handle* h);
