@@ -151,3 +151,16 @@ def test_stage_entry_points_refuse_other_forms(fsl):
                            v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         assert rc == -1  # FSL_E_ARG
         g.close()
+
+
+def test_precision_study_small(tmp_path):
+    """The study script end to end on a small case (64^3, 4,096 particles)."""
+    import precision_study
+    r = precision_study.main(["--cells", "64", "--np", "4096", "--steps", "6", "--oracle-steps", "1",
+                              "--json", str(tmp_path / "s.json"), "--md", str(tmp_path / "s.md")])
+    pin = r["oracle_pin"][0]
+    assert pin["fp64"]["dq_rel_inf"] < 1e-10 and pin["fp64"]["v_rel_inf"] < 1e-10
+    assert pin["fixed64"]["dq_rel_inf"] < 1e-5 and pin["float_atomic"]["dq_rel_inf"] < 1e-5
+    assert r["per_step_vs_fp64_form"]["fixed64"]["dq_rel_inf_max"] < 1e-5
+    assert r["reproducibility"]["fixed64"]["bit_identical"]
+    assert (tmp_path / "s.md").read_text().startswith("# Precision study")
