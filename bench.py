@@ -310,20 +310,13 @@ def serve_requests(n_per_s, duration, seed, steps_range):
         out.append((t, cfg, workloads.uniform(npart, m, int(rng.integers(1 << 30))), nst))
 
 
-def run_served(rate=100.0, duration=3.0, steps_range=(10, 500), seed=11, plain_sample=24):
-    """The serving loop under a Poisson stream; completion latency and
-    aggregate throughput, next to a sample of the same requests run one at a
-    time on the plain path (wall time of create + steps + read-back)."""
-    from fluam_b200 import Server, StokesLimit
-    reqs = serve_requests(rate, duration, seed, steps_range)
-    srv = Server(hbm_budget=150 * 10 ** 9)
-    # warm-up: one short request per size class builds the FFT plans
-    warm = {}
-    for _, c, q, _ in reqs:
-        warm.setdefault((c.mx, c.kernel), (c, q[:, :16]))
-    for rid in [srv.submit(c, q, 2) for c, q in warm.values()]:
-        srv.wait(rid)
-        srv.result(rid)
+# Arrival rates of the serving sweep (requests/s) and how long each stream
+# keeps arriving (s): 20, 60 and 120 requests.
+SERVE_SWEEP = ((10.0, 2.0), (100.0, 0.6), (1000.0, 0.12))
+
+
+def serve_stream(srv, reqs):
+    """Submits reqs at their arrival times; returns (infos, span s)."""
     ids = []
     t0 = time.perf_counter()
     for t, c, q, n in reqs:
@@ -334,15 +327,44 @@ def run_served(rate=100.0, duration=3.0, steps_range=(10, 500), seed=11, plain_s
     infos = [srv.wait(i) for i in ids]
     for i in ids:
         srv.result(i)
+    span = max(x["done_s"] for x in infos) - min(x["submit_s"] for x in infos)
+    return infos, span
+
+
+def run_served(sweep=SERVE_SWEEP, steps_range=(100, 5000), seed=11, plain_sample=12):
+    """The serving loop under open-loop Poisson streams at each rate of the
+    sweep: completion latency and aggregate throughput, next to a sample of
+    the same requests run one at a time on the plain path (wall time of
+    create + steps + read-back)."""
+    from fluam_b200 import Server, StokesLimit
+    streams = [serve_requests(rate, dur, seed + k, steps_range) for k, (rate, dur) in enumerate(sweep)]
+    srv = Server(hbm_budget=150 * 10 ** 9)
+    # warm-up: one short request per size class builds the FFT plans
+    warm = {}
+    for reqs in streams:
+        for _, c, q, _ in reqs:
+            warm.setdefault((c.mx, c.kernel), (c, q[:, :16]))
+    for rid in [srv.submit(c, q, 2) for c, q in warm.values()]:
+        srv.wait(rid)
+        srv.result(rid)
+    rows = []
+    for (rate, dur), reqs in zip(sweep, streams):
+        infos, span = serve_stream(srv, reqs)
+        lat = np.array([x["done_s"] - x["submit_s"] for x in infos])
+        work = sum(q.shape[1] * n for _, _, q, n in reqs)
+        rows.append({"rate_per_s": rate, "arrivals_s": dur, "requests": len(reqs),
+                     "completed": int(sum(x["state"] == 2 for x in infos)),
+                     "value": work / span, "unit": "particle-steps/s", "span_s": span,
+                     "latency_p50_s": float(np.percentile(lat, 50)),
+                     "latency_p99_s": float(np.percentile(lat, 99))})
     st = srv.stats()
     srv.close()
-    lat = np.array([x["done_s"] - x["submit_s"] for x in infos])
-    span = max(x["done_s"] for x in infos) - min(x["submit_s"] for x in infos)
-    work = sum(q.shape[1] * n for _, _, q, n in reqs)
-    ok = sum(x["state"] == 2 for x in infos)
-    # plain path, one request at a time
+    # plain path, one request at a time (a seeded sample across the sweep)
+    pool = [r for reqs in streams for r in reqs]
+    pick = np.random.default_rng(seed).choice(len(pool), size=min(plain_sample, len(pool)), replace=False)
     p_work, p_s = 0, 0.0
-    for _, c, q, n in reqs[:plain_sample]:
+    for k in pick:
+        _, c, q, n = pool[int(k)]
         a = time.perf_counter()
         g = StokesLimit(c, q)
         g.step(n)
@@ -351,17 +373,17 @@ def run_served(rate=100.0, duration=3.0, steps_range=(10, 500), seed=11, plain_s
         p_s += time.perf_counter() - a
         p_work += q.shape[1] * n
     plain = p_work / p_s
+    top = rows[-1]
     return {
-        "workload": f"Poisson {rate:g} req/s for {duration:g} s: edge U{{16,24,...,96}}, np "
-                    f"log-U[16,16384], steps log-U[{steps_range[0]},{steps_range[1]}], eta "
-                    "U[0.5,2], 3/4-pt kernel 50/50, soft repulsion, 150 GB budget",
-        "requests": len(reqs), "completed": ok, "value": work / span,
-        "unit": "particle-steps/s", "latency_p50_s": float(np.percentile(lat, 50)),
-        "latency_p99_s": float(np.percentile(lat, 99)), "span_s": span,
+        "workload": f"Poisson streams at {', '.join('%g' % r for r, _ in sweep)} req/s: edge "
+                    f"U{{16,24,...,96}}, np log-U[16,16384], steps log-U[{steps_range[0]},{steps_range[1]}], "
+                    "eta U[0.5,2], 3/4-pt kernel 50/50, soft repulsion, 150 GB budget",
+        "sweep": rows, "value": top["value"], "unit": "particle-steps/s",
+        "latency_p50_s": top["latency_p50_s"], "latency_p99_s": top["latency_p99_s"],
         "rounds": st["rounds"], "captures": st["captures"], "slots": st["slots"],
         "plain_one_at_a_time": {"value": plain, "unit": "particle-steps/s",
-                                "sample": f"first {plain_sample} requests, wall time"},
-        "speedup_vs_plain": (work / span) / plain,
+                                "sample": f"{len(pick)} requests of the sweep, wall time"},
+        "speedup_vs_plain": top["value"] / plain,
     }
 
 

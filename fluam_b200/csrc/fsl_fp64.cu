@@ -76,7 +76,7 @@ struct Stencil64 {
   double w[3][4];
 };
 
-// Stencil of component comp: the node choice of make_stencil (posc) and the
+// Stencil of component comp: the node choice of stencil_node (posc) and the
 // weights in FP64 (posw).
 __device__ __forceinline__ void stencil64(const Params& P, int comp, const double posc[3],
                                           const double posw[3], Stencil64& st) {
@@ -90,10 +90,10 @@ __device__ __forceinline__ void stencil64(const Params& P, int comp, const doubl
     const double off = (d == comp) ? __dmul_rn(0.5, h[d]) : 0.0;
     if (P.kernel == 3) {
       double r = minimage(__dsub_rn(posc[d], off), invL[d], L[d]);
-      st.j0[d] = (cellidx(r, invd[d], m[d]) - 1 + m[d]) % m[d];
+      st.j0[d] = wrap_add(cellidx(r, invd[d], m[d]), -1, m[d]);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        int j = (st.j0[d] + k) % m[d];
+        int j = wrap_add(st.j0[d], k, m[d]);
         double node = ((double)j + 0.5) * h[d] - 0.5 * L[d];
         double rr = minimage((posw[d] - node) - off, invL[d], L[d]);
         st.w[d][k] = delta3d(rr * invd[d]);
@@ -101,7 +101,7 @@ __device__ __forceinline__ void stencil64(const Params& P, int comp, const doubl
       st.w[d][3] = 0.0;
     } else {
       double r = minimage(__dsub_rn(__dsub_rn(posc[d], off), __dmul_rn(0.5, h[d])), invL[d], L[d]);
-      st.j0[d] = (cellidx(r, invd[d], m[d]) - 1 + m[d]) % m[d];
+      st.j0[d] = wrap_add(cellidx(r, invd[d], m[d]), -1, m[d]);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         int j = (st.j0[d] + k) % m[d];

@@ -112,8 +112,23 @@ __device__ __forceinline__ double minimage(double r, double invL, double L) {
 // coordinate beyond the int range) still lands in [0, m), so no index
 // derived from it can leave its array, and the caller flags the value.
 __device__ __forceinline__ int cellidx(double r, double invd, int m) {
-  int j = ((int)__dadd_rn(__dmul_rn(r, invd), __dmul_rn(0.5, (double)m))) % m;
-  return j < 0 ? j + m : j;
+  int j = (int)__dadd_rn(__dmul_rn(r, invd), __dmul_rn(0.5, (double)m));
+  // a wrapped coordinate gives j in [0, m] (m only at r = L/2): one
+  // comparison; anything else takes the general remainder
+  if (j == m) return 0;
+  if ((unsigned)j > (unsigned)m) {
+    j %= m;
+    j = j < 0 ? j + m : j;
+  }
+  return j;
+}
+
+// (j + k) mod m for j in [0, m), -1 <= k <= 2 and m >= 3 (stencil offsets)
+__device__ __forceinline__ int wrap_add(int j, int k, int m) {
+  int y = j + k;
+  y += y < 0 ? m : 0;
+  y -= y >= m ? m : 0;
+  return y;
 }
 
 __device__ __forceinline__ int nb_cell(const Params& P, double x, double y, double z) {
@@ -151,54 +166,10 @@ __device__ __forceinline__ float delta4f(float x) {
   return (5.0f - 2.0f * x - sqrtf(fmaxf(-7.0f + 12.0f * x - 4.0f * x * x, 0.0f))) * 0.125f;
 }
 
-// Stencil of one particle for field component comp: first node index per
-// dimension and the weights.  Nodes of component comp in dimension d sit at
+// Node k (0..n-1) of the stencil of field component comp in dimension d:
+// grid index j and its weight.  Nodes of component comp in dimension d sit at
 // (j + 1/2) h - L/2, plus h/2 when d == comp.  posc picks the nodes, posw sets
-// the weights (they differ only in the reference's RFD quirk).
-struct Stencil {
-  int j0[3];
-  float w[3][4];
-};
-
-__device__ __forceinline__ void make_stencil(const Params& P, int comp, const double posc[3],
-                                             const double posw[3], Stencil& st) {
-  const int m[3] = {P.mx, P.my, P.mz};
-  const double h[3] = {P.dx, P.dy, P.dz};
-  const double invd[3] = {P.invdx, P.invdy, P.invdz};
-  const double L[3] = {P.lx, P.ly, P.lz};
-  const double invL[3] = {P.invlx, P.invly, P.invlz};
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    double off = (d == comp) ? __dmul_rn(0.5, h[d]) : 0.0;
-    if (P.kernel == 3) {
-      double r = minimage(__dsub_rn(posc[d], off), invL[d], L[d]);
-      int jc = cellidx(r, invd[d], m[d]);
-      st.j0[d] = (jc - 1 + m[d]) % m[d];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        int j = (st.j0[d] + k) % m[d];
-        double node = ((double)j + 0.5) * h[d] - 0.5 * L[d];
-        double rr = minimage((posw[d] - node) - off, invL[d], L[d]);
-        st.w[d][k] = delta3f((float)(rr * invd[d]));
-      }
-      st.w[d][3] = 0.0f;
-    } else {
-      double r = minimage(__dsub_rn(__dsub_rn(posc[d], off), __dmul_rn(0.5, h[d])), invL[d], L[d]);
-      int jb = cellidx(r, invd[d], m[d]);
-      st.j0[d] = (jb - 1 + m[d]) % m[d];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        int j = (st.j0[d] + k) % m[d];
-        double node = ((double)j + 0.5) * h[d] - 0.5 * L[d] + off;
-        double rr = minimage(posw[d] - node, invL[d], L[d]);
-        st.w[d][k] = delta4f((float)(rr * invd[d]));
-      }
-    }
-  }
-}
-
-// Node k (0..n-1) of the stencil in dimension d alone: grid index j and its
-// weight (the same arithmetic as make_stencil for that dimension).
+// the weight (they differ only in the reference's RFD quirk).
 __device__ __forceinline__ void stencil_node(const Params& P, int d, int comp, double posc,
                                              double posw, int k, int& j, float& w) {
   const int m = d == 0 ? P.mx : (d == 1 ? P.my : P.mz);
@@ -210,14 +181,14 @@ __device__ __forceinline__ void stencil_node(const Params& P, int d, int comp, d
   if (P.kernel == 3) {
     double r = minimage(__dsub_rn(posc, off), invL, L);
     int jc = cellidx(r, invd, m);
-    j = (jc - 1 + k + m) % m;
+    j = wrap_add(jc, k - 1, m);
     double node = ((double)j + 0.5) * h - 0.5 * L;
     double rr = minimage((posw - node) - off, invL, L);
     w = delta3f((float)(rr * invd));
   } else {
     double r = minimage(__dsub_rn(__dsub_rn(posc, off), __dmul_rn(0.5, h)), invL, L);
     int jb = cellidx(r, invd, m);
-    j = (jb - 1 + k + m) % m;
+    j = wrap_add(jb, k - 1, m);
     double node = ((double)j + 0.5) * h - 0.5 * L + off;
     double rr = minimage(posw - node, invL, L);
     w = delta4f((float)(rr * invd));
@@ -256,8 +227,11 @@ __device__ __forceinline__ WarpStencil warp_stencil(const Params& P, const doubl
   if (lane < 6 * n) {
     int k = lane % n, fd = lane / n;
     int f = fd / 3, d = fd - 3 * f;
+    // selects, not posc[d]: a runtime index would put the arrays on the stack
+    const double pc = d == 0 ? posc[0] : (d == 1 ? posc[1] : posc[2]);
+    const double pw = d == 0 ? posw[0] : (d == 1 ? posw[1] : posw[2]);
     // family f = 1 is the face family of dimension d: use comp = d
-    stencil_node(P, d, f == 1 ? d : (d + 1) % 3, posc[d], posw[d], k, s.j, s.w);
+    stencil_node(P, d, f == 1 ? d : (d + 1) % 3, pc, pw, k, s.j, s.w);
   }
   return s;
 }

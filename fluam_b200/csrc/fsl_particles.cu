@@ -263,7 +263,7 @@ __device__ __forceinline__ void bond_force(double rx, double ry, double rz, doub
 // are read from the positions wrapped and stored in cell order by the cell
 // list build.  The partial forces are summed in a fixed butterfly order.
 template <bool ONE>
-__global__ void __launch_bounds__(kPartThreads) k_forces(FSL_KARGS, int which) {
+__global__ void __launch_bounds__(kPartThreads, 4) k_forces(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T8);
   __shared__ int s_pre[kPartThreads / 8][28];
   __shared__ int s_st[kPartThreads / 8][27];
@@ -297,7 +297,10 @@ __global__ void __launch_bounds__(kPartThreads) k_forces(FSL_KARGS, int which) {
     const double* __restrict__ ws = R.ws;  // wrapped, cell order
     const double wx = active ? ws[ig] : 0.0, wy = active ? ws[np + ig] : 0.0,
                  wz = active ? ws[2 * np + ig] : 0.0;
-    const int c = active ? R.cell_of[i] : 0;
+    // the cell of the wrapped position, the arithmetic of k_cell_count (no
+    // dependence on the load of i)
+    const int c = cellidx(wx, P.invdnx, P.mnx) + cellidx(wy, P.invdny, P.mny) * P.mnx +
+                  cellidx(wz, P.invdnz, P.mnz) * P.mnx * P.mny;
     const int cxy = c % (P.mnx * P.mny);
     const int cz = c / (P.mnx * P.mny), cy = cxy / P.mnx, cx = cxy - cy * P.mnx;
     // this lane's cells nn = sub + 8 m, in z-major order
@@ -379,10 +382,34 @@ void launch_forces(const Batch& B, int which, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------- spreading ---
-// One warp per entry (all three components of one spread of one particle);
-// lane l takes stencil nodes l, l+32, ... (x fastest, so a warp's atomics
-// fall on a few 32-byte sectors) and adds w * value in 64-bit fixed point
-// (in the float-atomic form: w * value as an FP32 atomic).
+// Node of a lane in the per-component node loops: the warp takes the n^3
+// nodes (a, b, c) of one component's stencil at a time, lane l fixed to
+// a = l mod n, b = (l / n) mod n, c = l / n^2 (n = 4: 64 nodes in two passes,
+// the second at c + 2; n = 3: lanes 27-31 idle).  x is fastest, so a pass's
+// accesses fall on few 32-byte sectors.
+template <int KN>
+struct LaneNode {
+  static constexpr int passes = KN == 4 ? 2 : 1;
+  int a, b, c0;
+  bool on;
+  __device__ __forceinline__ explicit LaneNode(int lane) {
+    if constexpr (KN == 4) {
+      a = lane & 3;
+      b = (lane >> 2) & 3;
+      c0 = lane >> 4;
+      on = true;
+    } else {
+      a = lane % 3;
+      b = (lane / 3) % 3;
+      c0 = lane < 27 ? lane / 9 : 0;  // idle lanes read a valid node
+      on = lane < 27;
+    }
+  }
+};
+
+// One warp per entry (all three components of one spread of one particle):
+// every lane adds w * value of its nodes in 64-bit fixed point (in the
+// float-atomic form: w * value as an FP32 atomic).
 // Replaces the slot writes of kernelSpreadParticlesForceStokesLimit and
 // kernelSpreadParticlesDrift + the gather of addSpreadedForcesStokesLimit
 // (src/stokesLimitFunctions.cu:659-1681, 1705-2255); the 1/dV of the gather
@@ -392,34 +419,36 @@ __device__ __forceinline__ void spread_entry(const Params& P, const double posc[
                                              const double posw[3], const double val[3],
                                              unsigned long long* __restrict__ grid, int lane,
                                              bool& sat) {
-  constexpr int n = KN, n3 = n * n * n, total = 3 * n3;
   const WarpStencil st = warp_stencil(P, posc, posw, lane);
-  constexpr int iters = (total + 31) >> 5;
+  const LaneNode<KN> ln(lane);
+  const bool fatom = P.prec == PREC_FLOAT;
 #pragma unroll
-  for (int it = 0; it < iters; ++it) {
-    const int id = (it << 5) + lane;
-    const bool valid = id < total;
-    const int idc = valid ? id : 0;  // every lane takes part in the shuffles
-    const int comp = idc / n3, r = idc - comp * n3;
-    const int a = r % n, b = (r / n) % n, c = r / (n * n);
-    int x, y, z;
-    float wx, wy, wz;
-    stencil_get(st, n, comp, 0, a, x, wx);
-    stencil_get(st, n, comp, 1, b, y, wy);
-    stencil_get(st, n, comp, 2, c, z, wz);
-    if (!valid) continue;
-    const double vc = comp == 0 ? val[0] : (comp == 1 ? val[1] : val[2]);
-    const size_t at = (size_t)comp * P.nc + x + (size_t)P.mx * (y + (size_t)P.my * z);
-    if (P.prec == PREC_FLOAT) {
-      // float-atomic form: the first 3 nc floats of the spread buffer
-      const float fv = (float)((double)(wx * (wy * wz)) * vc);
-      if (fv != 0.0f) atomicAdd(reinterpret_cast<float*>(grid) + at, fv);
-      continue;
+  for (int comp = 0; comp < 3; ++comp) {
+    int x, y;
+    float wx, wy;
+    stencil_get(st, KN, comp, 0, ln.a, x, wx);
+    stencil_get(st, KN, comp, 1, ln.b, y, wy);
+    const double vc = val[comp];
+    unsigned long long* gc = grid + (size_t)comp * P.nc;
+#pragma unroll
+    for (int h = 0; h < LaneNode<KN>::passes; ++h) {
+      int z;
+      float wz;
+      stencil_get(st, KN, comp, 2, ln.c0 + 2 * h, z, wz);
+      if (!ln.on) continue;
+      const int at = x + P.mx * (y + P.my * z);  // < nc <= 2^30
+      const float w = wx * (wy * wz);
+      if (fatom) {
+        // float-atomic form: the first 3 nc floats of the spread buffer
+        const float fv = (float)((double)w * vc);
+        if (fv != 0.0f) atomicAdd(reinterpret_cast<float*>(grid) + (size_t)comp * P.nc + at, fv);
+        continue;
+      }
+      const double v = (double)w * (vc * kFixedScale);
+      sat |= !(fabs(v) < kFixedMax);
+      const long long iv = sat ? 0ll : __double2ll_rn(v);
+      if (iv != 0) atomicAdd(gc + at, (unsigned long long)iv);
     }
-    double v = (double)(wx * (wy * wz)) * (vc * kFixedScale);
-    sat |= !(fabs(v) < kFixedMax);
-    long long iv = sat ? 0ll : __double2ll_rn(v);
-    if (iv != 0) atomicAdd(grid + at, (unsigned long long)iv);
   }
 }
 
@@ -467,7 +496,9 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
       bool same = true;
       if (lane < 6) {
         int f = lane / 3, d = lane - 3 * f;
-        same = stencil_base(P, d, f, pp[d]) == stencil_base(P, d, f, pm[d]);
+        const double a = d == 0 ? pp[0] : (d == 1 ? pp[1] : pp[2]);
+        const double b = d == 0 ? pm[0] : (d == 1 ? pm[1] : pm[2]);
+        same = stencil_base(P, d, f, a) == stencil_base(P, d, f, b);
       }
       if (__all_sync(0xffffffffu, same)) return;
       spread_entry<KN>(P, pp, pos, vp, R.grid, lane, sat);
@@ -491,7 +522,7 @@ void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s) {
 }
 
 // -------------------------------------------------------- interpolation ---
-// One warp per particle: lane l reads nodes l, l+32, ... of the three
+// One warp per particle: every lane reads its nodes (LaneNode) of the three
 // components' stencils and the warp sums w v per component in a fixed
 // butterfly order (src/stokesLimitFunctions.cu:2616-2642).  Every lane gets
 // the three sums.
@@ -499,49 +530,49 @@ template <int KN>
 __device__ __forceinline__ void interp_particle(const Params& P, const double pos[3],
                                                 const float* __restrict__ v, int lane,
                                                 float u[3]) {
-  constexpr int n = KN, n3 = n * n * n, total = 3 * n3;
-  constexpr int iters = (total + 31) >> 5;
+  constexpr int NH = LaneNode<KN>::passes;
   const WarpStencil st = warp_stencil(P, pos, pos, lane);
+  const LaneNode<KN> ln(lane);
   // every node's address and weight first, then all loads at once
-  float wt[iters];
-  const float* ad[iters];
+  float wt[3][NH];
+  const float* ad[3][NH];
 #pragma unroll
-  for (int it = 0; it < iters; ++it) {
-    const int id = (it << 5) + lane;
-    const bool valid = id < total;
-    const int idc = valid ? id : 0;
-    const int comp = idc / n3, r = idc - comp * n3;
-    const int a = r % n, b = (r / n) % n, c = r / (n * n);
-    int x, y, z;
-    float wx, wy, wz;
-    stencil_get(st, n, comp, 0, a, x, wx);
-    stencil_get(st, n, comp, 1, b, y, wy);
-    stencil_get(st, n, comp, 2, c, z, wz);
-    wt[it] = valid ? wx * (wy * wz) : 0.0f;
-    ad[it] = v + (size_t)comp * P.nc + x + (size_t)P.mx * (y + (size_t)P.my * z);
+  for (int comp = 0; comp < 3; ++comp) {
+    int x, y;
+    float wx, wy;
+    stencil_get(st, KN, comp, 0, ln.a, x, wx);
+    stencil_get(st, KN, comp, 1, ln.b, y, wy);
+    const float* vc = v + (size_t)comp * P.nc;
+#pragma unroll
+    for (int h = 0; h < NH; ++h) {
+      int z;
+      float wz;
+      stencil_get(st, KN, comp, 2, ln.c0 + 2 * h, z, wz);
+      wt[comp][h] = ln.on ? wx * (wy * wz) : 0.0f;
+      ad[comp][h] = vc + (x + P.mx * (y + P.my * z));
+    }
   }
-  float val[iters];
+  float val[3][NH];
 #pragma unroll
-  for (int it = 0; it < iters; ++it) val[it] = __ldg(ad[it]);
-  float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+  for (int comp = 0; comp < 3; ++comp)
 #pragma unroll
-  for (int it = 0; it < iters; ++it) {
-    const int id = (it << 5) + lane;
-    const int comp = (id < total ? id : 0) / n3;
-    float t = wt[it] * val[it];
-    if (comp == 0) s0 += t;
-    else if (comp == 1) s1 += t;
-    else s2 += t;
+    for (int h = 0; h < NH; ++h) val[comp][h] = __ldg(ad[comp][h]);
+  float s[3];
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    s[comp] = 0.0f;
+#pragma unroll
+    for (int h = 0; h < NH; ++h) s[comp] += wt[comp][h] * val[comp][h];
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    s[0] += __shfl_xor_sync(0xffffffffu, s[0], o);
+    s[1] += __shfl_xor_sync(0xffffffffu, s[1], o);
+    s[2] += __shfl_xor_sync(0xffffffffu, s[2], o);
   }
-  u[0] = s0;
-  u[1] = s1;
-  u[2] = s2;
+  u[0] = s[0];
+  u[1] = s[1];
+  u[2] = s[2];
 }
 
 // stage 1: q^{n+1/2} = q^n + dt/2 J(q^n) v (+ extraMobility terms),
