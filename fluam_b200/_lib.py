@@ -26,6 +26,7 @@ EXPORTS = [
     "fsl_get_status", "fsl_set_step", "fsl_clear_errors", "fsl_set_graph", "fsl_stream",
     "fsl_profile", "fsl_profile_read",
     "fsl_destroy", "fsl_last_error", "fsl_run_data_main", "fsl_parse_data_main",
+    "fsl_write_fluid_final", "fsl_write_fluid_vtk",
     "fsl_neighbor_grid", "fsl_cell_list", "fsl_compute_forces", "fsl_spread", "fsl_solve",
     "fsl_interpolate", "fsl_noise", "fsl_cell_list_noalloc",
     "fsl_batch_create", "fsl_batch_load_bonds", "fsl_batch_step", "fsl_batch_sync",
@@ -140,6 +141,9 @@ def load(path=None):
     L.fsl_destroy.restype = None
     L.fsl_last_error.restype = ctypes.c_char_p
     L.fsl_run_data_main.argtypes = [ctypes.c_char_p]
+    L.fsl_write_fluid_final.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config), ctypes.c_double, _D,
+                                        ctypes.c_int32, _D]
+    L.fsl_write_fluid_vtk.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _D]
     L.fsl_parse_data_main.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config),
                                       ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                       ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]

@@ -38,6 +38,10 @@ struct Run {
   int loadparticles = 0;
   std::string coordinates, outputname, bondfile;
   bool bonded = false;
+  // fluid output: saveFluid, saveVTK, savefreq, densfluid, pressureparameters
+  int save_fluid = 0, save_vtk = 0;
+  int64_t savefreq = 0;
+  double densfluid = 0.0, pressure[3] = {0.0, 0.0, 0.0};
   // scheme flags that select another fluam scheme (src/main.cpp:36-105)
   bool stokesLimit = false, first_order = false;
   std::vector<std::string> other_schemes;
@@ -177,6 +181,18 @@ int parse(const char* path, Run& r, std::string& err) {
         c.nonbonded = (int)I(0);
       } else if (word == "extraMobility") {
         c.extra_mobility = D(0);
+      } else if (word == "saveFluid") {
+        r.save_fluid = (int)I(0);
+      } else if (word == "saveVTK") {
+        r.save_vtk = (int)I(0);
+      } else if (word == "savefreq") {
+        r.savefreq = I(0);
+      } else if (word == "densfluid") {
+        r.densfluid = D(0);
+      } else if (word == "pressureparameters") {
+        r.pressure[0] = D(0);
+        r.pressure[1] = D(1);
+        r.pressure[2] = D(2);
       } else if (word == "setDevice") {
         c.device = (int)I(0);
       } else if (word == "stokesLimit") {
@@ -366,6 +382,47 @@ void write_sample(std::ofstream& f, int64_t np, const std::vector<double>& a, do
   for (int64_t i = 0; i < np; ++i) f << a[i] << " " << a[np + i] << " " << a[2 * np + i] << std::endl;
 }
 
+// ASCII number stream of the legacy VTK layout: "%20.12e " per value, a line
+// break after every ninth value of a run, a break before a new section when
+// the current line is open.
+struct VtkText {
+  FILE* f;
+  int col = 0;
+  void end_line() {
+    std::fputc('\n', f);
+    col = 0;
+  }
+  void section() {
+    if (col != 0) end_line();
+  }
+  void num(double x) {
+    std::fprintf(f, "%20.12e ", x);
+    if ((col++ % 9) == 8) end_line();
+  }
+};
+
+// One snapshot name: <out>.<index>.fluid.vtk (src/saveFluidVTK.cu:40-47)
+std::string vtk_name(const std::string& out, int64_t index) {
+  return out + "." + std::to_string(index) + ".fluid.vtk";
+}
+
+int fluid_outputs(fsl_handle* h, const Run& r, int final_call, int64_t step) {
+  const int mx = r.cfg.mx, my = r.cfg.my, mz = r.cfg.mz;
+  std::vector<double> v(3 * (size_t)mx * my * mz);
+  int rc = fsl_get_velocity_f64(h, v.data());
+  if (rc) return rc;
+  if (!final_call) {
+    return fsl_write_fluid_vtk(vtk_name(r.outputname, step / r.savefreq).c_str(), mx, my, mz, v.data());
+  }
+  if (r.save_fluid) {
+    rc = fsl_write_fluid_final((r.outputname + ".fluidFinalConfiguration").c_str(), &r.cfg,
+                               r.densfluid, r.pressure, 0, v.data());
+    if (rc) return rc;
+  }
+  if (r.save_vtk) rc = fsl_write_fluid_vtk((r.outputname + ".fluid.vtk").c_str(), mx, my, mz, v.data());
+  return rc;
+}
+
 }  // namespace
 
 extern "C" int fsl_parse_data_main(const char* path, fsl_config* cfg, int64_t* numsteps,
@@ -495,10 +552,20 @@ extern "C" int fsl_run_data_main(const char* path) {
       if ((rc = fsl_get_positions(h, pos.data())) || (rc = fsl_get_forces(h, frc.data()))) break;
       write_sample(fp, np, pos, step * r.cfg.dt);
       if (write_forces) write_sample(fv, np, frc, step * r.cfg.dt);
+      // fluid snapshots at sample steps that are multiples of savefreq, as
+      // the reference's other schemes do (src/saveFunctionsSchemeIncompressibleBoundary.cu:43-46)
+      if (r.save_vtk && r.savefreq > 0 && step % r.savefreq == 0 &&
+          (rc = fluid_outputs(h, r, 0, step)))
+        break;
     }
   }
   if (rc) std::cout << "ERROR: " << fsl_last_error() << std::endl;
   if (!rc) rc = fsl_sync(h);
+  // final fluid files (src/saveFunctionsSchemeIncompressibleBoundary.cu:57-59)
+  if (!rc && (r.save_fluid || r.save_vtk)) {
+    rc = fluid_outputs(h, r, 1, step);
+    if (rc) std::cout << "ERROR: " << fsl_last_error() << std::endl;
+  }
   time_t t1 = time(NULL) - t0;
   std::cout << std::endl << "TIME RUN_GPU                       " << t1 << std::endl << std::endl;
   {
@@ -508,4 +575,71 @@ extern "C" int fsl_run_data_main(const char* path) {
   fsl_destroy(h);
   if (!rc) std::cout << "END" << std::endl;
   return rc;
+}
+
+extern "C" int fsl_write_fluid_final(const char* path, const fsl_config* cfg, double density,
+                                     const double* pressure3, int32_t thermostat, const double* v) {
+  if (!path || !cfg || !v) return FSL_E_ARG;
+  std::ofstream f(path);
+  if (!f) return FSL_E_IO;
+  const int64_t nc = (int64_t)cfg->mx * cfg->my * cfg->mz;
+  const double p0 = pressure3 ? pressure3[0] : 0.0, p1 = pressure3 ? pressure3[1] : 0.0,
+               p2 = pressure3 ? pressure3[2] : 0.0;
+  f.precision(15);
+  f << "Number of cells " << nc << std::endl;
+  f << "mx my mz" << std::endl;
+  f << cfg->mx << " " << cfg->my << " " << cfg->mz << std::endl;
+  f << "lx ly lz" << std::endl;
+  f << cfg->lx << " " << cfg->ly << " " << cfg->lz << std::endl;
+  f << "Density " << density << std::endl;
+  f << "Pressure parameters " << p0 << " " << p1 << " " << p2 << std::endl;
+  f << "Thermostat " << thermostat << std::endl;
+  f << "Temperature " << cfg->temperature << std::endl;
+  f << "Cells properties " << std::endl;
+  f << "Density " << std::endl;
+  f << "Velocity" << std::endl;
+  for (int64_t i = 0; i < nc; ++i) {
+    f << density << std::endl;
+    f << v[i] << " " << v[nc + i] << " " << v[2 * nc + i] << std::endl;
+  }
+  return f.good() ? FSL_OK : FSL_E_IO;
+}
+
+extern "C" int fsl_write_fluid_vtk(const char* path, int32_t mx, int32_t my, int32_t mz,
+                                   const double* v) {
+  if (!path || !v || mx < 1 || my < 1 || mz < 1) return FSL_E_ARG;
+  FILE* fp = std::fopen(path, "w");
+  if (!fp) return FSL_E_IO;
+  VtkText t{fp};
+  const int dims[3] = {mx + 1, my + 1, mz + 1};
+  const int64_t nc = (int64_t)mx * my * mz;
+  std::fprintf(fp, "# vtk DataFile Version 2.0\n");
+  std::fprintf(fp, "Written using VisIt writer\n");
+  std::fprintf(fp, "ASCII\n");
+  std::fprintf(fp, "DATASET RECTILINEAR_GRID\n");
+  std::fprintf(fp, "DIMENSIONS %d %d %d\n", dims[0], dims[1], dims[2]);
+  const char* axis[3] = {"X", "Y", "Z"};
+  for (int a = 0; a < 3; ++a) {
+    if (a) t.section();
+    std::fprintf(fp, "%s_COORDINATES %d double\n", axis[a], dims[a]);
+    for (int i = 0; i < dims[a]; ++i) t.num((double)i);
+  }
+  t.section();
+  std::fprintf(fp, "CELL_DATA %lld\n", (long long)nc);
+  std::fprintf(fp, "VECTORS velocity double\n");
+  // cell-centred velocity: the mean of the two faces of each cell along its
+  // component (src/saveFluidVTK.cu:153-175)
+  for (int64_t i = 0; i < nc; ++i) {
+    const int x = (int)(i % mx), y = (int)((i / mx) % my), z = (int)(i / ((int64_t)mx * my));
+    const int64_t ixm = (x == 0 ? mx - 1 : x - 1) + (int64_t)mx * (y + (int64_t)my * z);
+    const int64_t iym = x + (int64_t)mx * ((y == 0 ? my - 1 : y - 1) + (int64_t)my * z);
+    const int64_t izm = x + (int64_t)mx * (y + (int64_t)my * (z == 0 ? mz - 1 : z - 1));
+    t.num(0.5 * (v[ixm] + v[i]));
+    t.num(0.5 * (v[nc + iym] + v[nc + i]));
+    t.num(0.5 * (v[2 * nc + izm] + v[2 * nc + i]));
+  }
+  t.end_line();
+  t.end_line();
+  const bool ok = std::ferror(fp) == 0;
+  return (std::fclose(fp) == 0 && ok) ? FSL_OK : FSL_E_IO;
 }

@@ -171,6 +171,20 @@ int fsl_run_data_main(const char* path);
 int fsl_parse_data_main(const char* path, fsl_config* cfg, int64_t* numsteps,
                         int64_t* samplefreq, int64_t* relax, int64_t* np);
 
+/* ---- fluid output (opt-in; the reference's Stokes path writes none) ------
+ * v is the staggered fluid velocity [3][mz][my][mx] (x fastest), e.g. from
+ * fsl_get_velocity_f64.  The drop-in driver calls these for the reference's
+ * keywords saveFluid 1 and saveVTK 1 (with savefreq). */
+/* <out>.fluidFinalConfiguration in the text format of
+ * saveFluidFinalConfiguration (src/saveFluidFinalConfiguration.cu:30-75):
+ * header, then per cell the density and the staggered velocity. */
+int fsl_write_fluid_final(const char* path, const fsl_config* cfg, double density,
+                          const double* pressure3, int32_t thermostat, const double* v);
+/* Legacy ASCII VTK rectilinear grid of (mx+1) x (my+1) x (mz+1) nodes with the
+ * cell-centred velocity as CELL_DATA, in the layout of the reference's VTK
+ * writer (src/saveFluidVTK.cu:33-250 via src/visit_writer.c:321-460,899-1015). */
+int fsl_write_fluid_vtk(const char* path, int32_t mx, int32_t my, int32_t mz, const double* v);
+
 /* ---- component entry points (one stage of the step each) --------------- */
 /* Non-bonded cell list at the current positions: cell of each particle, the
  * start offset of every neighbour-grid cell (mN+1 entries) and the particle

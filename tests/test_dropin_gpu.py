@@ -168,3 +168,47 @@ def test_errors_are_reported(tmp_path):
     p.write_text("incompressible\ncells 8 8 8\nsamplefreq 1\noutputname x\n")
     r = subprocess.run([FLUAM, str(p)], capture_output=True, text=True, cwd=tmp_path)
     assert r.returncode == 0 and "stokesLimit" in r.stdout
+
+
+def test_fluid_output_files(tmp_path, fsl):
+    """saveFluid 1 / saveVTK 1 / savefreq: <out>.fluidFinalConfiguration,
+    snapshots <out>.<step/savefreq>.fluid.vtk at sample steps and the final
+    <out>.fluid.vtk, holding the velocity field of the last solve."""
+    out = tmp_path / "run"
+    text = f"""stokesLimit
+particles 1
+numberparticles 27
+cutoff 1.5
+pairPotential soft
+densfluid 1
+shearviscosity 1
+temperature 0.01
+cells 16 16 16
+celldimension 16 16 16
+seed 3
+numsteps 4
+samplefreq 2
+savefreq 2
+saveFluid 1
+saveVTK 1
+dt 0.01
+outputname {out}
+"""
+    run_fluam(tmp_path, text)
+    for name in ("run.1.fluid.vtk", "run.2.fluid.vtk", "run.fluid.vtk", "run.fluidFinalConfiguration"):
+        assert (tmp_path / name).exists(), name
+    lines = (tmp_path / "run.fluidFinalConfiguration").read_text().split("\n")
+    assert lines[0] == "Number of cells 4096" and lines[2] == "16 16 16"
+    v_file = np.array([lines[13 + 2 * i].split() for i in range(4096)], dtype=float).T
+    # the same run through the API: same seed, same steps, same bits
+    c, run = fsl.parse_data_main(tmp_path / "data.main")
+    g3 = (np.arange(3) + 0.5) * (16.0 / 3) - 16.0 / 2  # src/simpleCubic.cpp arithmetic
+    q0 = np.stack(np.meshgrid(g3, g3, g3, indexing="ij"))[::-1].reshape(3, -1)
+    sim = fsl.StokesLimit(c, q0)
+    sim.step(4)
+    v_api = sim.velocity64().reshape(3, -1)
+    sim.close()
+    assert np.allclose(v_file, v_api, rtol=1e-13, atol=1e-300)
+    vtk = (tmp_path / "run.fluid.vtk").read_text()
+    assert vtk.startswith("# vtk DataFile Version 2.0\nWritten using VisIt writer\nASCII\n")
+    assert "DIMENSIONS 17 17 17" in vtk and "CELL_DATA 4096" in vtk
