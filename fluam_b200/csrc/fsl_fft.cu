@@ -803,8 +803,13 @@ static void pick_register_kernels(const Params& P, FftPlan* fp) {
       case 16: pick_plane_r<16, 16, 1, 16>(fp); break;
       case 24: pick_plane_r<24, 24, 1, 16>(fp); break;
       case 32: pick_plane_r<32, 16, 2, 4>(fp); break;
+      case 40: pick_plane_r<40, 8, 5, 4>(fp); break;
       case 48: pick_plane_r<48, 12, 4, 2>(fp); break;
+      case 56: pick_plane_r<56, 8, 7, 2>(fp); break;
       case 64: pick_plane_r<64, 16, 4, 2>(fp); break;
+      case 72: pick_plane_r<72, 12, 6, 1>(fp); break;
+      case 80: pick_plane_r<80, 20, 4, 1>(fp); break;
+      case 88: pick_plane_r<88, 8, 11, 1>(fp); break;
       case 96: pick_plane_r<96, 24, 4, 1>(fp); break;
       case 128: pick_plane_r<128, 16, 8, 1>(fp); break;
       default: break;
@@ -814,8 +819,13 @@ static void pick_register_kernels(const Params& P, FftPlan* fp) {
     case 16: pick_z_r<16, 16, 1, 9, 8>(fp); break;
     case 24: pick_z_r<24, 24, 1, 13, 8>(fp); break;
     case 32: pick_z_r<32, 16, 2, 17, 4>(fp); break;
+    case 40: pick_z_r<40, 8, 5, 21, 2>(fp); break;
     case 48: pick_z_r<48, 12, 4, 25, 1>(fp); break;
+    case 56: pick_z_r<56, 8, 7, 29, 1>(fp); break;
     case 64: pick_z_r<64, 16, 4, 33, 1>(fp); break;
+    case 72: pick_z_r<72, 12, 6, 19, 1>(fp); break;
+    case 80: pick_z_r<80, 20, 4, 21, 1>(fp); break;
+    case 88: pick_z_r<88, 8, 11, 9, 1>(fp); break;
     case 96: pick_z_r<96, 24, 4, 25, 1>(fp); break;
     case 128: pick_z_r<128, 16, 8, 13, 1>(fp); break;
     case 256: pick_z_r<256, 16, 16, 8, 1>(fp); break;
@@ -887,9 +897,9 @@ FftPlan* fft_plan_create(const Params& P) {
   cudaMemcpyToSymbol(c_w7, w7, sizeof(w7));
   cudaMemcpyToSymbol(c_w11, w11, sizeof(w11));
   {
-    static float2 rwt[33][32];
-    for (int R = 1; R <= 32; ++R)
-      for (int j = 0; j < 32; ++j)
+    static float2 rwt[kMaxRegR + 1][kMaxRegR];
+    for (int R = 1; R <= kMaxRegR; ++R)
+      for (int j = 0; j < kMaxRegR; ++j)
         rwt[R][j] = make_float2((float)cos(2 * M_PI * j / R), (float)-sin(2 * M_PI * j / R));
     cudaMemcpyToSymbol(c_rw, rwt, sizeof(rwt));
   }

@@ -13,8 +13,9 @@
 // mixed-radix (4, 2, 3) splits unrolled at compile time; their twiddles come
 // from a constant table read at warp-uniform addresses.
 
-// c_rw[R][j] = exp(-2 pi i j / R) for R <= 32 (filled by fft_plan_create)
-__constant__ float2 c_rw[33][32];
+// c_rw[R][j] = exp(-2 pi i j / R) for R <= kMaxRegR (filled by fft_plan_create)
+constexpr int kMaxRegR = 44;
+__constant__ float2 c_rw[kMaxRegR + 1][kMaxRegR];
 
 template <int R>
 __device__ __forceinline__ float2 rw(int j, int dir) {
@@ -29,7 +30,13 @@ template <int R>
 struct RDft {
   __device__ __forceinline__ static void run(float2 (&v)[R], int dir) {
     // R = P Q with the small radix P first: x = q + Q p, f = g + P h
-    constexpr int P = (R % 4 == 0) ? 4 : ((R % 2 == 0) ? 2 : 3);
+    constexpr int P = (R % 4 == 0) ? 4
+                      : (R % 2 == 0) ? 2
+                      : (R % 3 == 0) ? 3
+                      : (R % 5 == 0) ? 5
+                      : (R % 7 == 0) ? 7
+                                     : 11;
+    static_assert(R % P == 0 && R <= kMaxRegR, "register DFT sizes: 2,3,5,7,11-smooth, <= kMaxRegR");
     constexpr int Q = R / P;
     float2 Y[P][Q];
 #pragma unroll
@@ -65,6 +72,18 @@ template <>
 struct RDft<4> {
   __device__ __forceinline__ static void run(float2 (&v)[4], int dir) { dft<4>(v, dir); }
 };
+template <>
+struct RDft<5> {
+  __device__ __forceinline__ static void run(float2 (&v)[5], int dir) { dft<5>(v, dir); }
+};
+template <>
+struct RDft<7> {
+  __device__ __forceinline__ static void run(float2 (&v)[7], int dir) { dft<7>(v, dir); }
+};
+template <>
+struct RDft<11> {
+  __device__ __forceinline__ static void run(float2 (&v)[11], int dir) { dft<11>(v, dir); }
+};
 
 // Exchange layout of one line: Y_t[a] at [a (T + 1) + t]; the line pitch is
 // odd so that neighbouring lines fall on other banks.
@@ -74,8 +93,22 @@ struct LineGeom {
   static constexpr int XP = T + 1;                    // pitch of one a-row
   static constexpr int EX = (T > 1 ? R * XP : N) | 1;  // exchange floats2 per line
   static constexpr int LS = (EX > N + 1 ? EX : (N + 1)) | 1;  // line pitch (>= N + 1)
-  static constexpr int RT = R / T;                    // a values per thread after the exchange
+  // after the exchange thread t takes RT values of a: a = t RT + j when T
+  // divides R, else a = t + T j (j < RT, a < R)
+  static constexpr bool EVEN = R % T == 0;
+  static constexpr int RT = (R + T - 1) / T;
 };
+
+template <int R, int T>
+__device__ __forceinline__ int line_a(int t, int j) {
+  return LineGeom<R, T>::EVEN ? t * LineGeom<R, T>::RT + j : t + T * j;
+}
+
+// whether slot j of thread t holds a value
+template <int R, int T>
+__device__ __forceinline__ bool line_has(int t, int j) {
+  return LineGeom<R, T>::EVEN || line_a<R, T>(t, j) < R;
+}
 
 // Shared memory of one plane in the plane kernels (float2): the line buffer
 // of H lines or the row-major half plane of N rows, whichever is larger.
@@ -105,15 +138,20 @@ __device__ __forceinline__ void line_fft_a(float2 (&v)[R], int t, float2* ex,
   }
 }
 
-// Step 3 after a barrier: thread t takes a = t RT + j (j < RT) and all T
-// values of t; out[j][b] = X[a + R b].
+// Step 3 after a barrier: thread t takes its a values (line_a, j < RT) and
+// all T values of each; out[j][b] = X[a + R b] (zero where line_has fails).
 template <int R, int T>
 __device__ __forceinline__ void line_fft_b(const float2* ex, int t, int dir,
                                            float2 (&out)[LineGeom<R, T>::RT][T]) {
   using G = LineGeom<R, T>;
 #pragma unroll
   for (int j = 0; j < G::RT; ++j) {
-    const int a = t * G::RT + j;
+    const int a = line_a<R, T>(t, j);
+    if (!line_has<R, T>(t, j)) {
+#pragma unroll
+      for (int tt = 0; tt < T; ++tt) out[j][tt] = make_float2(0.f, 0.f);
+      continue;
+    }
 #pragma unroll
     for (int tt = 0; tt < T; ++tt) out[j][tt] = ex[a * G::XP + tt];
     RDft<T>::run(out[j], dir);
@@ -123,7 +161,7 @@ __device__ __forceinline__ void line_fft_b(const float2* ex, int t, int dir,
 // frequency of out[j][b] (or of v[j * T + b] when T == 1)
 template <int R, int T>
 __device__ __forceinline__ int line_freq(int t, int j, int b) {
-  return t * LineGeom<R, T>::RT + j + R * b;
+  return line_a<R, T>(t, j) + R * b;
 }
 
 // Real-to-complex transform of whole xy planes (x then y), PB planes per
@@ -174,8 +212,9 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < G::RT; ++j)
+      if (line_has<RR, T>(t, j))
 #pragma unroll
-      for (int b = 0; b < T; ++b) buf[p * LS + line_freq<RR, T>(t, j, b)] = out[j][b];
+        for (int b = 0; b < T; ++b) buf[p * LS + line_freq<RR, T>(t, j, b)] = out[j][b];
   }
   __syncthreads();
   // y pass: column c, thread t (c fastest, so the stores coalesce)
@@ -217,23 +256,26 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
     if (live && c != 0) {
 #pragma unroll
       for (int j = 0; j < G::RT; ++j)
+        if (line_has<RR, T>(t, j))
 #pragma unroll
-        for (int b = 0; b < T; ++b) out_g[(size_t)line_freq<RR, T>(t, j, b) * (H + 1) + c] = out[j][b];
+          for (int b = 0; b < T; ++b) out_g[(size_t)line_freq<RR, T>(t, j, b) * (H + 1) + c] = out[j][b];
     }
     __syncthreads();
     // the packed column: C = F0 + i FH, F0 = (C + conj C-)/2, FH = (C - conj C-)/(2i)
     if (c == 0) {
 #pragma unroll
       for (int j = 0; j < G::RT; ++j)
+        if (line_has<RR, T>(t, j))
 #pragma unroll
-        for (int b = 0; b < T; ++b) buf[line_freq<RR, T>(t, j, b)] = out[j][b];
+          for (int b = 0; b < T; ++b) buf[line_freq<RR, T>(t, j, b)] = out[j][b];
     }
     __syncthreads();
     if (c == 0 && live) {
 #pragma unroll
       for (int j = 0; j < G::RT; ++j)
+        if (line_has<RR, T>(t, j))
 #pragma unroll
-        for (int b = 0; b < T; ++b) {
+          for (int b = 0; b < T; ++b) {
           const int f = line_freq<RR, T>(t, j, b);
           const float2 C = out[j][b], Cm = buf[(N - f) % N];
           out_g[(size_t)f * (H + 1)] = make_float2(0.5f * (C.x + Cm.x), 0.5f * (C.y - Cm.y));
@@ -299,8 +341,9 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
       __syncthreads();
 #pragma unroll
       for (int j = 0; j < G::RT; ++j)
+        if (line_has<RR, T>(t, j))
 #pragma unroll
-        for (int b = 0; b < T; ++b) {
+          for (int b = 0; b < T; ++b) {
           const int y = line_freq<RR, T>(t, j, b);
           if (c == 0) {
             buf[y * PR] = make_float2(out[j][b].x, 0.f);
@@ -347,8 +390,9 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < G::RT; ++j)
+      if (line_has<RR, T>(t, j))
 #pragma unroll
-      for (int b = 0; b < T; ++b) {
+        for (int b = 0; b < T; ++b) {
         const int x = line_freq<RR, T>(t, j, b);
         fb[(2 * p) * (N + 1) + x] = out[j][b].x;
         fb[(2 * p + 1) * (N + 1) + x] = out[j][b].y;
@@ -402,8 +446,9 @@ __global__ void __launch_bounds__(3 * KX * KY * T)
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < G::RT; ++j)
+      if (line_has<RR, T>(t, j))
 #pragma unroll
-      for (int b = 0; b < T; ++b) lb[line_freq<RR, T>(t, j, b)] = out[j][b];
+        for (int b = 0; b < T; ++b) lb[line_freq<RR, T>(t, j, b)] = out[j][b];
   }
   __syncthreads();
   // the solve, one thread per (kx, ky, kz) mode
@@ -462,8 +507,9 @@ __global__ void __launch_bounds__(3 * KX * KY * T)
     if (live) {
 #pragma unroll
       for (int j = 0; j < G::RT; ++j)
+        if (line_has<RR, T>(t, j))
 #pragma unroll
-        for (int b = 0; b < T; ++b) col[(size_t)line_freq<RR, T>(t, j, b) * zstride] = out[j][b];
+          for (int b = 0; b < T; ++b) col[(size_t)line_freq<RR, T>(t, j, b) * zstride] = out[j][b];
     }
   }
 }

@@ -305,6 +305,9 @@ int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, c
   FSL_TRY(cudaMemsetAsync(r.bpp_off, 0, sizeof(int) * cap, st));
   FSL_TRY(cudaMemsetAsync(r.bfp_cnt, 0, sizeof(int) * cap, st));
   FSL_TRY(cudaMemsetAsync(r.bfp_off, 0, sizeof(int) * cap, st));
+  // the step's cell-list builds rely on cleared counters
+  FSL_TRY(cudaMemsetAsync(r.cnt, 0, sizeof(int) * (size_t)P.mN, st));
+  FSL_TRY(cudaMemsetAsync(r.fill, 0, sizeof(int) * (size_t)P.mN, st));
   FSL_TRY(cudaMemsetAsync(r.grid, 0, sizeof(unsigned long long) * 3 * (size_t)P.nc, st));
   if (P.prec == PREC_F64)
     FSL_TRY(cudaMemsetAsync(r.v64, 0, sizeof(double) * 3 * (size_t)P.nc, st));
@@ -507,7 +510,7 @@ void group_enqueue_step(Group& g) {
   };
   auto cells_forces = [&](int which) {
     pr.mark(s, "cells");
-    launch_cells(B, which, s);
+    launch_cells(B, which, s, false);
     chk("cells");
     pr.mark(s, "forces");
     launch_forces(B, which, s);

@@ -428,8 +428,10 @@ inline unsigned part_blocks(const Batch& B, int k) {
 void launch_noise(const Batch& B, cudaStream_t s);
 void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t count, float* out,
                         cudaStream_t s);
-// which = 0: cell list / forces at q, 1: at q^{n+1/2}
-void launch_cells(const Batch& B, int which, cudaStream_t s);
+// which = 0: cell list / forces at q, 1: at q^{n+1/2}.  The build leaves the
+// count and fill arrays cleared; zero_first clears them (and start, for an
+// instance without particles) first, for callers that cannot rely on that.
+void launch_cells(const Batch& B, int which, cudaStream_t s, bool zero_first = true);
 void launch_forces(const Batch& B, int which, cudaStream_t s);
 // drift = 0: spread F at q (cell-list order when ordered != 0);
 // drift = 1: spread F at q^{n+1/2} and the RFD drift at q;

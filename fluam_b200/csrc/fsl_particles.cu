@@ -128,7 +128,8 @@ __device__ __forceinline__ void block_scan(const int (&v)[kScanItems], int& incl
   total = warp_tot[32];
 }
 
-// Block-local exclusive scan of cnt into start, block totals into bsum.
+// Block-local exclusive scan of cnt into start, block totals into bsum.  The
+// counts are cleared behind the read, ready for the next build.
 template <bool ONE>
 __global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS) {
   FSL_REP_AT(blockIdx.y);
@@ -138,6 +139,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS) {
   int v[kScanItems];
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < n) ? R.cnt[base + k] : 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k)
+    if (base + k < n) R.cnt[base + k] = 0;
   int run, sum, total;
   block_scan(v, run, sum, warp_tot, total);
   if (threadIdx.x == 0) R.bsum[blockIdx.x] = total;
@@ -148,33 +152,28 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS) {
   }
 }
 
-// Exclusive scan of the block totals (at most kScanTile of them), in place;
-// also writes the grand total to start[mN].
+// Adds to every tile of start the sum of the block totals of the tiles
+// before it (a block reduction of at most kScanTile totals), and writes the
+// grand total to start[mN].
 template <bool ONE>
-__global__ void __launch_bounds__(kScanThreads) k_scan_top(FSL_KARGS) {
+__global__ void __launch_bounds__(kScanThreads) k_scan_add(FSL_KARGS) {
   FSL_REP_AT(blockIdx.y);
-  __shared__ int warp_tot[33];
-  const int nb = (P.mN + kScanTile - 1) / kScanTile;
-  int base = threadIdx.x * kScanItems;
-  int v[kScanItems];
+  __shared__ int warp_sum[32];
+  const int tile = blockIdx.x;
+  int part = 0;
+  for (int k = threadIdx.x; k < tile; k += blockDim.x) part += R.bsum[k];
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < nb) ? R.bsum[base + k] : 0;
-  int run, sum, total;
-  block_scan(v, run, sum, warp_tot, total);
-  if (threadIdx.x == 0) R.start[P.mN] = total;
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = part;
+  __syncthreads();
+  int prefix = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) prefix += warp_sum[w];
+  const int n = P.mN;
+  const int base = tile * kScanTile + threadIdx.x * kScanItems;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < nb) R.bsum[base + k] = run;
-    run += v[k];
-  }
-}
-
-template <bool ONE>
-__global__ void k_scan_add(FSL_KARGS) {
-  FSL_REP_AT(blockIdx.y);
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.mN) return;
-  R.start[i] += R.bsum[i / kScanTile];
+  for (int k = 0; k < kScanItems; ++k)
+    if (base + k < n) R.start[base + k] += prefix;
+  if (threadIdx.x == 0 && tile == (n + kScanTile - 1) / kScanTile - 1) R.start[n] = prefix + R.bsum[tile];
 }
 
 template <bool ONE>
@@ -198,6 +197,7 @@ __global__ void k_cell_rank(FSL_KARGS) {
   int rank = 0;
   for (int k = s; k < e; ++k) rank += R.tmp[k] < i;
   R.sorted[s + rank] = i;
+  R.fill[c] = 0;  // the scatter's slot counters, cleared for the next build
   if (R.ws) {  // wrapped positions in cell order for the pair loop
     R.ws[s + rank] = R.qw[i];
     R.ws[P.np + s + rank] = R.qw[P.np + i];
@@ -205,18 +205,19 @@ __global__ void k_cell_rank(FSL_KARGS) {
   }
 }
 
-void launch_cells(const Batch& B, int which, cudaStream_t s) {
+void launch_cells(const Batch& B, int which, cudaStream_t s, bool zero_first) {
   const int tb = kPartThreads;
-  unsigned zb = blocks_for(B.mN, tb);
-  if (zb > 1024) zb = 1024;
-  FSL_GO(k_zero_cells, dim3(zb, B.nrep), tb, 0, s, B);
+  if (zero_first) {
+    unsigned zb = blocks_for(B.mN, tb);
+    if (zb > 1024) zb = 1024;
+    FSL_GO(k_zero_cells, dim3(zb, B.nrep), tb, 0, s, B);
+  }
   if (B.max_np == 0) return;
   const unsigned pb = part_blocks(B, KIND_T1);
   FSL_GO(k_cell_count, pb, tb, 0, s, B, which);
-  unsigned nblk = blocks_for(B.mN, kScanTile);
+  const unsigned nblk = blocks_for(B.mN, kScanTile);
   FSL_GO(k_scan_local, dim3(nblk, B.nrep), kScanThreads, 0, s, B);
-  FSL_GO(k_scan_top, dim3(1, B.nrep), kScanThreads, 0, s, B);
-  FSL_GO(k_scan_add, dim3(blocks_for(B.mN, 256), B.nrep), 256, 0, s, B);
+  FSL_GO(k_scan_add, dim3(nblk, B.nrep), kScanThreads, 0, s, B);
   FSL_GO(k_cell_scatter, pb, tb, 0, s, B);
   FSL_GO(k_cell_rank, pb, tb, 0, s, B);
 }

@@ -45,7 +45,17 @@ struct SGroup {
   std::vector<std::unique_ptr<fsl::Slot>> slots;
   std::vector<Request*> owner;  // per slot; nullptr = free
   int busy = 0;
+  int idle_rounds = 0;  // rounds since a slot of this class was last busy
 };
+
+// Rounds a class without busy slots stays in the stepped set: a class that
+// comes and goes costs a graph capture each time, a class that stays costs
+// its (empty) launches every step.
+constexpr int kKeepIdleRounds = 4;
+// Longest round while no request waits for admission, in units of
+// max_round_steps (fewer host round trips; a new arrival waits at most one
+// round).
+constexpr int kQuietRoundFactor = 4;
 
 // particle capacity of a new slot: the next power of two, at least 64
 int capacity_for(int64_t np) {
@@ -234,15 +244,24 @@ void scheduler(fsl_server* s) {
       }
     }
     if (running.empty()) continue;
-    // one round: every class that holds slots (an idle class's kernels
-    // return at once, which costs far less than capturing a new graph each
-    // time the set of busy classes changes), as many steps as the nearest
-    // completion
+    // one round: the classes with busy slots plus those idle for fewer than
+    // kKeepIdleRounds rounds (an idle class's kernels return at once, which
+    // is cheaper than a new graph capture while classes come and go), as
+    // many steps as the nearest completion, at most max_round_steps (or a
+    // few times that while nothing waits for admission)
     std::vector<fsl::Group*> gl;
-    for (auto& kv : s->groups)
-      if (!kv.second->slots.empty()) gl.push_back(&kv.second->g);
+    for (auto& kv : s->groups) {
+      SGroup& G = *kv.second;
+      G.idle_rounds = G.busy > 0 ? 0 : G.idle_rounds + 1;
+      if (!G.slots.empty() && G.idle_rounds <= kKeepIdleRounds) gl.push_back(&G.g);
+    }
     if (gl != s->exec.groups) s->exec.groups = gl;
-    int64_t n = s->cfg.max_round_steps;
+    bool waiting;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      waiting = !s->queue.empty();
+    }
+    int64_t n = s->cfg.max_round_steps * (waiting ? 1 : kQuietRoundFactor);
     for (Request* r : running) n = std::min(n, r->remaining);
     const double ta = s->now();
     int rc = fsl::exec_step(s->exec, n);

@@ -115,7 +115,10 @@ def test_spread(fsl, oracle, kernel):
 
 @pytest.mark.parametrize("m", [(32, 32, 32), (16, 24, 40), (22, 18, 20), (56, 8, 12), (12, 10, 14),
                                (16, 16, 16), (24, 24, 24), (48, 48, 48), (64, 64, 64), (96, 96, 96),
-                               (128, 128, 128), (32, 32, 256), (64, 64, 24)])
+                               (128, 128, 128), (32, 32, 256), (64, 64, 24),
+                               # register passes with radix 5, 7, 11 and T = 6
+                               (40, 40, 40), (56, 56, 56), (72, 72, 72), (80, 80, 80), (88, 88, 88),
+                               (40, 40, 88), (88, 88, 56)])
 def test_solve(fsl, oracle, m):
     L = tuple(float(x) * 0.75 for x in m)
     q = uniform_positions(4, L, 1)
