@@ -412,10 +412,25 @@ int group_init(Group& g, const Params& P0) {
   g.P0 = P0;
   g.fft = fft_plan_create(P0);
   if (!g.fft) return errorf(FSL_E_ARG, "FFT plan creation failed (sizes or shared memory)");
+  // lowest priority: the block scheduler fills the SMs with the step's own
+  // (latency-bound) kernels first and the noise takes the rest
+  int lo = 0, hi = 0;
+  FSL_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  FSL_TRY(cudaStreamCreateWithPriority(&g.side, cudaStreamNonBlocking, lo));
+  FSL_TRY(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
+  FSL_TRY(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   return FSL_OK;
 }
 
 void group_destroy(Group& g) {
+  if (g.side) {
+    cudaStreamSynchronize(g.side);
+    cudaStreamDestroy(g.side);
+  }
+  if (g.ev_fork) cudaEventDestroy(g.ev_fork);
+  if (g.ev_join) cudaEventDestroy(g.ev_join);
+  g.side = nullptr;
+  g.ev_fork = g.ev_join = nullptr;
   fft_plan_destroy(g.fft);
   g.fft = nullptr;
   if (g.d_reps) cudaFree(g.d_reps);
@@ -519,15 +534,31 @@ void group_enqueue_step(Group& g) {
   };
   g.fail_stage = nullptr;
   chk("before the step");
-  pr.mark(s, "noise");
-  launch_noise(B, s);
+  // the noise of step t has no input but the step counter: it runs on the
+  // side stream beside the cell list and the forces, joined before its
+  // first reader (profiled steps keep one stream so that the stage
+  // intervals stay sequential)
+  const bool fork = !pr.on && g.side;
+  if (fork) {
+    cudaEventRecord(g.ev_fork, s);
+    cudaStreamWaitEvent(g.side, g.ev_fork, 0);
+    launch_noise(B, g.side);
+    cudaEventRecord(g.ev_join, g.side);
+  } else {
+    pr.mark(s, "noise");
+    launch_noise(B, s);
+  }
   chk("noise");
   pr.count(1);
+  auto join_noise = [&]() {
+    if (fork) cudaStreamWaitEvent(s, g.ev_join, 0);
+  };
   if (g.key.scheme == FSL_SCHEME_FIRST_ORDER) {
     // src/runSchemeStokesLimitFirstOrder.cu:163-241: f = S(q^n) F^n + RFD
     // drift, one solve with noise factor 1, predictor, forces at q^{n+1/2}
     // only with extraMobility (k_forces returns at once otherwise), corrector
     cells_forces(0);
+    join_noise();
     pr.mark(s, "spread_rfd");
     launch_spread(B, 2, 1, s);
     chk("spread_rfd");
@@ -559,6 +590,7 @@ void group_enqueue_step(Group& g) {
   launch_spread(B, 0, 1, s);
   chk("spread");
   pr.count(pk);
+  join_noise();
   launch_solve(B, g.fft, 1, 1.41421356237309504880, 0, s, &pr);
   chk("solve");
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
@@ -607,7 +639,10 @@ int group_prof_collect(Group& g) {
 int exec_init(Exec& e, int device) {
   e.device = device;
   FSL_TRY(cudaSetDevice(device));
-  FSL_TRY(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
+  // the step's streams take the highest priority, above the noise streams
+  int lo = 0, hi = 0;
+  FSL_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  FSL_TRY(cudaStreamCreateWithPriority(&e.stream, cudaStreamNonBlocking, hi));
   return FSL_OK;
 }
 
@@ -639,7 +674,9 @@ int exec_prepare(Exec& e) {
   const size_t ng = e.groups.size();
   while (e.side.size() + 1 < ng) {
     cudaStream_t s;
-    FSL_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int lo = 0, hi = 0;
+    FSL_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    FSL_TRY(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, hi));
     e.side.push_back(s);
   }
   while (e.ev.size() < ng + 1) {

@@ -84,6 +84,10 @@ struct Group {
   bool allow_one = true;        // a lone instance may travel by value (its
                                 // changes then need a new graph capture)
   cudaStream_t stream = nullptr;
+  // the noise of a step runs beside the cell list and forces on this stream
+  // (fork and join events); profiled steps keep everything on `stream`
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   Prof prof;
   std::map<std::string, std::pair<int64_t, double>> stage_acc;
   int launches = 0;             // kernels of this group in one step
