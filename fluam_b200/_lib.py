@@ -15,7 +15,7 @@ ERRORS = {-1: "FSL_E_ARG", -2: "FSL_E_CUDA", -3: "FSL_E_NOMEM", -4: "FSL_E_KERNE
           -5: "FSL_E_IO", -6: "FSL_E_INPUT"}
 PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
 RFD_REFERENCE, RFD_PAPER = 0, 1
-SCHEME_MIDPOINT, SCHEME_FIRST_ORDER = 0, 1
+SCHEME_MIDPOINT, SCHEME_FIRST_ORDER, SCHEME_QUASI2D, SCHEME_STOKES2D = 0, 1, 2, 3
 PRECISION_FIXED64, PRECISION_FLOAT_ATOMIC, PRECISION_FP64 = 0, 1, 2
 
 # Every symbol include/fluamsl.h declares.
@@ -53,6 +53,10 @@ class Config(ctypes.Structure):
         ("nonbonded", ctypes.c_int32), ("device", ctypes.c_int32),
         ("scheme", ctypes.c_int32),
         ("precision", ctypes.c_int32),
+        ("ndrift", ctypes.c_int32), ("use_rfd", ctypes.c_int32),
+        ("predictor_corrector", ctypes.c_int32), ("reserved_", ctypes.c_int32),
+        ("radius", ctypes.c_double), ("saffman_kc", ctypes.c_double),
+        ("saffman_width", ctypes.c_double), ("shear_amp", ctypes.c_double),
     ]
 
 

@@ -75,6 +75,10 @@ void fsl_config_defaults(fsl_config* c) {
   c->rfd = FSL_RFD_REFERENCE;
   c->nonbonded = 1;  // src/loadDataMain.cu:206
   c->device = -1;    // src/loadDataMain.cu:181
+  // src/loadDataMain.cu:260-272
+  c->radius = 1.0;
+  c->ndrift = 1;
+  c->use_rfd = 1;
 }
 
 int fsl_create(const fsl_config* cfg, int64_t np, const double* q, fsl_handle** out) {

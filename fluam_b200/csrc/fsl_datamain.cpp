@@ -43,7 +43,7 @@ struct Run {
   int64_t savefreq = 0;
   double densfluid = 0.0, pressure[3] = {0.0, 0.0, 0.0};
   // scheme flags that select another fluam scheme (src/main.cpp:36-105)
-  bool stokesLimit = false, first_order = false;
+  bool stokesLimit = false, first_order = false, quasi2D = false, stokes2D = false;
   std::vector<std::string> other_schemes;
   std::string wordfile;
 };
@@ -235,9 +235,26 @@ int parse(const char* path, Run& r, std::string& err) {
                  word == "incompressible" || word == "incompressibleBinaryMixture" ||
                  word == "incompressibleBinaryMixtureMidPoint" ||
                  word == "quasiNeutrallyBuoyant" || word == "quasiNeutrallyBuoyant2D" ||
-                 word == "quasiNeutrallyBuoyant4pt2D" || word == "quasi2D" ||
-                 word == "stokesLimit2D") {
+                 word == "quasiNeutrallyBuoyant4pt2D") {
         r.other_schemes.push_back(word);
+      } else if (word == "quasi2D") {
+        r.quasi2D = true;
+      } else if (word == "stokesLimit2D") {
+        r.stokes2D = true;
+      } else if (word == "hydrodynamicRadius") {
+        c.radius = D(0);
+      } else if (word == "nDrift") {
+        c.ndrift = (int)I(0);
+      } else if (word == "use_RFD") {
+        c.use_rfd = (int)I(0);
+      } else if (word == "predictorCorrector") {
+        c.predictor_corrector = (int)I(0);
+      } else if (word == "saffmanCutOffWaveNumber") {
+        c.saffman_kc = D(0);
+      } else if (word == "saffmanLayerWidth") {
+        c.saffman_width = D(0);
+      } else if (word == "viscosityMeasureAmplitude") {
+        c.shear_amp = D(0);
       }
     }
     oldword = word;
@@ -253,6 +270,11 @@ int parse(const char* path, Run& r, std::string& err) {
   // the cell centres in both cases, which is what the reference computes when
   // the file holds both keywords.
   if (r.first_order) r.cfg.scheme = FSL_SCHEME_FIRST_ORDER;
+  // quasi2D / stokesLimit2D precede both (src/main.cpp:91-93); with both
+  // keywords the quasi2D branches win (src/createCellsQuasi2DGPU.cu:53-61,
+  // src/runSchemeQuasi2D.cu:186-205)
+  if (r.quasi2D) r.cfg.scheme = FSL_SCHEME_QUASI2D;
+  else if (r.stokes2D) r.cfg.scheme = FSL_SCHEME_STOKES2D;
   return FSL_OK;
 }
 
@@ -274,11 +296,19 @@ bool read_coordinates(const std::string& file, std::vector<double>& q, int64_t& 
   return true;
 }
 
-void simple_cubic(const fsl_config& c, int64_t np, std::vector<double>& q) {
-  // src/simpleCubic.cpp:25-63 (dimension 3)
+void simple_cubic(const fsl_config& c, int64_t np, std::vector<double>& q, int dimension) {
+  // src/simpleCubic.cpp:25-63: a lattice in 3-D, or a single layer in 2-D
+  // (which the filling loop may still stack)
   double lx = c.lx, ly = c.ly, lz = c.lz;
-  double sigma = std::pow(lx * ly * lz / (np), 1. / 3.);
-  int nz = (int(lz / sigma) ? int(lz / sigma) : 1);
+  double sigma;
+  int nz;
+  if (dimension == 3) {
+    sigma = std::pow(lx * ly * lz / (np), 1. / 3.);
+    nz = (int(lz / sigma) ? int(lz / sigma) : 1);
+  } else {
+    sigma = std::sqrt(lx * ly / np);
+    nz = 1;
+  }
   int nx = (int(lx / sigma) ? int(lx / sigma) : 1);
   int ny = (int(ly / sigma) ? int(ly / sigma) : 1);
   while ((int64_t)nx * ny * nz < np) {
@@ -457,7 +487,7 @@ extern "C" int fsl_run_data_main(const char* path) {
     fo << r.wordfile << std::endl;
   }
   std::cout << "READ " << (path ? path : "data.main") << " :                DONE" << std::endl;
-  if (!r.other_schemes.empty() || !(r.stokesLimit || r.first_order)) {
+  if (!r.other_schemes.empty() || !(r.stokesLimit || r.first_order || r.quasi2D || r.stokes2D)) {
     std::cout << "ERROR: this build runs the stokesLimit and stokesLimitFirstOrder schemes only"
               << (r.other_schemes.empty() ? std::string(" (keyword stokesLimit missing)")
                                           : " (found " + r.other_schemes[0] + ")")
@@ -492,7 +522,8 @@ extern "C" int fsl_run_data_main(const char* path) {
       std::cout << "ERROR: numberparticles must be > 0" << std::endl;
       return FSL_E_INPUT;
     }
-    simple_cubic(r.cfg, np, q);
+    // src/createParticles.cpp:53-58
+    simple_cubic(r.cfg, np, q, r.cfg.scheme >= FSL_SCHEME_QUASI2D ? 2 : 3);
   }
   fsl_handle* h = nullptr;
   rc = fsl_create(&r.cfg, np, q.data(), &h);
@@ -522,7 +553,12 @@ extern "C" int fsl_run_data_main(const char* path) {
   }
   time_t t0 = time(NULL);
   // the first-order scheme writes no .velocityParticles (src/saveParticles.cu:43-46)
-  const bool write_forces = r.cfg.scheme != FSL_SCHEME_FIRST_ORDER;
+  // .velocityParticles: the midpoint scheme writes F^{n+1/2}; the first-order
+  // scheme and quasi2D write none; stokesLimit2D writes the particle velocity
+  // array, which that scheme never sets, so zeros (src/saveParticles.cu:43-47,
+  // src/gpuToHostStokesLimit.cu:41-43)
+  const bool q2 = r.cfg.scheme >= FSL_SCHEME_QUASI2D;
+  const bool write_forces = r.cfg.scheme == FSL_SCHEME_MIDPOINT || r.cfg.scheme == FSL_SCHEME_STOKES2D;
   std::ofstream fp(r.outputname + ".particles"), fv;
   if (write_forces) fv.open(r.outputname + ".velocityParticles");
   fp.precision(15);
@@ -530,9 +566,35 @@ extern "C" int fsl_run_data_main(const char* path) {
   fp << "#NUMBER PARTICLES " << np << std::endl;
   if (write_forces) fv << "#NUMBER PARTICLES " << np << std::endl;
   std::vector<double> pos(3 * np), frc(3 * np);
-  // src/runSchemeStokesLimit.cu:83, 163-285
   int64_t step = -r.relax;
-  while (step < r.numsteps) {
+  if (q2) {
+    // src/runSchemeQuasi2D.cu:99-252: a sample at the top of every step with
+    // step >= 0 and step % samplefreq == 0, and one after the last step
+    auto sample = [&]() -> int {
+      std::cout << (r.cfg.scheme == FSL_SCHEME_QUASI2D ? "Quasi 2D " : "stokesLimit 2D ") << step
+                << std::endl;
+      int e = fsl_sync(h);
+      if (e) {
+        std::cout << "ERROR IN KERNEL: " << fsl_last_error() << std::endl;
+        return e;
+      }
+      if ((e = fsl_get_positions(h, pos.data()))) return e;
+      write_sample(fp, np, pos, step * r.cfg.dt);
+      if (write_forces) write_sample(fv, np, std::vector<double>(3 * np, 0.0), step * r.cfg.dt);
+      return FSL_OK;
+    };
+    while (step < r.numsteps && !rc) {
+      if (step >= 0 && step % r.samplefreq == 0 && (rc = sample())) break;
+      int64_t next = step < 0 ? 0 : (step / r.samplefreq + 1) * r.samplefreq;
+      if (next > r.numsteps) next = r.numsteps;
+      rc = fsl_step(h, next - step);
+      if (rc) break;
+      step = next;
+    }
+    if (!rc && step % r.samplefreq == 0) rc = sample();
+  }
+  // src/runSchemeStokesLimit.cu:83, 163-285
+  while (!q2 && step < r.numsteps) {
     // next step index s > step with s % samplefreq == 0 and s > 0, or the end
     int64_t next = r.numsteps;
     int64_t s0 = step + 1;

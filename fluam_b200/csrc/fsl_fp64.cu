@@ -303,10 +303,11 @@ constexpr int kF64Elems = 1024;  // lines x length per block: 2 x 16 KB buffers
 
 // Lines of one block: axis 0 takes nl consecutive rows (contiguous);
 // axes 1 and 2 take nl consecutive x at one (comp, other index), element
-// stride mx or mx my.  to_real: the last inverse pass stores Re / nc to v64.
+// stride mx or mx my; ncomp field components.  to_real: the last inverse
+// pass stores Re / nc to v64.
 template <bool ONE>
 __global__ void __launch_bounds__(kF64Threads) k_fft64(FSL_KARGS, int axis, const Radix64 rad,
-                                                       int dir, int to_real) {
+                                                       int dir, int to_real, int ncomp) {
   FSL_REP_AT(blockIdx.y);
   __shared__ double2 sA[kF64Elems], sB[kF64Elems];
   const int n = rad.n;
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(kF64Threads) k_fft64(FSL_KARGS, int axis, cons
   size_t estride, lstride;
   int nvalid;
   if (axis == 0) {
-    const long nrows = 3L * my * mz;
+    const long nrows = (long)ncomp * my * mz;
     const long r0 = (long)blockIdx.x * nl;
     if (r0 >= nrows) return;
     base = (size_t)r0 * mx;
@@ -328,7 +329,7 @@ __global__ void __launch_bounds__(kF64Threads) k_fft64(FSL_KARGS, int axis, cons
     const int gx = (mx + nl - 1) / nl;
     const int other = axis == 1 ? mz : my;
     const long b = blockIdx.x;
-    if (b >= 3L * other * gx) return;
+    if (b >= (long)ncomp * other * gx) return;
     const int xg = (int)(b % gx);
     const long rest = b / gx;
     const int o = (int)(rest % other), comp = (int)(rest / other);
@@ -501,6 +502,29 @@ void launch_interp_update64(const Batch& B, int stage, cudaStream_t s) {
     FSL_GO_T(k_interp_update64, 3, g, kPartThreads, 0, s, B, stage);
 }
 
+// The line passes of a forward (dir -1: x, y[, z]) or inverse (dir +1:
+// [z,] y, x, the x pass storing Re / nc) transform of ncomp components over
+// the first naxes axes.
+static void fft64_passes(const Batch& B, int ncomp, int naxes, int dir, cudaStream_t s) {
+  const int m[3] = {B.mx, B.my, B.mz};
+  Radix64 rad[3];
+  unsigned gb[3];
+  for (int a = 0; a < naxes; ++a) {
+    rad[a] = radices(m[a]);
+    const int n = m[a];
+    const int nl = kF64Elems / n < 1 ? 1 : (kF64Elems / n > 32 ? 32 : kF64Elems / n);
+    if (a == 0) gb[a] = (unsigned)(((long)ncomp * B.my * B.mz + nl - 1) / nl);
+    else gb[a] = (unsigned)((long)ncomp * (a == 1 ? B.mz : B.my) * ((B.mx + nl - 1) / nl));
+  }
+  if (dir < 0) {
+    for (int a = 0; a < naxes; ++a)
+      FSL_GO(k_fft64, dim3(gb[a], B.nrep), kF64Threads, 0, s, B, a, rad[a], -1, 0, ncomp);
+  } else {
+    for (int a = naxes - 1; a >= 0; --a)
+      FSL_GO(k_fft64, dim3(gb[a], B.nrep), kF64Threads, 0, s, B, a, rad[a], +1, a == 0 ? 1 : 0, ncomp);
+  }
+}
+
 void launch_solve64(const Batch& B, int nsets, double nfac, cudaStream_t s, Prof* prof) {
   const int tb = 256;
   unsigned bc = blocks_for((long)B.nc, tb);
@@ -508,25 +532,15 @@ void launch_solve64(const Batch& B, int nsets, double nfac, cudaStream_t s, Prof
   if (bc > cap) bc = cap < 1 ? 1 : cap;
   if (prof) prof->mark(s, "wbuild64");
   FSL_GO(k_wbuild64, dim3(bc, B.nrep), tb, 0, s, B, nsets, nfac);
-  const int m[3] = {B.mx, B.my, B.mz};
-  Radix64 rad[3];
-  unsigned gb[3];
-  for (int a = 0; a < 3; ++a) {
-    rad[a] = radices(m[a]);
-    const int n = m[a];
-    const int nl = kF64Elems / n < 1 ? 1 : (kF64Elems / n > 32 ? 32 : kF64Elems / n);
-    if (a == 0) gb[a] = (unsigned)((3L * B.my * B.mz + nl - 1) / nl);
-    else gb[a] = (unsigned)(3L * (a == 1 ? B.mz : B.my) * ((B.mx + nl - 1) / nl));
-  }
   if (prof) prof->mark(s, "fft64");
-  for (int a = 0; a < 3; ++a)
-    FSL_GO(k_fft64, dim3(gb[a], B.nrep), kF64Threads, 0, s, B, a, rad[a], -1, 0);
+  fft64_passes(B, 3, 3, -1, s);
   if (prof) prof->mark(s, "solve64");
   FSL_GO(k_solve64, dim3(bc, B.nrep), tb, 0, s, B);
   if (prof) prof->mark(s, "fft64");
-  for (int a = 2; a >= 0; --a)
-    FSL_GO(k_fft64, dim3(gb[a], B.nrep), kF64Threads, 0, s, B, a, rad[a], +1, a == 0 ? 1 : 0);
+  fft64_passes(B, 3, 3, +1, s);
   if (prof) prof->count(1 + 3 + 1 + 3);
 }
+
+void launch_fft64_2d(const Batch& B, int dir, cudaStream_t s) { fft64_passes(B, 2, 2, dir, s); }
 
 }  // namespace fsl

@@ -38,7 +38,7 @@ SlotLayout layout(const Params& P, int np_cap) {
   };
   const size_t np = (size_t)np_cap, nc = (size_t)P.nc;
   const size_t mN = (size_t)P.mN;
-  const uint64_t noise = ((uint64_t)12 * nc + (uint64_t)9 * np + 3) / 4 * 4;
+  const uint64_t noise = (noise_count(P, np_cap) + 3) / 4 * 4;
   L.q = take(sizeof(double) * 3 * np);
   L.qp = take(sizeof(double) * 3 * np);
   L.F = take(sizeof(double) * 3 * np);
@@ -114,9 +114,12 @@ ClassKey class_of(const Params& P) {
 }
 
 int make_params(const fsl_config& c, int64_t np, Params& P) {
-  if (c.mx < 3 || c.my < 3 || c.mz < 3)
+  if (c.scheme < 0 || c.scheme > 3) return errorf(FSL_E_ARG, "unknown scheme %d", c.scheme);
+  const bool two_d = c.scheme >= FSL_SCHEME_QUASI2D;
+  if (two_d && c.mz != 1) return errorf(FSL_E_ARG, "the quasi-2D schemes need cells mx my 1");
+  if (c.mx < 3 || c.my < 3 || (!two_d && c.mz < 3))
     return errorf(FSL_E_ARG, "cells must be >= 3 in every direction");
-  if (!factor_ok(c.mx) || !factor_ok(c.my) || !factor_ok(c.mz))
+  if (!factor_ok(c.mx) || !factor_ok(c.my) || (!two_d && !factor_ok(c.mz)))
     return errorf(FSL_E_ARG, "cells %d %d %d: every extent must factor into 2,3,5,7,11", c.mx, c.my,
                   c.mz);
   if (c.mx > 1024 || c.my > 1024 || c.mz > 1024)
@@ -128,7 +131,6 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   if (c.kernel != 3 && c.kernel != 4) return errorf(FSL_E_ARG, "kernel must be 3 or 4");
   if (c.pair < 0 || c.pair > 2) return errorf(FSL_E_ARG, "unknown pair potential %d", c.pair);
   if (c.rfd < 0 || c.rfd > 1) return errorf(FSL_E_ARG, "unknown rfd mode %d", c.rfd);
-  if (c.scheme < 0 || c.scheme > 1) return errorf(FSL_E_ARG, "unknown scheme %d", c.scheme);
   if (c.precision < 0 || c.precision > 2)
     return errorf(FSL_E_ARG, "unknown precision form %d", c.precision);
   if (c.extra_mobility < 0) return errorf(FSL_E_ARG, "extraMobility must be >= 0");
@@ -168,6 +170,23 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   }
   if ((int64_t)P.mnx * P.mny * P.mnz > ((int64_t)1 << 28))
     return errorf(FSL_E_ARG, "cutoff too small for the box (neighbour grid too large)");
+  if (two_d) {
+    // src/createBoundariesQuasi2DGPU.cu:89-93: int(L / rc) cells per side in
+    // the plane (no lower bound: with fewer than 3 the 9-cell sweep visits a
+    // cell more than once, as the reference does), one layer
+    if (c.cutoff > 0) {
+      P.mnx = (int)(c.lx / c.cutoff);
+      P.mny = (int)(c.ly / c.cutoff);
+    }
+    P.mnz = 1;
+    if (c.nonbonded && np > 0 && (P.mnx < 1 || P.mny < 1))
+      return errorf(FSL_E_ARG, "cutoff larger than the box");
+    // without pair forces the cell list is unused; keep its extents valid
+    P.mnx = std::max(P.mnx, 1);
+    P.mny = std::max(P.mny, 1);
+    if (!(c.radius > 0)) return errorf(FSL_E_ARG, "hydrodynamicRadius must be > 0");
+    if (c.ndrift < 0) return errorf(FSL_E_ARG, "nDrift must be >= 0");
+  }
   P.mN = P.mnx * P.mny * P.mnz;
   if ((int64_t)((P.mN + 4095) / 4096) > 4096) return errorf(FSL_E_ARG, "neighbour grid too large");
   P.invdnx = double(P.mnx) / c.lx;
@@ -195,7 +214,24 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   P.fact4 = std::sqrt((2. * c.temperature * c.shearviscosity) / (P.dV * c.dt));
   P.fact2 = std::sqrt(c.temperature * c.extra_mobility * c.dt);
   P.seed = c.seed;
-  P.noise_n = (uint64_t)12 * P.nc + (uint64_t)9 * P.np;
+  if (two_d) {
+    // src/createCellsQuasi2DGPU.cu:49-79: blob variance by scheme, stencil
+    // half-width int(3 a mx / lx) + 1 (at most mx / 2), stochastic prefactor
+    const double a = c.radius, pi = 3.1415926535897932385;
+    P.q2_var = c.scheme == FSL_SCHEME_QUASI2D ? std::pow(a / std::sqrt(pi), 2)
+                                              : std::pow(a * 0.66556976637237890625, 2);
+    P.q2_kw = (int)(3.0 * a * c.mx / c.lx) + 1;
+    if (P.q2_kw > c.mx / 2) P.q2_kw = c.mx / 2;
+    P.q2_fact1 = std::sqrt(1.0 * c.temperature / (c.shearviscosity * c.dt * c.lx * c.ly)) * (double)P.nc;
+    P.q2_kc = c.saffman_kc;
+    P.q2_lw = c.saffman_width;
+    P.q2_shear = c.shear_amp;
+    P.q2_rfd = c.use_rfd ? 1 : 0;
+    P.q2_pc = c.predictor_corrector ? 1 : 0;
+    P.q2_ndrift = c.ndrift;
+    P.prec = PREC_F64;  // FP64 throughout, as the reference
+  }
+  P.noise_n = noise_count(P, P.np);
   return FSL_OK;
 }
 
@@ -459,7 +495,7 @@ int group_upload(Group& g) {
   B.max_noise_n = 0;
   for (const Slot* s : g.slots) {
     B.max_np = std::max(B.max_np, s->np_cap);
-    B.max_noise_n = std::max<uint64_t>(B.max_noise_n, (uint64_t)12 * B.nc + (uint64_t)9 * s->np_cap);
+    B.max_noise_n = std::max<uint64_t>(B.max_noise_n, noise_count(g.P0, s->np_cap));
   }
   if (n > g.d_cap) {
     if (g.d_reps || g.d_boff) {
@@ -553,6 +589,36 @@ void group_enqueue_step(Group& g) {
   auto join_noise = [&]() {
     if (fork) cudaStreamWaitEvent(s, g.ev_join, 0);
   };
+  if (g.key.scheme >= FSL_SCHEME_QUASI2D) {
+    // src/runSchemeQuasi2D.cu:108-250: 2-D cell list and forces, spread
+    // force and thermal drift, Fourier-space mobility and noise, update
+    pr.mark(s, "cells");
+    launch_cells(B, 0, s, false);
+    chk("cells");
+    pr.mark(s, "forces");
+    launch_q2_forces(B, s);
+    chk("forces");
+    pr.count(pk ? 6 : 1);
+    join_noise();
+    launch_q2_field(B, s, &pr);
+    chk("spread");
+    pr.count(2 + pk);
+    launch_q2_solve(B, s, &pr);
+    chk("solve");
+    pr.count(2 + 1 + 2);
+    pr.mark(s, "q2_update");
+    launch_q2_update(B, 1, s);
+    launch_q2_update(B, 2, s);
+    chk("update");
+    pr.count(2 * pk);
+    pr.mark(s, "counter");
+    launch_step_counter(B, s);
+    chk("counter");
+    pr.count(1);
+    pr.mark(s, nullptr);
+    g.launches = pr.launches;
+    return;
+  }
   if (g.key.scheme == FSL_SCHEME_FIRST_ORDER) {
     // src/runSchemeStokesLimitFirstOrder.cu:163-241: f = S(q^n) F^n + RFD
     // drift, one solve with noise factor 1, predictor, forces at q^{n+1/2}

@@ -45,14 +45,25 @@ struct Params {
   int np;
   int kernel;  // 3 or 4
   int pair, nonbonded, rfd, bonded;
-  int scheme;  // FSL_SCHEME_* (0 midpoint, 1 first order)
+  int scheme;  // FSL_SCHEME_* (0 midpoint, 1 first order, 2 quasi2D, 3 stokesLimit2D)
   int prec;    // FSL_PRECISION_* (0 fixed point, 1 float atomics, 2 FP64)
   int has_extra;
   double cutoff, cutoff2, invcut2, soft_eps;
   double eta, kT, dt, extra_mob, fact1, fact2, fact4;
   uint64_t seed;
-  uint64_t noise_n;  // 12 nc + 9 np
+  uint64_t noise_n;  // 12 nc + 9 np; quasi-2D family 4 (nc + mx + my) + 2 np nDrift
+  // quasi-2D family: Gaussian variance, stencil half-width, stochastic
+  // prefactor, options
+  double q2_var, q2_fact1, q2_kc, q2_lw, q2_shear;
+  int q2_kw, q2_rfd, q2_pc, q2_ndrift;
 };
+
+// noise count of an instance of P with np particles
+__host__ __device__ inline uint64_t noise_count(const Params& P, int np) {
+  if (P.scheme >= 2)
+    return (uint64_t)4 * ((uint64_t)P.nc + P.mx + P.my) + (uint64_t)2 * np * P.q2_ndrift;
+  return (uint64_t)12 * P.nc + (uint64_t)9 * np;
+}
 
 // ---------------------------------------------------------------- Philox ---
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): multipliers
@@ -446,6 +457,13 @@ void launch_noise64(const Batch& B, cudaStream_t s);
 void launch_spread64(const Batch& B, int drift, cudaStream_t s);
 void launch_interp_update64(const Batch& B, int stage, cudaStream_t s);
 void launch_solve64(const Batch& B, int nsets, double nfac, cudaStream_t s, Prof* prof);
+// 2-D transforms of two FP64 components (the quasi-2D family)
+void launch_fft64_2d(const Batch& B, int dir, cudaStream_t s);
+// The quasi-2D family (fsl_q2d.cu)
+void launch_q2_forces(const Batch& B, cudaStream_t s);
+void launch_q2_field(const Batch& B, cudaStream_t s, Prof* prof);
+void launch_q2_solve(const Batch& B, cudaStream_t s, Prof* prof);
+void launch_q2_update(const Batch& B, int stage, cudaStream_t s);
 
 struct FftPlan;  // defined in fsl_fft.cu
 FftPlan* fft_plan_create(const Params& P);

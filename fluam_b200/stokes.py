@@ -13,11 +13,11 @@ import numpy as np
 
 from . import _lib
 from ._lib import (PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE, SCHEME_FIRST_ORDER,
-                   SCHEME_MIDPOINT, check)
+                   SCHEME_MIDPOINT, SCHEME_QUASI2D, SCHEME_STOKES2D, check)
 
 __all__ = ["StokesLimit", "Batch", "Server", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
            "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE", "SCHEME_MIDPOINT",
-           "SCHEME_FIRST_ORDER"]
+           "SCHEME_FIRST_ORDER", "SCHEME_QUASI2D", "SCHEME_STOKES2D"]
 
 
 def _dp(a):
@@ -30,7 +30,8 @@ def _ip(a):
 
 def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair=PAIR_TABLE_LJ,
                 soft_epsilon=1.0, rfd=RFD_REFERENCE, nonbonded=1, extra_mobility=0.0, seed=0,
-                device=-1, scheme=0, precision=0):
+                device=-1, scheme=0, precision=0, radius=1.0, ndrift=1, use_rfd=1,
+                predictor_corrector=0, saffman_kc=0.0, saffman_width=0.0, shear_amp=0.0):
     c = _lib.Config()
     _lib.load().fsl_config_defaults(ctypes.byref(c))
     c.mx, c.my, c.mz = (int(x) for x in cells)
@@ -40,6 +41,9 @@ def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair
     c.nonbonded, c.extra_mobility, c.seed, c.device = nonbonded, extra_mobility, seed, device
     c.scheme = scheme
     c.precision = precision
+    # quasi-2D family (scheme SCHEME_QUASI2D / SCHEME_STOKES2D)
+    c.radius, c.ndrift, c.use_rfd, c.predictor_corrector = radius, ndrift, use_rfd, predictor_corrector
+    c.saffman_kc, c.saffman_width, c.shear_amp = saffman_kc, saffman_width, shear_amp
     return c
 
 

@@ -46,7 +46,12 @@ enum { FSL_RFD_REFERENCE = 0, FSL_RFD_PAPER = 1 };
  * (src/runSchemeStokesLimit.cu:163-285) or the first-order scheme of keyword
  * stokesLimitFirstOrder (src/runSchemeStokesLimitFirstOrder.cu:163-241: one
  * solve per step with the RFD drift, the same predictor and corrector). */
-enum { FSL_SCHEME_MIDPOINT = 0, FSL_SCHEME_FIRST_ORDER = 1 };
+/* The Gaussian-blob schemes of keywords quasi2D (RPY mobility of a blob in
+ * a quasi-2-D geometry) and stokesLimit2D (2-D Stokes, optionally Saffman-
+ * screened) on an mx x my grid (mz = 1): src/runSchemeQuasi2D.cu:20-260 with
+ * src/quasi2DFunctions.cu.  FP64 throughout, as the reference. */
+enum { FSL_SCHEME_MIDPOINT = 0, FSL_SCHEME_FIRST_ORDER = 1, FSL_SCHEME_QUASI2D = 2,
+       FSL_SCHEME_STOKES2D = 3 };
 /* Arithmetic of the fluid side (no counterpart in the reference, which is
  * FP64 throughout).  Particle positions, forces and the cell lists are FP64
  * in every form.
@@ -85,6 +90,15 @@ typedef struct fsl_config {
   int32_t device;                /* setDevice; -1 keeps the current device  */
   int32_t scheme;                /* FSL_SCHEME_*                            */
   int32_t precision;             /* FSL_PRECISION_*                         */
+  /* quasi-2D family only (FSL_SCHEME_QUASI2D / FSL_SCHEME_STOKES2D) */
+  int32_t ndrift;                /* nDrift (noise count only)               */
+  int32_t use_rfd;               /* use_RFD: the thermal drift spread       */
+  int32_t predictor_corrector;   /* predictorCorrector                      */
+  int32_t reserved_;
+  double radius;                 /* hydrodynamicRadius                      */
+  double saffman_kc;             /* saffmanCutOffWaveNumber (stokesLimit2D) */
+  double saffman_width;          /* saffmanLayerWidth                       */
+  double shear_amp;              /* viscosityMeasureAmplitude               */
 } fsl_config;
 
 typedef struct fsl_status {

@@ -269,6 +269,10 @@ struct orc_state {
   std::vector<double> noise;
   // non-bonded cell list (ascending particle index inside a cell)
   std::vector<int> cell_of, cstart, csorted;
+  // quasi-2D family (src/createCellsQuasi2DGPU.cu:49-98): Gaussian variance,
+  // stencil half-width, stochastic prefactor
+  double q2_var = 0.0, q2_fact1 = 0.0;
+  int q2_kw = 0;
   uint64_t t = 0;
 };
 
@@ -709,8 +713,11 @@ void one_step_first_order(orc_state* s) {
   s->t++;
 }
 
+void one_step_q2d(orc_state* s);
+
 void one_step(orc_state* s) {
   if (s->c.scheme == ORC_SCHEME_FIRST_ORDER) return one_step_first_order(s);
+  if (s->c.scheme == ORC_SCHEME_QUASI2D || s->c.scheme == ORC_SCHEME_STOKES2D) return one_step_q2d(s);
   const int np = s->np, nc = s->nc;
   const double dt = s->c.dt;
   draw_noise(s);
@@ -760,6 +767,387 @@ void one_step(orc_state* s) {
                               s->noise[(size_t)6 * nc + (size_t)(6 + d) * np + i]);
         s->q[k] = rnew;
       }
+  }
+  s->t++;
+}
+
+// ================================================ quasi-2D family (2D) ===
+// The Gaussian-blob Stokes schemes of keywords quasi2D (RPY mobility of a
+// blob in a quasi-2D geometry) and stokesLimit2D (2-D Stokes, optionally
+// Saffman-screened), src/runSchemeQuasi2D.cu:20-260.  Grid nodes sit at the
+// cell corners x_k = k dx - lx/2; a particle's stencil is the (2w+1)^2 nodes
+// around the node at or below it (w = kernelWidth).  Fields are complex
+// [2][my][mx] (x fastest), FP64 throughout as in the reference.
+
+inline bool q2_scheme(const orc_state* s) {
+  return s->c.scheme == ORC_SCHEME_QUASI2D || s->c.scheme == ORC_SCHEME_STOKES2D;
+}
+
+// src/deltaGPU.cu:114-117
+inline double gauss2d(double r2, double var) {
+  const double pi = 3.1415926535897932385;
+  return std::exp(-r2 / (2.0 * var)) / (2 * pi * var);
+}
+
+// (k + o) mod m: the reference's (k + o + m) % m wherever that is
+// non-negative (src/quasi2DFunctions.cu:260, 265)
+inline int q2_wrap(int k, int o, int m) {
+  int r = (k + o) % m;
+  return r < 0 ? r + m : r;
+}
+
+// The node at or below a coordinate (src/quasi2DFunctions.cu:243-252).
+inline int q2_node(double r, double invL, double L, double invd, int m) {
+  return cellidx(minimage(r, invL, L), invd, m);
+}
+
+// Wrapped distance from a coordinate to node k (src/quasi2DFunctions.cu:262-270).
+inline double q2_dist(double r, int k, double L, int m, double invL) {
+  double d = r - (k * L / m) + L * 0.5;
+  return minimage(d, invL, L);
+}
+
+// Adds g(r) * (ax, ay) of the stencil of (rx, ry) to the real parts of Z
+// (src/quasi2DFunctions.cu:255-281); with drift, -g(r) (kT/var) (dx, dy)
+// instead (src/quasi2DFunctions.cu:358-389).
+void q2_spread(orc_state* s, double rx, double ry, double ax, double ay, bool drift) {
+  const int mx = s->mx, my = s->my, w = s->q2_kw;
+  const double lx = s->c.lx, ly = s->c.ly;
+  const int kx = q2_node(rx, s->invlx, lx, s->invdx, mx);
+  const int ky = q2_node(ry, s->invly, ly, s->invdy, my);
+  cplx* Zx = s->Z.data();
+  cplx* Zy = s->Z.data() + s->nc;
+  for (int ix = -w; ix <= w; ++ix) {
+    const int kxn = q2_wrap(kx, ix, mx);
+    const double dxr = q2_dist(rx, kxn, lx, mx, s->invlx);
+    for (int iy = -w; iy <= w; ++iy) {
+      const int kyn = q2_wrap(ky, iy, my);
+      const int c = kxn + kyn * mx;
+      const double dyr = q2_dist(ry, kyn, ly, my, s->invly);
+      const double r2 = dxr * dxr + dyr * dyr;
+      if (drift) {
+        const double g = gauss2d(r2, s->q2_var) * s->c.temperature / s->q2_var;
+        Zx[c] += -g * dxr;
+        Zy[c] += -g * dyr;
+      } else {
+        const double g = gauss2d(r2, s->q2_var);
+        Zx[c] += g * ax;
+        Zy[c] += g * ay;
+      }
+    }
+  }
+}
+
+// u = sum_nodes g(r) v (src/quasi2DFunctions.cu:720-752)
+void q2_interp(const orc_state* s, double rx, double ry, double& ux, double& uy) {
+  const int mx = s->mx, my = s->my, w = s->q2_kw;
+  const double lx = s->c.lx, ly = s->c.ly;
+  const int kx = q2_node(rx, s->invlx, lx, s->invdx, mx);
+  const int ky = q2_node(ry, s->invly, ly, s->invdy, my);
+  const double* vx = s->v.data();
+  const double* vy = s->v.data() + s->nc;
+  ux = 0.0;
+  uy = 0.0;
+  for (int ix = -w; ix <= w; ++ix) {
+    const int kxn = q2_wrap(kx, ix, mx);
+    const double dxr = q2_dist(rx, kxn, lx, mx, s->invlx);
+    for (int iy = -w; iy <= w; ++iy) {
+      const int kyn = q2_wrap(ky, iy, my);
+      const double dyr = q2_dist(ry, kyn, ly, my, s->invly);
+      const double g = gauss2d(dxr * dxr + dyr * dyr, s->q2_var);
+      ux += g * vx[kxn + kyn * mx];
+      uy += g * vy[kxn + kyn * mx];
+    }
+  }
+}
+
+// Bonded (src/quasiNeutrallyBuoyantFunctions2D.cu:201-260) and pair forces
+// over the 9 neighbour cells of a 2-D cell list (src/quasi2DFunctions.cu:53-235).
+void q2_forces(orc_state* s) {
+  const int np = s->np;
+  const double* q = s->q.data();
+  build_cells(s, q);
+  s->F.assign(3 * (size_t)np, 0.0);
+  const double c1 = s->c.cutoff > 0 ? 2.0 * s->c.soft_epsilon / s->c.cutoff : 0.0;
+  const double c2 = s->c.cutoff > 0 ? 1.0 / s->c.cutoff : 0.0;
+  // own cell, -y, -x, +x, +y, then (+x,+y), (+x,-y), (-x,+y), (-x,-y)
+  const int order[9][2] = {{0, 0}, {0, -1}, {-1, 0}, {1, 0}, {0, 1}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < np; ++i) {
+    const double rx = q[i], ry = q[np + i];
+    double fx = 0.0, fy = 0.0;
+    if (s->bonded) {
+      for (int j = 0; j < s->bpp_cnt[i]; ++j) {
+        const int idx = s->bpp_idx[s->bpp_off[i] + j];
+        const double x = q[idx], y = q[np + idx];
+        const double r0 = s->bpp_r0[s->bpp_off[i] + j], k = s->bpp_k[s->bpp_off[i] + j];
+        if (r0 == 0) {
+          fx += -k * (rx - x);
+          fy += -k * (ry - y);
+        } else {
+          const double r = std::sqrt((x - rx) * (x - rx) + (y - ry) * (y - ry));
+          if (r > 0) {
+            fx += -k * (1 - r0 / r) * (rx - x);
+            fy += -k * (1 - r0 / r) * (ry - y);
+          }
+        }
+      }
+      for (int j = 0; j < s->bfp_cnt[i]; ++j) {
+        const int p = s->bfp_off[i] + j;
+        const double x = s->bfp_xyz[3 * p], y = s->bfp_xyz[3 * p + 1];
+        const double r0 = s->bfp_r0[p], k = s->bfp_k[p];
+        if (r0 == 0) {
+          fx += -k * (rx - x);
+          fy += -k * (ry - y);
+        } else {
+          const double r = std::sqrt((x - rx) * (x - rx) + (y - ry) * (y - ry));
+          if (r > 0) {
+            fx += -k * (1 - r0 / r) * (rx - x);
+            fy += -k * (1 - r0 / r) * (ry - y);
+          }
+        }
+      }
+    }
+    if (s->c.pair != ORC_PAIR_NONE) {
+      const int c = s->cell_of[i];
+      const int cx = c % s->mnx, cy = c / s->mnx;
+      for (int o = 0; o < 9; ++o) {
+        const int nx = (cx + order[o][0] + s->mnx) % s->mnx;
+        const int ny = (cy + order[o][1] + s->mny) % s->mny;
+        const int cc = nx + ny * s->mnx;
+        for (int k = s->cstart[cc]; k < s->cstart[cc + 1]; ++k) {
+          const int j = s->csorted[k];
+          double rxij = rx - q[j];
+          rxij = rxij - (double)(int)(rxij * s->invlx + 0.5 * sgn(rxij)) * s->c.lx;
+          double ryij = ry - q[np + j];
+          ryij = ryij - (double)(int)(ryij * s->invly + 0.5 * sgn(ryij)) * s->c.ly;
+          const double r2 = rxij * rxij + ryij * ryij;
+          double f;
+          if (s->c.pair == ORC_PAIR_TABLE_LJ) {
+            f = (double)tex_linear(s->ljtab.data(), 4096, (float)(r2 * s->invcut2));
+          } else {
+            if (j == i || r2 >= s->c.cutoff * s->c.cutoff || r2 == 0.0) continue;
+            f = c1 * (1.0 / std::sqrt(r2) - c2);
+          }
+          fx += f * rxij;
+          fy += f * ryij;
+        }
+      }
+    }
+    s->F[i] = fx;
+    s->F[np + i] = fy;
+  }
+}
+
+// Wave numbers of mode i for the deterministic updates
+// (src/quasi2DFunctions.cu:402-423): signed, with the Nyquist rows folded.
+inline void q2_k_det(const orc_state* s, int i, double& kx, double& ky) {
+  const int mx = s->mx, my = s->my;
+  int wy = i / mx, wx = i % mx;
+  if (wx > mx / 2) wx -= mx;
+  if (wy > my / 2) wy -= my;
+  const bool xHalf = (mx % 2) == 0 && (wx == mx / 2);
+  const bool yHalf = (my % 2) == 0 && (wy == my / 2);
+  if (xHalf && wy < 0) wx *= -1;
+  else if (yHalf && wx < 0) wy *= -1;
+  const double pi = 3.1415926535897932385;
+  kx = wx * 2 * pi / s->c.lx;
+  ky = wy * 2 * pi / s->c.ly;
+}
+
+// Noise bookkeeping of mode i (src/quasi2DFunctions.cu:598-635): the
+// canonical |wave numbers|, the noise index shared by i and -i, and whether
+// the imaginary part flips (the conjugate partner).
+struct Q2Mode {
+  double kx, ky;
+  int index;
+  bool xHalf, yHalf, flip;
+  int wx, wy;
+};
+inline Q2Mode q2_mode_noise(const orc_state* s, int i) {
+  const int mx = s->mx, my = s->my, nModes = s->nc + mx + my;
+  Q2Mode m;
+  int wy = i / mx, wx = i % mx, fx = wx, fy = wy, shift = 0;
+  if (wx > mx / 2) {
+    fx = wx - mx;
+    wx = mx - wx;
+  }
+  if (wy > my / 2) {
+    fy = wy - my;
+    wy = my - wy;
+  }
+  m.xHalf = (mx % 2) == 0 && (wx == mx / 2);
+  m.yHalf = (my % 2) == 0 && (wy == my / 2);
+  if (m.xHalf && fy < 0) fx *= -1;
+  else if (m.yHalf && fx < 0) fy *= -1;
+  const double pi = 3.1415926535897932385;
+  m.kx = wx * 2 * pi / s->c.lx;
+  m.ky = wy * 2 * pi / s->c.ly;
+  if (fx * fy < 0) {
+    shift = nModes / 2;
+    m.kx *= -1.0;
+  }
+  m.index = wy * mx + wx + shift;
+  m.flip = (fx < 0) || (fx == 0 && fy < 0);
+  m.wx = wx;
+  m.wy = wy;
+  return m;
+}
+
+// Fourier-space solve plus stochastic velocity of every mode.
+void q2_fourier(orc_state* s) {
+  const int nc = s->nc, mx = s->mx, my = s->my, nModes = nc + mx + my;
+  const double eta = s->c.shearviscosity, pi_half_inv = 0.56418958354775628695;
+  const double sigma = std::sqrt(s->q2_var), prefactor = s->q2_fact1;
+  const double* R = s->noise.data();
+  cplx* Zx = s->Z.data();
+  cplx* Zy = s->Z.data() + nc;
+  const bool rpy = s->c.scheme == ORC_SCHEME_QUASI2D;
+  const double kc = s->c.saffman_kc, lw = s->c.saffman_width;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nc; ++i) {
+    // deterministic part
+    double kx, ky;
+    q2_k_det(s, i, kx, ky);
+    const double vxr = Zx[i].real(), vxi = Zx[i].imag(), vyr = Zy[i].real(), vyi = Zy[i].imag();
+    double oxr = 0, oxi = 0, oyr = 0, oyi = 0;
+    if (i != 0) {
+      if (rpy) {
+        // src/quasi2DFunctions.cu:450-510
+        const double k_inv = 1.0 / std::sqrt(kx * kx + ky * ky);
+        const double k3_inv = k_inv * k_inv * k_inv;
+        const double k = 1.0 / k_inv, kn = sigma * k;
+        const double f = 0.5 * (std::erfc(kn) * (0.5 + kn * kn) * std::exp(kn * kn) - pi_half_inv * kn);
+        const double g = 0.5 * std::erfc(kn) * std::exp(kn * kn);
+        oxr = (k3_inv / eta) * (g * ky * (ky * vxr - kx * vyr) + f * kx * (kx * vxr + ky * vyr));
+        oxi = (k3_inv / eta) * (g * ky * (ky * vxi - kx * vyi) + f * kx * (kx * vxi + ky * vyi));
+        oyr = (k3_inv / eta) * (g * (-kx) * (ky * vxr - kx * vyr) + f * ky * (kx * vxr + ky * vyr));
+        oyi = (k3_inv / eta) * (g * (-kx) * (ky * vxi - kx * vyi) + f * ky * (kx * vxi + ky * vyi));
+      } else {
+        // src/quasi2DFunctions.cu:767-827 (Stokes) and 966-1035 (Saffman)
+        const double L = -(kx * kx) - (ky * ky);
+        double den;
+        if (kc != 0.0) {
+          const double kmod = std::sqrt(-L);
+          const double corr = lw != 0.0 ? std::tanh(kmod * lw) : 1.0;
+          den = eta * (kmod * (kmod + kc * corr));
+        } else {
+          den = -eta * L;
+        }
+        const double GWr = kx * vxr + ky * vyr, GWi = kx * vxi + ky * vyi;
+        oxr = (vxr + kx * GWr / L) / den;
+        oxi = (vxi + kx * GWi / L) / den;
+        oyr = (vyr + ky * GWr / L) / den;
+        oyi = (vyi + ky * GWi / L) / den;
+      }
+    }
+    // stochastic part
+    const Q2Mode m = q2_mode_noise(s, i);
+    double Wxr = 0, Wxi = 0, Wyr = 0, Wyi = 0;
+    const double mkx = m.kx, mky = m.ky;
+    const bool edge = (m.xHalf && m.wy == 0) || (m.yHalf && m.wx == 0) || (m.xHalf && m.yHalf);
+    if (rpy) {
+      // src/quasi2DFunctions.cu:590-678 (factorScheme 1)
+      if (i != 0) {
+        const double k = std::sqrt(mkx * mkx + mky * mky);
+        const double k3half_inv = 1.0 / std::sqrt(k * k * k);
+        const double kn = sigma * k;
+        const double f_half =
+            std::sqrt(0.5 * (std::erfc(kn) * (0.5 + kn * kn) * std::exp(kn * kn) - pi_half_inv * kn));
+        const double g_half = std::sqrt(0.5 * std::erfc(kn) * std::exp(kn * kn));
+        const double a = g_half * mky, b = f_half * mkx, c = g_half * (-mkx), d = f_half * mky;
+        if (edge) {
+          Wxr = std::sqrt(2.0) * prefactor * k3half_inv * (a * R[m.index] + b * R[nModes + m.index]);
+          Wyr = std::sqrt(2.0) * prefactor * k3half_inv * (c * R[m.index] + d * R[nModes + m.index]);
+        } else {
+          Wxr = prefactor * k3half_inv * (a * R[m.index] + b * R[nModes + m.index]);
+          Wyr = prefactor * k3half_inv * (c * R[m.index] + d * R[nModes + m.index]);
+          Wxi = prefactor * k3half_inv * (a * R[nModes * 2 + m.index] + b * R[nModes * 3 + m.index]);
+          Wyi = prefactor * k3half_inv * (c * R[nModes * 2 + m.index] + d * R[nModes * 3 + m.index]);
+        }
+      }
+    } else {
+      // src/quasi2DFunctions.cu:829-904 (Stokes) and 1037-1119 (Saffman)
+      const bool nyq = ((mx % 2) == 0 && (m.wx == mx / 2)) || ((my % 2) == 0 && (m.wy == my / 2)) || i == 0;
+      if (!nyq) {
+        double amp;
+        if (kc != 0.0) {
+          const double kmod2 = mkx * mkx + mky * mky, kmod = std::sqrt(kmod2);
+          const double corr = lw != 0.0 ? std::tanh(kmod * lw) : 1.0;
+          amp = 1.0 / std::sqrt(kmod * kmod2 * (kmod + kc * corr));
+        } else {
+          amp = 1.0 / (mkx * mkx + mky * mky);
+        }
+        if (edge) {
+          Wxr = std::sqrt(2.0) * prefactor * amp * (mky * R[m.index]);
+          Wyr = std::sqrt(2.0) * prefactor * amp * ((-mkx) * R[m.index]);
+        } else {
+          Wxr = prefactor * amp * (mky * R[m.index]);
+          Wyr = prefactor * amp * ((-mkx) * R[m.index]);
+          Wxi = prefactor * amp * (mky * R[nModes * 2 + m.index]);
+          Wyi = prefactor * amp * ((-mkx) * R[nModes * 2 + m.index]);
+        }
+      }
+    }
+    if (m.flip) {
+      Wxi = -Wxi;
+      Wyi = -Wyi;
+    }
+    Zx[i] = cplx(oxr + Wxr, oxi + Wxi);
+    Zy[i] = cplx(oyr + Wyr, oyi + Wyi);
+  }
+}
+
+// One step of runSchemeQuasi2D (src/runSchemeQuasi2D.cu:108-250).
+void one_step_q2d(orc_state* s) {
+  const int np = s->np, nc = s->nc, mx = s->mx, my = s->my;
+  {
+    const size_t n = (size_t)4 * (nc + mx + my) + (size_t)2 * np * s->c.ndrift;
+    s->noise.resize(n);
+    for (size_t k = 0; k < n; ++k) s->noise[k] = philox_normal(s->c.seed, s->t, k);
+  }
+  std::fill(s->Z.begin(), s->Z.end(), cplx(0, 0));
+  const double* q = s->q.data();
+  if (s->c.nonbonded) {
+    q2_forces(s);
+    for (int i = 0; i < np; ++i) q2_spread(s, q[i], q[np + i], s->F[i], s->F[np + i], false);
+  }
+  if (s->c.use_rfd)
+    for (int i = 0; i < np; ++i) q2_spread(s, q[i], q[np + i], 0.0, 0.0, true);
+  if (s->c.shear_amp != 0.0) {
+    // src/quasi2DFunctions.cu:3-12
+    const double pi2 = 2.0 * 3.1415926535897932385;
+    for (int i = 0; i < nc; ++i)
+      s->Z[nc + i] += s->c.shear_amp * std::sin(pi2 * ((i % mx) / (double)mx));
+  }
+  for (int comp = 0; comp < 2; ++comp)
+    fft3d(s->Z.data() + (size_t)comp * nc, mx, my, 1, s->Px, s->Py, s->Pz, -1);
+  q2_fourier(s);
+  for (int comp = 0; comp < 2; ++comp)
+    fft3d(s->Z.data() + (size_t)comp * nc, mx, my, 1, s->Px, s->Py, s->Pz, +1);
+  for (size_t k = 0; k < (size_t)2 * nc; ++k) s->v[k] = s->Z[k].real() / (double)nc;
+  // src/quasi2DFunctions.cu:681-760: q' = q + dx dy dt J(position) v
+  const double vol = s->dx * s->dy, dt = s->c.dt;
+  if (s->c.predictor_corrector) {
+    for (int i = 0; i < np; ++i) {
+      double ux, uy;
+      q2_interp(s, s->q[i], s->q[np + i], ux, uy);
+      s->qp[i] = s->q[i] + vol * ux * (0.5 * dt);
+      s->qp[np + i] = s->q[np + i] + vol * uy * (0.5 * dt);
+    }
+    for (int i = 0; i < np; ++i) {
+      double ux, uy;
+      q2_interp(s, s->qp[i], s->qp[np + i], ux, uy);
+      s->q[i] = s->q[i] + vol * ux * dt;
+      s->q[np + i] = s->q[np + i] + vol * uy * dt;
+    }
+  } else {
+    for (int i = 0; i < np; ++i) {
+      double ux, uy;
+      q2_interp(s, s->q[i], s->q[np + i], ux, uy);
+      s->q[i] = s->q[i] + vol * ux * dt;
+      s->q[np + i] = s->q[np + i] + vol * uy * dt;
+    }
   }
   s->t++;
 }
@@ -815,6 +1203,23 @@ orc_state* orc_create(const orc_config* cfg, int64_t np, const double* q) {
   } else {
     s->mnx = s->mny = s->mnz = 3;
     s->invcut2 = 0.0;
+  }
+  if (cfg->scheme == ORC_SCHEME_QUASI2D || cfg->scheme == ORC_SCHEME_STOKES2D) {
+    // src/createBoundariesQuasi2DGPU.cu:89-93: int(L / rc) cells per side
+    // (the callers keep at least 3), one layer in z
+    if (cfg->cutoff > 0) {
+      s->mnx = (int)(cfg->lx / cfg->cutoff);
+      s->mny = (int)(cfg->ly / cfg->cutoff);
+    }
+    s->mnz = 1;
+    // src/createCellsQuasi2DGPU.cu:49-79
+    const double a = cfg->radius;
+    s->q2_var = cfg->scheme == ORC_SCHEME_QUASI2D ? std::pow(a / std::sqrt(3.1415926535897932385), 2)
+                                                  : std::pow(a * 0.66556976637237890625, 2);
+    s->q2_kw = (int)(3.0 * a * s->mx / cfg->lx) + 1;
+    if (s->q2_kw > s->mx / 2) s->q2_kw = s->mx / 2;
+    s->q2_fact1 = std::sqrt(1.0 * cfg->temperature / (cfg->shearviscosity * cfg->dt * cfg->lx * cfg->ly)) *
+                  (s->mx * s->my * s->mz);
   }
   s->mN = s->mnx * s->mny * s->mnz;
   if (cfg->pair == ORC_PAIR_TABLE_LJ) build_ljtable(s);

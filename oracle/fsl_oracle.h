@@ -32,7 +32,11 @@ enum { ORC_RFD_REFERENCE = 0, ORC_RFD_PAPER = 1 };
 /* ORC_SCHEME_MIDPOINT: stokesLimit (src/runSchemeStokesLimit.cu:163-285);
  * ORC_SCHEME_FIRST_ORDER: stokesLimitFirstOrder
  * (src/runSchemeStokesLimitFirstOrder.cu:163-241). */
-enum { ORC_SCHEME_MIDPOINT = 0, ORC_SCHEME_FIRST_ORDER = 1 };
+/* ORC_SCHEME_QUASI2D / ORC_SCHEME_STOKES2D: the Gaussian-blob schemes of
+ * keywords quasi2D and stokesLimit2D on an mx x my grid (mz = 1),
+ * src/runSchemeQuasi2D.cu:20-260 with src/quasi2DFunctions.cu. */
+enum { ORC_SCHEME_MIDPOINT = 0, ORC_SCHEME_FIRST_ORDER = 1, ORC_SCHEME_QUASI2D = 2,
+       ORC_SCHEME_STOKES2D = 3 };
 
 typedef struct orc_config {
   int32_t mx, my, mz;
@@ -49,6 +53,15 @@ typedef struct orc_config {
   int32_t rfd;            /* ORC_RFD_*                                   */
   int32_t nonbonded;      /* computeNonBondedForces                      */
   int32_t scheme;         /* ORC_SCHEME_*                                */
+  /* quasi-2D family only */
+  int32_t ndrift;         /* nDrift (noise count only)                   */
+  int32_t use_rfd;        /* use_RFD                                     */
+  int32_t predictor_corrector; /* predictorCorrector                     */
+  int32_t pad_;
+  double radius;          /* hydrodynamicRadius                          */
+  double saffman_kc;      /* saffmanCutOffWaveNumber (stokesLimit2D)     */
+  double saffman_width;   /* saffmanLayerWidth                           */
+  double shear_amp;       /* viscosityMeasureAmplitude                   */
 } orc_config;
 
 typedef struct orc_state orc_state;

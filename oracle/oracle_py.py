@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
 RFD_REFERENCE, RFD_PAPER = 0, 1
-SCHEME_MIDPOINT, SCHEME_FIRST_ORDER = 0, 1
+SCHEME_MIDPOINT, SCHEME_FIRST_ORDER, SCHEME_QUASI2D, SCHEME_STOKES2D = 0, 1, 2, 3
 
 
 class OrcConfig(ctypes.Structure):
@@ -27,6 +27,10 @@ class OrcConfig(ctypes.Structure):
         ("seed", ctypes.c_uint64),
         ("pair", ctypes.c_int32), ("rfd", ctypes.c_int32),
         ("nonbonded", ctypes.c_int32), ("scheme", ctypes.c_int32),
+        ("ndrift", ctypes.c_int32), ("use_rfd", ctypes.c_int32),
+        ("predictor_corrector", ctypes.c_int32), ("pad_", ctypes.c_int32),
+        ("radius", ctypes.c_double), ("saffman_kc", ctypes.c_double),
+        ("saffman_width", ctypes.c_double), ("shear_amp", ctypes.c_double),
     ]
 
 
@@ -121,7 +125,9 @@ class Oracle:
 
     def __init__(self, mx, my, mz, lx, ly, lz, q, eta=1.0, kT=0.01, dt=0.01, cutoff=1.5,
                  kernel=3, pair=PAIR_SOFT, soft_epsilon=1.0, rfd=RFD_REFERENCE,
-                 nonbonded=1, extra_mobility=0.0, seed=1, scheme=0):
+                 nonbonded=1, extra_mobility=0.0, seed=1, scheme=0, radius=1.0, ndrift=1,
+                 use_rfd=1, predictor_corrector=0, saffman_kc=0.0, saffman_width=0.0,
+                 shear_amp=0.0):
         self.L = _load()
         q = np.ascontiguousarray(q, dtype=np.float64).reshape(3, -1)
         self.np = q.shape[1]
@@ -130,7 +136,10 @@ class Oracle:
         c = OrcConfig(mx=mx, my=my, mz=mz, kernel=kernel, lx=lx, ly=ly, lz=lz,
                       shearviscosity=eta, temperature=kT, dt=dt, cutoff=cutoff,
                       extra_mobility=extra_mobility, soft_epsilon=soft_epsilon,
-                      seed=seed, pair=pair, rfd=rfd, nonbonded=nonbonded, scheme=scheme)
+                      seed=seed, pair=pair, rfd=rfd, nonbonded=nonbonded, scheme=scheme,
+                      ndrift=ndrift, use_rfd=use_rfd, predictor_corrector=predictor_corrector,
+                      radius=radius, saffman_kc=saffman_kc, saffman_width=saffman_width,
+                      shear_amp=shear_amp)
         self.cfg = c
         self.h = self.L.orc_create(ctypes.byref(c), self.np, _dp(q))
         if not self.h:

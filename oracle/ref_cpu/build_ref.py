@@ -41,6 +41,10 @@ GPU_FILES = [
     "stokesLimitFunctions.cu", "boundaryParticlesFunctionStokesLimit.cu",
     "saveFunctionsSchemeStokesLimit.cu", "gpuToHostStokesLimit.cu", "runSchemeStokesLimit.cu",
     "boundaryParticlesFunctionStokesLimitFirstOrder.cu", "runSchemeStokesLimitFirstOrder.cu",
+    # the quasi-2D / stokesLimit2D family (src/GPU.cu:197, 279-287)
+    "quasiNeutrallyBuoyantFunctions2D.cu", "createCellsQuasi2DGPU.cu", "freeCellsQuasi2DGPU.cu",
+    "createBoundariesQuasi2DGPU.cu", "freeBoundariesQuasi2DGPU.cu", "quasi2DFunctions.cu",
+    "texturesCellsQuasi2D.cu", "runSchemeQuasi2D.cu",
 ]
 GPU_HEADERS = ["header.h", "cells.h", "fluid.h", "boundary.h", "headerOtherFluidVariables.h",
                "particles.h", "hydroAnalysis.h"]
@@ -48,7 +52,8 @@ GPU_HEADERS = ["header.h", "cells.h", "fluid.h", "boundary.h", "headerOtherFluid
 # reference's Makefile does).
 HOST_FILES = [
     "main.cpp", "loadDataMain.cu", "cudaDevice.cu", "initializeRandomNumber.cpp", "rantest.cu",
-    "gauss.cu", "schemeStokesLimit.cu", "schemeStokesLimitFirstOrder.cu", "createCells.cpp", "createParticles.cpp",
+    "gauss.cu", "schemeStokesLimit.cu", "schemeStokesLimitFirstOrder.cu", "schemeQuasi2D.cu",
+    "createCells.cpp", "createParticles.cpp",
     "simpleCubic.cpp", "initializeBondedForces.cpp", "initializeFluid.cpp", "modu.cu",
     "saveSeed.cpp", "saveTime.cpp", "saveParticles.cu", "freeParticles.cu", "random_frenk.cu",
 ]

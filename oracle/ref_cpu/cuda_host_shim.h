@@ -193,6 +193,11 @@ inline double fetch_double(const texture<int2, 1>& t, int i) {
   return reinterpret_cast<const double*>(t.ptr)[i];
 }
 
+// ------------------------------------------------------------ math -------
+// CUDA's double reciprocal square root, as 1 / sqrt on the host (the
+// quasi-2D kernels use it; within an ulp or two of the device function)
+inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
+
 // -------------------------------------------------------------- atomics ---
 inline int atomicAdd(int* p, int v) {
   int o = *p;

@@ -55,7 +55,6 @@ FLUAM_SCHEME_STUB(schemeIncompressibleBinaryMixtureMidPoint)
 FLUAM_SCHEME_STUB(schemeIncompressibleBoundary)
 FLUAM_SCHEME_STUB(schemeMomentumCoupling)
 FLUAM_SCHEME_STUB(schemeParticlesWall)
-FLUAM_SCHEME_STUB(schemeQuasi2D)
 FLUAM_SCHEME_STUB(schemeQuasiNeutrallyBuoyant)
 FLUAM_SCHEME_STUB(schemeQuasiNeutrallyBuoyant2D)
 FLUAM_SCHEME_STUB(schemeQuasiNeutrallyBuoyant4pt2D)

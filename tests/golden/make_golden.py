@@ -52,6 +52,20 @@ def chains(nch, beads, box, seed):
     return q, list(zip(idx[:, :-1].ravel(), idx[:, 1:].ravel()))
 
 
+def chains2d(nch, beads, box, seed):
+    """Chains in the plane z = 0: seeded starts, unit bonds in random directions."""
+    rng = np.random.default_rng(seed)
+    starts = rng.uniform(-0.5, 0.5, (nch, 2)) * np.asarray(box[:2])
+    # directions turn by at most 0.6 rad per bond, so a chain never folds back
+    phi = rng.uniform(0, 2 * np.pi, (nch, 1)) + np.cumsum(rng.uniform(-0.6, 0.6, (nch, beads - 1)), axis=1)
+    d = np.stack([np.cos(phi), np.sin(phi)], axis=2)
+    pos = np.concatenate([starts[:, None, :], starts[:, None, :] + np.cumsum(d, axis=1)], axis=1)
+    q = np.zeros((3, nch * beads))
+    q[:2] = pos.reshape(-1, 2).T
+    idx = np.arange(nch * beads).reshape(nch, beads)
+    return q, list(zip(idx[:, :-1].ravel(), idx[:, 1:].ravel()))
+
+
 def write_coor(path, q):
     with open(path, "w") as f:
         f.write(f"{q.shape[1]}\n")
@@ -139,6 +153,77 @@ numsteps 4
 samplefreq 2
 dt 0.01
 """, chains=(5, 7, (20.0, 16.0, 24.0), 12)),
+    # the quasi-2D family (keywords quasi2D / stokesLimit2D, src/runSchemeQuasi2D.cu):
+    # a Gaussian-blob RPY step with LJ forces through the 2-D cell list and
+    # the thermal drift (lz >= cutoff keeps the reference's neighbour grid
+    # non-empty, src/createBoundariesQuasi2DGPU.cu:89-95)
+    "q2d_rpy_lattice": dict(scheme="quasi2D", text="""numberparticles 100
+computeNonBondedForces 1
+cutoff 2.2449240966
+shearviscosity 1.2
+temperature 0.05
+hydrodynamicRadius 1.0
+cells 24 24 1
+celldimension 24 24 4
+seed 31
+numstepsRelaxation 1
+numsteps 6
+samplefreq 2
+dt 0.01
+"""),
+    # predictor-corrector with 2-D bonded chains and tethers (bonds act only
+    # with computeNonBondedForces 1 in this scheme; a fine grid keeps the
+    # hard-coded LJ table, sigma = 2 dx, short of the unit bonds)
+    "q2d_pc_chains": dict(scheme="quasi2D", dim=2, text="""loadparticles 1
+coordinates start.coor
+bondedForces bonds.dat
+computeNonBondedForces 1
+cutoff 0.5612310241
+predictorCorrector 1
+shearviscosity 0.8
+temperature 0.02
+hydrodynamicRadius 0.5
+cells 40 40 1
+celldimension 10 10 4
+seed 37
+numsteps 4
+samplefreq 2
+dt 0.01
+""", chains=(4, 5, (10.0, 10.0, 4.0), 17)),
+    # 2-D Stokes mobility, no thermal drift
+    "s2d_spectral": dict(scheme="stokesLimit2D", text="""numberparticles 25
+computeNonBondedForces 1
+cutoff 2.2449240966
+use_RFD 0
+shearviscosity 0.9
+temperature 0.1
+hydrodynamicRadius 1.2
+cells 30 20 1
+celldimension 30 20 4
+seed 41
+numsteps 4
+samplefreq 2
+dt 0.02
+"""),
+    # Saffman-screened 2-D mobility with the periodic layer correction and
+    # the shear forcing, predictor-corrector, no forces
+    "s2d_saffman_shear": dict(scheme="stokesLimit2D", text="""saffmanCutOffWaveNumber 0.3
+saffmanLayerWidth 2.0
+viscosityMeasureAmplitude 0.05
+numberparticles 16
+computeNonBondedForces 0
+cutoff 2.0
+predictorCorrector 1
+shearviscosity 1.0
+temperature 0.1
+hydrodynamicRadius 1.0
+cells 32 32 1
+celldimension 32 32 1
+seed 43
+numsteps 4
+samplefreq 2
+dt 0.05
+"""),
 }
 
 
@@ -156,7 +241,7 @@ def make_case(name, spec):
         write_coor(os.path.join(d, "start.coor"), spec["coor"]())
     if "chains" in spec:
         nch, beads, box, seed = spec["chains"]
-        q, bonds = chains(nch, beads, box, seed)
+        q, bonds = (chains2d if spec.get("dim") == 2 else chains)(nch, beads, box, seed)
         write_coor(os.path.join(d, "start.coor"), q)
         with open(os.path.join(d, "bonds.dat"), "w") as f:
             f.write(f"{len(bonds)}\n")

@@ -24,10 +24,15 @@ def read_particles(path):
     return n, out
 
 
-def simple_cubic(np_, lx, ly, lz):
-    """src/simpleCubic.cpp:25-63 (dimension 3)."""
-    sigma = (lx * ly * lz / np_) ** (1.0 / 3.0)
-    nz = int(lz / sigma) or 1
+def simple_cubic(np_, lx, ly, lz, dim=3):
+    """src/simpleCubic.cpp:25-63 (dimension 3, or 2: one layer that the
+    filling loop may still stack)."""
+    if dim == 3:
+        sigma = (lx * ly * lz / np_) ** (1.0 / 3.0)
+        nz = int(lz / sigma) or 1
+    else:
+        sigma = (lx * ly / np_) ** 0.5
+        nz = 1
     nx = int(lx / sigma) or 1
     ny = int(ly / sigma) or 1
     while nx * ny * nz < np_:
@@ -65,7 +70,8 @@ def load(name):
             n = int(f.readline())
             q0 = np.array([f.readline().split() for _ in range(n)], dtype=float).T.copy()
     else:
-        q0 = simple_cubic(run["numberparticles"], cfg.lx, cfg.ly, cfg.lz)
+        q0 = simple_cubic(run["numberparticles"], cfg.lx, cfg.ly, cfg.lz,
+                          2 if cfg.scheme >= 2 else 3)
     bonds = None
     if "bondedForces" in words:
         with open(os.path.join(d, "bonds.dat")) as f:
@@ -77,21 +83,36 @@ def load(name):
                      r0=bb[:, 3], fi=ff[:, 0].astype(np.int32), fk=ff[:, 1], fr0=ff[:, 2],
                      fxyz=ff[:, 3:6])
     _, pos = read_particles(os.path.join(d, "out.particles"))
-    # the first-order scheme writes no .velocityParticles (src/saveParticles.cu:43-46)
+    # the first-order scheme and quasi2D write no .velocityParticles
+    # (src/saveParticles.cu:43-46); stokesLimit2D writes zeros there (its
+    # particle velocity array is never set), which are not forces
     fv = os.path.join(d, "out.velocityParticles")
-    frc = read_particles(fv)[1] if os.path.exists(fv) else None
+    frc = read_particles(fv)[1] if os.path.exists(fv) and cfg.scheme < 2 else None
     seed = int(open(os.path.join(d, "out.seed")).read())
     return dict(dir=d, cfg=cfg, run=run, q0=q0, bonds=bonds, pos=pos, frc=frc, seed=seed)
 
 
-def sample_steps(run):
-    """Number of steps taken before each sample (src/runSchemeStokesLimit.cu:83, 280)."""
+def sample_steps(run, scheme=0):
+    """(step, steps taken) of each sample: after a step with step % samplefreq
+    == 0 and step > 0 (src/runSchemeStokesLimit.cu:83, 280); for the
+    quasi-2D family before each step with step >= 0 on the same condition,
+    plus one after the last (src/runSchemeQuasi2D.cu:99-252)."""
     out = []
     step = -run["numstepsRelaxation"]
     taken = 0
+    sf = run["samplefreq"]
+    if scheme >= 2:
+        while step < run["numsteps"]:
+            if step >= 0 and step % sf == 0:
+                out.append((step, taken))
+            step += 1
+            taken += 1
+        if step % sf == 0:
+            out.append((step, taken))
+        return out
     while step < run["numsteps"]:
         step += 1
         taken += 1
-        if step % run["samplefreq"] == 0 and step > 0:
+        if step % sf == 0 and step > 0:
             out.append((step, taken))
     return out

@@ -24,7 +24,10 @@ def _oracle_for(oracle, c):
                       eta=cfg.shearviscosity, kT=cfg.temperature, dt=cfg.dt, cutoff=cfg.cutoff,
                       kernel=cfg.kernel, pair=cfg.pair, soft_epsilon=cfg.soft_epsilon,
                       rfd=cfg.rfd, nonbonded=cfg.nonbonded, extra_mobility=cfg.extra_mobility,
-                      seed=c["seed"], scheme=cfg.scheme)
+                      seed=c["seed"], scheme=cfg.scheme, radius=cfg.radius, ndrift=cfg.ndrift,
+                      use_rfd=cfg.use_rfd, predictor_corrector=cfg.predictor_corrector,
+                      saffman_kc=cfg.saffman_kc, saffman_width=cfg.saffman_width,
+                      shear_amp=cfg.shear_amp)
     if c["bonds"] is not None:
         b = c["bonds"]
         o.set_bonds(b["bi"], b["bj"], b["k"], b["r0"], b["fi"], b["fk"], b["fr0"], b["fxyz"])
@@ -37,7 +40,7 @@ def test_oracle_reproduces_reference(oracle, name):
     o = _oracle_for(oracle, c)
     dt = c["cfg"].dt
     done = 0
-    samples = G.sample_steps(c["run"])
+    samples = G.sample_steps(c["run"], c["cfg"].scheme)
     assert len(samples) == len(c["pos"]) > 0
     for step, taken in samples:
         o.step(taken - done)
