@@ -7,10 +7,11 @@ ABI and the data.main driver), ``build.py`` (nvcc recipe), ``_lib.py``
 (ctypes binding) and ``stokes.py`` (the Python interface).
 """
 from .stokes import (PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE,
-                     SCHEME_FIRST_ORDER, SCHEME_MIDPOINT, SCHEME_QUASI2D, SCHEME_STOKES2D, Batch,
+                     SCHEME_FIRST_ORDER, SCHEME_INCOMPRESSIBLE, SCHEME_MIDPOINT, SCHEME_QUASI2D,
+                     SCHEME_STOKES2D, Batch,
                      Server, StokesLimit, make_config,
                      parse_data_main, run_data_main)
 
 __all__ = ["StokesLimit", "Batch", "Server", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
            "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE", "SCHEME_MIDPOINT",
-           "SCHEME_FIRST_ORDER", "SCHEME_QUASI2D", "SCHEME_STOKES2D"]
+           "SCHEME_FIRST_ORDER", "SCHEME_QUASI2D", "SCHEME_STOKES2D", "SCHEME_INCOMPRESSIBLE"]

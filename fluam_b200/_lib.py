@@ -15,14 +15,14 @@ ERRORS = {-1: "FSL_E_ARG", -2: "FSL_E_CUDA", -3: "FSL_E_NOMEM", -4: "FSL_E_KERNE
           -5: "FSL_E_IO", -6: "FSL_E_INPUT"}
 PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
 RFD_REFERENCE, RFD_PAPER = 0, 1
-SCHEME_MIDPOINT, SCHEME_FIRST_ORDER, SCHEME_QUASI2D, SCHEME_STOKES2D = 0, 1, 2, 3
+SCHEME_MIDPOINT, SCHEME_FIRST_ORDER, SCHEME_QUASI2D, SCHEME_STOKES2D, SCHEME_INCOMPRESSIBLE = 0, 1, 2, 3, 4
 PRECISION_FIXED64, PRECISION_FLOAT_ATOMIC, PRECISION_FP64 = 0, 1, 2
 
 # Every symbol include/fluamsl.h declares.
 EXPORTS = [
     "fsl_config_defaults", "fsl_create", "fsl_load_bonds", "fsl_step", "fsl_sync",
     "fsl_get_positions", "fsl_set_positions", "fsl_get_forces", "fsl_get_velocity",
-    "fsl_get_velocity_f64",
+    "fsl_get_velocity_f64", "fsl_set_velocity_f64",
     "fsl_get_status", "fsl_set_step", "fsl_clear_errors", "fsl_set_graph", "fsl_stream",
     "fsl_profile", "fsl_profile_read",
     "fsl_destroy", "fsl_last_error", "fsl_run_data_main", "fsl_parse_data_main",
@@ -57,6 +57,7 @@ class Config(ctypes.Structure):
         ("predictor_corrector", ctypes.c_int32), ("reserved_", ctypes.c_int32),
         ("radius", ctypes.c_double), ("saffman_kc", ctypes.c_double),
         ("saffman_width", ctypes.c_double), ("shear_amp", ctypes.c_double),
+        ("density", ctypes.c_double),
     ]
 
 
@@ -132,6 +133,7 @@ def load(path=None):
     L.fsl_get_forces.argtypes = [_VP, _D]
     L.fsl_get_velocity.argtypes = [_VP, _F]
     L.fsl_get_velocity_f64.argtypes = [_VP, _D]
+    L.fsl_set_velocity_f64.argtypes = [_VP, _D]
     L.fsl_get_status.argtypes = [_VP, ctypes.POINTER(Status)]
     L.fsl_set_step.argtypes = [_VP, ctypes.c_uint64]
     L.fsl_clear_errors.argtypes = [_VP]

@@ -79,6 +79,7 @@ void fsl_config_defaults(fsl_config* c) {
   c->radius = 1.0;
   c->ndrift = 1;
   c->use_rfd = 1;
+  c->density = 1.0;
 }
 
 int fsl_create(const fsl_config* cfg, int64_t np, const double* q, fsl_handle** out) {
@@ -226,6 +227,26 @@ int fsl_get_velocity_f64(fsl_handle* h, double* out) {
   FSL_TRY(cudaSetDevice(h->exec.device));
   FSL_TRY(cudaMemcpyAsync(out, rep(h).v64, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->exec.stream));
   FSL_TRY(cudaStreamSynchronize(h->exec.stream));
+  return FSL_OK;
+}
+
+int fsl_set_velocity_f64(fsl_handle* h, const double* in) {
+  if (!h || !in) return errorf(FSL_E_ARG, "null argument");
+  if (params(h).scheme != FSL_SCHEME_INCOMPRESSIBLE)
+    return errorf(FSL_E_ARG, "fsl_set_velocity_f64: the incompressible scheme only");
+  int rc = prepare(h);
+  if (rc) return rc;
+  const fsl::Batch& B = h->group.B;
+  cudaStream_t s = h->exec.stream;
+  FSL_TRY(cudaMemcpyAsync(rep(h).v64, in, sizeof(double) * 3 * (size_t)params(h).nc,
+                          cudaMemcpyHostToDevice, s));
+  // src/runSchemeIncompressible.cu:82-96: the projection of the initial field
+  fsl::launch_inc_load(B, s);
+  fsl::launch_fft64_3d(B, -1, 0, s);
+  fsl::launch_inc_fourier(B, 0, s);
+  fsl::launch_fft64_3d(B, +1, 1, s);
+  if ((rc = check_launch())) return rc;
+  FSL_TRY(cudaStreamSynchronize(s));
   return FSL_OK;
 }
 

@@ -43,7 +43,11 @@ struct Run {
   int64_t savefreq = 0;
   double densfluid = 0.0, pressure[3] = {0.0, 0.0, 0.0};
   // scheme flags that select another fluam scheme (src/main.cpp:36-105)
-  bool stokesLimit = false, first_order = false, quasi2D = false, stokes2D = false;
+  bool stokesLimit = false, first_order = false, quasi2D = false, stokes2D = false, incomp = false;
+  // initial fluid of the incompressible scheme (src/initializeFluid.cpp:28-82)
+  int64_t initfluid = 0;
+  bool setparticles = false;
+  double v0[3] = {0.0, 0.0, 0.0};
   std::vector<std::string> other_schemes;
   std::string wordfile;
 };
@@ -232,11 +236,21 @@ int parse(const char* path, Run& r, std::string& err) {
                  word == "binaryMixtureWall" || word == "binaryMixture" ||
                  word == "particlesWall" || word == "freeEnergyCompressibleParticles" ||
                  word == "semiImplicitCompressibleParticles" || word == "momentumCoupling" ||
-                 word == "incompressible" || word == "incompressibleBinaryMixture" ||
+                 word == "incompressibleBinaryMixture" ||
                  word == "incompressibleBinaryMixtureMidPoint" ||
                  word == "quasiNeutrallyBuoyant" || word == "quasiNeutrallyBuoyant2D" ||
                  word == "quasiNeutrallyBuoyant4pt2D") {
         r.other_schemes.push_back(word);
+      } else if (word == "incompressible") {
+        r.incomp = true;
+      } else if (word == "particles") {
+        r.setparticles = I(0) != 0;
+      } else if (word == "initfluid") {
+        r.initfluid = I(0);
+      } else if (word == "backgroundvelocity") {
+        r.v0[0] = D(0);
+        r.v0[1] = D(1);
+        r.v0[2] = D(2);
       } else if (word == "quasi2D") {
         r.quasi2D = true;
       } else if (word == "stokesLimit2D") {
@@ -275,6 +289,14 @@ int parse(const char* path, Run& r, std::string& err) {
   // src/runSchemeQuasi2D.cu:186-205)
   if (r.quasi2D) r.cfg.scheme = FSL_SCHEME_QUASI2D;
   else if (r.stokes2D) r.cfg.scheme = FSL_SCHEME_STOKES2D;
+  // incompressible comes before all of them in the reference's chain, and
+  // with particles it selects another scheme (src/main.cpp:70-75); densfluid
+  // is its fluid density
+  if (r.incomp && r.setparticles) r.other_schemes.push_back("incompressibleBoundary");
+  if (r.incomp) {
+    r.cfg.scheme = FSL_SCHEME_INCOMPRESSIBLE;
+    r.cfg.density = r.densfluid;
+  }
   return FSL_OK;
 }
 
@@ -453,6 +475,138 @@ int fluid_outputs(fsl_handle* h, const Run& r, int final_call, int64_t step) {
   return rc;
 }
 
+// Running averages of the fluid temperature diagnostic
+// (src/temperature.cu:32-205, indices 1 and 2).
+struct FluidTemperature {
+  double sigma = 0, mean = 0, txm = 0, tym = 0, tzm = 0;
+  // per sample: kinetic temperature of the staggered velocity about its mean
+  void sample(const Run& r, const std::vector<double>& v, int64_t step) {
+    const int64_t nc = (int64_t)r.cfg.mx * r.cfg.my * r.cfg.mz;
+    const double vol = (r.cfg.lx / r.cfg.mx) * (r.cfg.ly / r.cfg.my) * (r.cfg.lz / r.cfg.mz);
+    const double rho = r.cfg.density;
+    const int64_t n = step / r.samplefreq;
+    double m[3] = {0, 0, 0}, mass = 0;
+    for (int64_t i = 0; i < nc; ++i) {
+      for (int a = 0; a < 3; ++a) m[a] += v[a * nc + i];
+      mass += vol * rho;
+    }
+    for (int a = 0; a < 3; ++a) m[a] /= double(nc);
+    double t[3] = {0, 0, 0}, p[3] = {0, 0, 0};
+    for (int64_t i = 0; i < nc; ++i)
+      for (int a = 0; a < 3; ++a) {
+        const double d = v[a * nc + i] - m[a];
+        t[a] += 0.5 * vol * (rho + rho) * d * d;
+        p[a] += 0.5 * vol * (rho + rho) * v[a * nc + i];
+      }
+    for (int a = 0; a < 3; ++a) t[a] /= double(nc);
+    const double tt = (t[0] + t[1] + t[2]) / 3.;
+    const double T = r.cfg.temperature;
+    sigma += (tt - T) * (tt - T);
+    mean += tt;
+    txm += t[0];
+    tym += t[1];
+    tzm += t[2];
+    std::cout << "MASS FLUID    " << mass << std::endl;
+    std::cout << "TEMPERATURE FLUID " << tt << " " << mean / double(n) << " "
+              << (mean / double(n) - T) / T << " " << std::sqrt(sigma / double(n)) / T << "  " << n
+              << std::endl;
+    std::cout << "tx                " << t[0] << " " << txm / double(n) << std::endl;
+    std::cout << "ty                " << t[1] << " " << tym / double(n) << std::endl;
+    std::cout << "tz                " << t[2] << " " << tzm / double(n) << std::endl;
+    std::cout.precision(15);
+    std::cout << "PX " << p[0] << std::endl << "PY " << p[1] << std::endl << "PZ " << p[2] << std::endl
+              << std::endl;
+    std::cout.precision(6);
+  }
+  // <out>.temperature at the end, momenta of the last sampled field
+  void close(const Run& r, const std::vector<double>& v, int64_t step) const {
+    const int64_t nc = (int64_t)r.cfg.mx * r.cfg.my * r.cfg.mz;
+    const double vol = (r.cfg.lx / r.cfg.mx) * (r.cfg.ly / r.cfg.my) * (r.cfg.lz / r.cfg.mz);
+    const double rho = r.cfg.density, T = r.cfg.temperature;
+    const int64_t n = step / r.samplefreq;
+    std::ofstream f(r.outputname + ".temperature");
+    f.precision(15);
+    f << "TEMPERATURE FLUID " << mean / double(n) << " " << (mean / double(n) - T) / T << " "
+      << std::sqrt(sigma / double(n)) / T << "  " << n << std::endl;
+    f << "tx                " << txm / double(n) << std::endl;
+    f << "ty                " << tym / double(n) << std::endl;
+    f << "tz                " << tzm / double(n) << std::endl;
+    double p[3] = {0, 0, 0}, mass = 0;
+    for (int64_t i = 0; i < nc; ++i) {
+      for (int a = 0; a < 3; ++a) p[a] += 0.5 * vol * (rho + rho) * v[a * nc + i];
+      mass += vol * rho;
+    }
+    f << "PX " << p[0] << std::endl;
+    f << "PY " << p[1] << std::endl;
+    f << "PZ " << p[2] << std::endl << std::endl;
+    f << "MASS FLUID    " << mass << std::endl << std::endl;
+  }
+};
+
+// schemeIncompressible + runSchemeIncompressible (src/schemeIncompressible.cu:
+// 23-55, src/runSchemeIncompressible.cu:20-155): the initial field (a uniform
+// background velocity, initfluid 0; the other initfluid choices draw from the
+// reference's host generator and are not supported), samples after every
+// samplefreq-th step, the temperature diagnostic and the final fluid file.
+int run_incompressible(Run& r) {
+  if (r.initfluid != 0) {
+    std::cout << "ERROR: the incompressible scheme supports initfluid 0 (background velocity) only"
+              << std::endl;
+    return FSL_E_INPUT;
+  }
+  const int64_t nc = (int64_t)r.cfg.mx * r.cfg.my * r.cfg.mz;
+  std::vector<double> v(3 * nc);
+  for (int a = 0; a < 3; ++a) std::fill(v.begin() + a * nc, v.begin() + (a + 1) * nc, r.v0[a]);
+  fsl_handle* h = nullptr;
+  int rc = fsl_create(&r.cfg, 0, nullptr, &h);
+  if (!rc) rc = fsl_set_velocity_f64(h, v.data());
+  if (rc) {
+    std::cout << "ERROR: " << fsl_last_error() << std::endl;
+    if (h) fsl_destroy(h);
+    return rc;
+  }
+  {
+    std::ofstream fs(r.outputname + ".seed");
+    fs << r.cfg.seed << std::endl;
+  }
+  time_t t0 = time(NULL);
+  FluidTemperature temp;
+  // the host copy the final files read: the initial field until a sample
+  std::vector<double> last = v;
+  int64_t step = -r.relax;
+  while (step < r.numsteps) {
+    int64_t next = r.numsteps;
+    const int64_t s0 = step + 1;
+    int64_t cand = s0 <= 0 ? r.samplefreq : ((s0 + r.samplefreq - 1) / r.samplefreq) * r.samplefreq;
+    if (cand < next) next = cand;
+    rc = fsl_step(h, next - step);
+    if (rc) break;
+    step = next;
+    if (!(step % r.samplefreq) && step > 0) {
+      std::cout << "INCOMPRESSIBLE " << step << std::endl;
+      if ((rc = fsl_sync(h)) || (rc = fsl_get_velocity_f64(h, last.data()))) break;
+      temp.sample(r, last, step);
+    }
+  }
+  if (!rc) rc = fsl_sync(h);
+  time_t t1 = time(NULL) - t0;
+  std::cout << std::endl << "TIME RUN_GPU                       " << t1 << std::endl << std::endl;
+  {
+    std::ofstream ft(r.outputname + ".time");
+    ft << "TIME RUN GPU     " << t1 << std::endl;
+  }
+  if (!rc) {
+    temp.close(r, last, step);
+    const double p3[3] = {r.pressure[0], r.pressure[1], r.pressure[2]};
+    rc = fsl_write_fluid_final((r.outputname + ".fluidFinalConfiguration").c_str(), &r.cfg,
+                               r.densfluid, p3, 0, last.data());
+  }
+  if (rc) std::cout << "ERROR: " << fsl_last_error() << std::endl;
+  fsl_destroy(h);
+  if (!rc) std::cout << "END" << std::endl;
+  return rc;
+}
+
 }  // namespace
 
 extern "C" int fsl_parse_data_main(const char* path, fsl_config* cfg, int64_t* numsteps,
@@ -487,7 +641,8 @@ extern "C" int fsl_run_data_main(const char* path) {
     fo << r.wordfile << std::endl;
   }
   std::cout << "READ " << (path ? path : "data.main") << " :                DONE" << std::endl;
-  if (!r.other_schemes.empty() || !(r.stokesLimit || r.first_order || r.quasi2D || r.stokes2D)) {
+  if (!r.other_schemes.empty() ||
+      !(r.stokesLimit || r.first_order || r.quasi2D || r.stokes2D || r.incomp)) {
     std::cout << "ERROR: this build runs the stokesLimit and stokesLimitFirstOrder schemes only"
               << (r.other_schemes.empty() ? std::string(" (keyword stokesLimit missing)")
                                           : " (found " + r.other_schemes[0] + ")")
@@ -505,6 +660,7 @@ extern "C" int fsl_run_data_main(const char* path) {
     uint64_t s = (uint64_t)time(0);
     r.cfg.seed = s % 18671;
   }
+  if (r.incomp) return run_incompressible(r);
   // particles (src/createParticles.cpp:39-102)
   std::vector<double> q;
   int64_t np = r.np;
@@ -523,7 +679,8 @@ extern "C" int fsl_run_data_main(const char* path) {
       return FSL_E_INPUT;
     }
     // src/createParticles.cpp:53-58
-    simple_cubic(r.cfg, np, q, r.cfg.scheme >= FSL_SCHEME_QUASI2D ? 2 : 3);
+    simple_cubic(r.cfg, np, q,
+                 r.cfg.scheme == FSL_SCHEME_QUASI2D || r.cfg.scheme == FSL_SCHEME_STOKES2D ? 2 : 3);
   }
   fsl_handle* h = nullptr;
   rc = fsl_create(&r.cfg, np, q.data(), &h);
@@ -557,7 +714,7 @@ extern "C" int fsl_run_data_main(const char* path) {
   // scheme and quasi2D write none; stokesLimit2D writes the particle velocity
   // array, which that scheme never sets, so zeros (src/saveParticles.cu:43-47,
   // src/gpuToHostStokesLimit.cu:41-43)
-  const bool q2 = r.cfg.scheme >= FSL_SCHEME_QUASI2D;
+  const bool q2 = r.cfg.scheme == FSL_SCHEME_QUASI2D || r.cfg.scheme == FSL_SCHEME_STOKES2D;
   const bool write_forces = r.cfg.scheme == FSL_SCHEME_MIDPOINT || r.cfg.scheme == FSL_SCHEME_STOKES2D;
   std::ofstream fp(r.outputname + ".particles"), fv;
   if (write_forces) fv.open(r.outputname + ".velocityParticles");

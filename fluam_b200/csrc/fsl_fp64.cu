@@ -505,7 +505,8 @@ void launch_interp_update64(const Batch& B, int stage, cudaStream_t s) {
 // The line passes of a forward (dir -1: x, y[, z]) or inverse (dir +1:
 // [z,] y, x, the x pass storing Re / nc) transform of ncomp components over
 // the first naxes axes.
-static void fft64_passes(const Batch& B, int ncomp, int naxes, int dir, cudaStream_t s) {
+static void fft64_passes(const Batch& B, int ncomp, int naxes, int dir, cudaStream_t s,
+                         int to_real = 1) {
   const int m[3] = {B.mx, B.my, B.mz};
   Radix64 rad[3];
   unsigned gb[3];
@@ -521,7 +522,8 @@ static void fft64_passes(const Batch& B, int ncomp, int naxes, int dir, cudaStre
       FSL_GO(k_fft64, dim3(gb[a], B.nrep), kF64Threads, 0, s, B, a, rad[a], -1, 0, ncomp);
   } else {
     for (int a = naxes - 1; a >= 0; --a)
-      FSL_GO(k_fft64, dim3(gb[a], B.nrep), kF64Threads, 0, s, B, a, rad[a], +1, a == 0 ? 1 : 0, ncomp);
+      FSL_GO(k_fft64, dim3(gb[a], B.nrep), kF64Threads, 0, s, B, a, rad[a], +1, a == 0 ? to_real : 0,
+             ncomp);
   }
 }
 
@@ -542,5 +544,9 @@ void launch_solve64(const Batch& B, int nsets, double nfac, cudaStream_t s, Prof
 }
 
 void launch_fft64_2d(const Batch& B, int dir, cudaStream_t s) { fft64_passes(B, 2, 2, dir, s); }
+
+void launch_fft64_3d(const Batch& B, int dir, int to_real, cudaStream_t s) {
+  fft64_passes(B, 3, 3, dir, s, to_real);
+}
 
 }  // namespace fsl

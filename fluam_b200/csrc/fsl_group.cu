@@ -114,8 +114,11 @@ ClassKey class_of(const Params& P) {
 }
 
 int make_params(const fsl_config& c, int64_t np, Params& P) {
-  if (c.scheme < 0 || c.scheme > 3) return errorf(FSL_E_ARG, "unknown scheme %d", c.scheme);
-  const bool two_d = c.scheme >= FSL_SCHEME_QUASI2D;
+  if (c.scheme < 0 || c.scheme > 4) return errorf(FSL_E_ARG, "unknown scheme %d", c.scheme);
+  const bool two_d = c.scheme == FSL_SCHEME_QUASI2D || c.scheme == FSL_SCHEME_STOKES2D;
+  const bool incomp = c.scheme == FSL_SCHEME_INCOMPRESSIBLE;
+  if (incomp && np != 0) return errorf(FSL_E_ARG, "the incompressible scheme has no particles");
+  if (incomp && !(c.density > 0)) return errorf(FSL_E_ARG, "densfluid must be > 0");
   if (two_d && c.mz != 1) return errorf(FSL_E_ARG, "the quasi-2D schemes need cells mx my 1");
   if (c.mx < 3 || c.my < 3 || (!two_d && c.mz < 3))
     return errorf(FSL_E_ARG, "cells must be >= 3 in every direction");
@@ -229,6 +232,14 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
     P.q2_rfd = c.use_rfd ? 1 : 0;
     P.q2_pc = c.predictor_corrector ? 1 : 0;
     P.q2_ndrift = c.ndrift;
+    P.prec = PREC_F64;  // FP64 throughout, as the reference
+  }
+  if (incomp) {
+    // src/createCellsIncompressibleGPU.cu:60-63
+    const double rho = c.density, T = c.temperature, eta = c.shearviscosity, dt = c.dt;
+    P.rho = rho;
+    P.fact1 = std::sqrt((4. * T * eta * dt) / (P.dV * rho * rho));
+    P.fact4 = std::sqrt((2. * T * eta * dt) / (P.dV * rho * rho));
     P.prec = PREC_F64;  // FP64 throughout, as the reference
   }
   P.noise_n = noise_count(P, P.np);
@@ -589,6 +600,32 @@ void group_enqueue_step(Group& g) {
   auto join_noise = [&]() {
     if (fork) cudaStreamWaitEvent(s, g.ev_join, 0);
   };
+  if (g.key.scheme == FSL_SCHEME_INCOMPRESSIBLE) {
+    // src/runSchemeIncompressible.cu:98-141: two substeps on one noise draw,
+    // the advection of the second taken from the prediction
+    join_noise();
+    pr.mark(s, "inc_substep1");
+    launch_inc_w(B, 0, s);
+    launch_fft64_3d(B, -1, 0, s);
+    launch_inc_fourier(B, 1, s);
+    launch_fft64_3d(B, +1, 0, s);
+    launch_inc_pred(B, s);
+    chk("substep 1");
+    pr.mark(s, "inc_substep2");
+    launch_inc_w(B, 1, s);
+    launch_fft64_3d(B, -1, 0, s);
+    launch_inc_fourier(B, 1, s);
+    launch_fft64_3d(B, +1, 1, s);
+    chk("substep 2");
+    pr.count(2 * (1 + 3 + 1 + 3) + 1);
+    pr.mark(s, "counter");
+    launch_step_counter(B, s);
+    chk("counter");
+    pr.count(1);
+    pr.mark(s, nullptr);
+    g.launches = pr.launches;
+    return;
+  }
   if (g.key.scheme >= FSL_SCHEME_QUASI2D) {
     // src/runSchemeQuasi2D.cu:108-250: 2-D cell list and forces, spread
     // force and thermal drift, Fourier-space mobility and noise, update

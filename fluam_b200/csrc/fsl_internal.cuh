@@ -56,10 +56,13 @@ struct Params {
   // prefactor, options
   double q2_var, q2_fact1, q2_kc, q2_lw, q2_shear;
   int q2_kw, q2_rfd, q2_pc, q2_ndrift;
+  // incompressible scheme: fluid density
+  double rho;
 };
 
 // noise count of an instance of P with np particles
 __host__ __device__ inline uint64_t noise_count(const Params& P, int np) {
+  if (P.scheme == 4) return (uint64_t)6 * P.nc;
   if (P.scheme >= 2)
     return (uint64_t)4 * ((uint64_t)P.nc + P.mx + P.my) + (uint64_t)2 * np * P.q2_ndrift;
   return (uint64_t)12 * P.nc + (uint64_t)9 * np;
@@ -459,6 +462,14 @@ void launch_interp_update64(const Batch& B, int stage, cudaStream_t s);
 void launch_solve64(const Batch& B, int nsets, double nfac, cudaStream_t s, Prof* prof);
 // 2-D transforms of two FP64 components (the quasi-2D family)
 void launch_fft64_2d(const Batch& B, int dir, cudaStream_t s);
+// 3-D transforms of three FP64 components; to_real: the inverse's last pass
+// stores Re / nc to Rep::v64 instead of the spectrum
+void launch_fft64_3d(const Batch& B, int dir, int to_real, cudaStream_t s);
+// The incompressible scheme (fsl_inc.cu)
+void launch_inc_w(const Batch& B, int second, cudaStream_t s);
+void launch_inc_fourier(const Batch& B, int solve, cudaStream_t s);
+void launch_inc_pred(const Batch& B, cudaStream_t s);
+void launch_inc_load(const Batch& B, cudaStream_t s);
 // The quasi-2D family (fsl_q2d.cu)
 void launch_q2_forces(const Batch& B, cudaStream_t s);
 void launch_q2_field(const Batch& B, cudaStream_t s, Prof* prof);

@@ -13,11 +13,11 @@ import numpy as np
 
 from . import _lib
 from ._lib import (PAIR_NONE, PAIR_SOFT, PAIR_TABLE_LJ, RFD_PAPER, RFD_REFERENCE, SCHEME_FIRST_ORDER,
-                   SCHEME_MIDPOINT, SCHEME_QUASI2D, SCHEME_STOKES2D, check)
+                   SCHEME_INCOMPRESSIBLE, SCHEME_MIDPOINT, SCHEME_QUASI2D, SCHEME_STOKES2D, check)
 
 __all__ = ["StokesLimit", "Batch", "Server", "make_config", "run_data_main", "parse_data_main", "PAIR_NONE",
            "PAIR_SOFT", "PAIR_TABLE_LJ", "RFD_PAPER", "RFD_REFERENCE", "SCHEME_MIDPOINT",
-           "SCHEME_FIRST_ORDER", "SCHEME_QUASI2D", "SCHEME_STOKES2D"]
+           "SCHEME_FIRST_ORDER", "SCHEME_QUASI2D", "SCHEME_STOKES2D", "SCHEME_INCOMPRESSIBLE"]
 
 
 def _dp(a):
@@ -31,7 +31,8 @@ def _ip(a):
 def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair=PAIR_TABLE_LJ,
                 soft_epsilon=1.0, rfd=RFD_REFERENCE, nonbonded=1, extra_mobility=0.0, seed=0,
                 device=-1, scheme=0, precision=0, radius=1.0, ndrift=1, use_rfd=1,
-                predictor_corrector=0, saffman_kc=0.0, saffman_width=0.0, shear_amp=0.0):
+                predictor_corrector=0, saffman_kc=0.0, saffman_width=0.0, shear_amp=0.0,
+                density=1.0):
     c = _lib.Config()
     _lib.load().fsl_config_defaults(ctypes.byref(c))
     c.mx, c.my, c.mz = (int(x) for x in cells)
@@ -44,6 +45,7 @@ def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair
     # quasi-2D family (scheme SCHEME_QUASI2D / SCHEME_STOKES2D)
     c.radius, c.ndrift, c.use_rfd, c.predictor_corrector = radius, ndrift, use_rfd, predictor_corrector
     c.saffman_kc, c.saffman_width, c.shear_amp = saffman_kc, saffman_width, shear_amp
+    c.density = density  # incompressible scheme
     return c
 
 
@@ -115,6 +117,11 @@ class StokesLimit:
         out = np.empty((3, self.np))
         check(self.L.fsl_get_forces(self.h, _dp(out)))
         return out
+
+    def set_velocity64(self, v):
+        """Initial velocity of the incompressible scheme (projected)."""
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape((3,) + self.shape)
+        check(self.L.fsl_set_velocity_f64(self.h, v.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
 
     def velocity64(self):
         """The fluid velocity of the last solve as float64, in every precision form."""

@@ -50,8 +50,12 @@ enum { FSL_RFD_REFERENCE = 0, FSL_RFD_PAPER = 1 };
  * a quasi-2-D geometry) and stokesLimit2D (2-D Stokes, optionally Saffman-
  * screened) on an mx x my grid (mz = 1): src/runSchemeQuasi2D.cu:20-260 with
  * src/quasi2DFunctions.cu.  FP64 throughout, as the reference. */
+/* FSL_SCHEME_INCOMPRESSIBLE: the fluctuating incompressible Navier-Stokes
+ * solver of keyword incompressible (src/runSchemeIncompressible.cu:20-155),
+ * a fluid without particles (np = 0), FP64; its initial velocity is set by
+ * fsl_set_velocity_f64. */
 enum { FSL_SCHEME_MIDPOINT = 0, FSL_SCHEME_FIRST_ORDER = 1, FSL_SCHEME_QUASI2D = 2,
-       FSL_SCHEME_STOKES2D = 3 };
+       FSL_SCHEME_STOKES2D = 3, FSL_SCHEME_INCOMPRESSIBLE = 4 };
 /* Arithmetic of the fluid side (no counterpart in the reference, which is
  * FP64 throughout).  Particle positions, forces and the cell lists are FP64
  * in every form.
@@ -99,6 +103,8 @@ typedef struct fsl_config {
   double saffman_kc;             /* saffmanCutOffWaveNumber (stokesLimit2D) */
   double saffman_width;          /* saffmanLayerWidth                       */
   double shear_amp;              /* viscosityMeasureAmplitude               */
+  /* incompressible scheme only */
+  double density;                /* densfluid                               */
 } fsl_config;
 
 typedef struct fsl_status {
@@ -155,6 +161,10 @@ int fsl_get_velocity(fsl_handle* h, float* out);
 /* The same as double [3][nc], in every precision form (the only full-precision
  * read of the FP64 form's field). */
 int fsl_get_velocity_f64(fsl_handle* h, double* out);
+/* Incompressible scheme: upload the staggered velocity double [3][nc] and
+ * project it onto divergence-free fields, as the scheme does before its
+ * first step (src/runSchemeIncompressible.cu:82-96). */
+int fsl_set_velocity_f64(fsl_handle* h, const double* in);
 int fsl_get_status(fsl_handle* h, fsl_status* st);
 int fsl_set_step(fsl_handle* h, uint64_t step);
 int fsl_clear_errors(fsl_handle* h);

@@ -714,10 +714,12 @@ void one_step_first_order(orc_state* s) {
 }
 
 void one_step_q2d(orc_state* s);
+void one_step_incompressible(orc_state* s);
 
 void one_step(orc_state* s) {
   if (s->c.scheme == ORC_SCHEME_FIRST_ORDER) return one_step_first_order(s);
   if (s->c.scheme == ORC_SCHEME_QUASI2D || s->c.scheme == ORC_SCHEME_STOKES2D) return one_step_q2d(s);
+  if (s->c.scheme == ORC_SCHEME_INCOMPRESSIBLE) return one_step_incompressible(s);
   const int np = s->np, nc = s->nc;
   const double dt = s->c.dt;
   draw_noise(s);
@@ -768,6 +770,164 @@ void one_step(orc_state* s) {
         s->q[k] = rnew;
       }
   }
+  s->t++;
+}
+
+// ========================================= incompressible fluid (3D) ===
+// The fluctuating incompressible Navier-Stokes solver of keyword
+// incompressible (src/runSchemeIncompressible.cu:20-155): staggered
+// velocities, Crank-Nicolson viscous term and a midpoint advection in two
+// substeps sharing one noise draw, the projection done in Fourier space.
+
+// W = u + dt/2 (eta/rho) L u - (dt/4) A(a) + div(Sigma) per cell, the
+// advection A taken from field a (u in the first substep, the prediction in
+// the second), src/kernelConstructW.cu:32-265 and 266-521; written as the
+// real part of Z.
+void inc_build_W(orc_state* s, const double* a) {
+  const int mx = s->mx, my = s->my, mz = s->mz, nc = s->nc;
+  const double* u = s->v.data();
+  const double* R = s->noise.data();
+  const double idx = s->invdx, idy = s->invdy, idz = s->invdz, dt = s->c.dt;
+  const double nu = s->c.shearviscosity / s->c.density;
+  const double f1 = s->fact1, f4 = s->fact4;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nc; ++i) {
+    const int x = i % mx, y = (i / mx) % my, z = i / (mx * my);
+    auto at = [&](int dx, int dy, int dz) {
+      return (x + dx + mx) % mx + mx * (((y + dy + my) % my) + my * ((z + dz + mz) % mz));
+    };
+    const int v0 = at(0, 0, -1), v1 = at(0, -1, 0), v2 = at(-1, 0, 0), v3 = at(1, 0, 0),
+              v4 = at(0, 1, 0), v5 = at(0, 0, 1);
+    const int pxmy = at(1, -1, 0), pxmz = at(1, 0, -1), mxpy = at(-1, 1, 0), mxpz = at(-1, 0, 1),
+              pymz = at(0, 1, -1), mypz = at(0, -1, 1);
+    const double* ux = u;
+    const double* uy = u + nc;
+    const double* uz = u + 2 * (size_t)nc;
+    double wx = idx * idx * (ux[v3] - 2 * ux[i] + ux[v2]);
+    wx += idy * idy * (ux[v4] - 2 * ux[i] + ux[v1]);
+    wx += idz * idz * (ux[v5] - 2 * ux[i] + ux[v0]);
+    wx = 0.5 * dt * nu * wx;
+    double wy = idx * idx * (uy[v3] - 2 * uy[i] + uy[v2]);
+    wy += idy * idy * (uy[v4] - 2 * uy[i] + uy[v1]);
+    wy += idz * idz * (uy[v5] - 2 * uy[i] + uy[v0]);
+    wy = 0.5 * dt * nu * wy;
+    double wz = idx * idx * (uz[v3] - 2 * uz[i] + uz[v2]);
+    wz += idy * idy * (uz[v4] - 2 * uz[i] + uz[v1]);
+    wz += idz * idz * (uz[v5] - 2 * uz[i] + uz[v0]);
+    wz = 0.5 * dt * nu * wz;
+    wx += ux[i];
+    wy += uy[i];
+    wz += uz[i];
+    // advection of a (momentum flux differences at the faces)
+    const double* ax = a;
+    const double* ay = a + nc;
+    const double* az = a + 2 * (size_t)nc;
+    double advX = idx * ((ax[v3] + ax[i]) * (ax[v3] + ax[i]) - (ax[i] + ax[v2]) * (ax[i] + ax[v2]));
+    advX += idy * ((ax[v4] + ax[i]) * (ay[v3] + ay[i]) - (ax[i] + ax[v1]) * (ay[pxmy] + ay[v1]));
+    advX += idz * ((ax[v5] + ax[i]) * (az[v3] + az[i]) - (ax[i] + ax[v0]) * (az[pxmz] + az[v0]));
+    advX = 0.25 * dt * advX;
+    double advY = idx * ((ay[v3] + ay[i]) * (ax[v4] + ax[i]) - (ay[i] + ay[v2]) * (ax[mxpy] + ax[v2]));
+    advY += idy * ((ay[v4] + ay[i]) * (ay[v4] + ay[i]) - (ay[i] + ay[v1]) * (ay[i] + ay[v1]));
+    advY += idz * ((ay[v5] + ay[i]) * (az[v4] + az[i]) - (ay[i] + ay[v0]) * (az[pymz] + az[v0]));
+    advY = 0.25 * dt * advY;
+    double advZ = idx * ((az[v3] + az[i]) * (ax[v5] + ax[i]) - (az[i] + az[v2]) * (ax[mxpz] + ax[v2]));
+    advZ += idy * ((az[v4] + az[i]) * (ay[v5] + ay[i]) - (az[i] + az[v1]) * (ay[mypz] + ay[v1]));
+    advZ += idz * ((az[v5] + az[i]) * (az[v5] + az[i]) - (az[i] + az[v0]) * (az[i] + az[v0]));
+    advZ = 0.25 * dt * advZ;
+    wx -= advX;
+    wy -= advY;
+    wz -= advZ;
+    // divergence of the traceless symmetric random stress, layout
+    // XX, XY, XZ, YY, YZ, ZZ (src/kernelConstructW.cu:158-212)
+    const size_t n = nc;
+    auto trace = [&](int c) { return R[c] + R[c + 3 * n] + R[c + 5 * n]; };
+    wx += idx * f1 * (R[v3] - trace(v3) / 3.);
+    wy += idy * f1 * (R[v4 + 3 * n] - trace(v4) / 3.);
+    wz += idz * f1 * (R[v5 + 5 * n] - trace(v5) / 3.);
+    wx += idy * f4 * R[i + n];
+    wy += idx * f4 * R[i + n];
+    wx += idz * f4 * R[i + 2 * n];
+    wz += idx * f4 * R[i + 2 * n];
+    wy += idz * f4 * R[i + 4 * n];
+    wz += idy * f4 * R[i + 4 * n];
+    const double tr = trace(i);
+    wx -= idx * f1 * (R[i] - tr / 3.);
+    wy -= idy * f1 * (R[i + 3 * n] - tr / 3.);
+    wz -= idz * f1 * (R[i + 5 * n] - tr / 3.);
+    wx -= idy * f4 * R[v1 + n];
+    wx -= idz * f4 * R[v0 + 2 * n];
+    wy -= idx * f4 * R[v2 + n];
+    wy -= idz * f4 * R[v0 + 4 * n];
+    wz -= idx * f4 * R[v2 + 2 * n];
+    wz -= idy * f4 * R[v1 + 4 * n];
+    s->Z[i] = cplx(wx, 0.0);
+    s->Z[nc + i] = cplx(wy, 0.0);
+    s->Z[2 * nc + i] = cplx(wz, 0.0);
+  }
+}
+
+// Per mode of Z: shift(-1), then either the Crank-Nicolson solve
+// (src/kernelUpdateVIncompressible.cu:20-73) or the projection alone
+// (src/projectionDivergenceFree.cu:21-90), then shift(+1).
+void inc_fourier(orc_state* s, bool solve) {
+  const int mx = s->mx, my = s->my, nc = s->nc;
+  const double dt = s->c.dt, eta = s->c.shearviscosity, rho = s->c.density;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nc; ++i) {
+    const int kz = i / (mx * my), ky = (i % (mx * my)) / mx, kx = i % mx;
+    const int kk[3] = {kx, ky, kz};
+    cplx W[3] = {s->Z[i], s->Z[nc + i], s->Z[2 * (size_t)nc + i]};
+    for (int a = 0; a < 3; ++a) {
+      const double c = s->expKre[a][kk[a]], sn = s->expKim[a][kk[a]];
+      W[a] = cplx(W[a].real() * c + W[a].imag() * sn, W[a].imag() * c - W[a].real() * sn);
+    }
+    const double g[3] = {s->gradK[0][kx], s->gradK[1][ky], s->gradK[2][kz]};
+    const double GG = -(g[0] * g[0]) - (g[1] * g[1]) - (g[2] * g[2]);
+    const double GWr = g[0] * W[0].real() + g[1] * W[1].real() + g[2] * W[2].real();
+    const double GWi = g[0] * W[0].imag() + g[1] * W[1].imag() + g[2] * W[2].imag();
+    cplx V[3] = {W[0], W[1], W[2]};
+    if (i != 0) {
+      const double den = solve ? 1 - 0.5 * dt * eta * GG / rho : 1.0;
+      for (int a = 0; a < 3; ++a) {
+        if (solve)
+          V[a] = cplx((W[a].real() + g[a] * GWr / GG) / den, (W[a].imag() + g[a] * GWi / GG) / den);
+        else
+          V[a] = cplx(W[a].real() + g[a] * GWr / GG, W[a].imag() + g[a] * GWi / GG);
+      }
+    }
+    for (int a = 0; a < 3; ++a) {
+      const double c = s->expKre[a][kk[a]], sn = s->expKim[a][kk[a]];
+      s->Z[(size_t)a * nc + i] = cplx(V[a].real() * c - V[a].imag() * sn, V[a].imag() * c + V[a].real() * sn);
+    }
+  }
+}
+
+void inc_transform(orc_state* s, int sign) {
+  for (int comp = 0; comp < 3; ++comp)
+    fft3d(s->Z.data() + (size_t)comp * s->nc, s->mx, s->my, s->mz, s->Px, s->Py, s->Pz, sign);
+}
+
+// One step of runSchemeIncompressible (src/runSchemeIncompressible.cu:98-146).
+void one_step_incompressible(orc_state* s) {
+  const int nc = s->nc;
+  const size_t n3 = 3 * (size_t)nc;
+  {
+    const size_t n = (size_t)6 * nc;
+    s->noise.resize(n);
+    for (size_t k = 0; k < n; ++k) s->noise[k] = philox_normal(s->c.seed, s->t, k);
+  }
+  inc_build_W(s, s->v.data());
+  inc_transform(s, -1);
+  inc_fourier(s, true);
+  inc_transform(s, +1);
+  // prediction u^{n+1/2} = (u^n + u*) / 2 (src/realToComplex.cu:108-119)
+  std::vector<double> pred(n3);
+  for (size_t k = 0; k < n3; ++k) pred[k] = 0.5 * ((s->Z[k].real() / double(nc)) + s->v[k]);
+  inc_build_W(s, pred.data());
+  inc_transform(s, -1);
+  inc_fourier(s, true);
+  inc_transform(s, +1);
+  for (size_t k = 0; k < n3; ++k) s->v[k] = s->Z[k].real() / (double)nc;
   s->t++;
 }
 
@@ -1178,6 +1338,12 @@ orc_state* orc_create(const orc_config* cfg, int64_t np, const double* q) {
   double T = cfg->temperature, eta = cfg->shearviscosity, dt = cfg->dt;
   s->fact1 = std::sqrt((4. * T * eta) / (s->dV * dt));
   s->fact4 = std::sqrt((2. * T * eta) / (s->dV * dt));
+  if (cfg->scheme == ORC_SCHEME_INCOMPRESSIBLE) {
+    // src/createCellsIncompressibleGPU.cu:60-63
+    const double rho = cfg->density;
+    s->fact1 = std::sqrt((4. * T * eta * dt) / (s->dV * rho * rho));
+    s->fact4 = std::sqrt((2. * T * eta * dt) / (s->dV * rho * rho));
+  }
   s->fact2 = std::sqrt(T * cfg->extra_mobility * dt);
   s->Px.init(s->mx);
   s->Py.init(s->my);
@@ -1300,6 +1466,15 @@ int orc_set_bonds(orc_state* s, int64_t nbonds, const int32_t* bi, const int32_t
 int orc_step(orc_state* s, int64_t nsteps) {
   for (int64_t k = 0; k < nsteps; ++k) one_step(s);
   return 0;
+}
+
+void orc_set_velocity(orc_state* s, const double* v) {
+  const size_t n3 = 3 * (size_t)s->nc;
+  for (size_t k = 0; k < n3; ++k) s->Z[k] = cplx(v[k], 0.0);
+  inc_transform(s, -1);
+  inc_fourier(s, false);
+  inc_transform(s, +1);
+  for (size_t k = 0; k < n3; ++k) s->v[k] = s->Z[k].real() / (double)s->nc;
 }
 
 void orc_get_positions(const orc_state* s, double* out) {

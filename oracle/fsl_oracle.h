@@ -35,8 +35,11 @@ enum { ORC_RFD_REFERENCE = 0, ORC_RFD_PAPER = 1 };
 /* ORC_SCHEME_QUASI2D / ORC_SCHEME_STOKES2D: the Gaussian-blob schemes of
  * keywords quasi2D and stokesLimit2D on an mx x my grid (mz = 1),
  * src/runSchemeQuasi2D.cu:20-260 with src/quasi2DFunctions.cu. */
+/* ORC_SCHEME_INCOMPRESSIBLE: the fluctuating incompressible Navier-Stokes
+ * solver of keyword incompressible (no particles),
+ * src/runSchemeIncompressible.cu:20-155. */
 enum { ORC_SCHEME_MIDPOINT = 0, ORC_SCHEME_FIRST_ORDER = 1, ORC_SCHEME_QUASI2D = 2,
-       ORC_SCHEME_STOKES2D = 3 };
+       ORC_SCHEME_STOKES2D = 3, ORC_SCHEME_INCOMPRESSIBLE = 4 };
 
 typedef struct orc_config {
   int32_t mx, my, mz;
@@ -62,6 +65,7 @@ typedef struct orc_config {
   double saffman_kc;      /* saffmanCutOffWaveNumber (stokesLimit2D)     */
   double saffman_width;   /* saffmanLayerWidth                           */
   double shear_amp;       /* viscosityMeasureAmplitude                   */
+  double density;         /* densfluid (incompressible)                  */
 } orc_config;
 
 typedef struct orc_state orc_state;
@@ -77,6 +81,10 @@ void orc_set_positions(orc_state* s, const double* in);
 void orc_get_predictor(const orc_state* s, double* out);
 void orc_get_forces(const orc_state* s, double* out);
 void orc_get_velocity(const orc_state* s, double* out);
+/* Incompressible scheme: the initial staggered velocity [3][nc], projected
+ * onto divergence-free fields as the scheme does before its first step
+ * (src/runSchemeIncompressible.cu:82-96). */
+void orc_set_velocity(orc_state* s, const double* v);
 uint64_t orc_get_step(const orc_state* s);
 void orc_set_step(orc_state* s, uint64_t t);
 int orc_num_threads(void);

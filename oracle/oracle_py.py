@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 PAIR_NONE, PAIR_TABLE_LJ, PAIR_SOFT = 0, 1, 2
 RFD_REFERENCE, RFD_PAPER = 0, 1
-SCHEME_MIDPOINT, SCHEME_FIRST_ORDER, SCHEME_QUASI2D, SCHEME_STOKES2D = 0, 1, 2, 3
+SCHEME_MIDPOINT, SCHEME_FIRST_ORDER, SCHEME_QUASI2D, SCHEME_STOKES2D, SCHEME_INCOMPRESSIBLE = 0, 1, 2, 3, 4
 
 
 class OrcConfig(ctypes.Structure):
@@ -31,6 +31,7 @@ class OrcConfig(ctypes.Structure):
         ("predictor_corrector", ctypes.c_int32), ("pad_", ctypes.c_int32),
         ("radius", ctypes.c_double), ("saffman_kc", ctypes.c_double),
         ("saffman_width", ctypes.c_double), ("shear_amp", ctypes.c_double),
+        ("density", ctypes.c_double),
     ]
 
 
@@ -58,6 +59,7 @@ def _load():
     L.orc_destroy.argtypes = [vp]
     L.orc_set_bonds.argtypes = [vp, ctypes.c_int64, _I, _I, _D, _D, ctypes.c_int64, _I, _D, _D, _D]
     L.orc_step.argtypes = [vp, ctypes.c_int64]
+    L.orc_set_velocity.argtypes = [vp, _D]
     for name in ("orc_get_positions", "orc_set_positions", "orc_get_predictor",
                  "orc_get_forces", "orc_get_velocity"):
         getattr(L, name).argtypes = [vp, _D]
@@ -127,7 +129,7 @@ class Oracle:
                  kernel=3, pair=PAIR_SOFT, soft_epsilon=1.0, rfd=RFD_REFERENCE,
                  nonbonded=1, extra_mobility=0.0, seed=1, scheme=0, radius=1.0, ndrift=1,
                  use_rfd=1, predictor_corrector=0, saffman_kc=0.0, saffman_width=0.0,
-                 shear_amp=0.0):
+                 shear_amp=0.0, density=1.0):
         self.L = _load()
         q = np.ascontiguousarray(q, dtype=np.float64).reshape(3, -1)
         self.np = q.shape[1]
@@ -139,7 +141,7 @@ class Oracle:
                       seed=seed, pair=pair, rfd=rfd, nonbonded=nonbonded, scheme=scheme,
                       ndrift=ndrift, use_rfd=use_rfd, predictor_corrector=predictor_corrector,
                       radius=radius, saffman_kc=saffman_kc, saffman_width=saffman_width,
-                      shear_amp=shear_amp)
+                      shear_amp=shear_amp, density=density)
         self.cfg = c
         self.h = self.L.orc_create(ctypes.byref(c), self.np, _dp(q))
         if not self.h:
@@ -191,6 +193,12 @@ class Oracle:
         out = np.empty((3, self.np))
         self.L.orc_get_forces(self.h, _dp(out))
         return out
+
+    def set_velocity(self, v):
+        """Initial velocity of the incompressible scheme, projected as the
+        scheme does before its first step."""
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(3, self.nc)
+        self.L.orc_set_velocity(self.h, _dp(v))
 
     def velocity(self):
         out = np.empty((3,) + self.shape)

@@ -45,6 +45,10 @@ GPU_FILES = [
     "quasiNeutrallyBuoyantFunctions2D.cu", "createCellsQuasi2DGPU.cu", "freeCellsQuasi2DGPU.cu",
     "createBoundariesQuasi2DGPU.cu", "freeBoundariesQuasi2DGPU.cu", "quasi2DFunctions.cu",
     "texturesCellsQuasi2D.cu", "runSchemeQuasi2D.cu",
+    # the incompressible scheme (src/GPU.cu:158-171)
+    "projectionDivergenceFree.cu", "saveFunctionsSchemeIncompressible.cu",
+    "createCellsIncompressibleGPU.cu", "freeCellsIncompressibleGPU.cu", "gpuToHostIncompressible.cu",
+    "kernelConstructW.cu", "kernelUpdateVIncompressible.cu", "runSchemeIncompressible.cu",
 ]
 GPU_HEADERS = ["header.h", "cells.h", "fluid.h", "boundary.h", "headerOtherFluidVariables.h",
                "particles.h", "hydroAnalysis.h"]
@@ -53,6 +57,7 @@ GPU_HEADERS = ["header.h", "cells.h", "fluid.h", "boundary.h", "headerOtherFluid
 HOST_FILES = [
     "main.cpp", "loadDataMain.cu", "cudaDevice.cu", "initializeRandomNumber.cpp", "rantest.cu",
     "gauss.cu", "schemeStokesLimit.cu", "schemeStokesLimitFirstOrder.cu", "schemeQuasi2D.cu",
+    "schemeIncompressible.cu", "temperature.cu", "saveFluidFinalConfiguration.cu",
     "createCells.cpp", "createParticles.cpp",
     "simpleCubic.cpp", "initializeBondedForces.cpp", "initializeFluid.cpp", "modu.cu",
     "saveSeed.cpp", "saveTime.cpp", "saveParticles.cu", "freeParticles.cu", "random_frenk.cu",

@@ -49,7 +49,6 @@ FLUAM_SCHEME_STUB(schemeCompressibleParticles)
 FLUAM_SCHEME_STUB(schemeContinuousGradient)
 FLUAM_SCHEME_STUB(schemeFreeEnergyCompressibleParticles)
 FLUAM_SCHEME_STUB(schemeGiantFluctuations)
-FLUAM_SCHEME_STUB(schemeIncompressible)
 FLUAM_SCHEME_STUB(schemeIncompressibleBinaryMixture)
 FLUAM_SCHEME_STUB(schemeIncompressibleBinaryMixtureMidPoint)
 FLUAM_SCHEME_STUB(schemeIncompressibleBoundary)

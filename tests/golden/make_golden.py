@@ -224,6 +224,34 @@ numsteps 4
 samplefreq 2
 dt 0.05
 """),
+    # the incompressible fluctuating fluid (keyword incompressible, no
+    # particles): a uniform start, noise-driven with advection
+    "inc_fluid": dict(scheme="incompressible", fluid_only=True, text="""densfluid 1.3
+shearviscosity 0.7
+temperature 0.5
+cells 12 16 20
+celldimension 12 16 20
+initfluid 0
+backgroundvelocity 0.1 -0.05 0.02
+numstepsRelaxation 1
+numsteps 4
+samplefreq 2
+dt 0.05
+seed 3
+"""),
+    # a non-cubic box, stronger advection (large background flow)
+    "inc_fluid_flow": dict(scheme="incompressible", fluid_only=True, text="""densfluid 0.8
+shearviscosity 1.1
+temperature 0.05
+cells 16 10 14
+celldimension 24 15 14
+initfluid 0
+backgroundvelocity 0.8 0.3 -0.4
+numsteps 6
+samplefreq 3
+dt 0.1
+seed 8
+"""),
 }
 
 
@@ -236,6 +264,8 @@ def make_case(name, spec):
         common = COMMON
         if "scheme" in spec:
             common = common.replace("stokesLimit\n", spec["scheme"] + "\n", 1)
+        if spec.get("fluid_only"):  # a fluid without particles
+            common = spec["scheme"] + "\noutputname out\n"
         f.write(common + spec["text"])
     if "coor" in spec:
         write_coor(os.path.join(d, "start.coor"), spec["coor"]())
@@ -254,6 +284,10 @@ def make_case(name, spec):
         raise RuntimeError(f"{name}: reference run failed\n{r.stdout[-2000:]}")
     for ext in (".cuda", ".time", ".data.main"):
         os.remove(os.path.join(d, "out" + ext))
+    if spec.get("fluid_only"):
+        # the particle-free scheme writes its final field with the cells' full
+        # 15 digits; keep the fixtures small
+        assert os.path.getsize(os.path.join(d, "out.fluidFinalConfiguration")) < 400_000
 
 
 if __name__ == "__main__":

@@ -56,7 +56,37 @@ def simple_cubic(np_, lx, ly, lz, dim=3):
 
 
 def cases():
-    return sorted(d for d in os.listdir(GOLDEN) if os.path.isdir(os.path.join(GOLDEN, d)))
+    """Cases with particles (an out.particles file)."""
+    return sorted(d for d in os.listdir(GOLDEN)
+                  if os.path.exists(os.path.join(GOLDEN, d, "out.particles")))
+
+
+def fluid_cases():
+    """Cases of the particle-free incompressible scheme."""
+    return sorted(d for d in os.listdir(GOLDEN)
+                  if os.path.exists(os.path.join(GOLDEN, d, "out.fluidFinalConfiguration"))
+                  and not os.path.exists(os.path.join(GOLDEN, d, "out.particles")))
+
+
+def read_fluid_final(path, nc):
+    """The velocity [3][nc] of a .fluidFinalConfiguration file."""
+    lines = open(path).read().split("\n")
+    assert lines[11] == "Velocity"
+    return np.array([lines[13 + 2 * i].split() for i in range(nc)], dtype=float).T.copy()
+
+
+def load_fluid(name):
+    from fluam_b200 import parse_data_main
+    d = os.path.join(GOLDEN, name)
+    cfg, run = parse_data_main(os.path.join(d, "data.main"))
+    words = open(os.path.join(d, "data.main")).read().split()
+    k = words.index("backgroundvelocity")
+    v0 = [float(x) for x in words[k + 1:k + 4]]
+    nc = cfg.mx * cfg.my * cfg.mz
+    return dict(dir=d, cfg=cfg, run=run, v0=v0, nc=nc,
+                v=read_fluid_final(os.path.join(d, "out.fluidFinalConfiguration"), nc),
+                temperature=open(os.path.join(d, "out.temperature")).read(),
+                seed=int(open(os.path.join(d, "out.seed")).read()))
 
 
 def load(name):

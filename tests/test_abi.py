@@ -33,8 +33,8 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_config_layout_matches_header():
-    # fsl_config: 4 int32, 9 doubles, 1 uint64, 10 int32, 4 doubles
-    assert ctypes.sizeof(_lib.Config) == 4 * 4 + 9 * 8 + 8 + 10 * 4 + 4 * 8
+    # fsl_config: 4 int32, 9 doubles, 1 uint64, 10 int32, 5 doubles
+    assert ctypes.sizeof(_lib.Config) == 4 * 4 + 9 * 8 + 8 + 10 * 4 + 5 * 8
     assert ctypes.sizeof(_lib.Status) == 8 + 4 + 4 + 8 + 4 + 4
 
 

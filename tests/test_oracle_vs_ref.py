@@ -78,3 +78,32 @@ def test_golden_files_regenerate_identically(tmp_path, name):
         assert os.path.exists(mine) == os.path.exists(ref), ext
         if os.path.exists(ref):
             assert open(mine).read() == open(ref).read()
+
+
+@pytest.mark.parametrize("name", G.fluid_cases())
+def test_oracle_reproduces_reference_fluid(oracle, name):
+    """The incompressible scheme: the final field of the reference (the last
+    sample, here the last step) from the same uniform start and noise."""
+    c = G.load_fluid(name)
+    cfg = c["cfg"]
+    o = oracle.Oracle(cfg.mx, cfg.my, cfg.mz, cfg.lx, cfg.ly, cfg.lz, np.zeros((3, 0)),
+                      eta=cfg.shearviscosity, kT=cfg.temperature, dt=cfg.dt, seed=c["seed"],
+                      scheme=oracle.SCHEME_INCOMPRESSIBLE, density=cfg.density)
+    v0 = np.repeat(np.asarray(c["v0"])[:, None], c["nc"], axis=1)
+    o.set_velocity(v0)
+    o.step(c["run"]["numsteps"] + c["run"]["numstepsRelaxation"])
+    v = o.velocity().reshape(3, -1)
+    assert np.abs(v - c["v"]).max() <= 1e-12 * np.abs(c["v"]).max() * 10
+
+
+@pytest.mark.parametrize("name", G.fluid_cases())
+def test_fluid_golden_files_regenerate_identically(tmp_path, name):
+    if not (os.path.exists(FLUAM_REF) and os.path.isdir("/root/reference/src")):
+        pytest.skip("reference host build not available here")
+    src = os.path.join(G.GOLDEN, name)
+    shutil.copy(os.path.join(src, "data.main"), tmp_path / "data.main")
+    r = subprocess.run([FLUAM_REF, "data.main"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600)
+    assert "END" in r.stdout, r.stdout[-1000:]
+    for ext in (".fluidFinalConfiguration", ".temperature", ".seed"):
+        assert open(tmp_path / ("out" + ext)).read() == open(os.path.join(src, "out" + ext)).read()
