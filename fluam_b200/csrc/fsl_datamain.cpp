@@ -643,7 +643,8 @@ extern "C" int fsl_run_data_main(const char* path) {
   std::cout << "READ " << (path ? path : "data.main") << " :                DONE" << std::endl;
   if (!r.other_schemes.empty() ||
       !(r.stokesLimit || r.first_order || r.quasi2D || r.stokes2D || r.incomp)) {
-    std::cout << "ERROR: this build runs the stokesLimit and stokesLimitFirstOrder schemes only"
+    std::cout << "ERROR: this build runs the stokesLimit, stokesLimitFirstOrder, quasi2D, "
+                 "stokesLimit2D and incompressible schemes only"
               << (r.other_schemes.empty() ? std::string(" (keyword stokesLimit missing)")
                                           : " (found " + r.other_schemes[0] + ")")
               << std::endl;

@@ -171,9 +171,17 @@ def test_errors_are_reported(tmp_path):
     p.write_text("stokesLimit\ncells 8 8 8\nsamplefreq 0\noutputname x\n")
     r = subprocess.run([FLUAM, str(p)], capture_output=True, text=True, cwd=tmp_path)
     assert r.returncode == 0 and "samplefreq" in r.stdout
-    p.write_text("incompressible\ncells 8 8 8\nsamplefreq 1\noutputname x\n")
+    # a scheme this build does not run
+    p.write_text("incompressibleBinaryMixture\ncells 8 8 8\nsamplefreq 1\noutputname x\n")
     r = subprocess.run([FLUAM, str(p)], capture_output=True, text=True, cwd=tmp_path)
     assert r.returncode == 0 and "stokesLimit" in r.stdout
+    # the incompressible scheme needs a density and rejects particles
+    p.write_text("incompressible\ncells 8 8 8\nsamplefreq 1\noutputname x\n")
+    r = subprocess.run([FLUAM, str(p)], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 0 and "densfluid" in r.stdout
+    p.write_text("incompressible\nparticles 1\ndensfluid 1\ncells 8 8 8\nsamplefreq 1\noutputname x\n")
+    r = subprocess.run([FLUAM, str(p)], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 0 and "incompressibleBoundary" in r.stdout
 
 
 def test_fluid_output_files(tmp_path, fsl):
