@@ -453,30 +453,28 @@ __device__ __forceinline__ void spread_entry(const Params& P, const double posc[
   }
 }
 
-// drift = 0: entries [0, np) spread F at q; drift = 1: entries [0, np) spread
-// F at q^{n+1/2}, entries [np, 2np) the RFD drift of one particle each:
-// (kT/delta) sign W_p from q + sign (delta/2) W_p for both signs.  In
-// reference mode the drift's nodes come from the displaced position and its
-// weights from q, as the reference does.
+// One warp per particle (in cell order when ordered).  drift = 0: F at q;
+// drift = 1: F at q^{n+1/2}, then the particle's RFD drift (kT/delta) sign
+// W_p from q + sign (delta/2) W_p for both signs; drift = 2: F at q and the
+// drift.  In reference mode the drift's nodes come from the displaced
+// position and its weights from q, as the reference does.
 template <bool ONE, int KN>
 __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
-  FSL_REP_FLAT(drift ? KIND_T64 : KIND_T32);
+  FSL_REP_FLAT(KIND_T32);
   const int lane = threadIdx.x & 31;
   const long e = (long)((blk * (size_t)blockDim.x + threadIdx.x) >> 5);
   const int np = P.np;
-  const long nent = (long)np * (drift ? 2 : 1);
-  if (e >= nent) return;  // uniform per warp
-  const int* order = ordered ? R.sorted : nullptr;
+  if (e >= np) return;  // uniform per warp
+  const int i = ordered ? R.sorted[e] : (int)e;
   bool sat = false;
-  if (e < np) {
+  {
     const double* qf = drift == 1 ? R.qp : R.q;
-    int i = order ? order[e] : (int)e;
     double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
     double val[3] = {R.F[i], R.F[np + i], R.F[2 * (size_t)np + i]};
     spread_entry<KN>(P, pos, pos, val, R.grid, lane, sat);
-  } else {
-    int i = (int)(e - np);
-    if (order) i = order[i];
+  }
+  if (drift) {
+    // the RFD drift of the same particle, by the same warp
     const size_t wbase = (size_t)6 * P.nc;
     double W[3] = {(double)R.noise[wbase + i], (double)R.noise[wbase + np + i],
                    (double)R.noise[wbase + 2 * np + i]};
@@ -501,9 +499,10 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
         const double b = d == 0 ? pm[0] : (d == 1 ? pm[1] : pm[2]);
         same = stencil_base(P, d, f, a) == stencil_base(P, d, f, b);
       }
-      if (__all_sync(0xffffffffu, same)) return;
-      spread_entry<KN>(P, pp, pos, vp, R.grid, lane, sat);
-      spread_entry<KN>(P, pm, pos, vm, R.grid, lane, sat);
+      if (!__all_sync(0xffffffffu, same)) {
+        spread_entry<KN>(P, pp, pos, vp, R.grid, lane, sat);
+        spread_entry<KN>(P, pm, pos, vm, R.grid, lane, sat);
+      }
     } else {
       spread_entry<KN>(P, pp, pp, vp, R.grid, lane, sat);
       spread_entry<KN>(P, pm, pm, vm, R.grid, lane, sat);
@@ -515,7 +514,7 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
 void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s) {
   if (B.max_np == 0) return;
   if (B.prec == PREC_F64) return launch_spread64(B, drift, s);
-  const unsigned g = part_blocks(B, drift ? KIND_T64 : KIND_T32);
+  const unsigned g = part_blocks(B, KIND_T32);
   if (B.kernel == 4)
     FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered);
   else
