@@ -23,7 +23,7 @@ EXPORTS = [
     "fsl_config_defaults", "fsl_create", "fsl_load_bonds", "fsl_step", "fsl_sync",
     "fsl_get_positions", "fsl_set_positions", "fsl_get_forces", "fsl_get_velocity",
     "fsl_get_velocity_f64", "fsl_set_velocity_f64",
-    "fsl_get_status", "fsl_set_step", "fsl_clear_errors", "fsl_set_graph", "fsl_stream",
+    "fsl_get_status", "fsl_get_observables", "fsl_reset_observables", "fsl_set_step", "fsl_clear_errors", "fsl_set_graph", "fsl_stream",
     "fsl_profile", "fsl_profile_read",
     "fsl_destroy", "fsl_last_error", "fsl_run_data_main", "fsl_parse_data_main",
     "fsl_write_fluid_final", "fsl_write_fluid_vtk",
@@ -31,6 +31,7 @@ EXPORTS = [
     "fsl_interpolate", "fsl_noise", "fsl_cell_list_noalloc",
     "fsl_batch_create", "fsl_batch_load_bonds", "fsl_batch_step", "fsl_batch_sync",
     "fsl_batch_get_positions", "fsl_batch_get_forces", "fsl_batch_get_status",
+    "fsl_batch_get_observables", "fsl_batch_reset_observables",
     "fsl_batch_get_positions_packed", "fsl_batch_set_positions_packed",
     "fsl_batch_get_positions_packed_async", "fsl_batch_set_positions_packed_async",
     "fsl_batch_set_graph", "fsl_batch_get_info", "fsl_batch_stream", "fsl_batch_destroy",
@@ -54,7 +55,7 @@ class Config(ctypes.Structure):
         ("scheme", ctypes.c_int32),
         ("precision", ctypes.c_int32),
         ("ndrift", ctypes.c_int32), ("use_rfd", ctypes.c_int32),
-        ("predictor_corrector", ctypes.c_int32), ("reserved_", ctypes.c_int32),
+        ("predictor_corrector", ctypes.c_int32), ("observables", ctypes.c_int32),
         ("radius", ctypes.c_double), ("saffman_kc", ctypes.c_double),
         ("saffman_width", ctypes.c_double), ("shear_amp", ctypes.c_double),
         ("density", ctypes.c_double),
@@ -66,6 +67,19 @@ class Status(ctypes.Structure):
         ("step", ctypes.c_uint64), ("error_bits", ctypes.c_int32), ("np", ctypes.c_int32),
         ("nc", ctypes.c_int64), ("graph", ctypes.c_int32), ("launches_per_step", ctypes.c_int32),
     ]
+
+
+class Observables(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int64), ("msd", ctypes.c_double), ("msd_sum", ctypes.c_double),
+        ("displacement", ctypes.c_double * 3), ("force", ctypes.c_double * 3),
+        ("momentum", ctypes.c_double * 3), ("momentum_sum", ctypes.c_double * 3),
+    ]
+
+    def as_dict(self):
+        return dict(steps=self.steps, msd=self.msd, msd_sum=self.msd_sum,
+                    displacement=list(self.displacement), force=list(self.force),
+                    momentum=list(self.momentum), momentum_sum=list(self.momentum_sum))
 
 
 class StageTime(ctypes.Structure):
@@ -136,6 +150,8 @@ def load(path=None):
     L.fsl_set_velocity_f64.argtypes = [_VP, _D]
     L.fsl_get_status.argtypes = [_VP, ctypes.POINTER(Status)]
     L.fsl_set_step.argtypes = [_VP, ctypes.c_uint64]
+    L.fsl_get_observables.argtypes = [_VP, ctypes.POINTER(Observables)]
+    L.fsl_reset_observables.argtypes = [_VP]
     L.fsl_clear_errors.argtypes = [_VP]
     L.fsl_set_graph.argtypes = [_VP, ctypes.c_int]
     L.fsl_stream.argtypes = [_VP]
@@ -172,6 +188,8 @@ def load(path=None):
     L.fsl_batch_get_positions.argtypes = [_VP, ctypes.c_int32, _D]
     L.fsl_batch_get_forces.argtypes = [_VP, ctypes.c_int32, _D]
     L.fsl_batch_get_status.argtypes = [_VP, ctypes.c_int32, ctypes.POINTER(Status)]
+    L.fsl_batch_get_observables.argtypes = [_VP, ctypes.c_int32, ctypes.POINTER(Observables)]
+    L.fsl_batch_reset_observables.argtypes = [_VP, ctypes.c_int32]
     L.fsl_batch_get_positions_packed.argtypes = [_VP, _D]
     L.fsl_batch_set_positions_packed.argtypes = [_VP, _D]
     L.fsl_batch_get_positions_packed_async.argtypes = [_VP, _VP]

@@ -268,6 +268,19 @@ int fsl_get_status(fsl_handle* h, fsl_status* st) {
   return FSL_OK;
 }
 
+int fsl_get_observables(fsl_handle* h, fsl_observables* out) {
+  if (!h || !out) return errorf(FSL_E_ARG, "null argument");
+  FSL_TRY(cudaSetDevice(h->exec.device));
+  return fsl::slot_read_observables(h->slot, h->exec.stream, out);
+}
+
+int fsl_reset_observables(fsl_handle* h) {
+  if (!h) return errorf(FSL_E_ARG, "null handle");
+  if (!params(h).observe) return errorf(FSL_E_ARG, "observables are off (fsl_config.observables = 0)");
+  FSL_TRY(cudaSetDevice(h->exec.device));
+  return fsl::slot_reset_observables(h->slot, h->exec.stream);
+}
+
 int fsl_set_step(fsl_handle* h, uint64_t step) {
   if (!h) return errorf(FSL_E_ARG, "null handle");
   FSL_TRY(cudaSetDevice(h->exec.device));

@@ -250,6 +250,22 @@ int fsl_batch_get_status(fsl_batch* b, int32_t i, fsl_status* st) {
   return FSL_OK;
 }
 
+int fsl_batch_get_observables(fsl_batch* b, int32_t i, fsl_observables* out) {
+  int rc = check_index(b, i);
+  if (rc) return rc;
+  if (!out) return errorf(FSL_E_ARG, "null argument");
+  FSL_TRY(cudaSetDevice(b->exec.device));
+  return fsl::slot_read_observables(*b->slots[i], b->exec.stream, out);
+}
+
+int fsl_batch_reset_observables(fsl_batch* b, int32_t i) {
+  int rc = check_index(b, i);
+  if (rc) return rc;
+  if (!b->slots[i]->r.P.observe) return errorf(FSL_E_ARG, "instance %d: observables are off", i);
+  FSL_TRY(cudaSetDevice(b->exec.device));
+  return fsl::slot_reset_observables(*b->slots[i], b->exec.stream);
+}
+
 int fsl_batch_get_positions_packed_async(fsl_batch* b, double* host) {
   if (!b || !host) return errorf(FSL_E_ARG, "null argument");
   FSL_TRY(cudaSetDevice(b->exec.device));

@@ -5,10 +5,12 @@
 //   followed by a fixed number of values; '#' starts a comment to end of line;
 //   an unknown keyword is an error ("ERROR INPUT FILE").  Every keyword of the
 //   reference parser is accepted and consumes the same tokens; the ones that
-//   the Stokes-limit path does not read are ignored.  Five keywords are new
+//   the Stokes-limit path does not read are ignored.  Six keywords are new
 //   (the reference parser would reject them): pairPotential lj|soft|none,
 //   softEpsilon <eps>, kernelPoints 3|4, rfdMode reference|paper,
-//   precision fixed64|float_atomic|fp64.
+//   precision fixed64|float_atomic|fp64, observables 0|1 (3-D Stokes
+//   schemes: <out>.observables, one line per sample: step*dt, msd, msd summed
+//   over the steps, centre-of-mass displacement, total force, fluid momentum).
 // Output (src/saveFunctionsSchemeStokesLimit.cu, src/saveParticles.cu:32-82,
 //   src/saveSeed.cpp, src/saveTime.cpp, src/cudaDevice.cu):
 //   <out>.data.main echo, <out>.cuda, <out>.seed, <out>.time,
@@ -16,6 +18,7 @@
 //   per sample a line step*dt and np lines "x y z", precision 15).
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <ctime>
 #include <fstream>
@@ -84,7 +87,7 @@ const std::map<std::string, int>& keyword_arity() {
       {"stokesLimitFirstOrder", 0}, {"stokesLimit", 0}, {"extraMobility", 1},
       // extensions of this build
       {"pairPotential", 1}, {"softEpsilon", 1}, {"kernelPoints", 1}, {"rfdMode", 1},
-      {"precision", 1}, {"savedensity", -1}};
+      {"precision", 1}, {"observables", 1}, {"savedensity", -1}};
   return m;
 }
 
@@ -224,6 +227,8 @@ int parse(const char* path, Run& r, std::string& err) {
           err = "rfdMode must be reference or paper";
           return FSL_E_INPUT;
         }
+      } else if (word == "observables") {
+        c.observables = std::atoi(vals[0].c_str());
       } else if (word == "precision") {
         if (vals[0] == "fixed64") c.precision = FSL_PRECISION_FIXED64;
         else if (vals[0] == "float_atomic") c.precision = FSL_PRECISION_FLOAT_ATOMIC;
@@ -721,6 +726,12 @@ extern "C" int fsl_run_data_main(const char* path) {
   if (write_forces) fv.open(r.outputname + ".velocityParticles");
   fp.precision(15);
   fv.precision(15);
+  std::ofstream fo;
+  if (r.cfg.observables && !q2) {
+    fo.open(r.outputname + ".observables");
+    fo.precision(15);
+    fo << "# time msd msd_sum dx dy dz Fx Fy Fz Px Py Pz" << std::endl;
+  }
   fp << "#NUMBER PARTICLES " << np << std::endl;
   if (write_forces) fv << "#NUMBER PARTICLES " << np << std::endl;
   std::vector<double> pos(3 * np), frc(3 * np);
@@ -772,6 +783,15 @@ extern "C" int fsl_run_data_main(const char* path) {
       if ((rc = fsl_get_positions(h, pos.data())) || (rc = fsl_get_forces(h, frc.data()))) break;
       write_sample(fp, np, pos, step * r.cfg.dt);
       if (write_forces) write_sample(fv, np, frc, step * r.cfg.dt);
+      if (r.cfg.observables) {
+        fsl_observables o;
+        if ((rc = fsl_get_observables(h, &o))) break;
+        fo << step * r.cfg.dt << " " << o.msd << " " << o.msd_sum;
+        for (double x : o.displacement) fo << " " << x;
+        for (double x : o.force) fo << " " << x;
+        for (double x : o.momentum) fo << " " << x;
+        fo << std::endl;
+      }
       // fluid snapshots at sample steps that are multiples of savefreq, as
       // the reference's other schemes do (src/saveFunctionsSchemeIncompressibleBoundary.cu:43-46)
       if (r.save_vtk && r.savefreq > 0 && step % r.savefreq == 0 &&

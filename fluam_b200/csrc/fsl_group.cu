@@ -25,7 +25,8 @@ size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 // Byte offsets of one slot's buffers inside its arena.
 struct SlotLayout {
   size_t q, qp, F, u, qw, ws, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
-      bsum, ljtab, noise, grid, spec, v, wbuf, noise64, v64, z64, err, t, total;
+      bsum, ljtab, noise, grid, spec, v, wbuf, noise64, v64, z64, err, t, q0, obs, obs_part, obs_ticket,
+      total;
 };
 
 SlotLayout layout(const Params& P, int np_cap) {
@@ -71,6 +72,10 @@ SlotLayout layout(const Params& P, int np_cap) {
   L.z64 = take(f64 ? sizeof(double2) * 3 * nc : 0);
   L.err = take(sizeof(int) * 4);
   L.t = take(sizeof(uint64_t));
+  L.q0 = take(P.observe ? sizeof(double) * 3 * np : 0);
+  L.obs = take(sizeof(double) * kObsSlots);
+  L.obs_part = take(P.observe ? sizeof(double) * kObsVals * kObsMaxBlocks : 0);
+  L.obs_ticket = take(sizeof(unsigned));
   L.total = off;
   return L;
 }
@@ -103,14 +108,14 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 bool ClassKey::operator<(const ClassKey& o) const {
-  const int a[9] = {mx, my, mz, mnx, mny, mnz, kernel, scheme, prec};
-  const int b[9] = {o.mx, o.my, o.mz, o.mnx, o.mny, o.mnz, o.kernel, o.scheme, o.prec};
-  return std::lexicographical_compare(a, a + 9, b, b + 9);
+  const int a[10] = {mx, my, mz, mnx, mny, mnz, kernel, scheme, prec, observe};
+  const int b[10] = {o.mx, o.my, o.mz, o.mnx, o.mny, o.mnz, o.kernel, o.scheme, o.prec, o.observe};
+  return std::lexicographical_compare(a, a + 10, b, b + 10);
 }
 bool ClassKey::operator==(const ClassKey& o) const { return !(*this < o) && !(o < *this); }
 
 ClassKey class_of(const Params& P) {
-  return ClassKey{P.mx, P.my, P.mz, P.mnx, P.mny, P.mnz, P.kernel, P.scheme, P.prec};
+  return ClassKey{P.mx, P.my, P.mz, P.mnx, P.mny, P.mnz, P.kernel, P.scheme, P.prec, P.observe};
 }
 
 int make_params(const fsl_config& c, int64_t np, Params& P) {
@@ -137,6 +142,9 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   if (c.precision < 0 || c.precision > 2)
     return errorf(FSL_E_ARG, "unknown precision form %d", c.precision);
   if (c.extra_mobility < 0) return errorf(FSL_E_ARG, "extraMobility must be >= 0");
+  if (c.observables != 0 && c.observables != 1) return errorf(FSL_E_ARG, "observables must be 0 or 1");
+  if (c.observables && c.scheme > FSL_SCHEME_FIRST_ORDER)
+    return errorf(FSL_E_ARG, "observables: 3-D Stokes schemes only");
   if (np < 0 || np > (int64_t)1 << 28) return errorf(FSL_E_ARG, "bad particle count");
   bool pairs = c.nonbonded && c.pair != FSL_PAIR_NONE && np > 0;
   if (pairs && !(c.cutoff > 0)) return errorf(FSL_E_ARG, "cutoff must be > 0 with pair forces");
@@ -163,6 +171,7 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   P.invly = 1. / c.ly;
   P.invlz = 1. / c.lz;
   P.dV = P.dx * P.dy * P.dz;
+  P.observe = c.observables;
   // src/createBoundariesRK2GPU.cu:134-141
   if (c.cutoff > 0) {
     P.mnx = std::max(3, (int)(c.lx / c.cutoff));
@@ -315,6 +324,10 @@ int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st) {
   r.z64 = f64 ? (double2*)(base + L.z64) : nullptr;
   r.err = (int*)(base + L.err);
   r.t = (uint64_t*)(base + L.t);
+  r.q0 = P.observe ? (double*)(base + L.q0) : nullptr;
+  r.obs = (double*)(base + L.obs);
+  r.obs_part = P.observe ? (double*)(base + L.obs_part) : nullptr;
+  r.obs_ticket = (unsigned*)(base + L.obs_ticket);
   return FSL_OK;
 }
 
@@ -325,6 +338,34 @@ void slot_free(Slot& s) {
   s.bytes = 0;
   s.np_cap = 0;
   std::memset(&s.r, 0, sizeof(s.r));
+}
+
+int slot_read_observables(const Slot& s, cudaStream_t st, fsl_observables* out) {
+  const Rep& r = s.r;
+  if (!r.P.observe) return errorf(FSL_E_ARG, "observables are off (fsl_config.observables = 0)");
+  double o[kObsSlots];
+  FSL_TRY(cudaMemcpyAsync(o, r.obs, sizeof(o), cudaMemcpyDeviceToHost, st));
+  FSL_TRY(cudaStreamSynchronize(st));
+  std::memset(out, 0, sizeof(*out));
+  out->steps = (int64_t)o[0];
+  out->msd = o[1];
+  out->msd_sum = o[2];
+  for (int d = 0; d < 3; ++d) {
+    out->displacement[d] = o[3 + d];
+    out->force[d] = o[6 + d];
+    out->momentum[d] = o[9 + d];
+    out->momentum_sum[d] = o[12 + d];
+  }
+  return FSL_OK;
+}
+
+int slot_reset_observables(Slot& s, cudaStream_t st) {
+  Rep& r = s.r;
+  if (r.P.observe && r.P.np > 0)
+    FSL_TRY(cudaMemcpyAsync(r.q0, r.q, sizeof(double) * 3 * (size_t)r.P.np, cudaMemcpyDeviceToDevice, st));
+  FSL_TRY(cudaMemsetAsync(r.obs, 0, sizeof(double) * kObsSlots, st));
+  FSL_TRY(cudaMemsetAsync(r.obs_ticket, 0, sizeof(unsigned), st));
+  return FSL_OK;
 }
 
 int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, cudaStream_t st) {
@@ -362,6 +403,7 @@ int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, c
     FSL_TRY(cudaMemsetAsync(r.v, 0, sizeof(float) * 3 * (size_t)P.nc, st));
   FSL_TRY(cudaMemsetAsync(r.err, 0, sizeof(int) * 4, st));
   FSL_TRY(cudaMemsetAsync(r.t, 0, sizeof(uint64_t), st));
+  if (int rc = slot_reset_observables(s, st)) return rc;
   r.active = 1;
   return FSL_OK;
 }
@@ -600,6 +642,13 @@ void group_enqueue_step(Group& g) {
   auto join_noise = [&]() {
     if (fork) cudaStreamWaitEvent(s, g.ev_join, 0);
   };
+  auto observe = [&]() {
+    if (!g.key.observe) return;
+    pr.mark(s, "observe");
+    launch_observe(B, s);
+    chk("observe");
+    pr.count(1);
+  };
   if (g.key.scheme == FSL_SCHEME_INCOMPRESSIBLE) {
     // src/runSchemeIncompressible.cu:98-141: two substeps on one noise draw,
     // the advection of the second taken from the prediction
@@ -677,6 +726,7 @@ void group_enqueue_step(Group& g) {
     launch_interp_update(B, 2, s);
     chk("interp_update");
     pr.count(pk);
+    observe();
     pr.mark(s, "counter");
     launch_step_counter(B, s);
     chk("counter");
@@ -714,6 +764,7 @@ void group_enqueue_step(Group& g) {
   launch_interp_update(B, 2, s);
   chk("interp_update");
   pr.count(pk);
+  observe();
   pr.mark(s, "counter");
   launch_step_counter(B, s);
   chk("counter");

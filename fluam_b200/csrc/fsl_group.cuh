@@ -38,7 +38,7 @@ int make_params(const fsl_config& c, int64_t np, Params& P);
 
 // Size-class key: instances that can share every launch of a step.
 struct ClassKey {
-  int mx, my, mz, mnx, mny, mnz, kernel, scheme, prec;
+  int mx, my, mz, mnx, mny, mnz, kernel, scheme, prec, observe;
   bool operator<(const ClassKey& o) const;
   bool operator==(const ClassKey& o) const;
 };
@@ -64,6 +64,10 @@ void slot_free(Slot& s);
 // allocated slot of its class: positions, LJ table, cleared forces, error
 // word, step counter and bonds.  Enqueued on st.
 int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, cudaStream_t st);
+// q0 := q, observables accumulators cleared (enqueued on st).
+int slot_reset_observables(Slot& s, cudaStream_t st);
+// The accumulators of the slot (synchronises st).
+int slot_read_observables(const Slot& s, cudaStream_t st, fsl_observables* out);
 // Bond tables in the reference's CSR (src/initializeBondedForces.cpp:31-150).
 int slot_bonds(Slot& s, int64_t nbonds, const int32_t* bi, const int32_t* bj, const double* k,
                const double* r0, int64_t nfixed, const int32_t* fi, const double* fk,

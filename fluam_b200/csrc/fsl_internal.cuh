@@ -47,6 +47,7 @@ struct Params {
   int pair, nonbonded, rfd, bonded;
   int scheme;  // FSL_SCHEME_* (0 midpoint, 1 first order, 2 quasi2D, 3 stokesLimit2D)
   int prec;    // FSL_PRECISION_* (0 fixed point, 1 float atomics, 2 FP64)
+  int observe; // FP64 observables accumulated at the end of every step
   int has_extra;
   double cutoff, cutoff2, invcut2, soft_eps;
   double eta, kT, dt, extra_mob, fact1, fact2, fact4;
@@ -320,7 +321,17 @@ struct Rep {
   double2* z64;
   int* err;
   uint64_t* t;
+  // observables: reference positions q0 [3][np], accumulators (kObsSlots
+  // doubles, the fsl_observables fields in order after the step count),
+  // per-block partial sums and the ticket of the last block
+  double* q0;
+  double* obs;
+  double* obs_part;
+  unsigned* obs_ticket;
 };
+constexpr int kObsVals = 10;      // msd, displacement[3], force[3], momentum[3]
+constexpr int kObsSlots = 16;     // steps, msd, msd_sum, disp[3], force[3], mom[3], mom_sum[3]
+constexpr int kObsMaxBlocks = 148;
 
 // Launch kinds of the particle kernels (256-thread blocks): threads per
 // particle 1 (cell list), 8 (forces), 32 (one spread or interpolation per
@@ -454,6 +465,8 @@ void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s);
 void launch_interp_update(const Batch& B, int stage, cudaStream_t s);
 void launch_interp(const Batch& B, cudaStream_t s);  // u = J(q) v
 void launch_step_counter(const Batch& B, cudaStream_t s);
+// FP64 observables of every instance with P.observe (end of a step)
+void launch_observe(const Batch& B, cudaStream_t s);
 // The FP64 form (fsl_fp64.cu); the launchers above hand a class of that
 // form to these.
 void launch_noise64(const Batch& B, cudaStream_t s);

@@ -652,4 +652,92 @@ void launch_step_counter(const Batch& B, cudaStream_t s) {
   FSL_GO(k_step_counter, dim3(1, B.nrep), 32, 0, s, B);
 }
 
+// ------------------------------------------------------------ observables ---
+// FP64 sums over the particles (|q - q0|^2, q - q0, F) and the cells (v) of
+// one instance.  Each block sums its share in a fixed order (grid-stride
+// loops, butterfly within warps, warps in order) into its row of obs_part;
+// the last block to finish, known by a ticket, adds the rows in block order
+// and updates the accumulators, so the result does not depend on how the
+// blocks were scheduled.
+constexpr int kObsThreads = 256;
+
+template <bool ONE>
+__global__ void __launch_bounds__(kObsThreads) k_observe(FSL_KARGS) {
+  FSL_REP_AT(blockIdx.y);
+  if (!P.observe) return;
+  __shared__ double red[kObsThreads / 32][kObsVals];
+  __shared__ double tot[kObsVals];
+  __shared__ int last;
+  double acc[kObsVals];
+#pragma unroll
+  for (int k = 0; k < kObsVals; ++k) acc[k] = 0.0;
+  const int np = P.np;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double dd = R.q[(size_t)d * np + i] - R.q0[(size_t)d * np + i];
+      acc[0] += dd * dd;
+      acc[1 + d] += dd;
+      acc[4 + d] += R.F[(size_t)d * np + i];
+    }
+  }
+  const size_t nc = (size_t)P.nc;
+  const bool f64 = P.prec == PREC_F64;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += stride)
+      acc[7 + d] += f64 ? R.v64[d * nc + c] : (double)R.v[d * nc + c];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kObsVals; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (lane == 0) red[warp][k] = acc[k];
+  }
+  __syncthreads();
+  double* part = R.obs_part + (size_t)blockIdx.x * kObsVals;
+  if (threadIdx.x < kObsVals) {
+    double sum = 0.0;
+    for (int w = 0; w < kObsThreads / 32; ++w) sum += red[w][threadIdx.x];
+    part[threadIdx.x] = sum;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(R.obs_ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < kObsVals) {
+    double sum = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) sum += __ldcg(R.obs_part + (size_t)b * kObsVals + threadIdx.x);
+    tot[threadIdx.x] = sum;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // steps, msd, msd_sum, displacement[3], force[3], momentum[3], momentum_sum[3]
+    double* o = R.obs;
+    const double inv_np = np > 0 ? 1.0 / np : 0.0;
+    const double msd = tot[0] * inv_np;
+    o[0] += 1.0;
+    o[1] = msd;
+    o[2] += msd;
+    for (int d = 0; d < 3; ++d) {
+      o[3 + d] = tot[1 + d] * inv_np;
+      o[6 + d] = tot[4 + d];
+      const double mom = tot[7 + d] * P.dV;
+      o[9 + d] = mom;
+      o[12 + d] += mom;
+    }
+    *R.obs_ticket = 0u;  // ready for the next launch
+  }
+}
+
+void launch_observe(const Batch& B, cudaStream_t s) {
+  long work = std::max<long>((long)B.max_np, (long)B.nc) / (kObsThreads * 16);
+  const unsigned nb = (unsigned)std::min<long>(kObsMaxBlocks, std::max<long>(1, work));
+  FSL_GO(k_observe, dim3(nb, B.nrep), kObsThreads, 0, s, B);
+}
+
 }  // namespace fsl

@@ -32,7 +32,7 @@ def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair
                 soft_epsilon=1.0, rfd=RFD_REFERENCE, nonbonded=1, extra_mobility=0.0, seed=0,
                 device=-1, scheme=0, precision=0, radius=1.0, ndrift=1, use_rfd=1,
                 predictor_corrector=0, saffman_kc=0.0, saffman_width=0.0, shear_amp=0.0,
-                density=1.0):
+                density=1.0, observables=0):
     c = _lib.Config()
     _lib.load().fsl_config_defaults(ctypes.byref(c))
     c.mx, c.my, c.mz = (int(x) for x in cells)
@@ -46,6 +46,7 @@ def make_config(cells, box, eta=1.0, kT=0.0, dt=0.01, cutoff=0.0, kernel=3, pair
     c.radius, c.ndrift, c.use_rfd, c.predictor_corrector = radius, ndrift, use_rfd, predictor_corrector
     c.saffman_kc, c.saffman_width, c.shear_amp = saffman_kc, saffman_width, shear_amp
     c.density = density  # incompressible scheme
+    c.observables = observables  # FP64 accumulators on the device (3-D Stokes schemes)
     return c
 
 
@@ -133,6 +134,17 @@ class StokesLimit:
         out = np.empty((3,) + self.shape, dtype=np.float32)
         check(self.L.fsl_get_velocity(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
+
+    def observables(self):
+        """FP64 device accumulators (config observables=1): msd, displacement,
+        total force, fluid momentum and their sums over the steps."""
+        o = _lib.Observables()
+        check(self.L.fsl_get_observables(self.h, ctypes.byref(o)))
+        return o.as_dict()
+
+    def reset_observables(self):
+        """q0 := the current positions, accumulators := 0."""
+        check(self.L.fsl_reset_observables(self.h))
 
     def status(self):
         st = _lib.Status()
@@ -270,6 +282,14 @@ class Batch:
         out = np.empty((3, int(self.nps[i])))
         check(self.L.fsl_batch_get_forces(self.h, int(i), _dp(out)))
         return out
+
+    def observables(self, i):
+        o = _lib.Observables()
+        check(self.L.fsl_batch_get_observables(self.h, int(i), ctypes.byref(o)))
+        return o.as_dict()
+
+    def reset_observables(self, i):
+        check(self.L.fsl_batch_reset_observables(self.h, int(i)))
 
     def status(self, i):
         st = _lib.Status()

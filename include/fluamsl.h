@@ -98,7 +98,9 @@ typedef struct fsl_config {
   int32_t ndrift;                /* nDrift (noise count only)               */
   int32_t use_rfd;               /* use_RFD: the thermal drift spread       */
   int32_t predictor_corrector;   /* predictorCorrector                      */
-  int32_t reserved_;
+  /* 3-D Stokes schemes: 1 = accumulate fsl_observables in FP64 on the
+   * device at the end of every step (one extra launch per step) */
+  int32_t observables;
   double radius;                 /* hydrodynamicRadius                      */
   double saffman_kc;             /* saffmanCutOffWaveNumber (stokesLimit2D) */
   double saffman_width;          /* saffmanLayerWidth                       */
@@ -166,6 +168,26 @@ int fsl_get_velocity_f64(fsl_handle* h, double* out);
  * first step (src/runSchemeIncompressible.cu:82-96). */
 int fsl_set_velocity_f64(fsl_handle* h, const double* in);
 int fsl_get_status(fsl_handle* h, fsl_status* st);
+
+/* FP64 accumulators kept on the device when fsl_config.observables is 1
+ * (3-D Stokes schemes).  No counterpart in the reference, which computes no
+ * observables on this path.  q0 are the reference positions: the positions
+ * given to fsl_create, or those at the last fsl_reset_observables. */
+typedef struct fsl_observables {
+  int64_t steps;                 /* steps accumulated since q0 was set        */
+  double msd;                    /* (1/np) sum_i |q_i - q0_i|^2 after the last step */
+  double msd_sum;                /* sum of msd over the accumulated steps     */
+  double displacement[3];        /* (1/np) sum_i (q_i - q0_i): centre-of-mass drift */
+  double force[3];               /* sum_i F_i of the step's last force evaluation */
+  double momentum[3];            /* sum over cells of v dV of the last solve (the
+                                    fluid momentum per unit density)         */
+  double momentum_sum[3];        /* sum of momentum over the accumulated steps */
+} fsl_observables;
+/* Read the accumulators (waits for the handle's queued work). */
+int fsl_get_observables(fsl_handle* h, fsl_observables* out);
+/* q0 := the current positions; accumulators := 0 (queued on the stream). */
+int fsl_reset_observables(fsl_handle* h);
+
 int fsl_set_step(fsl_handle* h, uint64_t step);
 int fsl_clear_errors(fsl_handle* h);
 /* Capture one step into a CUDA graph and replay it from then on (on by
@@ -272,6 +294,9 @@ int fsl_batch_sync(fsl_batch* b);
 int fsl_batch_get_positions(fsl_batch* b, int32_t i, double* out);
 int fsl_batch_get_forces(fsl_batch* b, int32_t i, double* out);
 int fsl_batch_get_status(fsl_batch* b, int32_t i, fsl_status* st);
+/* fsl_get_observables / fsl_reset_observables of instance i. */
+int fsl_batch_get_observables(fsl_batch* b, int32_t i, fsl_observables* out);
+int fsl_batch_reset_observables(fsl_batch* b, int32_t i);
 /* All instances' positions in one packed array (one copy each way plus one
  * gather/scatter kernel). */
 int fsl_batch_get_positions_packed(fsl_batch* b, double* out);
