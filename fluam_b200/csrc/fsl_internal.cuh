@@ -334,11 +334,11 @@ constexpr int kObsSlots = 16;     // steps, msd, msd_sum, disp[3], force[3], mom
 constexpr int kObsMaxBlocks = 148;
 
 // Launch kinds of the particle kernels (256-thread blocks): threads per
-// particle 1 (cell list), 8 (forces), 32 (one spread or interpolation per
-// particle), 64 (force spread plus drift spread per particle).
-enum { KIND_T1 = 0, KIND_T8 = 1, KIND_T32 = 2, KIND_T64 = 3, NKIND = 4 };
+// particle 1 (cell list), 8 (forces), 32 (one warp per particle), 4 (one
+// quad per particle: spreading and interpolation).
+enum { KIND_T1 = 0, KIND_T8 = 1, KIND_T32 = 2, KIND_T4 = 3, NKIND = 4 };
 constexpr int kPartThreads = 256;
-__host__ __device__ constexpr int kind_threads(int k) { return k == 0 ? 1 : k == 1 ? 8 : k == 2 ? 32 : 64; }
+__host__ __device__ constexpr int kind_threads(int k) { return k == 0 ? 1 : k == 1 ? 8 : k == 2 ? 32 : 4; }
 __host__ __device__ constexpr int kind_ppb(int k) { return kPartThreads / kind_threads(k); }
 
 // Where a batched kernel finds its instance: the device table, and for the

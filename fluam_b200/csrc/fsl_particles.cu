@@ -382,99 +382,160 @@ void launch_forces(const Batch& B, int which, cudaStream_t s) {
   FSL_GO(k_forces, part_blocks(B, KIND_T8), kPartThreads, 0, s, B, which);
 }
 
-// ------------------------------------------------------------- spreading ---
-// Node of a lane in the per-component node loops: the warp takes the n^3
-// nodes (a, b, c) of one component's stencil at a time, lane l fixed to
-// a = l mod n, b = (l / n) mod n, c = l / n^2 (n = 4: 64 nodes in two passes,
-// the second at c + 2; n = 3: lanes 27-31 idle).  x is fastest, so a pass's
-// accesses fall on few 32-byte sectors.
+// ------------------------------------------------------------ quad layout ---
+// Spreading and interpolation take four lanes per particle (eight particles
+// per warp).  Lane a = lane & 3 of a quad computes node a of the six stencil
+// families (the cell-centre and face node families of each dimension),
+// keeps its own x nodes and takes all y and z nodes of the quad by
+// shuffles; it then handles x node a of every stencil, the KN^2 (y, z)
+// nodes of each component (a = 3 idles for the 3-point kernel).  A warp
+// instruction touches eight particles' x-runs of four consecutive values.
 template <int KN>
-struct LaneNode {
-  static constexpr int passes = KN == 4 ? 2 : 1;
-  int a, b, c0;
-  bool on;
-  __device__ __forceinline__ explicit LaneNode(int lane) {
-    if constexpr (KN == 4) {
-      a = lane & 3;
-      b = (lane >> 2) & 3;
-      c0 = lane >> 4;
-      on = true;
-    } else {
-      a = lane % 3;
-      b = (lane / 3) % 3;
-      c0 = lane < 27 ? lane / 9 : 0;  // idle lanes read a valid node
-      on = lane < 27;
-    }
-  }
+struct QuadStencil {
+  int jx[2], jy[2][KN], jz[2][KN];  // family 0: cell centres, 1: faces
+  float wx[2], wy[2][KN], wz[2][KN];
 };
 
-// One warp per entry (all three components of one spread of one particle):
-// every lane adds w * value of its nodes in 64-bit fixed point (in the
-// float-atomic form: w * value as an FP32 atomic).
-// Replaces the slot writes of kernelSpreadParticlesForceStokesLimit and
-// kernelSpreadParticlesDrift + the gather of addSpreadedForcesStokesLimit
-// (src/stokesLimitFunctions.cu:659-1681, 1705-2255); the 1/dV of the gather
-// is applied when the field is read back.
-template <int KN>  // kernel width 3 or 4
-__device__ __forceinline__ void spread_entry(const Params& P, const double posc[3],
-                                             const double posw[3], const double val[3],
-                                             unsigned long long* __restrict__ grid, int lane,
-                                             bool& sat) {
-  const WarpStencil st = warp_stencil(P, posc, posw, lane);
-  const LaneNode<KN> ln(lane);
-  const bool fatom = P.prec == PREC_FLOAT;
+// Every lane of the warp calls this (shuffles); qb is the first lane of the
+// quad.  Node k of family f in dimension d is the stencil_node of component
+// d (faces) or (d + 1) mod 3 (centres).
+template <int KN>
+__device__ __forceinline__ void quad_stencil(const Params& P, const double posc[3],
+                                             const double posw[3], int a, int qb,
+                                             QuadStencil<KN>& S) {
+  int j[2][3];
+  float w[2][3];
 #pragma unroll
-  for (int comp = 0; comp < 3; ++comp) {
-    int x, y;
-    float wx, wy;
-    stencil_get(st, KN, comp, 0, ln.a, x, wx);
-    stencil_get(st, KN, comp, 1, ln.b, y, wy);
-    const double vc = val[comp];
-    unsigned long long* gc = grid + (size_t)comp * P.nc;
+  for (int f = 0; f < 2; ++f)
 #pragma unroll
-    for (int h = 0; h < LaneNode<KN>::passes; ++h) {
-      int z;
-      float wz;
-      stencil_get(st, KN, comp, 2, ln.c0 + 2 * h, z, wz);
-      if (!ln.on) continue;
-      const int at = x + P.mx * (y + P.my * z);  // < nc <= 2^30
-      const float w = wx * (wy * wz);
-      if (fatom) {
-        // float-atomic form: the first 3 nc floats of the spread buffer
-        const float fv = (float)((double)w * vc);
-        if (fv != 0.0f) atomicAdd(reinterpret_cast<float*>(grid) + (size_t)comp * P.nc + at, fv);
-        continue;
-      }
-      const double v = (double)w * (vc * kFixedScale);
-      sat |= !(fabs(v) < kFixedMax);
-      const long long iv = sat ? 0ll : __double2ll_rn(v);
-      if (iv != 0) atomicAdd(gc + at, (unsigned long long)iv);
+    for (int d = 0; d < 3; ++d) {
+      j[f][d] = 0;
+      w[f][d] = 0.0f;
+      if (a < KN) stencil_node(P, d, f == 1 ? d : (d + 1) % 3, posc[d], posw[d], a, j[f][d], w[f][d]);
+    }
+#pragma unroll
+  for (int f = 0; f < 2; ++f) {
+    S.jx[f] = j[f][0];
+    S.wx[f] = w[f][0];
+#pragma unroll
+    for (int k = 0; k < KN; ++k) {
+      S.jy[f][k] = __shfl_sync(0xffffffffu, j[f][1], qb + k);
+      S.wy[f][k] = __shfl_sync(0xffffffffu, w[f][1], qb + k);
+      S.jz[f][k] = __shfl_sync(0xffffffffu, j[f][2], qb + k);
+      S.wz[f][k] = __shfl_sync(0xffffffffu, w[f][2], qb + k);
     }
   }
 }
 
-// One warp per particle (in cell order when ordered).  drift = 0: F at q;
+// One spread of one particle by its quad: every lane adds w * value of its
+// nodes in 64-bit fixed point (in the float-atomic form: w * value as an
+// FP32 atomic).  Replaces the slot writes of
+// kernelSpreadParticlesForceStokesLimit and kernelSpreadParticlesDrift + the
+// gather of addSpreadedForcesStokesLimit (src/stokesLimitFunctions.cu:
+// 659-1681, 1705-2255); the 1/dV of the gather is applied when the field is
+// read back.  No shuffles: lanes may skip it.
+template <int KN>
+__device__ __forceinline__ void quad_spread(const Params& P, const QuadStencil<KN>& S, int a,
+                                            const double val[3],
+                                            unsigned long long* __restrict__ grid, bool& sat) {
+  if (a >= KN) return;
+  const bool fatom = P.prec == PREC_FLOAT;
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    const int x = S.jx[comp == 0];
+    const float wx = S.wx[comp == 0];
+    const double vc = val[comp];
+    const double vs = vc * kFixedScale;
+    unsigned long long* gc = grid + (size_t)comp * P.nc;
+#pragma unroll
+    for (int b = 0; b < KN; ++b) {
+      const int y = S.jy[comp == 1][b];
+      const float wy = S.wy[comp == 1][b];
+#pragma unroll
+      for (int c = 0; c < KN; ++c) {
+        const int at = x + P.mx * (y + P.my * S.jz[comp == 2][c]);  // < nc <= 2^30
+        const float w = wx * (wy * S.wz[comp == 2][c]);
+        if (fatom) {
+          // float-atomic form: the first 3 nc floats of the spread buffer
+          const float fv = (float)((double)w * vc);
+          if (fv != 0.0f) atomicAdd(reinterpret_cast<float*>(grid) + (size_t)comp * P.nc + at, fv);
+          continue;
+        }
+        const double v = (double)w * vs;
+        sat |= !(fabs(v) < kFixedMax);
+        const long long iv = sat ? 0ll : __double2ll_rn(v);
+        if (iv != 0) atomicAdd(gc + at, (unsigned long long)iv);
+      }
+    }
+  }
+}
+
+// J v of one particle by its quad: each lane sums w v over its nodes per
+// component, then the quad adds its four partial sums (xor 1, then xor 2);
+// every lane of the quad gets the three sums
+// (src/stokesLimitFunctions.cu:2616-2642).
+template <int KN>
+__device__ __forceinline__ void quad_interp(const Params& P, const QuadStencil<KN>& S, int a,
+                                            const float* __restrict__ v, float u[3]) {
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    const float* vc = v + (size_t)comp * P.nc;
+    const int x = S.jx[comp == 0];
+    const float wx = S.wx[comp == 0];
+    float val[KN * KN];
+#pragma unroll
+    for (int b = 0; b < KN; ++b)
+#pragma unroll
+      for (int c = 0; c < KN; ++c)
+        val[b * KN + c] = a < KN ? __ldg(vc + (x + P.mx * (S.jy[comp == 1][b] + P.my * S.jz[comp == 2][c]))) : 0.0f;
+    float s = 0.0f;
+#pragma unroll
+    for (int b = 0; b < KN; ++b)
+#pragma unroll
+      for (int c = 0; c < KN; ++c) s += (wx * (S.wy[comp == 1][b] * S.wz[comp == 2][c])) * val[b * KN + c];
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    u[comp] = s;
+  }
+}
+
+// The quad of this thread in a KIND_T4 launch: particle index e (in the
+// instance), lane a in the quad, first lane qb of the quad; returns false
+// when the whole warp is past the last particle (uniform per warp).
+__device__ __forceinline__ bool quad_of(int blk, int np, long& e, int& a, int& qb) {
+  const long t = blk * (long)blockDim.x + threadIdx.x;
+  e = t >> 2;
+  a = threadIdx.x & 3;
+  qb = (threadIdx.x & 31) & ~3;
+  return ((t & ~31L) >> 2) < np;
+}
+
+// ------------------------------------------------------------- spreading ---
+// One quad per particle (in cell order when ordered).  drift = 0: F at q;
 // drift = 1: F at q^{n+1/2}, then the particle's RFD drift (kT/delta) sign
 // W_p from q + sign (delta/2) W_p for both signs; drift = 2: F at q and the
 // drift.  In reference mode the drift's nodes come from the displaced
 // position and its weights from q, as the reference does.
 template <bool ONE, int KN>
 __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
-  FSL_REP_FLAT(KIND_T32);
-  const int lane = threadIdx.x & 31;
-  const long e = (long)((blk * (size_t)blockDim.x + threadIdx.x) >> 5);
+  FSL_REP_FLAT(KIND_T4);
+  long e;
+  int a, qb;
   const int np = P.np;
-  if (e >= np) return;  // uniform per warp
-  const int i = ordered ? R.sorted[e] : (int)e;
+  if (!quad_of(blk, np, e, a, qb)) return;
+  const bool on = e < np;  // lanes past the end join the shuffles only
+  const int i = on ? (ordered ? R.sorted[e] : (int)e) : 0;
   bool sat = false;
+  QuadStencil<KN> S;
   {
     const double* qf = drift == 1 ? R.qp : R.q;
     double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
     double val[3] = {R.F[i], R.F[np + i], R.F[2 * (size_t)np + i]};
-    spread_entry<KN>(P, pos, pos, val, R.grid, lane, sat);
+    quad_stencil<KN>(P, pos, pos, a, qb, S);
+    if (on) quad_spread<KN>(P, S, a, val, R.grid, sat);
   }
   if (drift) {
-    // the RFD drift of the same particle, by the same warp
+    // the RFD drift of the same particle, by the same quad
     const size_t wbase = (size_t)6 * P.nc;
     double W[3] = {(double)R.noise[wbase + i], (double)R.noise[wbase + np + i],
                    (double)R.noise[wbase + 2 * np + i]};
@@ -491,21 +552,33 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
       // Reference mode weighs both spreads at q: where both displaced
       // positions pick the same nodes the two fixed-point spreads are exact
       // negatives of each other (same weights, opposite values, symmetric
-      // rounding), so they are skipped without changing the result.
-      bool same = true;
-      if (lane < 6) {
-        int f = lane / 3, d = lane - 3 * f;
-        const double a = d == 0 ? pp[0] : (d == 1 ? pp[1] : pp[2]);
-        const double b = d == 0 ? pm[0] : (d == 1 ? pm[1] : pm[2]);
-        same = stencil_base(P, d, f, a) == stencil_base(P, d, f, b);
+      // rounding), so they are skipped without changing the result.  Lane a
+      // checks the node families a and a + 4 of the six.
+      int same = 1;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int fd = a + 4 * r;
+        if (fd < 6) {
+          const int f = fd / 3, d = fd - 3 * f;
+          const double x = d == 0 ? pp[0] : (d == 1 ? pp[1] : pp[2]);
+          const double y = d == 0 ? pm[0] : (d == 1 ? pm[1] : pm[2]);
+          same &= stencil_base(P, d, f, x) == stencil_base(P, d, f, y);
+        }
       }
-      if (!__all_sync(0xffffffffu, same)) {
-        spread_entry<KN>(P, pp, pos, vp, R.grid, lane, sat);
-        spread_entry<KN>(P, pm, pos, vm, R.grid, lane, sat);
+      same &= __shfl_xor_sync(0xffffffffu, same, 1);
+      same &= __shfl_xor_sync(0xffffffffu, same, 2);
+      if (!__all_sync(0xffffffffu, same || !on)) {
+        // a quad whose nodes agree spreads nothing; the others do both
+        quad_stencil<KN>(P, pp, pos, a, qb, S);
+        if (on && !same) quad_spread<KN>(P, S, a, vp, R.grid, sat);
+        quad_stencil<KN>(P, pm, pos, a, qb, S);
+        if (on && !same) quad_spread<KN>(P, S, a, vm, R.grid, sat);
       }
     } else {
-      spread_entry<KN>(P, pp, pp, vp, R.grid, lane, sat);
-      spread_entry<KN>(P, pm, pm, vm, R.grid, lane, sat);
+      quad_stencil<KN>(P, pp, pp, a, qb, S);
+      if (on) quad_spread<KN>(P, S, a, vp, R.grid, sat);
+      quad_stencil<KN>(P, pm, pm, a, qb, S);
+      if (on) quad_spread<KN>(P, S, a, vm, R.grid, sat);
     }
   }
   if (sat) set_err(R.err, 1);
@@ -514,7 +587,7 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
 void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s) {
   if (B.max_np == 0) return;
   if (B.prec == PREC_F64) return launch_spread64(B, drift, s);
-  const unsigned g = part_blocks(B, KIND_T32);
+  const unsigned g = part_blocks(B, KIND_T4);
   if (B.kernel == 4)
     FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered);
   else
@@ -522,78 +595,29 @@ void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s) {
 }
 
 // -------------------------------------------------------- interpolation ---
-// One warp per particle: every lane reads its nodes (LaneNode) of the three
-// components' stencils and the warp sums w v per component in a fixed
-// butterfly order (src/stokesLimitFunctions.cu:2616-2642).  Every lane gets
-// the three sums.
-template <int KN>
-__device__ __forceinline__ void interp_particle(const Params& P, const double pos[3],
-                                                const float* __restrict__ v, int lane,
-                                                float u[3]) {
-  constexpr int NH = LaneNode<KN>::passes;
-  const WarpStencil st = warp_stencil(P, pos, pos, lane);
-  const LaneNode<KN> ln(lane);
-  // every node's address and weight first, then all loads at once
-  float wt[3][NH];
-  const float* ad[3][NH];
-#pragma unroll
-  for (int comp = 0; comp < 3; ++comp) {
-    int x, y;
-    float wx, wy;
-    stencil_get(st, KN, comp, 0, ln.a, x, wx);
-    stencil_get(st, KN, comp, 1, ln.b, y, wy);
-    const float* vc = v + (size_t)comp * P.nc;
-#pragma unroll
-    for (int h = 0; h < NH; ++h) {
-      int z;
-      float wz;
-      stencil_get(st, KN, comp, 2, ln.c0 + 2 * h, z, wz);
-      wt[comp][h] = ln.on ? wx * (wy * wz) : 0.0f;
-      ad[comp][h] = vc + (x + P.mx * (y + P.my * z));
-    }
-  }
-  float val[3][NH];
-#pragma unroll
-  for (int comp = 0; comp < 3; ++comp)
-#pragma unroll
-    for (int h = 0; h < NH; ++h) val[comp][h] = __ldg(ad[comp][h]);
-  float s[3];
-#pragma unroll
-  for (int comp = 0; comp < 3; ++comp) {
-    s[comp] = 0.0f;
-#pragma unroll
-    for (int h = 0; h < NH; ++h) s[comp] += wt[comp][h] * val[comp][h];
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    s[0] += __shfl_xor_sync(0xffffffffu, s[0], o);
-    s[1] += __shfl_xor_sync(0xffffffffu, s[1], o);
-    s[2] += __shfl_xor_sync(0xffffffffu, s[2], o);
-  }
-  u[0] = s[0];
-  u[1] = s[1];
-  u[2] = s[2];
-}
-
 // stage 1: q^{n+1/2} = q^n + dt/2 J(q^n) v (+ extraMobility terms),
 //          src/stokesLimitFunctions.cu:2646-2650
 // stage 2: q^{n+1}   = q^n + dt J(q^{n+1/2}) v (+ extraMobility terms),
 //          src/stokesLimitFunctions.cu:3676-3681
+// One quad per particle; lanes 0, 1, 2 of the quad update x, y, z.
 template <bool ONE, int KN>
 __global__ void k_interp_update(FSL_KARGS, int stage) {
-  FSL_REP_FLAT(KIND_T32);
-  const int lane = threadIdx.x & 31;
-  const long t = (long)((blk * (size_t)blockDim.x + threadIdx.x) >> 5);
-  if (t >= P.np) return;  // uniform per warp
-  const int i = (int)t;
+  FSL_REP_FLAT(KIND_T4);
+  long e;
+  int a, qb;
   const int np = P.np;
+  if (!quad_of(blk, np, e, a, qb)) return;
+  const bool on = e < np;
+  const int i = on ? (int)e : 0;
   const double* qpos = stage == 1 ? R.q : R.qp;
   double* qout = stage == 1 ? R.qp : R.q;
   double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
+  QuadStencil<KN> S;
+  quad_stencil<KN>(P, pos, pos, a, qb, S);
   float us[3];
-  interp_particle<KN>(P, pos, R.v, lane, us);
-  if (lane >= 3) return;
-  const int comp = lane;  // lanes 0, 1, 2 update x, y, z
+  quad_interp<KN>(P, S, a, R.v, us);
+  if (!on || a >= 3) return;
+  const int comp = a;
   const double u = (double)(comp == 0 ? us[0] : (comp == 1 ? us[1] : us[2]));
   size_t k = (size_t)comp * np + i;
   double h = stage == 1 ? 0.5 * P.dt : P.dt;
@@ -610,22 +634,25 @@ __global__ void k_interp_update(FSL_KARGS, int stage) {
 
 template <bool ONE, int KN>
 __global__ void k_interp(FSL_KARGS) {
-  FSL_REP_FLAT(KIND_T32);
-  const int lane = threadIdx.x & 31;
-  const long t = (long)((blk * (size_t)blockDim.x + threadIdx.x) >> 5);
-  if (t >= P.np) return;  // uniform per warp
-  const int i = (int)t;
+  FSL_REP_FLAT(KIND_T4);
+  long e;
+  int a, qb;
   const int np = P.np;
+  if (!quad_of(blk, np, e, a, qb)) return;
+  const bool on = e < np;
+  const int i = on ? (int)e : 0;
   double pos[3] = {R.q[i], R.q[np + i], R.q[2 * np + i]};
+  QuadStencil<KN> S;
+  quad_stencil<KN>(P, pos, pos, a, qb, S);
   float us[3];
-  interp_particle<KN>(P, pos, R.v, lane, us);
-  if (lane < 3) R.u[(size_t)lane * np + i] = (double)(lane == 0 ? us[0] : (lane == 1 ? us[1] : us[2]));
+  quad_interp<KN>(P, S, a, R.v, us);
+  if (on && a < 3) R.u[(size_t)a * np + i] = (double)(a == 0 ? us[0] : (a == 1 ? us[1] : us[2]));
 }
 
 void launch_interp_update(const Batch& B, int stage, cudaStream_t s) {
   if (B.max_np == 0) return;
   if (B.prec == PREC_F64) return launch_interp_update64(B, stage, s);
-  const unsigned g = part_blocks(B, KIND_T32);
+  const unsigned g = part_blocks(B, KIND_T4);
   if (B.kernel == 4)
     FSL_GO_T(k_interp_update, 4, g, kPartThreads, 0, s, B, stage);
   else
@@ -634,7 +661,7 @@ void launch_interp_update(const Batch& B, int stage, cudaStream_t s) {
 
 void launch_interp(const Batch& B, cudaStream_t s) {
   if (B.max_np == 0) return;
-  const unsigned g = part_blocks(B, KIND_T32);
+  const unsigned g = part_blocks(B, KIND_T4);
   if (B.kernel == 4)
     FSL_GO_T(k_interp, 4, g, kPartThreads, 0, s, B);
   else
