@@ -274,35 +274,6 @@ constexpr int kYTile = 16;   // y pass: kx columns per block
 constexpr int kZTile = 8;    // z pass: kx columns per block (x 3 components)
 constexpr int kFftThreads = 512;
 
-// Noise terms of W for component comp at cell i (x,y,z) for one stress
-// sample d (src/stokesLimitFunctions.cu:2323-2367): the divergence of the
-// stochastic stress with diagonals at cell centres and off-diagonals on edges.
-__device__ __forceinline__ float stress_div(const Params& P, const float* __restrict__ d, int comp,
-                                            int x, int y, int z, int i, float a1x, float a1y,
-                                            float a1z, float a4x, float a4y, float a4z) {
-  const size_t nc = (size_t)P.nc;
-  const int mx = P.mx, my = P.my, mz = P.mz;
-  int xm = x == 0 ? mx - 1 : x - 1, xp = x == mx - 1 ? 0 : x + 1;
-  int ym = y == 0 ? my - 1 : y - 1, yp = y == my - 1 ? 0 : y + 1;
-  int zm = z == 0 ? mz - 1 : z - 1, zp = z == mz - 1 ? 0 : z + 1;
-  int rowyz = mx * (y + my * z);
-  if (comp == 0) {
-    int v3 = xp + rowyz, v1 = x + mx * (ym + my * z), v0 = x + mx * (y + my * zm);
-    return a1x * (__ldg(d + v3) - __ldg(d + i)) + a4y * (__ldg(d + nc + i) - __ldg(d + nc + v1)) +
-           a4z * (__ldg(d + 2 * nc + i) - __ldg(d + 2 * nc + v0));
-  } else if (comp == 1) {
-    int v4 = x + mx * (yp + my * z), v2 = xm + rowyz, v0 = x + mx * (y + my * zm);
-    return a1y * (__ldg(d + 3 * nc + v4) - __ldg(d + 3 * nc + i)) +
-           a4x * (__ldg(d + nc + i) - __ldg(d + nc + v2)) +
-           a4z * (__ldg(d + 4 * nc + i) - __ldg(d + 4 * nc + v0));
-  } else {
-    int v5 = x + mx * (y + my * zp), v2 = xm + rowyz, v1 = x + mx * (ym + my * z);
-    return a1z * (__ldg(d + 5 * nc + v5) - __ldg(d + 5 * nc + i)) +
-           a4x * (__ldg(d + 2 * nc + i) - __ldg(d + 2 * nc + v2)) +
-           a4y * (__ldg(d + 4 * nc + i) - __ldg(d + 4 * nc + v1));
-  }
-}
-
 // W = f + c div(Sigma) of all three components of every cell
 // (src/stokesLimitFunctions.cu:2281-2378, 3922-4069): the fixed-point spread
 // field times 2^-40/dV plus the stochastic stress divergence, with
@@ -343,54 +314,6 @@ __global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
       if (nsets > 1) w += stress_div(P, n2, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
       R.wbuf[comp * nc + i] = w;
     }
-  }
-}
-
-// Four consecutive x cells of a row for one stress sample d: the x, y, z
-// neighbours as 16-byte rows (aligned: the sample's base is a multiple of 4
-// floats; otherwise four scalar loads) plus the two x-edge scalars.
-__device__ __forceinline__ float4 ld_row4(const float* __restrict__ p, bool aligned) {
-  if (aligned) return __ldg(reinterpret_cast<const float4*>(p));
-  return make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3));
-}
-
-// w[comp][c] += the stress divergence of cells x0 .. x0+3 (the arithmetic of
-// stress_div, four cells at a time).
-__device__ __forceinline__ void stress_div4(const Params& P, const float* __restrict__ d,
-                                            bool aligned, int x0, int y, int z, size_t i0,
-                                            float a1x, float a1y, float a1z, float a4x,
-                                            float a4y, float a4z, float (&w)[3][4]) {
-  const size_t nc = (size_t)P.nc;
-  const int mx = P.mx, my = P.my, mz = P.mz;
-  const size_t row = i0 - x0;  // first cell of the row
-  const long dym = (y == 0 ? (long)(my - 1) * mx : -(long)mx);
-  const long dyp = (y == my - 1 ? -(long)(my - 1) * mx : (long)mx);
-  const long dzm = (z == 0 ? (long)(mz - 1) * my * mx : -(long)my * mx);
-  const long dzp = (z == mz - 1 ? -(long)(mz - 1) * my * mx : (long)my * mx);
-  const int xl = x0 == 0 ? mx - 1 : x0 - 1, xr = x0 + 4 == mx ? 0 : x0 + 4;
-  const float4 r0 = ld_row4(d + i0, aligned);
-  const float e0 = __ldg(d + row + xr);
-  const float4 r1 = ld_row4(d + nc + i0, aligned), r1ym = ld_row4(d + nc + i0 + dym, aligned);
-  const float e1 = __ldg(d + nc + row + xl);
-  const float4 r2 = ld_row4(d + 2 * nc + i0, aligned), r2zm = ld_row4(d + 2 * nc + i0 + dzm, aligned);
-  const float e2 = __ldg(d + 2 * nc + row + xl);
-  const float4 r3 = ld_row4(d + 3 * nc + i0, aligned), r3yp = ld_row4(d + 3 * nc + i0 + dyp, aligned);
-  const float4 r4 = ld_row4(d + 4 * nc + i0, aligned), r4zm = ld_row4(d + 4 * nc + i0 + dzm, aligned),
-               r4ym = ld_row4(d + 4 * nc + i0 + dym, aligned);
-  const float4 r5 = ld_row4(d + 5 * nc + i0, aligned), r5zp = ld_row4(d + 5 * nc + i0 + dzp, aligned);
-  const float d0[5] = {r0.x, r0.y, r0.z, r0.w, e0};          // d0[x .. x+4]
-  const float d1[5] = {e1, r1.x, r1.y, r1.z, r1.w};          // d1[x-1 .. x+3]
-  const float d2[5] = {e2, r2.x, r2.y, r2.z, r2.w};          // d2[x-1 .. x+3]
-  const float d1ym[4] = {r1ym.x, r1ym.y, r1ym.z, r1ym.w}, d2zm[4] = {r2zm.x, r2zm.y, r2zm.z, r2zm.w};
-  const float d3[4] = {r3.x, r3.y, r3.z, r3.w}, d3yp[4] = {r3yp.x, r3yp.y, r3yp.z, r3yp.w};
-  const float d4[4] = {r4.x, r4.y, r4.z, r4.w}, d4zm[4] = {r4zm.x, r4zm.y, r4zm.z, r4zm.w},
-              d4ym[4] = {r4ym.x, r4ym.y, r4ym.z, r4ym.w};
-  const float d5[4] = {r5.x, r5.y, r5.z, r5.w}, d5zp[4] = {r5zp.x, r5zp.y, r5zp.z, r5zp.w};
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    w[0][c] += a1x * (d0[c + 1] - d0[c]) + a4y * (d1[c + 1] - d1ym[c]) + a4z * (d2[c + 1] - d2zm[c]);
-    w[1][c] += a1y * (d3yp[c] - d3[c]) + a4x * (d1[c + 1] - d1[c]) + a4z * (d4[c] - d4zm[c]);
-    w[2][c] += a1z * (d5zp[c] - d5[c]) + a4x * (d2[c + 1] - d2[c]) + a4y * (d4[c] - d4ym[c]);
   }
 }
 

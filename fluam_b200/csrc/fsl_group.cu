@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "fsl_group.cuh"
@@ -26,7 +27,7 @@ size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 struct SlotLayout {
   size_t q, qp, F, u, qw, ws, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
       bsum, ljtab, noise, grid, spec, v, wbuf, noise64, v64, z64, err, t, q0, obs, obs_part, obs_ticket,
-      total;
+      start1, sorted1, ws1, total;
 };
 
 SlotLayout layout(const Params& P, int np_cap) {
@@ -76,6 +77,11 @@ SlotLayout layout(const Params& P, int np_cap) {
   L.obs = take(sizeof(double) * kObsSlots);
   L.obs_part = take(P.observe ? sizeof(double) * kObsVals * kObsMaxBlocks : 0);
   L.obs_ticket = take(sizeof(unsigned));
+  // the 3-D Stokes schemes build two cell lists per step and keep both
+  const bool two_lists = P.scheme <= FSL_SCHEME_FIRST_ORDER;
+  L.start1 = take(two_lists ? sizeof(int) * (mN + 1) : 0);
+  L.sorted1 = take(two_lists ? sizeof(int) * np : 0);
+  L.ws1 = take(two_lists ? sizeof(double) * 3 * np : 0);
   L.total = off;
   return L;
 }
@@ -328,6 +334,10 @@ int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st) {
   r.obs = (double*)(base + L.obs);
   r.obs_part = P.observe ? (double*)(base + L.obs_part) : nullptr;
   r.obs_ticket = (unsigned*)(base + L.obs_ticket);
+  const bool two_lists = P.scheme <= FSL_SCHEME_FIRST_ORDER;
+  r.start1 = two_lists ? (int*)(base + L.start1) : nullptr;
+  r.sorted1 = two_lists ? (int*)(base + L.sorted1) : nullptr;
+  r.ws1 = two_lists ? (double*)(base + L.ws1) : nullptr;
   return FSL_OK;
 }
 
@@ -508,6 +518,7 @@ int group_init(Group& g, const Params& P0) {
   FSL_TRY(cudaStreamCreateWithPriority(&g.side, cudaStreamNonBlocking, lo));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
+  tile_init();
   return FSL_OK;
 }
 
@@ -546,9 +557,14 @@ int group_upload(Group& g) {
   B.prec = g.P0.prec;
   B.max_np = 0;
   B.max_noise_n = 0;
+  // FLUAMSL_TILED_SPREAD=0 keeps the fixed-point form on the global-atomic
+  // spread and the separate W build (same bits; for comparisons)
+  const char* env = std::getenv("FLUAMSL_TILED_SPREAD");
+  B.tiled = !(env && env[0] == '0') && tile_eligible(g.P0);
   for (const Slot* s : g.slots) {
     B.max_np = std::max(B.max_np, s->np_cap);
     B.max_noise_n = std::max<uint64_t>(B.max_noise_n, noise_count(g.P0, s->np_cap));
+    B.tiled = B.tiled && tile_eligible(s->r.P);  // per instance: the cell sizes
   }
   if (n > g.d_cap) {
     if (g.d_reps || g.d_boff) {
@@ -711,11 +727,18 @@ void group_enqueue_step(Group& g) {
     // only with extraMobility (k_forces returns at once otherwise), corrector
     cells_forces(0);
     join_noise();
-    pr.mark(s, "spread_rfd");
-    launch_spread(B, 2, 1, s);
-    chk("spread_rfd");
-    pr.count(pk);
-    launch_solve(B, g.fft, 1, 1.0, 0, s, &pr);
+    if (B.tiled) {
+      pr.mark(s, "spread_w");
+      launch_spread_w(B, 2, 1, 1.0, s);
+      chk("spread_w");
+      pr.count(1);
+    } else {
+      pr.mark(s, "spread_rfd");
+      launch_spread(B, 2, 1, s);
+      chk("spread_rfd");
+      pr.count(pk);
+    }
+    launch_solve(B, g.fft, 1, 1.0, B.tiled, s, &pr);
     chk("solve");
     pr.mark(s, "interp_update");
     launch_interp_update(B, 1, s);
@@ -739,12 +762,20 @@ void group_enqueue_step(Group& g) {
   // spread field is all zeros here: it starts cleared and every W build
   // clears what it reads.
   cells_forces(0);
-  pr.mark(s, "spread");
-  launch_spread(B, 0, 1, s);
-  chk("spread");
-  pr.count(pk);
-  join_noise();
-  launch_solve(B, g.fft, 1, 1.41421356237309504880, 0, s, &pr);
+  if (B.tiled) {
+    join_noise();
+    pr.mark(s, "spread_w");
+    launch_spread_w(B, 0, 1, 1.41421356237309504880, s);
+    chk("spread_w");
+    pr.count(1);
+  } else {
+    pr.mark(s, "spread");
+    launch_spread(B, 0, 1, s);
+    chk("spread");
+    pr.count(pk);
+    join_noise();
+  }
+  launch_solve(B, g.fft, 1, 1.41421356237309504880, B.tiled, s, &pr);
   chk("solve");
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
   // sqrt(1/2) (stress 1 + stress 2)
@@ -753,11 +784,18 @@ void group_enqueue_step(Group& g) {
   chk("interp_update");
   pr.count(pk);
   cells_forces(1);
-  pr.mark(s, "spread_rfd");
-  launch_spread(B, 1, 1, s);
-  chk("spread_rfd");
-  pr.count(pk);
-  launch_solve(B, g.fft, 2, 0.70710678118654752440, 0, s, &pr);
+  if (B.tiled) {
+    pr.mark(s, "spread_w_rfd");
+    launch_spread_w(B, 1, 2, 0.70710678118654752440, s);
+    chk("spread_w_rfd");
+    pr.count(1);
+  } else {
+    pr.mark(s, "spread_rfd");
+    launch_spread(B, 1, 1, s);
+    chk("spread_rfd");
+    pr.count(pk);
+  }
+  launch_solve(B, g.fft, 2, 0.70710678118654752440, B.tiled, s, &pr);
   chk("solve");
   // option 2: corrector
   pr.mark(s, "interp_update");

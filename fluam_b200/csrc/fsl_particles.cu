@@ -6,6 +6,8 @@
 // kernels over particles run a flat grid whose blocks map to instances
 // through the block-offset table.  ONE = true compiles the single-instance
 // form, whose instance is a by-value parameter.
+#include <algorithm>
+
 #include "fsl_internal.cuh"
 
 namespace fsl {
@@ -131,8 +133,9 @@ __device__ __forceinline__ void block_scan(const int (&v)[kScanItems], int& incl
 // Block-local exclusive scan of cnt into start, block totals into bsum.  The
 // counts are cleared behind the read, ready for the next build.
 template <bool ONE>
-__global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS) {
+__global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS, int which) {
   FSL_REP_AT(blockIdx.y);
+  int* start = which && R.start1 ? R.start1 : R.start;
   __shared__ int warp_tot[33];
   const int n = P.mN;
   int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
@@ -147,7 +150,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS) {
   if (threadIdx.x == 0) R.bsum[blockIdx.x] = total;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < n) R.start[base + k] = run;
+    if (base + k < n) start[base + k] = run;
     run += v[k];
   }
 }
@@ -156,8 +159,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS) {
 // before it (a block reduction of at most kScanTile totals), and writes the
 // grand total to start[mN].
 template <bool ONE>
-__global__ void __launch_bounds__(kScanThreads) k_scan_add(FSL_KARGS) {
+__global__ void __launch_bounds__(kScanThreads) k_scan_add(FSL_KARGS, int which) {
   FSL_REP_AT(blockIdx.y);
+  int* start = which && R.start1 ? R.start1 : R.start;
   __shared__ int warp_sum[32];
   const int tile = blockIdx.x;
   int part = 0;
@@ -172,36 +176,41 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(FSL_KARGS) {
   const int base = tile * kScanTile + threadIdx.x * kScanItems;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k)
-    if (base + k < n) R.start[base + k] += prefix;
-  if (threadIdx.x == 0 && tile == (n + kScanTile - 1) / kScanTile - 1) R.start[n] = prefix + R.bsum[tile];
+    if (base + k < n) start[base + k] += prefix;
+  if (threadIdx.x == 0 && tile == (n + kScanTile - 1) / kScanTile - 1) start[n] = prefix + R.bsum[tile];
 }
 
 template <bool ONE>
-__global__ void k_cell_scatter(FSL_KARGS) {
+__global__ void k_cell_scatter(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T1);
   int i = blk * blockDim.x + threadIdx.x;
   if (i >= P.np) return;
+  const int* start = which && R.start1 ? R.start1 : R.start;
   int c = R.cell_of[i];
-  R.tmp[R.start[c] + atomicAdd(&R.fill[c], 1)] = i;
+  R.tmp[start[c] + atomicAdd(&R.fill[c], 1)] = i;
 }
 
 // Rank of particle i among the particles of its cell = number of smaller
 // indices in the (unordered) bucket; gives the ascending order.
 template <bool ONE>
-__global__ void k_cell_rank(FSL_KARGS) {
+__global__ void k_cell_rank(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T1);
   int i = blk * blockDim.x + threadIdx.x;
   if (i >= P.np) return;
+  const bool second = which && R.start1;
+  const int* start = second ? R.start1 : R.start;
+  int* sorted = second ? R.sorted1 : R.sorted;
+  double* ws = second ? R.ws1 : R.ws;
   int c = R.cell_of[i];
-  int s = R.start[c], e = R.start[c + 1];
+  int s = start[c], e = start[c + 1];
   int rank = 0;
   for (int k = s; k < e; ++k) rank += R.tmp[k] < i;
-  R.sorted[s + rank] = i;
+  sorted[s + rank] = i;
   R.fill[c] = 0;  // the scatter's slot counters, cleared for the next build
-  if (R.ws) {  // wrapped positions in cell order for the pair loop
-    R.ws[s + rank] = R.qw[i];
-    R.ws[P.np + s + rank] = R.qw[P.np + i];
-    R.ws[2 * P.np + s + rank] = R.qw[2 * P.np + i];
+  if (ws) {  // wrapped positions in cell order for the pair loop
+    ws[s + rank] = R.qw[i];
+    ws[P.np + s + rank] = R.qw[P.np + i];
+    ws[2 * P.np + s + rank] = R.qw[2 * P.np + i];
   }
 }
 
@@ -216,10 +225,10 @@ void launch_cells(const Batch& B, int which, cudaStream_t s, bool zero_first) {
   const unsigned pb = part_blocks(B, KIND_T1);
   FSL_GO(k_cell_count, pb, tb, 0, s, B, which);
   const unsigned nblk = blocks_for(B.mN, kScanTile);
-  FSL_GO(k_scan_local, dim3(nblk, B.nrep), kScanThreads, 0, s, B);
-  FSL_GO(k_scan_add, dim3(nblk, B.nrep), kScanThreads, 0, s, B);
-  FSL_GO(k_cell_scatter, pb, tb, 0, s, B);
-  FSL_GO(k_cell_rank, pb, tb, 0, s, B);
+  FSL_GO(k_scan_local, dim3(nblk, B.nrep), kScanThreads, 0, s, B, which);
+  FSL_GO(k_scan_add, dim3(nblk, B.nrep), kScanThreads, 0, s, B, which);
+  FSL_GO(k_cell_scatter, pb, tb, 0, s, B, which);
+  FSL_GO(k_cell_rank, pb, tb, 0, s, B, which);
 }
 
 // ----------------------------------------------------------------- forces ---
@@ -276,7 +285,8 @@ __global__ void __launch_bounds__(kPartThreads, 4) k_forces(FSL_KARGS, int which
   // first-order scheme: forces at q^{n+1/2} only with extraMobility
   // (src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:170-180)
   if (which == 1 && P.scheme == 1 && !P.has_extra) return;
-  const int i = active ? R.sorted[ig] : 0;
+  const CellList cl = cell_list(R, which);
+  const int i = active ? cl.sorted[ig] : 0;
   const double* __restrict__ q = which ? R.qp : R.q;
   double fx = 0.0, fy = 0.0, fz = 0.0;
   if (P.bonded && active) {
@@ -295,7 +305,7 @@ __global__ void __launch_bounds__(kPartThreads, 4) k_forces(FSL_KARGS, int which
     }
   }
   if (P.nonbonded && P.pair != 0) {
-    const double* __restrict__ ws = R.ws;  // wrapped, cell order
+    const double* __restrict__ ws = cl.ws;  // wrapped, cell order
     const double wx = active ? ws[ig] : 0.0, wy = active ? ws[np + ig] : 0.0,
                  wz = active ? ws[2 * np + ig] : 0.0;
     // the cell of the wrapped position, the arithmetic of k_cell_count (no
@@ -317,8 +327,8 @@ __global__ void __launch_bounds__(kPartThreads, 4) k_forces(FSL_KARGS, int which
         oy += oy < 0 ? P.mny : (oy >= P.mny ? -P.mny : 0);
         oz += oz < 0 ? P.mnz : (oz >= P.mnz ? -P.mnz : 0);
         const int cc = ox + oy * P.mnx + oz * P.mnx * P.mny;
-        st[m] = R.start[cc];
-        cnt[m] = R.start[cc + 1] - st[m];
+        st[m] = cl.start[cc];
+        cnt[m] = cl.start[cc + 1] - st[m];
       }
     }
     // exclusive scan of the 27 counts in cell order, within the 8 lanes
@@ -510,6 +520,59 @@ __device__ __forceinline__ bool quad_of(int blk, int np, long& e, int& a, int& q
   return ((t & ~31L) >> 2) < np;
 }
 
+// The RFD drift of particle i by its quad: (kT/delta) sign W_p spread from
+// q + sign (delta/2) W_p for both signs through add(stencil, values).  In
+// reference mode the drift's nodes come from the displaced position and its
+// weights from q, as the reference does; where both displaced positions pick
+// the same nodes the two fixed-point spreads are exact negatives of each
+// other (same weights, opposite values, symmetric rounding), so they are
+// skipped without changing the result.  Every lane of the warp calls this.
+template <int KN, class Add>
+__device__ __forceinline__ void rfd_drift(const Params& P, const Rep& R, int i, int a, int qb,
+                                          bool on, Add&& add) {
+  const int np = P.np;
+  const size_t wbase = (size_t)6 * P.nc;
+  double W[3] = {(double)R.noise[wbase + i], (double)R.noise[wbase + np + i],
+                 (double)R.noise[wbase + 2 * np + i]};
+  double pos[3] = {R.q[i], R.q[np + i], R.q[2 * np + i]};
+  double pp[3], pm[3], vp[3], vm[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    pp[d] = pos[d] + 0.5 * kRfdDelta * W[d];
+    pm[d] = pos[d] - 0.5 * kRfdDelta * W[d];
+    vp[d] = (P.kT / kRfdDelta) * W[d];
+    vm[d] = (P.kT / kRfdDelta) * -1 * W[d];
+  }
+  QuadStencil<KN> S;
+  if (P.rfd != 1) {
+    // lane a checks the node families a and a + 4 of the six
+    int same = 1;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int fd = a + 4 * r;
+      if (fd < 6) {
+        const int f = fd / 3, d = fd - 3 * f;
+        const double x = d == 0 ? pp[0] : (d == 1 ? pp[1] : pp[2]);
+        const double y = d == 0 ? pm[0] : (d == 1 ? pm[1] : pm[2]);
+        same &= stencil_base(P, d, f, x) == stencil_base(P, d, f, y);
+      }
+    }
+    same &= __shfl_xor_sync(0xffffffffu, same, 1);
+    same &= __shfl_xor_sync(0xffffffffu, same, 2);
+    if (!__all_sync(0xffffffffu, same || !on)) {
+      quad_stencil<KN>(P, pp, pos, a, qb, S);
+      if (on && !same) add(S, vp);
+      quad_stencil<KN>(P, pm, pos, a, qb, S);
+      if (on && !same) add(S, vm);
+    }
+  } else {
+    quad_stencil<KN>(P, pp, pp, a, qb, S);
+    if (on) add(S, vp);
+    quad_stencil<KN>(P, pm, pm, a, qb, S);
+    if (on) add(S, vm);
+  }
+}
+
 // ------------------------------------------------------------- spreading ---
 // One quad per particle (in cell order when ordered).  drift = 0: F at q;
 // drift = 1: F at q^{n+1/2}, then the particle's RFD drift (kT/delta) sign
@@ -524,7 +587,7 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
   const int np = P.np;
   if (!quad_of(blk, np, e, a, qb)) return;
   const bool on = e < np;  // lanes past the end join the shuffles only
-  const int i = on ? (ordered ? R.sorted[e] : (int)e) : 0;
+  const int i = on ? (ordered ? cell_list(R, drift == 1).sorted[e] : (int)e) : 0;
   bool sat = false;
   QuadStencil<KN> S;
   {
@@ -536,50 +599,9 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
   }
   if (drift) {
     // the RFD drift of the same particle, by the same quad
-    const size_t wbase = (size_t)6 * P.nc;
-    double W[3] = {(double)R.noise[wbase + i], (double)R.noise[wbase + np + i],
-                   (double)R.noise[wbase + 2 * np + i]};
-    double pos[3] = {R.q[i], R.q[np + i], R.q[2 * np + i]};
-    double pp[3], pm[3], vp[3], vm[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      pp[d] = pos[d] + 0.5 * kRfdDelta * W[d];
-      pm[d] = pos[d] - 0.5 * kRfdDelta * W[d];
-      vp[d] = (P.kT / kRfdDelta) * W[d];
-      vm[d] = (P.kT / kRfdDelta) * -1 * W[d];
-    }
-    if (P.rfd != 1) {
-      // Reference mode weighs both spreads at q: where both displaced
-      // positions pick the same nodes the two fixed-point spreads are exact
-      // negatives of each other (same weights, opposite values, symmetric
-      // rounding), so they are skipped without changing the result.  Lane a
-      // checks the node families a and a + 4 of the six.
-      int same = 1;
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int fd = a + 4 * r;
-        if (fd < 6) {
-          const int f = fd / 3, d = fd - 3 * f;
-          const double x = d == 0 ? pp[0] : (d == 1 ? pp[1] : pp[2]);
-          const double y = d == 0 ? pm[0] : (d == 1 ? pm[1] : pm[2]);
-          same &= stencil_base(P, d, f, x) == stencil_base(P, d, f, y);
-        }
-      }
-      same &= __shfl_xor_sync(0xffffffffu, same, 1);
-      same &= __shfl_xor_sync(0xffffffffu, same, 2);
-      if (!__all_sync(0xffffffffu, same || !on)) {
-        // a quad whose nodes agree spreads nothing; the others do both
-        quad_stencil<KN>(P, pp, pos, a, qb, S);
-        if (on && !same) quad_spread<KN>(P, S, a, vp, R.grid, sat);
-        quad_stencil<KN>(P, pm, pos, a, qb, S);
-        if (on && !same) quad_spread<KN>(P, S, a, vm, R.grid, sat);
-      }
-    } else {
-      quad_stencil<KN>(P, pp, pp, a, qb, S);
-      if (on) quad_spread<KN>(P, S, a, vp, R.grid, sat);
-      quad_stencil<KN>(P, pm, pm, a, qb, S);
-      if (on) quad_spread<KN>(P, S, a, vm, R.grid, sat);
-    }
+    rfd_drift<KN>(P, R, i, a, qb, on, [&](const QuadStencil<KN>& T, const double val[3]) {
+      quad_spread<KN>(P, T, a, val, R.grid, sat);
+    });
   }
   if (sat) set_err(R.err, 1);
 }
@@ -592,6 +614,304 @@ void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s) {
     FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered);
   else
     FSL_GO_T(k_spread, 3, g, kPartThreads, 0, s, B, drift, ordered);
+}
+
+// ------------------------------------------------ tiled spread + W build ---
+// The fixed-point form's spread and W build in one pass, without the spread
+// field in HBM.  A block owns a tile of kTileX x kTileY x kTileZ cells: it
+// takes from the cell lists every particle whose stencils can reach the
+// tile, adds the fixed-point products of the stencil nodes inside the tile
+// with shared-memory 64-bit atomics (the same integers the global spread
+// adds, so every node's sum is the same integer), then builds W = f +
+// c div(Sigma) of its cells with the arithmetic of k_wbuild4 (k_wbuild when
+// mx is not a multiple of 4) and stores it with coalesced 16-byte writes.
+// Replaces the slot writes and gathers of the reference's spreading
+// (src/stokesLimitFunctions.cu:659-1681, 1705-2255) and
+// kernelConstructWstokesLimit(_2) (:2281-2378, 3922-4069).
+
+constexpr int kTileX = 32, kTileY = 8, kTileZ = 8;
+constexpr int kTileCells = kTileX * kTileY * kTileZ;
+constexpr int kTileThreads = 256;
+constexpr int kTileMaxRuns = 1024;
+
+// Neighbour cells [a, b] (up to two intervals after the periodic wrap, no
+// cell twice) holding every particle whose stencil nodes can reach the cells
+// [x0, x1) of a grid of m cells: a stencil node lies within H cells of the
+// particle's grid coordinate, and one neighbour cell more on each side
+// absorbs the rounding of the cell assignment.
+struct NbRange {
+  int n, a[2], b[2];
+  __host__ __device__ int cells() const { return (b[0] - a[0] + 1) + (n > 1 ? b[1] - a[1] + 1 : 0); }
+  __host__ __device__ int at(int k) const { return k <= b[0] - a[0] ? a[0] + k : a[1] + k - (b[0] - a[0] + 1); }
+};
+
+__host__ __device__ inline int floor_div(long p, long q) {
+  return (int)(p >= 0 ? p / q : -((-p + q - 1) / q));
+}
+
+__host__ __device__ inline NbRange nb_range(int x0, int x1, int m, int mn, int H) {
+  const int lo = floor_div((long)(x0 - H) * mn, m) - 1;
+  const int hi = floor_div((long)(x1 + H) * mn, m) + 1;
+  NbRange r;
+  r.n = 1;
+  r.a[1] = r.b[1] = 0;
+  if (hi - lo + 1 >= mn) {
+    r.a[0] = 0;
+    r.b[0] = mn - 1;
+  } else if (lo < 0) {
+    r.n = 2;
+    r.a[0] = lo + mn;
+    r.b[0] = mn - 1;
+    r.a[1] = 0;
+    r.b[1] = hi;
+  } else if (hi >= mn) {
+    r.n = 2;
+    r.a[0] = lo;
+    r.b[0] = mn - 1;
+    r.a[1] = 0;
+    r.b[1] = hi - mn;
+  } else {
+    r.a[0] = lo;
+    r.b[0] = hi;
+  }
+  return r;
+}
+
+__host__ __device__ constexpr int tile_halo(int kn) { return kn / 2 + 2; }
+
+size_t tile_smem_bytes() {
+  return sizeof(unsigned long long) * 3 * kTileCells + sizeof(int) * (2 * kTileMaxRuns + 1);
+}
+
+// The runs of the block's candidates: for every (y, z) neighbour cell pair
+// and x interval, the particles start[c(a, y, z)] .. start[c(b, y, z) + 1]
+// of the cell-ordered list; run_pre gets the exclusive prefix of the run
+// lengths (run_pre[nruns] = all candidates).  All threads call this.
+__device__ void tile_runs(const int* __restrict__ start, const NbRange& ix, const NbRange& iy,
+                          const NbRange& iz, int mnx, int mny, int* run_st, int* run_pre, int nruns) {
+  const int ny = iy.cells();
+  for (int r = threadIdx.x; r < nruns; r += blockDim.x) {
+    const int xi = r % ix.n, pr = r / ix.n;
+    const int y = iy.at(pr % ny), z = iz.at(pr / ny);
+    const int row = mnx * (y + mny * z);
+    const int s0 = start[ix.a[xi] + row];
+    run_st[r] = s0;
+    run_pre[r] = start[ix.b[xi] + row + 1] - s0;
+  }
+  __syncthreads();
+  // exclusive scan: four entries per thread, then the threads' sums
+  __shared__ int wsum[kTileThreads / 32];
+  const int base = threadIdx.x * 4;
+  int v[4], sum = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = base + k < nruns ? run_pre[base + k] : 0;
+    sum += v[k];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  int off = 0;
+  for (int w = 0; w < warp; ++w) off += wsum[w];
+  int run = off + incl - sum;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (base + k < nruns) run_pre[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == blockDim.x - 1) run_pre[nruns] = run;
+  __syncthreads();
+}
+
+// The products of the nodes of one spread that fall in the tile, added to
+// the tile's accumulators (shared memory).  No shuffles.
+template <int KN>
+__device__ __forceinline__ void tile_spread(const Params& P, const QuadStencil<KN>& S, int a,
+                                            const double val[3], unsigned long long* acc, int x0,
+                                            int y0, int z0, bool& sat) {
+  if (a >= KN) return;
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    const int lx = S.jx[comp == 0] - x0;
+    if ((unsigned)lx >= (unsigned)kTileX) continue;
+    const float wx = S.wx[comp == 0];
+    const double vs = val[comp] * kFixedScale;
+    unsigned long long* ac = acc + comp * kTileCells + lx;
+#pragma unroll
+    for (int b = 0; b < KN; ++b) {
+      const int ly = S.jy[comp == 1][b] - y0;
+      if ((unsigned)ly >= (unsigned)kTileY) continue;
+      const float wy = S.wy[comp == 1][b];
+#pragma unroll
+      for (int c = 0; c < KN; ++c) {
+        const int lz = S.jz[comp == 2][c] - z0;
+        if ((unsigned)lz >= (unsigned)kTileZ) continue;
+        const float w = wx * (wy * S.wz[comp == 2][c]);
+        const double v = (double)w * vs;
+        sat |= !(fabs(v) < kFixedMax);
+        const long long iv = sat ? 0ll : __double2ll_rn(v);
+        if (iv != 0) atomicAdd(ac + (lz * kTileY + ly) * kTileX, (unsigned long long)iv);
+      }
+    }
+  }
+}
+
+// drift: as k_spread (0: F at q; 1: F at q^{n+1/2} and the RFD drift at q^n;
+// 2: F and the drift at q^n); the forces come from the list of their
+// positions, the drift from the list at q^n.  nsets, nfac: the stress
+// samples and factor of k_wbuild.
+template <bool ONE, int KN>
+__global__ void __launch_bounds__(kTileThreads) k_spread_w(FSL_KARGS, int drift, int nsets,
+                                                            double nfac, int tiles_x, int tiles_y) {
+  FSL_REP_AT(blockIdx.y);
+  extern __shared__ unsigned long long tsm[];
+  unsigned long long* acc = tsm;  // [3][kTileZ][kTileY][kTileX]
+  int* run_st = reinterpret_cast<int*>(acc + 3 * kTileCells);
+  int* run_pre = run_st + kTileMaxRuns;
+  const int bt = blockIdx.x;
+  const int x0 = (bt % tiles_x) * kTileX, y0 = ((bt / tiles_x) % tiles_y) * kTileY,
+            z0 = (bt / (tiles_x * tiles_y)) * kTileZ;
+  for (int k = threadIdx.x; k < 3 * kTileCells; k += blockDim.x) acc[k] = 0ull;
+  bool sat = false;
+  const int np = P.np;
+  if (np > 0) {
+    constexpr int H = tile_halo(KN);
+    const NbRange ix = nb_range(x0, min(x0 + kTileX, P.mx), P.mx, P.mnx, H);
+    const NbRange iy = nb_range(y0, min(y0 + kTileY, P.my), P.my, P.mny, H);
+    const NbRange iz = nb_range(z0, min(z0 + kTileZ, P.mz), P.mz, P.mnz, H);
+    const int nruns = ix.n * iy.cells() * iz.cells();  // <= kTileMaxRuns (checked on the host)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int a = lane & 3, qb = lane & ~3;
+    auto add = [&](const QuadStencil<KN>& S, const double val[3]) {
+      tile_spread<KN>(P, S, a, val, acc, x0, y0, z0, sat);
+    };
+    const int passes = drift == 1 ? 2 : 1;
+    for (int pass = 0; pass < passes; ++pass) {
+      const CellList cl = cell_list(R, drift == 1 && pass == 0 ? 1 : 0);
+      __syncthreads();  // the runs of the previous pass are read
+      tile_runs(cl.start, ix, iy, iz, P.mnx, P.mny, run_st, run_pre, nruns);
+      const int K = run_pre[nruns];
+      for (int k0 = warp * 8; k0 < K; k0 += (kTileThreads / 32) * 8) {
+        const int k = k0 + (lane >> 2);
+        const bool on = k < K;
+        int i = 0;
+        if (on) {
+          int lo = 0, hi = nruns;  // run_pre[lo] <= k < run_pre[hi]
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (run_pre[mid] <= k) lo = mid;
+            else hi = mid;
+          }
+          i = cl.sorted[run_st[lo] + (k - run_pre[lo])];
+        }
+        if (pass == 0) {
+          const double* qf = drift == 1 ? R.qp : R.q;
+          double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
+          double val[3] = {R.F[i], R.F[np + i], R.F[2 * (size_t)np + i]};
+          QuadStencil<KN> S;
+          quad_stencil<KN>(P, pos, pos, a, qb, S);
+          if (on) add(S, val);
+        }
+        if ((pass == 0 && drift == 2) || pass == 1) rfd_drift<KN>(P, R, i, a, qb, on, add);
+      }
+    }
+  }
+  __syncthreads();
+  // W of the tile's cells
+  const float scale = (float)(kFixedInv / P.dV);
+  const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
+  const float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
+  const float a4x = (float)P.invdx * f4, a4y = (float)P.invdy * f4, a4z = (float)P.invdz * f4;
+  const float* n1 = R.noise;
+  const size_t off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
+  const float* n2 = R.noise + off2;
+  const size_t nc = (size_t)P.nc;
+  const int ex = min(kTileX, P.mx - x0), ey = min(kTileY, P.my - y0), ez = min(kTileZ, P.mz - z0);
+  if ((P.mx & 3) == 0) {
+    const bool al2 = (off2 & 3) == 0;
+    constexpr int GX = kTileX / 4;
+    for (int g = threadIdx.x; g < GX * kTileY * kTileZ; g += blockDim.x) {
+      const int lx = 4 * (g % GX), ly = (g / GX) % kTileY, lz = g / (GX * kTileY);
+      if (lx >= ex || ly >= ey || lz >= ez) continue;
+      const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+      const size_t i0 = (size_t)x + (size_t)P.mx * ((size_t)y + (size_t)P.my * z);
+      float w[3][4];
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          w[comp][c] = (float)((double)(long long)acc[comp * kTileCells + (lz * kTileY + ly) * kTileX + lx + c] *
+                               (double)scale);
+      stress_div4(P, n1, true, x, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
+      if (nsets > 1) stress_div4(P, n2, al2, x, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp)
+        *reinterpret_cast<float4*>(R.wbuf + comp * nc + i0) =
+            make_float4(w[comp][0], w[comp][1], w[comp][2], w[comp][3]);
+    }
+  } else {
+    for (int c = threadIdx.x; c < kTileCells; c += blockDim.x) {
+      const int lx = c % kTileX, ly = (c / kTileX) % kTileY, lz = c / (kTileX * kTileY);
+      if (lx >= ex || ly >= ey || lz >= ez) continue;
+      const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+      const int i = x + P.mx * (y + P.my * z);
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp) {
+        float w = (float)((double)(long long)acc[comp * kTileCells + c] * (double)scale);
+        w += stress_div(P, n1, comp, x, y, z, i, a1x, a1y, a1z, a4x, a4y, a4z);
+        if (nsets > 1) w += stress_div(P, n2, comp, x, y, z, i, a1x, a1y, a1z, a4x, a4y, a4z);
+        R.wbuf[comp * nc + i] = w;
+      }
+    }
+  }
+  if (sat) set_err(R.err, 1);
+}
+
+void tile_init() {
+  const int sm = (int)tile_smem_bytes();
+  cudaFuncSetAttribute(k_spread_w<true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_spread_w<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_spread_w<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_spread_w<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+bool tile_eligible(const Params& P) {
+  if (P.prec != PREC_FIXED || P.scheme > 1) return false;  // 3-D Stokes schemes
+  // the drift's displacement (delta/2 |W| <= 0.003 for FP32 normals) must
+  // stay well inside the halo's spare cell
+  if (std::min(P.dx, std::min(P.dy, P.dz)) < 0.01) return false;
+  // a block scans about (tile + 2 halo + 2 neighbour cells)^3: only worth it
+  // while a neighbour cell spans at most four grid cells
+  if (P.mx > 4 * P.mnx || P.my > 4 * P.mny || P.mz > 4 * P.mnz) return false;
+  const int H = tile_halo(P.kernel);
+  int runs = 1;
+  const int m[3] = {P.mx, P.my, P.mz}, mn[3] = {P.mnx, P.mny, P.mnz}, t[3] = {kTileX, kTileY, kTileZ};
+  for (int d = 0; d < 3; ++d) {
+    int worst = 0;
+    for (int x0 = 0; x0 < m[d]; x0 += t[d]) {
+      const NbRange r = nb_range(x0, std::min(x0 + t[d], m[d]), m[d], mn[d], H);
+      worst = std::max(worst, d == 0 ? r.n : r.cells());
+    }
+    runs *= worst;
+  }
+  return runs <= kTileMaxRuns;
+}
+
+void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStream_t s) {
+  const int tx = (B.mx + kTileX - 1) / kTileX, ty = (B.my + kTileY - 1) / kTileY,
+            tz = (B.mz + kTileZ - 1) / kTileZ;
+  const dim3 g((unsigned)(tx * ty * tz), (unsigned)B.nrep);
+  const size_t sm = tile_smem_bytes();
+  if (B.kernel == 4)
+    FSL_GO_T(k_spread_w, 4, g, kTileThreads, sm, s, B, drift, nsets, nfac, tx, ty);
+  else
+    FSL_GO_T(k_spread_w, 3, g, kTileThreads, sm, s, B, drift, nsets, nfac, tx, ty);
 }
 
 // -------------------------------------------------------- interpolation ---
