@@ -31,6 +31,12 @@ def _run(fsl, c, tiled, steps=6):
     L = c["L"]
     if c["n"] is None:
         q, bi, bj = chains(16, 16, L, 3)
+    elif c["pair"] == "lj":
+        # a jittered lattice of spacing 3: no overlaps for the LJ table
+        g = [np.arange(int(x // 3)) * 3.0 - x / 2 + 1.5 for x in L]
+        q = np.stack(np.meshgrid(*g, indexing="ij")).reshape(3, -1)[:, :c["n"]]
+        q = q + 0.2 * (uniform_positions(q.shape[1], (1.0,) * 3, 5))
+        bi = None
     else:
         q, bi = uniform_positions(c["n"], L, 17), None
     cfg = fsl.make_config(c["m"], L, eta=1.0, kT=0.01, dt=0.01, cutoff=1.5, kernel=c["kernel"],
