@@ -633,6 +633,7 @@ constexpr int kTileX = 32, kTileY = 8, kTileZ = 8;
 constexpr int kTileCells = kTileX * kTileY * kTileZ;
 constexpr int kTileThreads = 256;
 constexpr int kTileMaxRuns = 1024;
+constexpr int kTileChunk = 1024;  // candidates filtered per round
 
 // Neighbour cells [a, b] (up to two intervals after the periodic wrap, no
 // cell twice) holding every particle whose stencil nodes can reach the cells
@@ -680,7 +681,7 @@ __host__ __device__ inline NbRange nb_range(int x0, int x1, int m, int mn, int H
 __host__ __device__ constexpr int tile_halo(int kn) { return kn / 2 + 2; }
 
 size_t tile_smem_bytes() {
-  return sizeof(unsigned long long) * 3 * kTileCells + sizeof(int) * (2 * kTileMaxRuns + 1);
+  return sizeof(unsigned long long) * 3 * kTileCells + sizeof(int) * (2 * kTileMaxRuns + 1 + kTileChunk);
 }
 
 // The runs of the block's candidates: for every (y, z) neighbour cell pair
@@ -774,6 +775,9 @@ __global__ void __launch_bounds__(kTileThreads) k_spread_w(FSL_KARGS, int drift,
   unsigned long long* acc = tsm;  // [3][kTileZ][kTileY][kTileX]
   int* run_st = reinterpret_cast<int*>(acc + 3 * kTileCells);
   int* run_pre = run_st + kTileMaxRuns;
+  int* acc_list = run_pre + kTileMaxRuns + 1;  // [kTileChunk] accepted particles
+  __shared__ int n_acc_s;
+  int* n_acc = &n_acc_s;
   const int bt = blockIdx.x;
   const int x0 = (bt % tiles_x) * kTileX, y0 = ((bt / tiles_x) % tiles_y) * kTileY,
             z0 = (bt / (tiles_x * tiles_y)) * kTileZ;
@@ -791,34 +795,58 @@ __global__ void __launch_bounds__(kTileThreads) k_spread_w(FSL_KARGS, int drift,
     auto add = [&](const QuadStencil<KN>& S, const double val[3]) {
       tile_spread<KN>(P, S, a, val, acc, x0, y0, z0, sat);
     };
+    // a particle's stencil nodes lie within [u - 3, u + 1.5] (4-point) or
+    // [u - 2.5, u + 1] (3-point) of its grid coordinate u; 0.05 more absorbs
+    // the drift's displacement and rounding
+    const double mlo = (KN == 4 ? 1.5 : 1.0) + 0.05, mhi = (KN == 4 ? 2.0 : 1.5) + 0.05;
+    const int ex1 = min(x0 + kTileX, P.mx), ey1 = min(y0 + kTileY, P.my), ez1 = min(z0 + kTileZ, P.mz);
+    auto near = [&](double w, double halfL, double invd, int lo, int hi, int m) {
+      const double u = (w + halfL) * invd, a0 = lo - mlo, b0 = hi + mhi;
+      return (u >= a0 && u < b0) || (u - m >= a0 && u - m < b0) || (u + m >= a0 && u + m < b0);
+    };
     const int passes = drift == 1 ? 2 : 1;
     for (int pass = 0; pass < passes; ++pass) {
       const CellList cl = cell_list(R, drift == 1 && pass == 0 ? 1 : 0);
-      __syncthreads();  // the runs of the previous pass are read
+      __syncthreads();  // the runs and accepted list of the previous pass are read
       tile_runs(cl.start, ix, iy, iz, P.mnx, P.mny, run_st, run_pre, nruns);
       const int K = run_pre[nruns];
-      for (int k0 = warp * 8; k0 < K; k0 += (kTileThreads / 32) * 8) {
-        const int k = k0 + (lane >> 2);
-        const bool on = k < K;
-        int i = 0;
-        if (on) {
+      for (int c0 = 0; c0 < K; c0 += kTileChunk) {
+        // the candidates whose stencils can reach the tile, from their
+        // wrapped positions in list order (the order of acceptance does not
+        // matter: the fixed-point sums are exact)
+        if (threadIdx.x == 0) *n_acc = 0;
+        __syncthreads();
+        const int c1 = min(K, c0 + kTileChunk);
+        for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
           int lo = 0, hi = nruns;  // run_pre[lo] <= k < run_pre[hi]
           while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
             if (run_pre[mid] <= k) lo = mid;
             else hi = mid;
           }
-          i = cl.sorted[run_st[lo] + (k - run_pre[lo])];
+          const int e = run_st[lo] + (k - run_pre[lo]);
+          if (near(cl.ws[e], 0.5 * P.lx, P.invdx, x0, ex1, P.mx) &&
+              near(cl.ws[np + e], 0.5 * P.ly, P.invdy, y0, ey1, P.my) &&
+              near(cl.ws[2 * np + e], 0.5 * P.lz, P.invdz, z0, ez1, P.mz))
+            acc_list[atomicAdd(n_acc, 1)] = cl.sorted[e];
         }
-        if (pass == 0) {
-          const double* qf = drift == 1 ? R.qp : R.q;
-          double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
-          double val[3] = {R.F[i], R.F[np + i], R.F[2 * (size_t)np + i]};
-          QuadStencil<KN> S;
-          quad_stencil<KN>(P, pos, pos, a, qb, S);
-          if (on) add(S, val);
+        __syncthreads();
+        const int na = *n_acc;
+        for (int k0 = warp * 8; k0 < na; k0 += (kTileThreads / 32) * 8) {
+          const int k = k0 + (lane >> 2);
+          const bool on = k < na;
+          const int i = on ? acc_list[k] : acc_list[0];
+          if (pass == 0) {
+            const double* qf = drift == 1 ? R.qp : R.q;
+            double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
+            double val[3] = {R.F[i], R.F[np + i], R.F[2 * (size_t)np + i]};
+            QuadStencil<KN> S;
+            quad_stencil<KN>(P, pos, pos, a, qb, S);
+            if (on) add(S, val);
+          }
+          if ((pass == 0 && drift == 2) || pass == 1) rfd_drift<KN>(P, R, i, a, qb, on, add);
         }
-        if ((pass == 0 && drift == 2) || pass == 1) rfd_drift<KN>(P, R, i, a, qb, on, add);
+        __syncthreads();  // acc_list is read
       }
     }
   }
@@ -884,8 +912,8 @@ void tile_init() {
 bool tile_eligible(const Params& P) {
   if (P.prec != PREC_FIXED || P.scheme > 1) return false;  // 3-D Stokes schemes
   // the drift's displacement (delta/2 |W| <= 0.003 for FP32 normals) must
-  // stay well inside the halo's spare cell
-  if (std::min(P.dx, std::min(P.dy, P.dz)) < 0.01) return false;
+  // stay well inside the candidates' spare 0.05 cells
+  if (std::min(P.dx, std::min(P.dy, P.dz)) < 0.1) return false;
   // a block scans about (tile + 2 halo + 2 neighbour cells)^3: only worth it
   // while a neighbour cell spans at most four grid cells
   if (P.mx > 4 * P.mnx || P.my > 4 * P.mny || P.mz > 4 * P.mnz) return false;
