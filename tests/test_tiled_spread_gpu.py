@@ -1,8 +1,9 @@
 """The tiled spread + W build of the fixed-point form against the global-atomic
 spread and the separate W build: every node's fixed-point sum is the same
 integer and W is built with the same arithmetic, so positions, forces and
-the velocity field agree bit for bit.  FLUAMSL_TILED_SPREAD=0 selects the
-global-atomic path when an instance is created."""
+the velocity field agree bit for bit.  FLUAMSL_TILED_SPREAD=1 selects the
+tiled path when an instance is created (the global-atomic path is the
+default)."""
 import os
 
 import numpy as np
