@@ -190,6 +190,7 @@ int fsl_set_positions(fsl_handle* h, const double* in) {
   FSL_TRY(cudaSetDevice(h->exec.device));
   FSL_TRY(cudaMemcpyAsync(rep(h).q, in, sizeof(double) * 3 * (size_t)params(h).np,
                           cudaMemcpyHostToDevice, h->exec.stream));
+  if (int rc = fsl::slot_mark_moved(h->slot, h->exec.stream)) return rc;
   FSL_TRY(cudaStreamSynchronize(h->exec.stream));
   return FSL_OK;
 }
@@ -311,6 +312,7 @@ int fsl_cell_list(fsl_handle* h, int32_t* cell_of, int32_t* start, int32_t* sort
   int rc = prepare(h);
   if (rc) return rc;
   const fsl::Params& P = params(h);
+  if ((rc = fsl::slot_request_lists(h->slot, h->exec.stream))) return rc;
   fsl::launch_cells(h->group.B, 0, h->exec.stream);
   if ((rc = check_launch())) return rc;
   FSL_TRY(cudaStreamSynchronize(h->exec.stream));
@@ -326,7 +328,8 @@ int fsl_compute_forces(fsl_handle* h, double* F) {
   if (!h || !F) return errorf(FSL_E_ARG, "null argument");
   int rc = prepare(h);
   if (rc) return rc;
-  fsl::launch_cells(h->group.B, 0, h->exec.stream);
+  if ((rc = fsl::slot_request_lists(h->slot, h->exec.stream))) return rc;
+  fsl::launch_pair_lists(h->group.B, 0, h->exec.stream);
   fsl::launch_forces(h->group.B, 0, h->exec.stream);
   if ((rc = check_launch())) return rc;
   return fsl_get_forces(h, F);

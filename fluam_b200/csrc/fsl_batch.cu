@@ -19,6 +19,7 @@ struct PackEnt {
   long long off;  // first double of the instance in the packed array
   int np;
   int pad;
+  uint64_t* vl_flag;  // set [2] when the positions are replaced
 };
 
 // dir = 0: packed <- q of every instance; dir = 1: q <- packed.
@@ -31,6 +32,8 @@ __global__ void k_pack(const PackEnt* __restrict__ ents, double* __restrict__ pa
     if (dir == 0) packed[e.off + k] = e.q[k];
     else e.q[k] = packed[e.off + k];
   }
+  // new positions: the pair list is rebuilt at the next force evaluation
+  if (dir == 1 && blockIdx.x == 0 && threadIdx.x == 0) e.vl_flag[2] = 1;
 }
 
 // errs[i] = error bits of instance i with bit 30 set, or 0 if its word is clear
@@ -137,7 +140,7 @@ int fsl_batch_create(int32_t n, const fsl_config* cfgs, const int64_t* np, const
       it = b->groups.emplace(key, std::move(g)).first;
     }
     it->second->slots.push_back(&s);
-    ents[i] = PackEnt{s.r.q, s.r.err, off, (int)np[i], 0};
+    ents[i] = PackEnt{s.r.q, s.r.err, off, (int)np[i], 0, s.r.vl_flag};
     off += 3ll * np[i];
     b->max_np = std::max(b->max_np, (int)np[i]);
     b->nc_total += P[i].nc;

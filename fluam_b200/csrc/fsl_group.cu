@@ -27,7 +27,7 @@ size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 struct SlotLayout {
   size_t q, qp, F, u, qw, ws, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
       bsum, ljtab, noise, grid, spec, v, wbuf, noise64, v64, z64, err, t, q0, obs, obs_part, obs_ticket,
-      start1, sorted1, ws1, total;
+      start1, sorted1, ws1, vl_cnt, vl_idx, qref, vl_flag, total;
 };
 
 SlotLayout layout(const Params& P, int np_cap) {
@@ -82,6 +82,10 @@ SlotLayout layout(const Params& P, int np_cap) {
   L.start1 = take(two_lists ? sizeof(int) * (mN + 1) : 0);
   L.sorted1 = take(two_lists ? sizeof(int) * np : 0);
   L.ws1 = take(two_lists ? sizeof(double) * 3 * np : 0);
+  L.vl_cnt = take(P.verlet ? sizeof(int) * np : 0);
+  L.vl_idx = take(P.verlet ? sizeof(int) * (size_t)kVlCap * np : 0);
+  L.qref = take(P.verlet ? sizeof(double) * 3 * np : 0);
+  L.vl_flag = take(sizeof(uint64_t) * 3);
   L.total = off;
   return L;
 }
@@ -223,6 +227,25 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   P.cutoff2 = c.cutoff * c.cutoff;
   P.invcut2 = c.cutoff > 0 ? 1. / (c.cutoff * c.cutoff) : 0.0;
   P.soft_eps = c.soft_epsilon;
+  // 3-D Stokes schemes: soft repulsion through a Verlet list (when the
+  // neighbour cells are at least rc wide, so that the list holds exactly
+  // the reference's pair set; skin <= 2 cells - rc keeps the list build
+  // within two cells), no list at all without pair forces.
+  // FLUAMSL_VERLET=0 keeps soft repulsion on the cell-list kernel.
+  if (c.scheme <= FSL_SCHEME_FIRST_ORDER && np > 0) {
+    const bool pairs_on = c.nonbonded && c.pair != FSL_PAIR_NONE;
+    P.nolist = !pairs_on;
+    const double cell = std::min(c.lx / P.mnx, std::min(c.ly / P.mny, c.lz / P.mnz));
+    const double skin = std::min(0.25 * c.cutoff, 2.0 * cell - c.cutoff);
+    const char* env = std::getenv("FLUAMSL_VERLET");
+    if (pairs_on && c.pair == FSL_PAIR_SOFT && cell >= c.cutoff && skin >= 0.05 * c.cutoff &&
+        !(env && env[0] == '0')) {
+      P.verlet = 1;
+      P.skin = skin;
+      P.vl_cut2 = (c.cutoff + skin) * (c.cutoff + skin);
+      P.vl_half2 = 0.25 * skin * skin;
+    }
+  }
   P.eta = c.shearviscosity;
   P.kT = c.temperature;
   P.dt = c.dt;
@@ -338,6 +361,10 @@ int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st) {
   r.start1 = two_lists ? (int*)(base + L.start1) : nullptr;
   r.sorted1 = two_lists ? (int*)(base + L.sorted1) : nullptr;
   r.ws1 = two_lists ? (double*)(base + L.ws1) : nullptr;
+  r.vl_cnt = P.verlet ? (int*)(base + L.vl_cnt) : nullptr;
+  r.vl_idx = P.verlet ? (int*)(base + L.vl_idx) : nullptr;
+  r.qref = P.verlet ? (double*)(base + L.qref) : nullptr;
+  r.vl_flag = (uint64_t*)(base + L.vl_flag);
   return FSL_OK;
 }
 
@@ -366,6 +393,18 @@ int slot_read_observables(const Slot& s, cudaStream_t st, fsl_observables* out) 
     out->momentum[d] = o[9 + d];
     out->momentum_sum[d] = o[12 + d];
   }
+  return FSL_OK;
+}
+
+int slot_mark_moved(Slot& s, cudaStream_t st) {
+  static const uint64_t flags[3] = {0, 0, 1};
+  FSL_TRY(cudaMemcpyAsync(s.r.vl_flag, flags, sizeof(flags), cudaMemcpyHostToDevice, st));
+  return FSL_OK;
+}
+
+int slot_request_lists(Slot& s, cudaStream_t st) {
+  static const uint64_t two = 2;
+  FSL_TRY(cudaMemcpyAsync(s.r.vl_flag + 2, &two, sizeof(two), cudaMemcpyHostToDevice, st));
   return FSL_OK;
 }
 
@@ -414,6 +453,7 @@ int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, c
   FSL_TRY(cudaMemsetAsync(r.err, 0, sizeof(int) * 4, st));
   FSL_TRY(cudaMemsetAsync(r.t, 0, sizeof(uint64_t), st));
   if (int rc = slot_reset_observables(s, st)) return rc;
+  if (int rc = slot_mark_moved(s, st)) return rc;
   r.active = 1;
   return FSL_OK;
 }
@@ -562,10 +602,13 @@ int group_upload(Group& g) {
   // particle density the global-atomic spread plus the W build is faster.
   const char* env = std::getenv("FLUAMSL_TILED_SPREAD");
   B.tiled = env && env[0] == '1' && tile_eligible(g.P0);
+  B.has_vl = B.has_cl = 0;
   for (const Slot* s : g.slots) {
     B.max_np = std::max(B.max_np, s->np_cap);
     B.max_noise_n = std::max<uint64_t>(B.max_noise_n, noise_count(g.P0, s->np_cap));
     B.tiled = B.tiled && tile_eligible(s->r.P);  // per instance: the cell sizes
+    if (s->r.P.verlet || s->r.P.nolist) B.has_vl = 1;
+    else B.has_cl = 1;
   }
   if (n > g.d_cap) {
     if (g.d_reps || g.d_boff) {
@@ -631,12 +674,12 @@ void group_enqueue_step(Group& g) {
   };
   auto cells_forces = [&](int which) {
     pr.mark(s, "cells");
-    launch_cells(B, which, s, false);
+    launch_pair_lists(B, which, s);
     chk("cells");
     pr.mark(s, "forces");
     launch_forces(B, which, s);
     chk("forces");
-    pr.count(pk ? 8 : 1);
+    pr.count(pk ? 5 + (B.has_vl ? 2 : 0) + (B.has_cl ? 1 : 0) : 0);
   };
   g.fail_stage = nullptr;
   chk("before the step");

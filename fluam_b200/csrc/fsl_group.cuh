@@ -64,6 +64,11 @@ void slot_free(Slot& s);
 // allocated slot of its class: positions, LJ table, cleared forces, error
 // word, step counter and bonds.  Enqueued on st.
 int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, cudaStream_t st);
+// Positions changed from the host: the pair list is rebuilt at the next
+// force evaluation.  slot_request_lists: the next launch_pair_lists builds
+// the cell list whatever the path (the component entry points).
+int slot_mark_moved(Slot& s, cudaStream_t st);
+int slot_request_lists(Slot& s, cudaStream_t st);
 // q0 := q, observables accumulators cleared (enqueued on st).
 int slot_reset_observables(Slot& s, cudaStream_t st);
 // The accumulators of the slot (synchronises st).

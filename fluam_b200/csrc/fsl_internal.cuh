@@ -48,6 +48,11 @@ struct Params {
   int scheme;  // FSL_SCHEME_* (0 midpoint, 1 first order, 2 quasi2D, 3 stokesLimit2D)
   int prec;    // FSL_PRECISION_* (0 fixed point, 1 float atomics, 2 FP64)
   int observe; // FP64 observables accumulated at the end of every step
+  // pair forces from a Verlet list (soft repulsion): pairs within
+  // rc + skin at the reference positions qref, rebuilt when a particle has
+  // moved more than skin / 2 since; nolist: no pair forces, no cell list
+  int verlet, nolist;
+  double skin, vl_cut2, vl_half2;  // skin, (rc + skin)^2, (skin / 2)^2
   int has_extra;
   double cutoff, cutoff2, invcut2, soft_eps;
   double eta, kT, dt, extra_mob, fact1, fact2, fact4;
@@ -412,7 +417,16 @@ struct Rep {
   double* obs;
   double* obs_part;
   unsigned* obs_ticket;
+  // Verlet list: per particle count and kVlCap neighbour slots ([slot][np]),
+  // reference positions, and the rebuild word vl_flag: [0], [1] the step
+  // (counter + 1) at whose force evaluation at q (0) or q^{n+1/2} (1) the
+  // list must be rebuilt, [2] nonzero: rebuild at the next evaluation
+  int* vl_cnt;
+  int* vl_idx;
+  double* qref;
+  uint64_t* vl_flag;
 };
+constexpr int kVlCap = 64;
 constexpr int kObsVals = 10;      // msd, displacement[3], force[3], momentum[3]
 constexpr int kObsSlots = 16;     // steps, msd, msd_sum, disp[3], force[3], mom[3], mom_sum[3]
 constexpr int kObsMaxBlocks = 148;
@@ -426,6 +440,17 @@ struct CellList {
 __device__ __forceinline__ CellList cell_list(const Rep& R, int which) {
   if (which && R.start1) return CellList{R.start1, R.sorted1, R.ws1};
   return CellList{R.start, R.sorted, R.ws};
+}
+
+// Whether the list-building kernels of force evaluation `which` run: always
+// for the cell-list path, never without pair forces, and for the Verlet path
+// only when the list must be rebuilt.
+__device__ __forceinline__ bool list_needed(const Rep& R, int which) {
+  if (!R.P.verlet && !R.P.nolist) return true;
+  const uint64_t f = R.vl_flag[2];  // 2: requested by a component entry point
+  if (f == 2) return true;
+  if (R.P.nolist) return false;
+  return f != 0 || R.vl_flag[which] == *R.t + 1;
 }
 
 // Launch kinds of the particle kernels (256-thread blocks): threads per
@@ -457,6 +482,7 @@ struct Batch {
   int max_np;
   uint64_t max_noise_n;
   int tiled;        // spread and W build by launch_spread_w
+  int has_vl, has_cl;  // instances on the Verlet path / on the cell-list pair path
   int nblk[NKIND];  // total blocks of each particle launch kind
   const Rep* one;   // host copy of the single instance (nrep == 1), else null
   RepSrc src() const { return RepSrc{reps, boff, nrep}; }
@@ -568,6 +594,9 @@ void launch_step_counter(const Batch& B, cudaStream_t s);
 void tile_init();
 bool tile_eligible(const Params& P);
 void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStream_t s);
+// The cell list of force evaluation `which` and, for Verlet-list
+// instances, the pair list (each only where list_needed says so).
+void launch_pair_lists(const Batch& B, int which, cudaStream_t s);
 // FP64 observables of every instance with P.observe (end of a step)
 void launch_observe(const Batch& B, cudaStream_t s);
 // The FP64 form (fsl_fp64.cu); the launchers above hand a class of that

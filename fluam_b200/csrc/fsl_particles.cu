@@ -76,7 +76,7 @@ template <bool ONE>
 __global__ void k_cell_count(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T1);
   int i = blk * blockDim.x + threadIdx.x;
-  if (i >= P.np) return;
+  if (i >= P.np || !list_needed(R, which)) return;
   const double* q = which ? R.qp : R.q;
   double x = q[i], y = q[P.np + i], z = q[2 * P.np + i];
   // a coordinate this large or non-finite means the run has blown up
@@ -135,6 +135,7 @@ __device__ __forceinline__ void block_scan(const int (&v)[kScanItems], int& incl
 template <bool ONE>
 __global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS, int which) {
   FSL_REP_AT(blockIdx.y);
+  if (!list_needed(R, which)) return;
   int* start = which && R.start1 ? R.start1 : R.start;
   __shared__ int warp_tot[33];
   const int n = P.mN;
@@ -161,6 +162,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_local(FSL_KARGS, int whic
 template <bool ONE>
 __global__ void __launch_bounds__(kScanThreads) k_scan_add(FSL_KARGS, int which) {
   FSL_REP_AT(blockIdx.y);
+  if (!list_needed(R, which)) return;
   int* start = which && R.start1 ? R.start1 : R.start;
   __shared__ int warp_sum[32];
   const int tile = blockIdx.x;
@@ -184,7 +186,7 @@ template <bool ONE>
 __global__ void k_cell_scatter(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T1);
   int i = blk * blockDim.x + threadIdx.x;
-  if (i >= P.np) return;
+  if (i >= P.np || !list_needed(R, which)) return;
   const int* start = which && R.start1 ? R.start1 : R.start;
   int c = R.cell_of[i];
   R.tmp[start[c] + atomicAdd(&R.fill[c], 1)] = i;
@@ -196,7 +198,7 @@ template <bool ONE>
 __global__ void k_cell_rank(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T1);
   int i = blk * blockDim.x + threadIdx.x;
-  if (i >= P.np) return;
+  if (i >= P.np || !list_needed(R, which)) return;
   const bool second = which && R.start1;
   const int* start = second ? R.start1 : R.start;
   int* sorted = second ? R.sorted1 : R.sorted;
@@ -282,6 +284,7 @@ __global__ void __launch_bounds__(kPartThreads, 4) k_forces(FSL_KARGS, int which
   if ((ig & ~3) >= P.np) return;  // uniform per warp (4 particles per warp)
   const bool active = ig < P.np;  // inactive lanes still join the shuffles
   const int np = P.np;
+  if (P.verlet || P.nolist) return;  // k_forces_vl
   // first-order scheme: forces at q^{n+1/2} only with extraMobility
   // (src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:170-180)
   if (which == 1 && P.scheme == 1 && !P.has_extra) return;
@@ -387,9 +390,124 @@ __global__ void __launch_bounds__(kPartThreads, 4) k_forces(FSL_KARGS, int which
   R.F[2 * np + i] = fz;
 }
 
+// ------------------------------------------------------------ Verlet list ---
+// Soft repulsion has an explicit cutoff, so its pair forces can come from a
+// list of the pairs within rc + skin at reference positions qref: every pair
+// within rc at positions that moved at most skin / 2 from qref is on it.
+// The list is rebuilt from a cell list of the current positions (the cells
+// are at least rc wide, so the pairs within rc + skin <= 2 rc lie within two
+// cells) when the update kernels have flagged a particle that moved further,
+// after positions were set from the host, and at the first evaluation.
+// Neighbours are stored in the cell order of the scan (deterministic).
+template <bool ONE>
+__global__ void k_vl_build(FSL_KARGS, int which) {
+  FSL_REP_FLAT(KIND_T1);
+  const int i = blk * blockDim.x + threadIdx.x;
+  const int np = P.np;
+  if (i >= np || !P.verlet || !list_needed(R, which)) return;
+  const CellList cl = cell_list(R, which);
+  const double* __restrict__ q = which ? R.qp : R.q;
+  const double xi = q[i], yi = q[np + i], zi = q[2 * np + i];
+  const double wx = minimage(xi, P.invlx, P.lx), wy = minimage(yi, P.invly, P.ly),
+               wz = minimage(zi, P.invlz, P.lz);
+  const int cx = cellidx(wx, P.invdnx, P.mnx), cy = cellidx(wy, P.invdny, P.mny),
+            cz = cellidx(wz, P.invdnz, P.mnz);
+  // per direction the cells within two of the particle's, each once
+  const int nx = min(P.mnx, 5), ny = min(P.mny, 5), nz = min(P.mnz, 5);
+  const int bx = P.mnx <= 5 ? 0 : cx - 2, by = P.mny <= 5 ? 0 : cy - 2, bz = P.mnz <= 5 ? 0 : cz - 2;
+  int n = 0;
+  bool over = false;
+  for (int oz = 0; oz < nz; ++oz) {
+    const int z = wrap_add(bz, oz, P.mnz);
+    for (int oy = 0; oy < ny; ++oy) {
+      const int y = wrap_add(by, oy, P.mny);
+      for (int ox = 0; ox < nx; ++ox) {
+        const int c = wrap_add(bx, ox, P.mnx) + P.mnx * (y + P.mny * z);
+        for (int e = cl.start[c]; e < cl.start[c + 1]; ++e) {
+          const int j = cl.sorted[e];
+          if (j == i) continue;
+          const double rx = minimage(xi - q[j], P.invlx, P.lx);
+          const double ry = minimage(yi - q[np + j], P.invly, P.ly);
+          const double rz = minimage(zi - q[2 * np + j], P.invlz, P.lz);
+          if (rx * rx + ry * ry + rz * rz >= P.vl_cut2) continue;
+          if (n < kVlCap) R.vl_idx[(size_t)n * np + i] = j;
+          else over = true;
+          ++n;
+        }
+      }
+    }
+  }
+  R.vl_cnt[i] = min(n, kVlCap);
+  R.qref[i] = xi;
+  R.qref[np + i] = yi;
+  R.qref[2 * np + i] = zi;
+  if (over) set_err(R.err, 8);
+}
+
+// Pair forces from the Verlet list (soft repulsion with the cutoff test and
+// arithmetic of k_forces, on the minimum image of the unwrapped positions as
+// the reference takes it) plus the bonded forces; one thread per particle.
+// Also the force kernel of instances without pair forces (bonds only).
+template <bool ONE>
+__global__ void k_forces_vl(FSL_KARGS, int which) {
+  FSL_REP_FLAT(KIND_T1);
+  const int i = blk * blockDim.x + threadIdx.x;
+  const int np = P.np;
+  if (!(P.verlet || P.nolist)) return;
+  if (blk == 0 && threadIdx.x == 0 && R.vl_flag) R.vl_flag[2] = 0;  // rebuilt by now
+  if (i >= np) return;
+  // first-order scheme: forces at q^{n+1/2} only with extraMobility
+  // (src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:170-180)
+  if (which == 1 && P.scheme == 1 && !P.has_extra) return;
+  const double* __restrict__ q = which ? R.qp : R.q;
+  const double rx = q[i], ry = q[np + i], rz = q[2 * np + i];
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  if (P.bonded) {
+    int nb = R.bpp_cnt[i], off = R.bpp_off[i];
+    for (int j = 0; j < nb; ++j) {
+      const int idx = R.bpp_idx[off + j];
+      bond_force(rx, ry, rz, q[idx], q[np + idx], q[2 * np + idx], R.bpp_k[off + j], R.bpp_r0[off + j],
+                 fx, fy, fz);
+    }
+    nb = R.bfp_cnt[i];
+    off = R.bfp_off[i];
+    for (int j = 0; j < nb; ++j) {
+      const double* p = R.bfp_xyz + 3 * (off + j);
+      bond_force(rx, ry, rz, p[0], p[1], p[2], R.bfp_k[off + j], R.bfp_r0[off + j], fx, fy, fz);
+    }
+  }
+  if (P.verlet) {
+    const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
+    const int n = R.vl_cnt[i];
+    for (int k = 0; k < n; ++k) {
+      const int j = R.vl_idx[(size_t)k * np + i];
+      const double rxij = minimage(rx - q[j], P.invlx, P.lx);
+      const double ryij = minimage(ry - q[np + j], P.invly, P.ly);
+      const double rzij = minimage(rz - q[2 * np + j], P.invlz, P.lz);
+      const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rxij, rxij), __dmul_rn(ryij, ryij)),
+                                  __dmul_rn(rzij, rzij));
+      if (r2 >= P.cutoff2 || r2 == 0.0) continue;
+      const double f = c1 * (rsqrt(r2) - c2);
+      fx += f * rxij;
+      fy += f * ryij;
+      fz += f * rzij;
+    }
+  }
+  if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) set_err(R.err, 2);
+  R.F[i] = fx;
+  R.F[np + i] = fy;
+  R.F[2 * np + i] = fz;
+}
+
 void launch_forces(const Batch& B, int which, cudaStream_t s) {
   if (B.max_np == 0) return;
-  FSL_GO(k_forces, part_blocks(B, KIND_T8), kPartThreads, 0, s, B, which);
+  if (B.has_cl) FSL_GO(k_forces, part_blocks(B, KIND_T8), kPartThreads, 0, s, B, which);
+  if (B.has_vl) FSL_GO(k_forces_vl, part_blocks(B, KIND_T1), kPartThreads, 0, s, B, which);
+}
+
+void launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
+  launch_cells(B, which, s, false);
+  if (B.max_np > 0 && B.has_vl) FSL_GO(k_vl_build, part_blocks(B, KIND_T1), kPartThreads, 0, s, B, which);
 }
 
 // ------------------------------------------------------------ quad layout ---
@@ -587,7 +705,9 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
   const int np = P.np;
   if (!quad_of(blk, np, e, a, qb)) return;
   const bool on = e < np;  // lanes past the end join the shuffles only
-  const int i = on ? (ordered ? cell_list(R, drift == 1).sorted[e] : (int)e) : 0;
+  // cell order on the cell-list path (a list the step has just built)
+  const bool by_cell = ordered && !P.verlet && !P.nolist;
+  const int i = on ? (by_cell ? cell_list(R, drift == 1).sorted[e] : (int)e) : 0;
   bool sat = false;
   QuadStencil<KN> S;
   {
@@ -911,6 +1031,7 @@ void tile_init() {
 
 bool tile_eligible(const Params& P) {
   if (P.prec != PREC_FIXED || P.scheme > 1) return false;  // 3-D Stokes schemes
+  if (P.verlet || P.nolist) return false;  // needs both cell lists of every step
   // the drift's displacement (delta/2 |W| <= 0.003 for FP32 normals) must
   // stay well inside the candidates' spare 0.05 cells
   if (std::min(P.dx, std::min(P.dy, P.dz)) < 0.1) return false;
@@ -964,8 +1085,7 @@ __global__ void k_interp_update(FSL_KARGS, int stage) {
   quad_stencil<KN>(P, pos, pos, a, qb, S);
   float us[3];
   quad_interp<KN>(P, S, a, R.v, us);
-  if (!on || a >= 3) return;
-  const int comp = a;
+  const int comp = a < 3 ? a : 0;
   const double u = (double)(comp == 0 ? us[0] : (comp == 1 ? us[1] : us[2]));
   size_t k = (size_t)comp * np + i;
   double h = stage == 1 ? 0.5 * P.dt : P.dt;
@@ -976,6 +1096,17 @@ __global__ void k_interp_update(FSL_KARGS, int stage) {
     if (stage == 2) xi += (double)R.noise[nb + (size_t)3 * np];
     r += h * P.extra_mob * R.F[k] + P.fact2 * xi;
   }
+  if (P.verlet) {
+    // the Verlet list must be rebuilt before the next force evaluation
+    // (at q^{n+1/2} in this step, or at q of the next) once a particle has
+    // moved more than skin / 2 from its reference position
+    const double d = a < 3 ? r - R.qref[k] : 0.0;
+    double d2 = d * d;
+    d2 += __shfl_xor_sync(0xffffffffu, d2, 1);
+    d2 += __shfl_xor_sync(0xffffffffu, d2, 2);
+    if (on && a == 0 && d2 > P.vl_half2) R.vl_flag[stage == 1 ? 1 : 0] = *R.t + stage;
+  }
+  if (!on || a >= 3) return;
   if (!isfinite(r)) set_err(R.err, 2);
   qout[k] = r;
 }
