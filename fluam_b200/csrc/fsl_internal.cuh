@@ -453,6 +453,17 @@ __device__ __forceinline__ bool list_needed(const Rep& R, int which) {
   return f != 0 || R.vl_flag[which] == *R.t + 1;
 }
 
+// The quad of this thread in a KIND_T4 launch: particle index e (in the
+// instance), lane a in the quad, first lane qb of the quad; returns false
+// when the whole warp is past the last particle (uniform per warp).
+__device__ __forceinline__ bool quad_of(int blk, int np, long& e, int& a, int& qb) {
+  const long t = blk * (long)blockDim.x + threadIdx.x;
+  e = t >> 2;
+  a = threadIdx.x & 3;
+  qb = (threadIdx.x & 31) & ~3;
+  return ((t & ~31L) >> 2) < np;
+}
+
 // Launch kinds of the particle kernels (256-thread blocks): threads per
 // particle 1 (cell list), 8 (forces), 32 (one warp per particle), 4 (one
 // quad per particle: spreading and interpolation).
@@ -597,6 +608,8 @@ void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStre
 // The cell list of force evaluation `which` and, for Verlet-list
 // instances, the pair list (each only where list_needed says so).
 void launch_pair_lists(const Batch& B, int which, cudaStream_t s);
+// The condition h of a graph IF node: 1 if launch_pair_lists(which) has work.
+void launch_lists_gate(const Batch& B, int which, cudaGraphConditionalHandle h, cudaStream_t s);
 // FP64 observables of every instance with P.observe (end of a step)
 void launch_observe(const Batch& B, cudaStream_t s);
 // The FP64 form (fsl_fp64.cu); the launchers above hand a class of that

@@ -446,40 +446,45 @@ __global__ void k_vl_build(FSL_KARGS, int which) {
 
 // Pair forces from the Verlet list (soft repulsion with the cutoff test and
 // arithmetic of k_forces, on the minimum image of the unwrapped positions as
-// the reference takes it) plus the bonded forces; one thread per particle.
-// Also the force kernel of instances without pair forces (bonds only).
+// the reference takes it) plus the bonded forces; one quad per particle, lane
+// a taking list entries and bonds a, a + 4, ..., the partial forces summed
+// in a fixed butterfly order.  Also the force kernel of instances without
+// pair forces (bonds only).
 template <bool ONE>
 __global__ void k_forces_vl(FSL_KARGS, int which) {
-  FSL_REP_FLAT(KIND_T1);
-  const int i = blk * blockDim.x + threadIdx.x;
+  FSL_REP_FLAT(KIND_T4);
+  long e;
+  int a, qb;
   const int np = P.np;
   if (!(P.verlet || P.nolist)) return;
   if (blk == 0 && threadIdx.x == 0 && R.vl_flag) R.vl_flag[2] = 0;  // rebuilt by now
-  if (i >= np) return;
+  if (!quad_of(blk, np, e, a, qb)) return;
   // first-order scheme: forces at q^{n+1/2} only with extraMobility
   // (src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:170-180)
   if (which == 1 && P.scheme == 1 && !P.has_extra) return;
+  const bool on = e < np;
+  const int i = on ? (int)e : 0;
   const double* __restrict__ q = which ? R.qp : R.q;
   const double rx = q[i], ry = q[np + i], rz = q[2 * np + i];
   double fx = 0.0, fy = 0.0, fz = 0.0;
-  if (P.bonded) {
+  if (P.bonded && on) {
     int nb = R.bpp_cnt[i], off = R.bpp_off[i];
-    for (int j = 0; j < nb; ++j) {
+    for (int j = a; j < nb; j += 4) {
       const int idx = R.bpp_idx[off + j];
       bond_force(rx, ry, rz, q[idx], q[np + idx], q[2 * np + idx], R.bpp_k[off + j], R.bpp_r0[off + j],
                  fx, fy, fz);
     }
     nb = R.bfp_cnt[i];
     off = R.bfp_off[i];
-    for (int j = 0; j < nb; ++j) {
+    for (int j = a; j < nb; j += 4) {
       const double* p = R.bfp_xyz + 3 * (off + j);
       bond_force(rx, ry, rz, p[0], p[1], p[2], R.bfp_k[off + j], R.bfp_r0[off + j], fx, fy, fz);
     }
   }
-  if (P.verlet) {
+  if (P.verlet && on) {
     const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
     const int n = R.vl_cnt[i];
-    for (int k = 0; k < n; ++k) {
+    for (int k = a; k < n; k += 4) {
       const int j = R.vl_idx[(size_t)k * np + i];
       const double rxij = minimage(rx - q[j], P.invlx, P.lx);
       const double ryij = minimage(ry - q[np + j], P.invly, P.ly);
@@ -493,6 +498,13 @@ __global__ void k_forces_vl(FSL_KARGS, int which) {
       fz += f * rzij;
     }
   }
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (!on || a != 0) return;
   if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) set_err(R.err, 2);
   R.F[i] = fx;
   R.F[np + i] = fy;
@@ -502,7 +514,26 @@ __global__ void k_forces_vl(FSL_KARGS, int which) {
 void launch_forces(const Batch& B, int which, cudaStream_t s) {
   if (B.max_np == 0) return;
   if (B.has_cl) FSL_GO(k_forces, part_blocks(B, KIND_T8), kPartThreads, 0, s, B, which);
-  if (B.has_vl) FSL_GO(k_forces_vl, part_blocks(B, KIND_T1), kPartThreads, 0, s, B, which);
+  if (B.has_vl) FSL_GO(k_forces_vl, part_blocks(B, KIND_T4), kPartThreads, 0, s, B, which);
+}
+
+// Sets the condition of the graph's IF node around the list kernels of
+// force evaluation `which`: whether any instance of the class needs them.
+template <bool ONE>
+__global__ void k_lists_gate(const RepSrc src, const __grid_constant__ Rep one, int which,
+                             cudaGraphConditionalHandle h) {
+  int need = 0;
+  const int n = ONE ? 1 : src.nrep;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const Rep& R = ONE ? one : src.reps[r];
+    if (R.active && R.P.np > 0 && list_needed(R, which)) need = 1;
+  }
+  need = __syncthreads_or(need);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, need ? 1u : 0u);
+}
+
+void launch_lists_gate(const Batch& B, int which, cudaGraphConditionalHandle h, cudaStream_t s) {
+  FSL_GO(k_lists_gate, 1, 256, 0, s, B, which, h);
 }
 
 void launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
@@ -627,16 +658,6 @@ __device__ __forceinline__ void quad_interp(const Params& P, const QuadStencil<K
   }
 }
 
-// The quad of this thread in a KIND_T4 launch: particle index e (in the
-// instance), lane a in the quad, first lane qb of the quad; returns false
-// when the whole warp is past the last particle (uniform per warp).
-__device__ __forceinline__ bool quad_of(int blk, int np, long& e, int& a, int& qb) {
-  const long t = blk * (long)blockDim.x + threadIdx.x;
-  e = t >> 2;
-  a = threadIdx.x & 3;
-  qb = (threadIdx.x & 31) & ~3;
-  return ((t & ~31L) >> 2) < np;
-}
 
 // The RFD drift of particle i by its quad: (kT/delta) sign W_p spread from
 // q + sign (delta/2) W_p for both signs through add(stencil, values).  In
