@@ -558,7 +558,6 @@ int group_init(Group& g, const Params& P0) {
   FSL_TRY(cudaStreamCreateWithPriority(&g.side, cudaStreamNonBlocking, lo));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
-  FSL_TRY(cudaStreamCreateWithFlags(&g.cond, cudaStreamNonBlocking));
   tile_init();
   return FSL_OK;
 }
@@ -568,8 +567,6 @@ void group_destroy(Group& g) {
     cudaStreamSynchronize(g.side);
     cudaStreamDestroy(g.side);
   }
-  if (g.cond) cudaStreamDestroy(g.cond);
-  g.cond = nullptr;
   if (g.ev_fork) cudaEventDestroy(g.ev_fork);
   if (g.ev_join) cudaEventDestroy(g.ev_join);
   g.side = nullptr;
@@ -660,43 +657,6 @@ int group_upload(Group& g) {
 
 // One midpoint step (src/runSchemeStokesLimit.cu:163-275) of every active
 // instance of the group.
-bool capturing(cudaStream_t s) {
-  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-  return cudaStreamIsCapturing(s, &st) == cudaSuccess && st == cudaStreamCaptureStatusActive;
-}
-
-// Gate kernel on s, then an IF node whose body (captured on g.cond) holds
-// the list kernels of evaluation `which`; the capture of s continues after
-// the node.
-int enqueue_gated_lists(Group& g, int which, cudaStream_t s) {
-  cudaStreamCaptureStatus st;
-  cudaGraph_t graph = nullptr;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t ndeps = 0;
-  FSL_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &graph, &deps, &ndeps));
-  cudaGraphConditionalHandle h;
-  FSL_TRY(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
-  launch_lists_gate(g.B, which, h, s);
-  FSL_TRY(cudaGetLastError());
-  FSL_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &graph, &deps, &ndeps));
-  cudaGraphNodeParams np{};
-  np.type = cudaGraphNodeTypeConditional;
-  np.conditional.handle = h;
-  np.conditional.type = cudaGraphCondTypeIf;
-  np.conditional.size = 1;
-  cudaGraphNode_t node;
-  FSL_TRY(cudaGraphAddNode(&node, graph, deps, ndeps, &np));
-  cudaGraph_t body = np.conditional.phGraph_out[0];
-  FSL_TRY(cudaStreamBeginCaptureToGraph(g.cond, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  launch_pair_lists(g.B, which, g.cond);
-  cudaError_t le = cudaGetLastError();
-  cudaGraph_t out = nullptr;
-  FSL_TRY(cudaStreamEndCapture(g.cond, &out));
-  FSL_TRY(le);
-  FSL_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
-  return FSL_OK;
-}
-
 void group_enqueue_step(Group& g) {
   const Batch& B = g.B;
   cudaStream_t s = g.stream;
@@ -714,16 +674,10 @@ void group_enqueue_step(Group& g) {
   };
   auto cells_forces = [&](int which) {
     pr.mark(s, "cells");
-    if (B.has_vl && B.max_np > 0 && capturing(s) && g.cond) {
-      // captured steps: the list kernels sit in a conditional node that a
-      // gate kernel switches on only when some instance needs new lists
-      // (counted: the gate; the body runs on the steps that rebuild)
-      if (enqueue_gated_lists(g, which, s) != FSL_OK && !g.fail_stage) g.fail_stage = "cells (graph)";
-      pr.count(1);
-    } else {
-      launch_pair_lists(B, which, s);
-      pr.count(pk ? 5 + (B.has_vl ? 1 : 0) : 0);
-    }
+    // (on the Verlet path the list kernels return at once unless a rebuild
+    // is due)
+    launch_pair_lists(B, which, s);
+    pr.count(pk ? 5 + (B.has_vl ? 1 : 0) : 0);
     chk("cells");
     pr.mark(s, "forces");
     launch_forces(B, which, s);

@@ -608,8 +608,6 @@ void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStre
 // The cell list of force evaluation `which` and, for Verlet-list
 // instances, the pair list (each only where list_needed says so).
 void launch_pair_lists(const Batch& B, int which, cudaStream_t s);
-// The condition h of a graph IF node: 1 if launch_pair_lists(which) has work.
-void launch_lists_gate(const Batch& B, int which, cudaGraphConditionalHandle h, cudaStream_t s);
 // FP64 observables of every instance with P.observe (end of a step)
 void launch_observe(const Batch& B, cudaStream_t s);
 // The FP64 form (fsl_fp64.cu); the launchers above hand a class of that

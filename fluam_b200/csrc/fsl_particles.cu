@@ -517,25 +517,6 @@ void launch_forces(const Batch& B, int which, cudaStream_t s) {
   if (B.has_vl) FSL_GO(k_forces_vl, part_blocks(B, KIND_T4), kPartThreads, 0, s, B, which);
 }
 
-// Sets the condition of the graph's IF node around the list kernels of
-// force evaluation `which`: whether any instance of the class needs them.
-template <bool ONE>
-__global__ void k_lists_gate(const RepSrc src, const __grid_constant__ Rep one, int which,
-                             cudaGraphConditionalHandle h) {
-  int need = 0;
-  const int n = ONE ? 1 : src.nrep;
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
-    const Rep& R = ONE ? one : src.reps[r];
-    if (R.active && R.P.np > 0 && list_needed(R, which)) need = 1;
-  }
-  need = __syncthreads_or(need);
-  if (threadIdx.x == 0) cudaGraphSetConditional(h, need ? 1u : 0u);
-}
-
-void launch_lists_gate(const Batch& B, int which, cudaGraphConditionalHandle h, cudaStream_t s) {
-  FSL_GO(k_lists_gate, 1, 256, 0, s, B, which, h);
-}
-
 void launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
   launch_cells(B, which, s, false);
   if (B.max_np > 0 && B.has_vl) FSL_GO(k_vl_build, part_blocks(B, KIND_T1), kPartThreads, 0, s, B, which);
