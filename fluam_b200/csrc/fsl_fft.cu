@@ -282,7 +282,7 @@ constexpr int kFftThreads = 512;
 // field is cleared behind the read, ready for the next spread.  One thread
 // per cell: the loads of a warp are coalesced rows, full occupancy.
 template <bool ONE>
-__global__ void k_wbuild(FSL_KARGS, int nsets, double nfac, int clear) {
+__global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
   FSL_REP_AT(blockIdx.y);
   const float scale = (float)(kFixedInv / P.dV);
   const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
@@ -304,11 +304,11 @@ __global__ void k_wbuild(FSL_KARGS, int nsets, double nfac, int clear) {
       float w;
       if (fatom) {
         w = gf[comp * nc + i] * fscale;
-        if (clear) gf[comp * nc + i] = 0.0f;
+        gf[comp * nc + i] = 0.0f;
       } else {
         long long g = (long long)R.grid[comp * nc + i];
         w = (float)((double)g * (double)scale);
-        if (clear) R.grid[comp * nc + i] = 0ull;
+        R.grid[comp * nc + i] = 0ull;
       }
       w += stress_div(P, n1, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
       if (nsets > 1) w += stress_div(P, n2, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
@@ -320,7 +320,7 @@ __global__ void k_wbuild(FSL_KARGS, int nsets, double nfac, int clear) {
 // k_wbuild for mx a multiple of 4: one thread per four x cells, 16-byte loads
 // of the fixed-point field, the noise rows and W, and 16-byte clears.
 template <bool ONE>
-__global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac, int clear) {
+__global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
   FSL_REP_AT(blockIdx.y);
   const float scale = (float)(kFixedInv / P.dV);
   const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
@@ -352,7 +352,7 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac, int clear) {
         w[comp][1] = ga.y * fscale;
         w[comp][2] = ga.z * fscale;
         w[comp][3] = ga.w * fscale;
-        if (clear) *fp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        *fp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         continue;
       }
       const longlong2* gp = reinterpret_cast<const longlong2*>(R.grid + comp * nc + i0);
@@ -368,7 +368,7 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac, int clear) {
     for (int comp = 0; comp < 3; ++comp) {
       *reinterpret_cast<float4*>(R.wbuf + comp * nc + i0) =
           make_float4(w[comp][0], w[comp][1], w[comp][2], w[comp][3]);
-      if (fatom || !clear) continue;  // cleared at the read, or by k_zero_grid
+      if (fatom) continue;  // cleared at the read
       longlong2* gq = reinterpret_cast<longlong2*>(R.grid + comp * nc + i0);
       gq[0] = make_longlong2(0, 0);
       gq[1] = make_longlong2(0, 0);
@@ -942,53 +942,28 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
 }
 
-void launch_wbuild(const Batch& B, int nsets, double nfac, int clear, cudaStream_t s, Prof* prof) {
-  Prof dummy;
-  Prof& pr = prof ? *prof : dummy;
-  const int nrep = B.nrep;
-  pr.mark(s, "wbuild");
-  int tb = 256;
-  long blocks = ((long)B.nc + tb - 1) / tb;
-  long cap = (148L * 64 + nrep - 1) / nrep;
-  if (blocks > cap) blocks = cap < 1 ? 1 : cap;
-  if ((B.mx & 3) == 0) {
-    long b4 = ((long)B.nc / 4 + tb - 1) / tb;
-    if (b4 > cap) b4 = cap < 1 ? 1 : cap;
-    FSL_GO(k_wbuild4, dim3((unsigned)b4, nrep), tb, 0, s, B, nsets, nfac, clear);
-  } else {
-    FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets, nfac, clear);
-  }
-  pr.count(1);
-}
-
-// The spread field of every instance set to zero (16-byte stores).
-template <bool ONE>
-__global__ void k_zero_grid(FSL_KARGS) {
-  FSL_REP_AT(blockIdx.y);
-  longlong2* g = reinterpret_cast<longlong2*>(R.grid);
-  const size_t n = (size_t)3 * P.nc / 2;  // pairs of the 3 nc 8-byte entries
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-    g[k] = make_longlong2(0, 0);
-  if (((size_t)3 * P.nc) & 1) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) R.grid[(size_t)3 * P.nc - 1] = 0ull;
-  }
-}
-
-void launch_zero_grid(const Batch& B, cudaStream_t s) {
-  const int tb = 256;
-  long blocks = ((long)3 * B.nc / 2 + tb - 1) / tb;
-  const long cap = (148L * 16 + B.nrep - 1) / B.nrep;
-  if (blocks > cap) blocks = cap < 1 ? 1 : cap;
-  FSL_GO(k_zero_grid, dim3((unsigned)blocks, B.nrep), tb, 0, s, B);
-}
-
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof) {
   if (B.prec == PREC_F64) return launch_solve64(B, nsets, nfac, s, prof);
   Prof dummy;
   Prof& pr = prof ? *prof : dummy;
   const int nrep = B.nrep;
-  if (!w_given) launch_wbuild(B, nsets, nfac, 1, s, &pr);
+  if (!w_given) {
+    // W from the spread field and the noise; clears the spread field
+    pr.mark(s, "wbuild");
+    int tb = 256;
+    long blocks = ((long)B.nc + tb - 1) / tb;
+    long cap = (148L * 64 + nrep - 1) / nrep;
+    if (blocks > cap) blocks = cap < 1 ? 1 : cap;
+    if ((B.mx & 3) == 0) {
+      long b4 = ((long)B.nc / 4 + tb - 1) / tb;
+      if (b4 > cap) b4 = cap < 1 ? 1 : cap;
+      FSL_GO(k_wbuild4, dim3((unsigned)b4, nrep), tb, 0, s, B, nsets, nfac);
+    } else {
+      FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets, nfac);
+    }
+    pr.count(1);
+  }
   if (fp->plane_fwd_r[0]) {
     dim3 gp((3 * B.mz + fp->plane_pb - 1) / fp->plane_pb, 1, nrep);
     const int tb = fp->plane_threads;

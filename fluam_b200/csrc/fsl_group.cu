@@ -558,8 +558,6 @@ int group_init(Group& g, const Params& P0) {
   FSL_TRY(cudaStreamCreateWithPriority(&g.side, cudaStreamNonBlocking, lo));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
-  FSL_TRY(cudaEventCreateWithFlags(&g.ev_cfork, cudaEventDisableTiming));
-  FSL_TRY(cudaEventCreateWithFlags(&g.ev_cjoin, cudaEventDisableTiming));
   tile_init();
   return FSL_OK;
 }
@@ -569,9 +567,6 @@ void group_destroy(Group& g) {
     cudaStreamSynchronize(g.side);
     cudaStreamDestroy(g.side);
   }
-  if (g.ev_cfork) cudaEventDestroy(g.ev_cfork);
-  if (g.ev_cjoin) cudaEventDestroy(g.ev_cjoin);
-  g.ev_cfork = g.ev_cjoin = nullptr;
   if (g.ev_fork) cudaEventDestroy(g.ev_fork);
   if (g.ev_join) cudaEventDestroy(g.ev_join);
   g.side = nullptr;
@@ -710,29 +705,6 @@ void group_enqueue_step(Group& g) {
   auto join_noise = [&]() {
     if (fork) cudaStreamWaitEvent(s, g.ev_join, 0);
   };
-  // W build, then the transforms and the Stokes solve.  On the FP32 forms
-  // the W build leaves the spread field as it is and a zeroing kernel on the
-  // side stream clears it while the transforms run; it is joined before the
-  // next spread and at the end of the step.
-  bool clear_pending = false;
-  auto solve = [&](int nsets, double nfac) {
-    if (B.tiled || B.prec == PREC_F64 || !fork) {
-      launch_solve(B, g.fft, nsets, nfac, B.tiled, s, &pr);
-      return;
-    }
-    launch_wbuild(B, nsets, nfac, 0, s, &pr);
-    cudaEventRecord(g.ev_cfork, s);
-    cudaStreamWaitEvent(g.side, g.ev_cfork, 0);
-    launch_zero_grid(B, g.side);
-    cudaEventRecord(g.ev_cjoin, g.side);
-    clear_pending = true;
-    pr.count(1);
-    launch_solve(B, g.fft, nsets, nfac, 1, s, &pr);
-  };
-  auto join_clear = [&]() {
-    if (clear_pending) cudaStreamWaitEvent(s, g.ev_cjoin, 0);
-    clear_pending = false;
-  };
   auto observe = [&]() {
     if (!g.key.observe) return;
     pr.mark(s, "observe");
@@ -813,7 +785,7 @@ void group_enqueue_step(Group& g) {
       chk("spread_rfd");
       pr.count(pk);
     }
-    solve(1, 1.0);
+    launch_solve(B, g.fft, 1, 1.0, B.tiled, s, &pr);
     chk("solve");
     pr.mark(s, "interp_update");
     launch_interp_update(B, 1, s);
@@ -824,7 +796,6 @@ void group_enqueue_step(Group& g) {
     launch_interp_update(B, 2, s);
     chk("interp_update");
     pr.count(pk);
-    join_clear();
     observe();
     pr.mark(s, "counter");
     launch_step_counter(B, s);
@@ -851,7 +822,7 @@ void group_enqueue_step(Group& g) {
     pr.count(pk);
     join_noise();
   }
-  solve(1, 1.41421356237309504880);
+  launch_solve(B, g.fft, 1, 1.41421356237309504880, B.tiled, s, &pr);
   chk("solve");
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
   // sqrt(1/2) (stress 1 + stress 2)
@@ -866,20 +837,18 @@ void group_enqueue_step(Group& g) {
     chk("spread_w_rfd");
     pr.count(1);
   } else {
-    join_clear();
     pr.mark(s, "spread_rfd");
     launch_spread(B, 1, 1, s);
     chk("spread_rfd");
     pr.count(pk);
   }
-  solve(2, 0.70710678118654752440);
+  launch_solve(B, g.fft, 2, 0.70710678118654752440, B.tiled, s, &pr);
   chk("solve");
   // option 2: corrector
   pr.mark(s, "interp_update");
   launch_interp_update(B, 2, s);
   chk("interp_update");
   pr.count(pk);
-  join_clear();
   observe();
   pr.mark(s, "counter");
   launch_step_counter(B, s);

@@ -97,8 +97,6 @@ struct Group {
   // (fork and join events); profiled steps keep everything on `stream`
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  // the clearing of the spread field on the side stream (fork and join)
-  cudaEvent_t ev_cfork = nullptr, ev_cjoin = nullptr;
   Prof prof;
   std::map<std::string, std::pair<int64_t, double>> stage_acc;
   int launches = 0;             // kernels of this group in one step

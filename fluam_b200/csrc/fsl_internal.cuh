@@ -638,11 +638,6 @@ void fft_plan_destroy(FftPlan* fp);
 // v = solve(W).  W = f + nfac div(stress 1 [+ stress 2 when nsets == 2]) is
 // built from the spread field (which is cleared on the way) and the noise
 // into Rep::wbuf, unless w_given, in which case Rep::wbuf already holds W.
-// W from the spread field and the noise (FP32 forms); clear: also set the
-// spread field back to zero (else launch_zero_grid must, before the next
-// spread).
-void launch_wbuild(const Batch& B, int nsets, double nfac, int clear, cudaStream_t s, Prof* prof);
-void launch_zero_grid(const Batch& B, cudaStream_t s);
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof = nullptr);
 }  // namespace fsl
