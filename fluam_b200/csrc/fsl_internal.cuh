@@ -420,7 +420,10 @@ struct Rep {
   // Verlet list: per particle count and kVlCap neighbour slots ([slot][np]),
   // reference positions, and the rebuild word vl_flag: [0], [1] the step
   // (counter + 1) at whose force evaluation at q (0) or q^{n+1/2} (1) the
-  // list must be rebuilt, [2] nonzero: rebuild at the next evaluation
+  // list must be rebuilt; [2] 1: rebuild at the next evaluation, 2: cell
+  // list requested by an entry point, 3: cell mode (a particle had more
+  // than kVlCap neighbours: the pair forces come from the cell list of every
+  // evaluation until the positions are set again)
   int* vl_cnt;
   int* vl_idx;
   double* qref;
@@ -450,6 +453,7 @@ __device__ __forceinline__ bool list_needed(const Rep& R, int which) {
   const uint64_t f = R.vl_flag[2];  // 2: requested by a component entry point
   if (f == 2) return true;
   if (R.P.nolist) return false;
+  // 3: cell mode (the list overflowed): a cell list at every evaluation
   return f != 0 || R.vl_flag[which] == *R.t + 1;
 }
 

@@ -404,7 +404,7 @@ __global__ void k_vl_build(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T1);
   const int i = blk * blockDim.x + threadIdx.x;
   const int np = P.np;
-  if (i >= np || !P.verlet || !list_needed(R, which)) return;
+  if (i >= np || !P.verlet || !list_needed(R, which) || R.vl_flag[2] == 3) return;
   const CellList cl = cell_list(R, which);
   const double* __restrict__ q = which ? R.qp : R.q;
   const double xi = q[i], yi = q[np + i], zi = q[2 * np + i];
@@ -441,7 +441,7 @@ __global__ void k_vl_build(FSL_KARGS, int which) {
   R.qref[i] = xi;
   R.qref[np + i] = yi;
   R.qref[2 * np + i] = zi;
-  if (over) set_err(R.err, 8);
+  if (over) R.vl_flag[2] = 3;  // cell mode from now on
 }
 
 // Pair forces from the Verlet list (soft repulsion with the cutoff test and
@@ -457,7 +457,9 @@ __global__ void k_forces_vl(FSL_KARGS, int which) {
   int a, qb;
   const int np = P.np;
   if (!(P.verlet || P.nolist)) return;
-  if (blk == 0 && threadIdx.x == 0 && R.vl_flag) R.vl_flag[2] = 0;  // rebuilt by now
+  const bool cell_mode = P.verlet && R.vl_flag[2] == 3;
+  __syncthreads();  // every thread has read the word before it is cleared
+  if (blk == 0 && threadIdx.x == 0 && R.vl_flag && !cell_mode) R.vl_flag[2] = 0;  // rebuilt by now
   if (!quad_of(blk, np, e, a, qb)) return;
   // first-order scheme: forces at q^{n+1/2} only with extraMobility
   // (src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:170-180)
@@ -481,7 +483,32 @@ __global__ void k_forces_vl(FSL_KARGS, int which) {
       bond_force(rx, ry, rz, p[0], p[1], p[2], R.bfp_k[off + j], R.bfp_r0[off + j], fx, fy, fz);
     }
   }
-  if (P.verlet && on) {
+  if (P.verlet && on && cell_mode) {
+    // the 27 neighbour cells of the current cell list, lanes taking cells
+    // a, a + 4, ...
+    const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
+    const CellList cl = cell_list(R, which);
+    const int cx = cellidx(minimage(rx, P.invlx, P.lx), P.invdnx, P.mnx),
+              cy = cellidx(minimage(ry, P.invly, P.ly), P.invdny, P.mny),
+              cz = cellidx(minimage(rz, P.invlz, P.lz), P.invdnz, P.mnz);
+    for (int nn = a; nn < 27; nn += 4) {
+      const int c = wrap_add(cx, nn % 3 - 1, P.mnx) +
+                    P.mnx * (wrap_add(cy, (nn / 3) % 3 - 1, P.mny) + P.mny * wrap_add(cz, nn / 9 - 1, P.mnz));
+      for (int e2 = cl.start[c]; e2 < cl.start[c + 1]; ++e2) {
+        const int j = cl.sorted[e2];
+        const double rxij = minimage(rx - q[j], P.invlx, P.lx);
+        const double ryij = minimage(ry - q[np + j], P.invly, P.ly);
+        const double rzij = minimage(rz - q[2 * np + j], P.invlz, P.lz);
+        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rxij, rxij), __dmul_rn(ryij, ryij)),
+                                    __dmul_rn(rzij, rzij));
+        if (j == i || r2 >= P.cutoff2 || r2 == 0.0) continue;
+        const double f = c1 * (rsqrt(r2) - c2);
+        fx += f * rxij;
+        fy += f * ryij;
+        fz += f * rzij;
+      }
+    }
+  } else if (P.verlet && on) {
     const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
     const int n = R.vl_cnt[i];
     for (int k = a; k < n; k += 4) {

@@ -72,9 +72,7 @@ enum { FSL_PRECISION_FIXED64 = 0, FSL_PRECISION_FLOAT_ATOMIC = 1, FSL_PRECISION_
 enum {
   FSL_ERRBIT_FIXED_SAT = 1,   /* fixed-point spread value out of range      */
   FSL_ERRBIT_NONFINITE = 2,   /* non-finite force or position               */
-  FSL_ERRBIT_GRID = 4,        /* internal index check failed (access skipped) */
-  FSL_ERRBIT_NEIGHBORS = 8    /* a particle has more than 64 neighbours within
-                                 cutoff + skin (Verlet list of soft repulsion) */
+  FSL_ERRBIT_GRID = 4         /* internal index check failed (access skipped) */
 };
 
 /* Configuration of one instance.  Field names follow data.main keywords

@@ -81,11 +81,19 @@ def test_verlet_after_set_positions_and_entry_points(fsl):
         np.testing.assert_allclose(b.positions(), a.positions(), rtol=0, atol=1e-12)
 
 
-def test_verlet_capacity_is_reported(fsl):
-    """More than 64 neighbours within rc + skin: the error word says so."""
-    rng = np.random.default_rng(1)
-    q = rng.uniform(-0.4, 0.4, (3, 100))
-    s = _make(fsl, q, True, kT=0.0, dt=1e-4)
-    with s:
-        s.step(1)
-        assert s.status()["error_bits"] & 8
+def test_verlet_overflow_falls_back_to_cells(fsl):
+    """More than 64 neighbours within rc + skin (a dense random box, as the
+    served workload draws): the instance switches to the cell-list pair
+    forces and follows the cell-list kernel."""
+    q = uniform_positions(4000, (10.0,) * 3, 2)
+    kw = dict(kT=0.01, dt=0.01, kernel=3, m=(16, 16, 16), L=10.0)
+    a, b = _pair(fsl, q, **kw)
+    with a, b:
+        for _ in range(3):
+            a.step(2)
+            b.step(2)
+            assert a.status()["error_bits"] == 0 and b.status()["error_bits"] == 0
+            qa = a.positions()
+            np.testing.assert_allclose(b.positions(), qa, rtol=0, atol=1e-12 * max(1.0, np.abs(qa).max()))
+            Fa = a.forces()
+            np.testing.assert_allclose(b.forces(), Fa, rtol=0, atol=1e-11 * max(1.0, np.abs(Fa).max()))
