@@ -750,7 +750,7 @@ static void pick_register_kernels(const Params& P, FftPlan* fp) {
     case 80: pick_z_r<80, 20, 4, 21, 1>(fp); break;
     case 88: pick_z_r<88, 8, 11, 9, 1>(fp); break;
     case 96: pick_z_r<96, 24, 4, 25, 1>(fp); break;
-    case 128: pick_z_r<128, 16, 8, 13, 1>(fp); break;
+    case 128: pick_z_r<128, 16, 8, 8, 2>(fp); break;
     case 256: pick_z_r<256, 16, 16, 8, 1>(fp); break;
     default: break;
   }
