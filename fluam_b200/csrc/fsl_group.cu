@@ -27,7 +27,7 @@ size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 struct SlotLayout {
   size_t q, qp, F, u, qw, ws, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
       bsum, ljtab, noise, grid, spec, v, wbuf, noise64, v64, z64, err, t, q0, obs, obs_part, obs_ticket,
-      start1, sorted1, ws1, vl_cnt, vl_idx, qref, vl_flag, total;
+      start1, sorted1, ws1, vl_cnt, vl_idx, qref, vl_flag, bar, total;
 };
 
 SlotLayout layout(const Params& P, int np_cap) {
@@ -57,7 +57,7 @@ SlotLayout layout(const Params& P, int np_cap) {
   L.cnt = take(sizeof(int) * mN);
   L.fill = take(sizeof(int) * mN);
   L.start = take(sizeof(int) * (mN + 1));
-  L.bsum = take(sizeof(int) * ((mN + 4095) / 4096 + 1));
+  L.bsum = take(sizeof(int) * std::max<size_t>((mN + 4095) / 4096 + 1, kCoopMaxBlocks + 1));
   L.ljtab = take(sizeof(float) * kLjTableSize);
   // the FP32 field buffers, or their FP64 counterparts (the spread field has
   // 8-byte entries in every form: fixed point, or FP64; the float-atomic
@@ -86,6 +86,7 @@ SlotLayout layout(const Params& P, int np_cap) {
   L.vl_idx = take(P.verlet ? sizeof(int) * (size_t)kVlCap * np : 0);
   L.qref = take(P.verlet ? sizeof(double) * 3 * np : 0);
   L.vl_flag = take(sizeof(uint64_t) * 3);
+  L.bar = take(sizeof(unsigned) * 2);
   L.total = off;
   return L;
 }
@@ -365,6 +366,7 @@ int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st) {
   r.vl_idx = P.verlet ? (int*)(base + L.vl_idx) : nullptr;
   r.qref = P.verlet ? (double*)(base + L.qref) : nullptr;
   r.vl_flag = (uint64_t*)(base + L.vl_flag);
+  r.bar = (unsigned*)(base + L.bar);  // zeroed with the slot
   return FSL_OK;
 }
 
@@ -674,10 +676,10 @@ void group_enqueue_step(Group& g) {
   };
   auto cells_forces = [&](int which) {
     pr.mark(s, "cells");
-    // (on the Verlet path the list kernels return at once unless a rebuild
-    // is due)
+    // (one cooperative launch for a single instance; on the Verlet path the
+    // list kernels return at once unless a rebuild is due)
     launch_pair_lists(B, which, s);
-    pr.count(pk ? 5 + (B.has_vl ? 1 : 0) : 0);
+    pr.count(!pk ? 0 : (B.one && B.one->bar) ? 1 : 5 + (B.has_vl ? 1 : 0));
     chk("cells");
     pr.mark(s, "forces");
     launch_forces(B, which, s);

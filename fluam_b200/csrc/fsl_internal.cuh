@@ -428,7 +428,10 @@ struct Rep {
   int* vl_idx;
   double* qref;
   uint64_t* vl_flag;
+  // grid barrier of the single-launch list build (count, generation)
+  unsigned* bar;
 };
+constexpr int kCoopMaxBlocks = 1024;
 constexpr int kVlCap = 64;
 constexpr int kObsVals = 10;      // msd, displacement[3], force[3], momentum[3]
 constexpr int kObsSlots = 16;     // steps, msd, msd_sum, disp[3], force[3], mom[3], mom_sum[3]

@@ -72,11 +72,10 @@ __global__ void k_zero_cells(FSL_KARGS) {
   if (P.np == 0 && blockIdx.x == 0 && threadIdx.x == 0) R.start[P.mN] = 0;
 }
 
-template <bool ONE>
-__global__ void k_cell_count(FSL_KARGS, int which) {
-  FSL_REP_FLAT(KIND_T1);
-  int i = blk * blockDim.x + threadIdx.x;
-  if (i >= P.np || !list_needed(R, which)) return;
+// one particle of each phase of the build (the kernels below, and the
+// cooperative single-launch build)
+__device__ __forceinline__ void cell_count_one(const Rep& R, int i, int which) {
+  const Params& P = R.P;
   const double* q = which ? R.qp : R.q;
   double x = q[i], y = q[P.np + i], z = q[2 * P.np + i];
   // a coordinate this large or non-finite means the run has blown up
@@ -93,6 +92,14 @@ __global__ void k_cell_count(FSL_KARGS, int which) {
     R.qw[2 * P.np + i] = wz;
   }
   atomicAdd(&R.cnt[c], 1);
+}
+
+template <bool ONE>
+__global__ void k_cell_count(FSL_KARGS, int which) {
+  FSL_REP_FLAT(KIND_T1);
+  int i = blk * blockDim.x + threadIdx.x;
+  if (i >= P.np || !list_needed(R, which)) return;
+  cell_count_one(R, i, which);
 }
 
 constexpr int kScanThreads = 1024;
@@ -182,23 +189,24 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(FSL_KARGS, int which)
   if (threadIdx.x == 0 && tile == (n + kScanTile - 1) / kScanTile - 1) start[n] = prefix + R.bsum[tile];
 }
 
-template <bool ONE>
-__global__ void k_cell_scatter(FSL_KARGS, int which) {
-  FSL_REP_FLAT(KIND_T1);
-  int i = blk * blockDim.x + threadIdx.x;
-  if (i >= P.np || !list_needed(R, which)) return;
+__device__ __forceinline__ void cell_scatter_one(const Rep& R, int i, int which) {
   const int* start = which && R.start1 ? R.start1 : R.start;
   int c = R.cell_of[i];
   R.tmp[start[c] + atomicAdd(&R.fill[c], 1)] = i;
 }
 
-// Rank of particle i among the particles of its cell = number of smaller
-// indices in the (unordered) bucket; gives the ascending order.
 template <bool ONE>
-__global__ void k_cell_rank(FSL_KARGS, int which) {
+__global__ void k_cell_scatter(FSL_KARGS, int which) {
   FSL_REP_FLAT(KIND_T1);
   int i = blk * blockDim.x + threadIdx.x;
   if (i >= P.np || !list_needed(R, which)) return;
+  cell_scatter_one(R, i, which);
+}
+
+// Rank of particle i among the particles of its cell = number of smaller
+// indices in the (unordered) bucket; gives the ascending order.
+__device__ __forceinline__ void cell_rank_one(const Rep& R, int i, int which) {
+  const Params& P = R.P;
   const bool second = which && R.start1;
   const int* start = second ? R.start1 : R.start;
   int* sorted = second ? R.sorted1 : R.sorted;
@@ -214,6 +222,14 @@ __global__ void k_cell_rank(FSL_KARGS, int which) {
     ws[P.np + s + rank] = R.qw[P.np + i];
     ws[2 * P.np + s + rank] = R.qw[2 * P.np + i];
   }
+}
+
+template <bool ONE>
+__global__ void k_cell_rank(FSL_KARGS, int which) {
+  FSL_REP_FLAT(KIND_T1);
+  int i = blk * blockDim.x + threadIdx.x;
+  if (i >= P.np || !list_needed(R, which)) return;
+  cell_rank_one(R, i, which);
 }
 
 void launch_cells(const Batch& B, int which, cudaStream_t s, bool zero_first) {
@@ -399,12 +415,9 @@ __global__ void __launch_bounds__(kPartThreads, 4) k_forces(FSL_KARGS, int which
 // cells) when the update kernels have flagged a particle that moved further,
 // after positions were set from the host, and at the first evaluation.
 // Neighbours are stored in the cell order of the scan (deterministic).
-template <bool ONE>
-__global__ void k_vl_build(FSL_KARGS, int which) {
-  FSL_REP_FLAT(KIND_T1);
-  const int i = blk * blockDim.x + threadIdx.x;
+__device__ void vl_build_one(const Rep& R, int i, int which) {
+  const Params& P = R.P;
   const int np = P.np;
-  if (i >= np || !P.verlet || !list_needed(R, which) || R.vl_flag[2] == 3) return;
   const CellList cl = cell_list(R, which);
   const double* __restrict__ q = which ? R.qp : R.q;
   const double xi = q[i], yi = q[np + i], zi = q[2 * np + i];
@@ -442,6 +455,106 @@ __global__ void k_vl_build(FSL_KARGS, int which) {
   R.qref[np + i] = yi;
   R.qref[2 * np + i] = zi;
   if (over) R.vl_flag[2] = 3;  // cell mode from now on
+}
+
+template <bool ONE>
+__global__ void k_vl_build(FSL_KARGS, int which) {
+  FSL_REP_FLAT(KIND_T1);
+  const int i = blk * blockDim.x + threadIdx.x;
+  if (i >= P.np || !P.verlet || !list_needed(R, which) || R.vl_flag[2] == 3) return;
+  vl_build_one(R, i, which);
+}
+
+// ----------------------------------------------- single-launch list build ---
+// The cell list (and the Verlet list) of one instance in one cooperative
+// launch: the phases of the kernels above separated by grid barriers, so a
+// force evaluation that needs no rebuild costs one near-empty launch instead
+// of six.  The barrier spins with a bound; if it ever gives up (the blocks
+// are co-resident by the cooperative launch, so it should not) the instance's
+// error word gets FSL_ERRBIT_GRID.
+constexpr int kCoopThreads = 256;
+
+__device__ void grid_barrier(const Rep& R) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = R.bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(R.bar, 1u) == gridDim.x - 1) {
+      R.bar[0] = 0u;
+      __threadfence();
+      atomicAdd(R.bar + 1, 1u);
+    } else {
+      long spins = 0;
+      while (*gen == g) {
+        if (++spins > 20000000L) {  // about seconds: give up, flag it
+          set_err(R.err, 4);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kCoopThreads) k_lists_coop(const __grid_constant__ Rep R, int which) {
+  const Params& P = R.P;
+  if (!R.active || P.np == 0 || !list_needed(R, which)) return;
+  const int np = P.np, nb = gridDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = nb * blockDim.x;
+  for (int i = tid; i < np; i += nth) cell_count_one(R, i, which);
+  grid_barrier(R);
+  // exclusive scan of the counts: block b takes a contiguous chunk, the
+  // block totals go through bsum, the counts are cleared behind the read
+  int* start = which && R.start1 ? R.start1 : R.start;
+  __shared__ int wsum[kCoopThreads / 32];
+  __shared__ int s_off;
+  const int n = P.mN, chunk = (n + nb - 1) / nb;
+  const int c0 = min(n, blockIdx.x * chunk), c1 = min(n, c0 + chunk);
+  const int per = (c1 - c0 + blockDim.x - 1) / blockDim.x;
+  const int t0 = min(c1, c0 + (int)threadIdx.x * per), t1 = min(c1, t0 + per);
+  int sum = 0;
+  for (int c = t0; c < t1; ++c) sum += R.cnt[c];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  int woff = 0, btot = 0;
+  for (int w = 0; w < kCoopThreads / 32; ++w) {
+    if (w < warp) woff += wsum[w];
+    btot += wsum[w];
+  }
+  if (threadIdx.x == 0) R.bsum[blockIdx.x] = btot;
+  grid_barrier(R);
+  if (threadIdx.x == 0) {
+    int off = 0;
+    for (int b = 0; b < (int)blockIdx.x; ++b) off += R.bsum[b];
+    s_off = off;
+    if (blockIdx.x == nb - 1) start[n] = off + btot;
+  }
+  __syncthreads();
+  int run = s_off + woff + incl - sum;
+  for (int c = t0; c < t1; ++c) {
+    const int v = R.cnt[c];
+    start[c] = run;
+    R.cnt[c] = 0;
+    run += v;
+  }
+  grid_barrier(R);
+  for (int i = tid; i < np; i += nth) cell_scatter_one(R, i, which);
+  grid_barrier(R);
+  for (int i = tid; i < np; i += nth) cell_rank_one(R, i, which);
+  if (!P.verlet) return;
+  grid_barrier(R);
+  if (R.vl_flag[2] == 3) return;  // cell mode: no pair list
+  for (int i = tid; i < np; i += nth) vl_build_one(R, i, which);
 }
 
 // Pair forces from the Verlet list (soft repulsion with the cutoff test and
@@ -544,7 +657,37 @@ void launch_forces(const Batch& B, int which, cudaStream_t s) {
   if (B.has_vl) FSL_GO(k_forces_vl, part_blocks(B, KIND_T4), kPartThreads, 0, s, B, which);
 }
 
+// Blocks of the cooperative build: all co-resident (cached per device).
+static unsigned coop_blocks() {
+  static int dev_cached = -1;
+  static unsigned blocks = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev != dev_cached) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lists_coop, kCoopThreads, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long b = (long)per_sm * sms;
+    blocks = (unsigned)std::max(1L, std::min(b, (long)kCoopMaxBlocks));
+    dev_cached = dev;
+  }
+  return blocks;
+}
+
 void launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
+  if (B.one && B.one->bar && B.max_np > 0) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(coop_blocks());
+    cfg.blockDim = dim3(kCoopThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_lists_coop, *B.one, which);
+    return;
+  }
   launch_cells(B, which, s, false);
   if (B.max_np > 0 && B.has_vl) FSL_GO(k_vl_build, part_blocks(B, KIND_T1), kPartThreads, 0, s, B, which);
 }
