@@ -19,7 +19,10 @@ struct PackEnt {
   long long off;  // first double of the instance in the packed array
   int np;
   int pad;
-  uint64_t* vl_flag;  // set [2] when the positions are replaced
+  uint64_t* vl_flag;  // Verlet list: rebuild word, reference positions,
+  const double* qref;  // (skin / 2)^2 and the step counter (null qref: no list)
+  double vl_half2;
+  const uint64_t* t;
 };
 
 // dir = 0: packed <- q of every instance; dir = 1: q <- packed.
@@ -32,8 +35,19 @@ __global__ void k_pack(const PackEnt* __restrict__ ents, double* __restrict__ pa
     if (dir == 0) packed[e.off + k] = e.q[k];
     else e.q[k] = packed[e.off + k];
   }
-  // new positions: the pair list is rebuilt at the next force evaluation
-  if (dir == 1 && blockIdx.x == 0 && threadIdx.x == 0) e.vl_flag[2] = 1;
+  // new positions: the Verlet list is rebuilt at the next evaluation at q
+  // if a particle left its skin (as k_moved_check)
+  if (dir == 1 && e.qref) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < e.np;
+         i += (long long)gridDim.x * blockDim.x) {
+      double d2 = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        const double v = packed[e.off + d * (long long)e.np + i] - e.qref[d * (long long)e.np + i];
+        d2 += v * v;
+      }
+      if (d2 > e.vl_half2) e.vl_flag[0] = *e.t + 1;
+    }
+  }
 }
 
 // errs[i] = error bits of instance i with bit 30 set, or 0 if its word is clear
@@ -140,7 +154,8 @@ int fsl_batch_create(int32_t n, const fsl_config* cfgs, const int64_t* np, const
       it = b->groups.emplace(key, std::move(g)).first;
     }
     it->second->slots.push_back(&s);
-    ents[i] = PackEnt{s.r.q, s.r.err, off, (int)np[i], 0, s.r.vl_flag};
+    ents[i] = PackEnt{s.r.q, s.r.err, off, (int)np[i], 0, s.r.vl_flag, s.r.P.verlet ? s.r.qref : nullptr,
+                      s.r.P.vl_half2, s.r.t};
     off += 3ll * np[i];
     b->max_np = std::max(b->max_np, (int)np[i]);
     b->nc_total += P[i].nc;

@@ -398,9 +398,15 @@ int slot_read_observables(const Slot& s, cudaStream_t st, fsl_observables* out) 
   return FSL_OK;
 }
 
-int slot_mark_moved(Slot& s, cudaStream_t st) {
+int slot_force_lists(Slot& s, cudaStream_t st) {
   static const uint64_t flags[3] = {0, 0, 1};
   FSL_TRY(cudaMemcpyAsync(s.r.vl_flag, flags, sizeof(flags), cudaMemcpyHostToDevice, st));
+  return FSL_OK;
+}
+
+int slot_mark_moved(Slot& s, cudaStream_t st) {
+  launch_moved_check(s.r, st);
+  FSL_TRY(cudaGetLastError());
   return FSL_OK;
 }
 
@@ -455,7 +461,7 @@ int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, c
   FSL_TRY(cudaMemsetAsync(r.err, 0, sizeof(int) * 4, st));
   FSL_TRY(cudaMemsetAsync(r.t, 0, sizeof(uint64_t), st));
   if (int rc = slot_reset_observables(s, st)) return rc;
-  if (int rc = slot_mark_moved(s, st)) return rc;
+  if (int rc = slot_force_lists(s, st)) return rc;
   r.active = 1;
   return FSL_OK;
 }

@@ -64,9 +64,12 @@ void slot_free(Slot& s);
 // allocated slot of its class: positions, LJ table, cleared forces, error
 // word, step counter and bonds.  Enqueued on st.
 int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, cudaStream_t st);
-// Positions changed from the host: the pair list is rebuilt at the next
-// force evaluation.  slot_request_lists: the next launch_pair_lists builds
-// the cell list whatever the path (the component entry points).
+// slot_force_lists: the pair list is rebuilt at the next force evaluation
+// (a new instance).  slot_mark_moved: positions changed from the host, the
+// list is rebuilt if a particle left its skin.  slot_request_lists: the next
+// launch_pair_lists builds the cell list whatever the path (the component
+// entry points).
+int slot_force_lists(Slot& s, cudaStream_t st);
 int slot_mark_moved(Slot& s, cudaStream_t st);
 int slot_request_lists(Slot& s, cudaStream_t st);
 // q0 := q, observables accumulators cleared (enqueued on st).

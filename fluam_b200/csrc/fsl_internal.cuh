@@ -615,6 +615,9 @@ void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStre
 // The cell list of force evaluation `which` and, for Verlet-list
 // instances, the pair list (each only where list_needed says so).
 void launch_pair_lists(const Batch& B, int which, cudaStream_t s);
+// After positions were replaced from the host: flag a Verlet-list rebuild if
+// a particle moved more than skin / 2 from its reference position.
+void launch_moved_check(const Rep& r, cudaStream_t s);
 // FP64 observables of every instance with P.observe (end of a step)
 void launch_observe(const Batch& B, cudaStream_t s);
 // The FP64 form (fsl_fp64.cu); the launchers above hand a class of that

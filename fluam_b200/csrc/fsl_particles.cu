@@ -465,6 +465,25 @@ __global__ void k_vl_build(FSL_KARGS, int which) {
   vl_build_one(R, i, which);
 }
 
+// Positions replaced from the host: the Verlet list is rebuilt at the next
+// evaluation at q only if a particle now lies more than skin / 2 from its
+// reference position (a host loop that feeds back the positions it read
+// keeps its list).
+__global__ void k_moved_check(const __grid_constant__ Rep R) {
+  const Params& P = R.P;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.np; i += gridDim.x * blockDim.x) {
+    const double dx = R.q[i] - R.qref[i], dy = R.q[P.np + i] - R.qref[P.np + i],
+                 dz = R.q[2 * P.np + i] - R.qref[2 * P.np + i];
+    if (dx * dx + dy * dy + dz * dz > P.vl_half2) R.vl_flag[0] = *R.t + 1;
+  }
+}
+
+void launch_moved_check(const Rep& r, cudaStream_t s) {
+  if (!r.P.verlet || r.P.np == 0) return;
+  const unsigned b = (unsigned)std::min<long>(148L * 4, ((long)r.P.np + 255) / 256);
+  k_moved_check<<<b, 256, 0, s>>>(r);
+}
+
 // ----------------------------------------------- single-launch list build ---
 // The cell list (and the Verlet list) of one instance in one cooperative
 // launch: the phases of the kernels above separated by grid barriers, so a
