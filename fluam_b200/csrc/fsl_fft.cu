@@ -927,18 +927,18 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
   if (fp->zsolve_r[0]) {
     dim3 g((B.mxh + fp->z_kx - 1) / fp->z_kx, (B.my + fp->z_ky - 1) / fp->z_ky, B.nrep);
     if (B.one)
-      fsl_launch(fp->zsolve_r[1], dim3(g), dim3(fp->z_threads), fp->smem_z_r, s, RepSrc{}, *B.one, fp->twz, fp->sx, fp->sy,
+      fp->zsolve_r[1]<<<g, fp->z_threads, fp->smem_z_r, s>>>(RepSrc{}, *B.one, fp->twz, fp->sx, fp->sy,
                                                              fp->sz, fp->ex, fp->ey, fp->ez);
     else
-      fsl_launch(fp->zsolve_r[0], dim3(g), dim3(fp->z_threads), fp->smem_z_r, s, B.src(), Rep{}, fp->twz, fp->sx, fp->sy,
+      fp->zsolve_r[0]<<<g, fp->z_threads, fp->smem_z_r, s>>>(B.src(), Rep{}, fp->twz, fp->sx, fp->sy,
                                                              fp->sz, fp->ex, fp->ey, fp->ez);
     return;
   }
   if (B.one)
-    fsl_launch(fp->zsolve[1], dim3(gz), dim3(kFftThreads), fp->smem_z, s, RepSrc{}, *B.one, fp->rz, fp->twz, fp->sx, fp->sy,
+    fp->zsolve[1]<<<gz, kFftThreads, fp->smem_z, s>>>(RepSrc{}, *B.one, fp->rz, fp->twz, fp->sx, fp->sy,
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
   else
-    fsl_launch(fp->zsolve[0], dim3(gz), dim3(kFftThreads), fp->smem_z, s, B.src(), Rep{}, fp->rz, fp->twz, fp->sx, fp->sy,
+    fp->zsolve[0]<<<gz, kFftThreads, fp->smem_z, s>>>(B.src(), Rep{}, fp->rz, fp->twz, fp->sx, fp->sy,
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
 }
 
@@ -969,16 +969,16 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_giv
     const int tb = fp->plane_threads;
     pr.mark(s, "plane_fwd");
     if (B.one)
-      fsl_launch(fp->plane_fwd_r[1], dim3(gp), dim3(tb), fp->smem_plane_r, s, RepSrc{}, *B.one, fp->twx);
+      fp->plane_fwd_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
     else
-      fsl_launch(fp->plane_fwd_r[0], dim3(gp), dim3(tb), fp->smem_plane_r, s, B.src(), Rep{}, fp->twx);
+      fp->plane_fwd_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
     pr.mark(s, "zsolve");
     zsolve(B, fp, dim3((B.mxh + kZTile - 1) / kZTile, B.my, nrep), s);
     pr.mark(s, "plane_inv");
     if (B.one)
-      fsl_launch(fp->plane_inv_r[1], dim3(gp), dim3(tb), fp->smem_plane_r, s, RepSrc{}, *B.one, fp->twx);
+      fp->plane_inv_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
     else
-      fsl_launch(fp->plane_inv_r[0], dim3(gp), dim3(tb), fp->smem_plane_r, s, B.src(), Rep{}, fp->twx);
+      fp->plane_inv_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
     pr.count(3);
     return;
   }
@@ -986,17 +986,17 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_giv
     dim3 gp(B.mz, 3, nrep);
     pr.mark(s, "plane_fwd");
     if (B.one)
-      fsl_launch(fp->plane_fwd[1], dim3(gp), dim3(kFftThreads), fp->smem_plane, s, RepSrc{}, *B.one, fp->rx, fp->ry, fp->twx, fp->twy);
+      fp->plane_fwd[1]<<<gp, kFftThreads, fp->smem_plane, s>>>(RepSrc{}, *B.one, fp->rx, fp->ry, fp->twx, fp->twy);
     else
-      fsl_launch(fp->plane_fwd[0], dim3(gp), dim3(kFftThreads), fp->smem_plane, s, B.src(), Rep{}, fp->rx, fp->ry, fp->twx, fp->twy);
+      fp->plane_fwd[0]<<<gp, kFftThreads, fp->smem_plane, s>>>(B.src(), Rep{}, fp->rx, fp->ry, fp->twx, fp->twy);
     dim3 gz((B.mxh + kZTile - 1) / kZTile, B.my, nrep);
     pr.mark(s, "zsolve");
     zsolve(B, fp, gz, s);
     pr.mark(s, "plane_inv");
     if (B.one)
-      fsl_launch(fp->plane_inv[1], dim3(gp), dim3(kFftThreads), fp->smem_plane, s, RepSrc{}, *B.one, fp->rx, fp->ry, fp->twx, fp->twy);
+      fp->plane_inv[1]<<<gp, kFftThreads, fp->smem_plane, s>>>(RepSrc{}, *B.one, fp->rx, fp->ry, fp->twx, fp->twy);
     else
-      fsl_launch(fp->plane_inv[0], dim3(gp), dim3(kFftThreads), fp->smem_plane, s, B.src(), Rep{}, fp->rx, fp->ry, fp->twx, fp->twy);
+      fp->plane_inv[0]<<<gp, kFftThreads, fp->smem_plane, s>>>(B.src(), Rep{}, fp->rx, fp->ry, fp->twx, fp->twy);
     pr.count(3);
     return;
   }

@@ -129,14 +129,6 @@ ClassKey class_of(const Params& P) {
   return ClassKey{P.mx, P.my, P.mz, P.mnx, P.mny, P.mnz, P.kernel, P.scheme, P.prec, P.observe};
 }
 
-bool pdl_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("FLUAMSL_PDL");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
 int make_params(const fsl_config& c, int64_t np, Params& P) {
   if (c.scheme < 0 || c.scheme > 4) return errorf(FSL_E_ARG, "unknown scheme %d", c.scheme);
   const bool two_d = c.scheme == FSL_SCHEME_QUASI2D || c.scheme == FSL_SCHEME_STOKES2D;

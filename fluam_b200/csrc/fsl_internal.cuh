@@ -17,7 +17,6 @@
 #pragma once
 
 #include <cstdint>
-#include <utility>
 #include <cuda_runtime.h>
 
 namespace fsl {
@@ -555,22 +554,9 @@ __device__ __forceinline__ const Rep& rep_flat(const RepSrc& src, const Rep& one
 
 #define FSL_KARGS const RepSrc src, const __grid_constant__ Rep one
 
-// Programmatic dependent launch: the kernels are launched with programmatic
-// stream serialization, so a kernel's blocks may be scheduled while the
-// previous kernel on the stream drains.  Every kernel waits for the previous
-// grid's completion and memory (griddepcontrol.wait) before it reads
-// anything a kernel wrote (only its instance table, written by the host, is
-// read before), then lets the next kernel be scheduled once all of its own
-// blocks have started.
-__device__ __forceinline__ void pdl_wait_and_release() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 #define FSL_REP_AT(IDX)                                            \
   __shared__ Rep fsl_sh_rep_;                                      \
   const Rep& R = rep_copy<ONE>(src, one, (int)(IDX), fsl_sh_rep_); \
-  pdl_wait_and_release();                                          \
   if (!R.active) return;                                           \
   const Params& P = R.P
 
@@ -578,45 +564,24 @@ __device__ __forceinline__ void pdl_wait_and_release() {
   __shared__ Rep fsl_sh_rep_;                                      \
   int blk;                                                         \
   const Rep& R = rep_flat<ONE>(src, one, (KIND), blk, fsl_sh_rep_); \
-  pdl_wait_and_release();                                          \
   if (!R.active) return;                                           \
   const Params& P = R.P
 
-// Whether launches carry the programmatic-serialization attribute
-// (FLUAMSL_PDL=0 turns it off; read once).
-bool pdl_enabled();
-
-template <typename... KArgs, typename... Args>
-inline void fsl_launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                       Args&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
-}
-
 // Launch of a kernel template whose first template argument is ONE.
-#define FSL_GO(KERN, GRID, BLOCK, SMEM, S, B, ...)                                              \
-  do {                                                                                          \
-    if ((B).one)                                                                                \
-      fsl_launch(KERN<true>, dim3(GRID), dim3(BLOCK), (SMEM), (S), RepSrc{}, *(B).one, ##__VA_ARGS__); \
-    else                                                                                        \
-      fsl_launch(KERN<false>, dim3(GRID), dim3(BLOCK), (SMEM), (S), (B).src(), Rep{}, ##__VA_ARGS__);  \
+#define FSL_GO(KERN, GRID, BLOCK, SMEM, S, B, ...)                                     \
+  do {                                                                                 \
+    if ((B).one)                                                                       \
+      KERN<true><<<(GRID), (BLOCK), (SMEM), (S)>>>(RepSrc{}, *(B).one, ##__VA_ARGS__); \
+    else                                                                               \
+      KERN<false><<<(GRID), (BLOCK), (SMEM), (S)>>>((B).src(), Rep{}, ##__VA_ARGS__);  \
   } while (0)
 // ... with a second template argument T
-#define FSL_GO_T(KERN, T, GRID, BLOCK, SMEM, S, B, ...)                                            \
-  do {                                                                                             \
-    if ((B).one)                                                                                   \
-      fsl_launch(KERN<true, T>, dim3(GRID), dim3(BLOCK), (SMEM), (S), RepSrc{}, *(B).one, ##__VA_ARGS__); \
-    else                                                                                           \
-      fsl_launch(KERN<false, T>, dim3(GRID), dim3(BLOCK), (SMEM), (S), (B).src(), Rep{}, ##__VA_ARGS__);  \
+#define FSL_GO_T(KERN, T, GRID, BLOCK, SMEM, S, B, ...)                                   \
+  do {                                                                                    \
+    if ((B).one)                                                                          \
+      KERN<true, T><<<(GRID), (BLOCK), (SMEM), (S)>>>(RepSrc{}, *(B).one, ##__VA_ARGS__); \
+    else                                                                                  \
+      KERN<false, T><<<(GRID), (BLOCK), (SMEM), (S)>>>((B).src(), Rep{}, ##__VA_ARGS__);  \
   } while (0)
 
 // Blocks of a particle launch of kind k.
