@@ -164,107 +164,6 @@ __device__ __forceinline__ int line_freq(int t, int j, int b) {
   return line_a<R, T>(t, j) + R * b;
 }
 
-// W of component comp at cells x0 .. x0+3 of row y, plane z, for one stress
-// sample d: the terms of stress_div4 for that component, the same
-// expressions.
-__device__ __forceinline__ void stress_div4_comp(const Params& P, const float* __restrict__ d, bool aligned,
-                                                 int comp, int x0, int y, int z, size_t i0, const WCoef& k,
-                                                 float (&w)[4]) {
-  const size_t nc = (size_t)P.nc;
-  const int mx = P.mx, my = P.my, mz = P.mz;
-  const size_t row = i0 - x0;
-  const long dym = (y == 0 ? (long)(my - 1) * mx : -(long)mx);
-  const long dyp = (y == my - 1 ? -(long)(my - 1) * mx : (long)mx);
-  const long dzm = (z == 0 ? (long)(mz - 1) * my * mx : -(long)my * mx);
-  const long dzp = (z == mz - 1 ? -(long)(mz - 1) * my * mx : (long)my * mx);
-  const int xl = x0 == 0 ? mx - 1 : x0 - 1, xr = x0 + 4 == mx ? 0 : x0 + 4;
-  if (comp == 0) {
-    const float4 r0 = ld_row4(d + i0, aligned);
-    const float e0 = __ldg(d + row + xr);
-    const float4 r1 = ld_row4(d + nc + i0, aligned), r1ym = ld_row4(d + nc + i0 + dym, aligned);
-    const float4 r2 = ld_row4(d + 2 * nc + i0, aligned), r2zm = ld_row4(d + 2 * nc + i0 + dzm, aligned);
-    const float d0[5] = {r0.x, r0.y, r0.z, r0.w, e0};
-    const float d1[5] = {0.f, r1.x, r1.y, r1.z, r1.w};
-    const float d2[5] = {0.f, r2.x, r2.y, r2.z, r2.w};
-    const float d1ym[4] = {r1ym.x, r1ym.y, r1ym.z, r1ym.w}, d2zm[4] = {r2zm.x, r2zm.y, r2zm.z, r2zm.w};
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-      w[c] += k.a1x * (d0[c + 1] - d0[c]) + k.a4y * (d1[c + 1] - d1ym[c]) + k.a4z * (d2[c + 1] - d2zm[c]);
-  } else if (comp == 1) {
-    const float4 r1 = ld_row4(d + nc + i0, aligned);
-    const float e1 = __ldg(d + nc + row + xl);
-    const float4 r3 = ld_row4(d + 3 * nc + i0, aligned), r3yp = ld_row4(d + 3 * nc + i0 + dyp, aligned);
-    const float4 r4 = ld_row4(d + 4 * nc + i0, aligned), r4zm = ld_row4(d + 4 * nc + i0 + dzm, aligned);
-    const float d1[5] = {e1, r1.x, r1.y, r1.z, r1.w};
-    const float d3[4] = {r3.x, r3.y, r3.z, r3.w}, d3yp[4] = {r3yp.x, r3yp.y, r3yp.z, r3yp.w};
-    const float d4[4] = {r4.x, r4.y, r4.z, r4.w}, d4zm[4] = {r4zm.x, r4zm.y, r4zm.z, r4zm.w};
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-      w[c] += k.a1y * (d3yp[c] - d3[c]) + k.a4x * (d1[c + 1] - d1[c]) + k.a4z * (d4[c] - d4zm[c]);
-  } else {
-    const float4 r2 = ld_row4(d + 2 * nc + i0, aligned);
-    const float e2 = __ldg(d + 2 * nc + row + xl);
-    const float4 r4 = ld_row4(d + 4 * nc + i0, aligned), r4ym = ld_row4(d + 4 * nc + i0 + dym, aligned);
-    const float4 r5 = ld_row4(d + 5 * nc + i0, aligned), r5zp = ld_row4(d + 5 * nc + i0 + dzp, aligned);
-    const float d2[5] = {e2, r2.x, r2.y, r2.z, r2.w};
-    const float d4[4] = {r4.x, r4.y, r4.z, r4.w}, d4ym[4] = {r4ym.x, r4ym.y, r4ym.z, r4ym.w};
-    const float d5[4] = {r5.x, r5.y, r5.z, r5.w}, d5zp[4] = {r5zp.x, r5zp.y, r5zp.z, r5zp.w};
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-      w[c] += k.a1z * (d5zp[c] - d5[c]) + k.a4x * (d2[c + 1] - d2[c]) + k.a4y * (d4[c] - d4ym[c]);
-  }
-}
-
-// W of plane (comp, z) (an N x N register-edge plane, mx = my = N) into fb
-// with row pitch N + 1, four x cells per item: the spread field over dV and
-// the stress divergence of nsets samples, as k_wbuild4.  Loads only.
-template <int N>
-__device__ void w_plane_stage(const Rep& R, const Params& P, int comp, int z, int nsets, const WCoef& k,
-                              float* fb, int r, int nthr) {
-  const size_t nc = (size_t)P.nc;
-  const size_t off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
-  const bool al2 = (off2 & 3) == 0;
-  for (int g = r; g < N * N / 4; g += nthr) {
-    const int x0 = (g % (N / 4)) * 4, y = g / (N / 4);
-    const size_t i0 = (size_t)x0 + (size_t)N * ((size_t)y + (size_t)N * z);
-    float w[4];
-    if (P.prec == PREC_FLOAT) {
-      const float4 ga = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(R.grid) + comp * nc + i0);
-      w[0] = ga.x * k.fscale;
-      w[1] = ga.y * k.fscale;
-      w[2] = ga.z * k.fscale;
-      w[3] = ga.w * k.fscale;
-    } else {
-      const longlong2* gp = reinterpret_cast<const longlong2*>(R.grid + comp * nc + i0);
-      const longlong2 ga = gp[0], gb = gp[1];
-      w[0] = (float)((double)ga.x * (double)k.scale);
-      w[1] = (float)((double)ga.y * (double)k.scale);
-      w[2] = (float)((double)gb.x * (double)k.scale);
-      w[3] = (float)((double)gb.y * (double)k.scale);
-    }
-    stress_div4_comp(P, R.noise, true, comp, x0, y, z, i0, k, w);
-    if (nsets > 1) stress_div4_comp(P, R.noise + off2, al2, comp, x0, y, z, i0, k, w);
-    float* row = fb + y * (N + 1) + x0;
-    row[0] = w[0];
-    row[1] = w[1];
-    row[2] = w[2];
-    row[3] = w[3];
-  }
-}
-
-// The plane (comp, z) of the spread field set to zero (16-byte stores).
-template <int N>
-__device__ void w_plane_clear(const Rep& R, const Params& P, int comp, int z, int r, int nthr) {
-  const size_t base = (size_t)comp * P.nc + (size_t)z * N * N;
-  if (P.prec == PREC_FLOAT) {
-    float4* g = reinterpret_cast<float4*>(reinterpret_cast<float*>(R.grid) + base);
-    for (int i = r; i < N * N / 4; i += nthr) g[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-  } else {
-    longlong2* g = reinterpret_cast<longlong2*>(R.grid + base);
-    for (int i = r; i < N * N / 2; i += nthr) g[i] = make_longlong2(0, 0);
-  }
-}
-
 // Real-to-complex transform of whole xy planes (x then y), PB planes per
 // block, H * T threads per plane (H = N / 2).  x: the row pair (2p, 2p+1) is
 // one complex line; y: columns kx = 1 .. H-1 are complex lines and columns 0
@@ -289,22 +188,18 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
   const bool live = pl < 3 * P.mz;
   const int comp = live ? pl / P.mz : 0, z = live ? pl - comp * P.mz : 0;
   const float* W = R.wbuf + (size_t)comp * P.nc + (size_t)z * N * N;
-  float* fb = reinterpret_cast<float*>(buf);  // a real plane, row pitch N + 1
-  if constexpr (WB) {
-    // W of the plane into shared memory (loads only), then the plane of the
-    // spread field cleared
-    __syncthreads();
-    if (live) w_plane_stage<N>(R, P, comp, z, nsets, wcoef(P, nfac), fb, r, TPP);
-    else
-      for (int i = r; i < N * (N + 1); i += TPP) fb[i] = 0.0f;
-    __syncthreads();
-    if (live) w_plane_clear<N>(R, P, comp, z, r, TPP);
-  }
+  WCoef wc;
+  if constexpr (WB) wc = wcoef(P, nfac);
+  // W at (x, y) of this plane
+  auto wat = [&](int x, int y) -> float {
+    if constexpr (WB) return w_cell(R, P, comp, x, y, z, nsets, wc);
+    else return W[y * N + x];
+  };
   float2 v[RR];
   if constexpr (T == 1) {
     // stage the plane through shared memory so the global reads coalesce
-    if constexpr (!WB)
-      for (int i = r; i < N * N; i += TPP) fb[i + (i / N)] = live ? W[i] : 0.0f;  // row pitch N + 1
+    float* fb = reinterpret_cast<float*>(buf);
+    for (int i = r; i < N * N; i += TPP) fb[i + (i / N)] = live ? wat(i % N, i / N) : 0.0f;  // row pitch N + 1
     __syncthreads();
     const int p = r;
 #pragma unroll
@@ -319,12 +214,8 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
 #pragma unroll
     for (int k = 0; k < RR; ++k) {
       const int x = t + T * k;
-      if constexpr (WB)
-        v[k] = make_float2(fb[(2 * p) * (N + 1) + x], fb[(2 * p + 1) * (N + 1) + x]);
-      else
-        v[k] = live ? make_float2(W[(2 * p) * N + x], W[(2 * p + 1) * N + x]) : make_float2(0.f, 0.f);
+      v[k] = live ? make_float2(wat(x, 2 * p), wat(x, 2 * p + 1)) : make_float2(0.f, 0.f);
     }
-    if constexpr (WB) __syncthreads();  // the staged plane is read before the exchange reuses it
     line_fft_a<RR, T>(v, t, buf + p * LS, stw, -1);
     __syncthreads();
     float2 out[G::RT][T];

@@ -452,6 +452,29 @@ __device__ __forceinline__ WCoef wcoef(const Params& P, double nfac) {
   return c;
 }
 
+// W of component comp at cell (x, y, z) with the arithmetic of k_wbuild: the
+// spread field (fixed point or FP32) over dV plus the stress divergence of
+// nsets samples; the spread entry is cleared behind the read.
+__device__ __forceinline__ float w_cell(const Rep& R, const Params& P, int comp, int x, int y, int z,
+                                        int nsets, const WCoef& c) {
+  const size_t nc = (size_t)P.nc;
+  const int i = x + P.mx * (y + P.my * z);
+  float w;
+  if (P.prec == PREC_FLOAT) {
+    float* gf = reinterpret_cast<float*>(R.grid);
+    w = gf[comp * nc + i] * c.fscale;
+    gf[comp * nc + i] = 0.0f;
+  } else {
+    const long long g = (long long)R.grid[comp * nc + i];
+    w = (float)((double)g * (double)c.scale);
+    R.grid[comp * nc + i] = 0ull;
+  }
+  w += stress_div(P, R.noise, comp, x, y, z, i, c.a1x, c.a1y, c.a1z, c.a4x, c.a4y, c.a4z);
+  if (nsets > 1)
+    w += stress_div(P, R.noise + (size_t)6 * P.nc + (size_t)9 * P.np, comp, x, y, z, i, c.a1x, c.a1y, c.a1z,
+                    c.a4x, c.a4y, c.a4z);
+  return w;
+}
 constexpr int kVlCap = 64;
 constexpr int kObsVals = 10;      // msd, displacement[3], force[3], momentum[3]
 constexpr int kObsSlots = 16;     // steps, msd, msd_sum, disp[3], force[3], mom[3], mom_sum[3]
