@@ -949,6 +949,15 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
 }
 
+// FLUAMSL_FUSED_W=0 keeps the separate W build (read once).
+static bool fused_w_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("FLUAMSL_FUSED_W");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof) {
   if (B.prec == PREC_F64) return launch_solve64(B, nsets, nfac, s, prof);
@@ -956,7 +965,7 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_giv
   Prof& pr = prof ? *prof : dummy;
   const int nrep = B.nrep;
   // the register plane path builds W inside its first pass
-  const bool fused = !w_given && fp->plane_fwd_rw[0] && B.fused_w;
+  const bool fused = !w_given && fp->plane_fwd_rw[0] && fused_w_enabled();
   if (!w_given && !fused) {
     // W from the spread field and the noise; clears the spread field
     pr.mark(s, "wbuild");

@@ -611,9 +611,6 @@ int group_upload(Group& g) {
   const char* env = std::getenv("FLUAMSL_TILED_SPREAD");
   B.tiled = env && env[0] == '1' && tile_eligible(g.P0);
   B.has_vl = B.has_cl = 0;
-  // FLUAMSL_FUSED_W=0 keeps the separate W build
-  const char* fenv = std::getenv("FLUAMSL_FUSED_W");
-  B.fused_w = !(fenv && fenv[0] == '0');
   for (const Slot* s : g.slots) {
     B.max_np = std::max(B.max_np, s->np_cap);
     B.max_noise_n = std::max<uint64_t>(B.max_noise_n, noise_count(g.P0, s->np_cap));

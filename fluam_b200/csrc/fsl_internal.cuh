@@ -544,7 +544,6 @@ struct Batch {
   uint64_t max_noise_n;
   int tiled;        // spread and W build by launch_spread_w
   int has_vl, has_cl;  // instances on the Verlet path / on the cell-list pair path
-  int fused_w;         // the register plane path builds W in its first pass
   int nblk[NKIND];  // total blocks of each particle launch kind
   const Rep* one;   // host copy of the single instance (nrep == 1), else null
   RepSrc src() const { return RepSrc{reps, boff, nrep}; }

@@ -46,11 +46,9 @@ def _run(fsl, c, tiled, steps=6):
                           rfd=fsl.RFD_PAPER if c.get("rfd") == "paper" else fsl.RFD_REFERENCE,
                           scheme=fsl.SCHEME_FIRST_ORDER if c.get("scheme") == "first" else 0,
                           seed=21)
-    keys = ("FLUAMSL_TILED_SPREAD", "FLUAMSL_VERLET", "FLUAMSL_FUSED_W")
-    old = tuple(os.environ.get(k) for k in keys)
+    old = os.environ.get("FLUAMSL_TILED_SPREAD"), os.environ.get("FLUAMSL_VERLET")
     os.environ["FLUAMSL_TILED_SPREAD"] = "1" if tiled else "0"
     os.environ["FLUAMSL_VERLET"] = "0"  # the tiles read the cell lists of every step
-    os.environ["FLUAMSL_FUSED_W"] = "0"  # the W build of both paths: k_wbuild's arithmetic
     try:
         with fsl.StokesLimit(cfg, q) as s:
             if bi is not None:
@@ -60,7 +58,7 @@ def _run(fsl, c, tiled, steps=6):
             assert st["error_bits"] == 0
             return s.positions(), s.forces(), s.velocity(), st["launches_per_step"]
     finally:
-        for key, val in zip(keys, old):
+        for key, val in zip(("FLUAMSL_TILED_SPREAD", "FLUAMSL_VERLET"), old):
             if val is None:
                 del os.environ[key]
             else:
