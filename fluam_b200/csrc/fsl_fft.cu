@@ -22,8 +22,6 @@
 #include <cstdio>
 #include <vector>
 
-#include <cstdlib>
-
 #include "fsl_internal.cuh"
 
 namespace fsl {
@@ -51,8 +49,7 @@ struct FftPlan {
   void (*zsolve[2])(RepSrc, Rep, Radices, const float2*, const float*, const float*, const float*,
                     const float2*, const float2*, const float2*) = {};
   // register-resident passes for compiled edges (null: not available)
-  void (*plane_fwd_r[2])(RepSrc, Rep, const float2*, int, double) = {};
-  void (*plane_fwd_rw[2])(RepSrc, Rep, const float2*, int, double) = {};  // W built in the pass
+  void (*plane_fwd_r[2])(RepSrc, Rep, const float2*) = {};
   void (*plane_inv_r[2])(RepSrc, Rep, const float2*) = {};
   void (*zsolve_r[2])(RepSrc, Rep, const float2*, const float*, const float*, const float*,
                       const float2*, const float2*, const float2*) = {};
@@ -703,10 +700,8 @@ __global__ void __launch_bounds__(kFftThreads)
 // ------------------------------------------------------------ host side ---
 template <int N, int R, int T, int PB>
 static void pick_plane_r(FftPlan* fp) {
-  fp->plane_fwd_r[0] = k_plane_fwd_r<false, N, R, T, PB, false>;
-  fp->plane_fwd_r[1] = k_plane_fwd_r<true, N, R, T, PB, false>;
-  fp->plane_fwd_rw[0] = k_plane_fwd_r<false, N, R, T, PB, true>;
-  fp->plane_fwd_rw[1] = k_plane_fwd_r<true, N, R, T, PB, true>;
+  fp->plane_fwd_r[0] = k_plane_fwd_r<false, N, R, T, PB>;
+  fp->plane_fwd_r[1] = k_plane_fwd_r<true, N, R, T, PB>;
   fp->plane_inv_r[0] = k_plane_inv_r<false, N, R, T, PB>;
   fp->plane_inv_r[1] = k_plane_inv_r<true, N, R, T, PB>;
   fp->plane_pb = PB;
@@ -898,10 +893,8 @@ FftPlan* fft_plan_create(const Params& P) {
   for (int v = 0; v < 2; ++v) {
     if (fp->plane_fwd_r[0] &&
         !(allow((const void*)fp->plane_fwd_r[v], fp->smem_plane_r) &&
-          allow((const void*)fp->plane_fwd_rw[v], fp->smem_plane_r) &&
           allow((const void*)fp->plane_inv_r[v], fp->smem_plane_r)))
-      fp->plane_fwd_r[0] = fp->plane_fwd_r[1] = fp->plane_fwd_rw[0] = fp->plane_fwd_rw[1] = nullptr,
-      fp->plane_inv_r[0] = fp->plane_inv_r[1] = nullptr;
+      fp->plane_fwd_r[0] = fp->plane_fwd_r[1] = fp->plane_inv_r[0] = fp->plane_inv_r[1] = nullptr;
     if (fp->zsolve_r[0] && !allow((const void*)fp->zsolve_r[v], fp->smem_z_r))
       fp->zsolve_r[0] = fp->zsolve_r[1] = nullptr;
   }
@@ -949,24 +942,13 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
 }
 
-// FLUAMSL_FUSED_W=0 keeps the separate W build (read once).
-static bool fused_w_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("FLUAMSL_FUSED_W");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof) {
   if (B.prec == PREC_F64) return launch_solve64(B, nsets, nfac, s, prof);
   Prof dummy;
   Prof& pr = prof ? *prof : dummy;
   const int nrep = B.nrep;
-  // the register plane path builds W inside its first pass
-  const bool fused = !w_given && fp->plane_fwd_rw[0] && fused_w_enabled();
-  if (!w_given && !fused) {
+  if (!w_given) {
     // W from the spread field and the noise; clears the spread field
     pr.mark(s, "wbuild");
     int tb = 256;
@@ -985,12 +967,11 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_giv
   if (fp->plane_fwd_r[0]) {
     dim3 gp((3 * B.mz + fp->plane_pb - 1) / fp->plane_pb, 1, nrep);
     const int tb = fp->plane_threads;
-    pr.mark(s, fused ? "wbuild_plane_fwd" : "plane_fwd");
-    auto k = fused ? fp->plane_fwd_rw : fp->plane_fwd_r;
+    pr.mark(s, "plane_fwd");
     if (B.one)
-      k[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx, nsets, nfac);
+      fp->plane_fwd_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
     else
-      k[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx, nsets, nfac);
+      fp->plane_fwd_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
     pr.mark(s, "zsolve");
     zsolve(B, fp, dim3((B.mxh + kZTile - 1) / kZTile, B.my, nrep), s);
     pr.mark(s, "plane_inv");

@@ -169,13 +169,9 @@ __device__ __forceinline__ int line_freq(int t, int j, int b) {
 // one complex line; y: columns kx = 1 .. H-1 are complex lines and columns 0
 // and H (real after the x transform) travel together as one complex line.
 // Output: the half spectrum spec[comp][z][ky][kx], kx <= H.
-//
-// WB: W is built on the fly from the spread field and the noise (the
-// arithmetic of k_wbuild, w_cell) instead of read, and the spread field of
-// the plane is cleared; nsets and nfac as k_wbuild.
-template <bool ONE, int N, int RR, int T, int PB, bool WB>
+template <bool ONE, int N, int RR, int T, int PB>
 __global__ void __launch_bounds__(PB * (N / 2) * T)
-    k_plane_fwd_r(FSL_KARGS, const float2* __restrict__ twn, int nsets, double nfac) {
+    k_plane_fwd_r(FSL_KARGS, const float2* __restrict__ twn) {
   FSL_REP_AT(blockIdx.z);
   using G = LineGeom<RR, T>;
   constexpr int H = N / 2, TPP = H * T, LS = G::LS;
@@ -188,18 +184,11 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
   const bool live = pl < 3 * P.mz;
   const int comp = live ? pl / P.mz : 0, z = live ? pl - comp * P.mz : 0;
   const float* W = R.wbuf + (size_t)comp * P.nc + (size_t)z * N * N;
-  WCoef wc;
-  if constexpr (WB) wc = wcoef(P, nfac);
-  // W at (x, y) of this plane
-  auto wat = [&](int x, int y) -> float {
-    if constexpr (WB) return w_cell(R, P, comp, x, y, z, nsets, wc);
-    else return W[y * N + x];
-  };
   float2 v[RR];
   if constexpr (T == 1) {
     // stage the plane through shared memory so the global reads coalesce
     float* fb = reinterpret_cast<float*>(buf);
-    for (int i = r; i < N * N; i += TPP) fb[i + (i / N)] = live ? wat(i % N, i / N) : 0.0f;  // row pitch N + 1
+    for (int i = r; i < N * N; i += TPP) fb[i + (i / N)] = live ? W[i] : 0.0f;  // row pitch N + 1
     __syncthreads();
     const int p = r;
 #pragma unroll
@@ -214,7 +203,7 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
 #pragma unroll
     for (int k = 0; k < RR; ++k) {
       const int x = t + T * k;
-      v[k] = live ? make_float2(wat(x, 2 * p), wat(x, 2 * p + 1)) : make_float2(0.f, 0.f);
+      v[k] = live ? make_float2(W[(2 * p) * N + x], W[(2 * p + 1) * N + x]) : make_float2(0.f, 0.f);
     }
     line_fft_a<RR, T>(v, t, buf + p * LS, stw, -1);
     __syncthreads();

@@ -270,11 +270,6 @@ __device__ __forceinline__ void set_err(int* err, int bit) {
 }
 
 // ---------------------------------------------------- stress divergence ---
-// Coefficients of the W build (k_wbuild) for the noise factor nfac.
-struct WCoef {
-  float scale, fscale, a1x, a1y, a1z, a4x, a4y, a4z;
-};
-
 // Noise terms of W for component comp at cell i (x,y,z) for one stress
 // sample d (src/stokesLimitFunctions.cu:2323-2367): the divergence of the
 // stochastic stress with diagonals at cell centres and off-diagonals on edges.
@@ -437,44 +432,6 @@ struct Rep {
   unsigned* bar;
 };
 constexpr int kCoopMaxBlocks = 1024;
-
-__device__ __forceinline__ WCoef wcoef(const Params& P, double nfac) {
-  WCoef c;
-  c.scale = (float)(kFixedInv / P.dV);
-  c.fscale = (float)(1.0 / P.dV);
-  const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
-  c.a1x = (float)P.invdx * f1;
-  c.a1y = (float)P.invdy * f1;
-  c.a1z = (float)P.invdz * f1;
-  c.a4x = (float)P.invdx * f4;
-  c.a4y = (float)P.invdy * f4;
-  c.a4z = (float)P.invdz * f4;
-  return c;
-}
-
-// W of component comp at cell (x, y, z) with the arithmetic of k_wbuild: the
-// spread field (fixed point or FP32) over dV plus the stress divergence of
-// nsets samples; the spread entry is cleared behind the read.
-__device__ __forceinline__ float w_cell(const Rep& R, const Params& P, int comp, int x, int y, int z,
-                                        int nsets, const WCoef& c) {
-  const size_t nc = (size_t)P.nc;
-  const int i = x + P.mx * (y + P.my * z);
-  float w;
-  if (P.prec == PREC_FLOAT) {
-    float* gf = reinterpret_cast<float*>(R.grid);
-    w = gf[comp * nc + i] * c.fscale;
-    gf[comp * nc + i] = 0.0f;
-  } else {
-    const long long g = (long long)R.grid[comp * nc + i];
-    w = (float)((double)g * (double)c.scale);
-    R.grid[comp * nc + i] = 0ull;
-  }
-  w += stress_div(P, R.noise, comp, x, y, z, i, c.a1x, c.a1y, c.a1z, c.a4x, c.a4y, c.a4z);
-  if (nsets > 1)
-    w += stress_div(P, R.noise + (size_t)6 * P.nc + (size_t)9 * P.np, comp, x, y, z, i, c.a1x, c.a1y, c.a1z,
-                    c.a4x, c.a4y, c.a4z);
-  return w;
-}
 constexpr int kVlCap = 64;
 constexpr int kObsVals = 10;      // msd, displacement[3], force[3], momentum[3]
 constexpr int kObsSlots = 16;     // steps, msd, msd_sum, disp[3], force[3], mom[3], mom_sum[3]
