@@ -601,49 +601,24 @@ __global__ void k_forces_vl(FSL_KARGS, int which) {
   const double* __restrict__ q = which ? R.qp : R.q;
   const double rx = q[i], ry = q[np + i], rz = q[2 * np + i];
   double fx = 0.0, fy = 0.0, fz = 0.0;
-  const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
-  // soft pair force of neighbour j (the arithmetic of k_forces)
-  auto pair = [&](int j) {
-    const double rxij = minimage(rx - q[j], P.invlx, P.lx);
-    const double ryij = minimage(ry - q[np + j], P.invly, P.ly);
-    const double rzij = minimage(rz - q[2 * np + j], P.invlz, P.lz);
-    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rxij, rxij), __dmul_rn(ryij, ryij)),
-                                __dmul_rn(rzij, rzij));
-    if (r2 >= P.cutoff2 || r2 == 0.0) return;
-    const double f = c1 * (rsqrt(r2) - c2);
-    fx += f * rxij;
-    fy += f * ryij;
-    fz += f * rzij;
-  };
-  // this lane's first bond and first two list entries are fetched together,
-  // so that the dependent loads of bonds and pairs overlap
-  const bool bonded = P.bonded && on, listed = P.verlet && on && !cell_mode;
-  const int nb = bonded ? R.bpp_cnt[i] : 0, boff = bonded ? R.bpp_off[i] : 0;
-  const int n = listed ? R.vl_cnt[i] : 0;
-  const int b0 = a < nb ? R.bpp_idx[boff + a] : -1;
-  const int j0 = a < n ? R.vl_idx[(size_t)a * np + i] : -1;
-  const int j1 = a + 4 < n ? R.vl_idx[(size_t)(a + 4) * np + i] : -1;
-  if (b0 >= 0)
-    bond_force(rx, ry, rz, q[b0], q[np + b0], q[2 * np + b0], R.bpp_k[boff + a], R.bpp_r0[boff + a], fx,
-               fy, fz);
-  for (int j = a + 4; j < nb; j += 4) {
-    const int idx = R.bpp_idx[boff + j];
-    bond_force(rx, ry, rz, q[idx], q[np + idx], q[2 * np + idx], R.bpp_k[boff + j], R.bpp_r0[boff + j], fx,
-               fy, fz);
-  }
-  if (bonded) {
-    const int nf = R.bfp_cnt[i], off = R.bfp_off[i];
-    for (int j = a; j < nf; j += 4) {
+  if (P.bonded && on) {
+    int nb = R.bpp_cnt[i], off = R.bpp_off[i];
+    for (int j = a; j < nb; j += 4) {
+      const int idx = R.bpp_idx[off + j];
+      bond_force(rx, ry, rz, q[idx], q[np + idx], q[2 * np + idx], R.bpp_k[off + j], R.bpp_r0[off + j],
+                 fx, fy, fz);
+    }
+    nb = R.bfp_cnt[i];
+    off = R.bfp_off[i];
+    for (int j = a; j < nb; j += 4) {
       const double* p = R.bfp_xyz + 3 * (off + j);
       bond_force(rx, ry, rz, p[0], p[1], p[2], R.bfp_k[off + j], R.bfp_r0[off + j], fx, fy, fz);
     }
   }
-  if (j0 >= 0) pair(j0);
-  if (j1 >= 0) pair(j1);
-  for (int k = a + 8; k < n; k += 4) pair(R.vl_idx[(size_t)k * np + i]);
   if (P.verlet && on && cell_mode) {
     // the 27 neighbour cells of the current cell list, lanes taking cells
     // a, a + 4, ...
+    const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
     const CellList cl = cell_list(R, which);
     const int cx = cellidx(minimage(rx, P.invlx, P.lx), P.invdnx, P.mnx),
               cy = cellidx(minimage(ry, P.invly, P.ly), P.invdny, P.mny),
@@ -653,8 +628,33 @@ __global__ void k_forces_vl(FSL_KARGS, int which) {
                     P.mnx * (wrap_add(cy, (nn / 3) % 3 - 1, P.mny) + P.mny * wrap_add(cz, nn / 9 - 1, P.mnz));
       for (int e2 = cl.start[c]; e2 < cl.start[c + 1]; ++e2) {
         const int j = cl.sorted[e2];
-        if (j != i) pair(j);
+        const double rxij = minimage(rx - q[j], P.invlx, P.lx);
+        const double ryij = minimage(ry - q[np + j], P.invly, P.ly);
+        const double rzij = minimage(rz - q[2 * np + j], P.invlz, P.lz);
+        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rxij, rxij), __dmul_rn(ryij, ryij)),
+                                    __dmul_rn(rzij, rzij));
+        if (j == i || r2 >= P.cutoff2 || r2 == 0.0) continue;
+        const double f = c1 * (rsqrt(r2) - c2);
+        fx += f * rxij;
+        fy += f * ryij;
+        fz += f * rzij;
       }
+    }
+  } else if (P.verlet && on) {
+    const double c1 = 2.0 * P.soft_eps / P.cutoff, c2 = 1.0 / P.cutoff;
+    const int n = R.vl_cnt[i];
+    for (int k = a; k < n; k += 4) {
+      const int j = R.vl_idx[(size_t)k * np + i];
+      const double rxij = minimage(rx - q[j], P.invlx, P.lx);
+      const double ryij = minimage(ry - q[np + j], P.invly, P.ly);
+      const double rzij = minimage(rz - q[2 * np + j], P.invlz, P.lz);
+      const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rxij, rxij), __dmul_rn(ryij, ryij)),
+                                  __dmul_rn(rzij, rzij));
+      if (r2 >= P.cutoff2 || r2 == 0.0) continue;
+      const double f = c1 * (rsqrt(r2) - c2);
+      fx += f * rxij;
+      fy += f * ryij;
+      fz += f * rzij;
     }
   }
 #pragma unroll
