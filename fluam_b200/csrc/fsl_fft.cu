@@ -56,6 +56,17 @@ struct FftPlan {
   int plane_pb = 0, plane_threads = 0;      // planes per block, threads per block
   int z_kx = 0, z_ky = 0, z_threads = 0;    // zsolve tile and threads per block
   size_t smem_plane_r = 0, smem_z_r = 0;
+  // tile candidates of the register z pass (same arithmetic, other (kx, ky)
+  // tiles per block); the first is the default, fft_autotune picks one
+  struct ZCand {
+    void (*k[2])(RepSrc, Rep, const float2*, const float*, const float*, const float*, const float2*,
+                 const float2*, const float2*);
+    int kx, ky, threads;
+    size_t smem;
+  } zc[4];
+  int nzc = 0;
+  bool tuned = false;
+  float zc_us[4] = {};  // measured time per candidate (us per launch)
 };
 
 static bool factorize(int n, Radices& R) {
@@ -709,14 +720,27 @@ static void pick_plane_r(FftPlan* fp) {
   fp->smem_plane_r = sizeof(float2) * (N + (size_t)PB * plane_buf<N, R, T>());
 }
 
+static void use_zcand(FftPlan* fp, int i) {
+  const FftPlan::ZCand& c = fp->zc[i];
+  fp->zsolve_r[0] = c.k[0];
+  fp->zsolve_r[1] = c.k[1];
+  fp->z_kx = c.kx;
+  fp->z_ky = c.ky;
+  fp->z_threads = c.threads;
+  fp->smem_z_r = c.smem;
+}
+
 template <int MZ, int R, int T, int KX, int KY>
 static void pick_z_r(FftPlan* fp) {
-  fp->zsolve_r[0] = k_zsolve_r<false, MZ, R, T, KX, KY>;
-  fp->zsolve_r[1] = k_zsolve_r<true, MZ, R, T, KX, KY>;
-  fp->z_kx = KX;
-  fp->z_ky = KY;
-  fp->z_threads = 3 * KX * KY * T;
-  fp->smem_z_r = sizeof(float2) * (MZ + (size_t)3 * KX * KY * LineGeom<R, T>::LS);
+  if (fp->nzc >= 4) return;
+  FftPlan::ZCand& c = fp->zc[fp->nzc++];
+  c.k[0] = k_zsolve_r<false, MZ, R, T, KX, KY>;
+  c.k[1] = k_zsolve_r<true, MZ, R, T, KX, KY>;
+  c.kx = KX;
+  c.ky = KY;
+  c.threads = 3 * KX * KY * T;
+  c.smem = sizeof(float2) * (MZ + (size_t)3 * KX * KY * LineGeom<R, T>::LS);
+  if (fp->nzc == 1) use_zcand(fp, 0);
 }
 
 // Register-pass shapes per edge: N = R x T; planes per block; z tiles.
@@ -741,17 +765,37 @@ static void pick_register_kernels(const Params& P, FftPlan* fp) {
   switch (P.mz) {
     case 16: pick_z_r<16, 16, 1, 9, 8>(fp); break;
     case 24: pick_z_r<24, 24, 1, 13, 8>(fp); break;
-    case 32: pick_z_r<32, 16, 2, 17, 4>(fp); break;
+    case 32:
+      pick_z_r<32, 16, 2, 17, 4>(fp);
+      pick_z_r<32, 16, 2, 9, 8>(fp);
+      break;
     case 40: pick_z_r<40, 8, 5, 21, 2>(fp); break;
-    case 48: pick_z_r<48, 12, 4, 25, 1>(fp); break;
+    case 48:
+      pick_z_r<48, 12, 4, 25, 1>(fp);
+      pick_z_r<48, 12, 4, 13, 2>(fp);
+      break;
     case 56: pick_z_r<56, 8, 7, 29, 1>(fp); break;
-    case 64: pick_z_r<64, 16, 4, 33, 1>(fp); break;
+    case 64:
+      pick_z_r<64, 16, 4, 33, 1>(fp);
+      pick_z_r<64, 16, 4, 17, 2>(fp);
+      pick_z_r<64, 16, 4, 8, 4>(fp);
+      break;
     case 72: pick_z_r<72, 12, 6, 19, 1>(fp); break;
     case 80: pick_z_r<80, 20, 4, 21, 1>(fp); break;
     case 88: pick_z_r<88, 8, 11, 9, 1>(fp); break;
-    case 96: pick_z_r<96, 24, 4, 25, 1>(fp); break;
-    case 128: pick_z_r<128, 16, 8, 8, 2>(fp); break;
-    case 256: pick_z_r<256, 16, 16, 8, 1>(fp); break;
+    case 96:
+      pick_z_r<96, 24, 4, 25, 1>(fp);
+      pick_z_r<96, 24, 4, 13, 2>(fp);
+      break;
+    case 128:
+      pick_z_r<128, 16, 8, 8, 2>(fp);
+      pick_z_r<128, 16, 8, 13, 1>(fp);
+      pick_z_r<128, 16, 8, 4, 2>(fp);
+      break;
+    case 256:
+      pick_z_r<256, 16, 16, 8, 1>(fp);
+      pick_z_r<256, 16, 16, 4, 2>(fp);
+      break;
     default: break;
   }
 }
@@ -895,8 +939,16 @@ FftPlan* fft_plan_create(const Params& P) {
         !(allow((const void*)fp->plane_fwd_r[v], fp->smem_plane_r) &&
           allow((const void*)fp->plane_inv_r[v], fp->smem_plane_r)))
       fp->plane_fwd_r[0] = fp->plane_fwd_r[1] = fp->plane_inv_r[0] = fp->plane_inv_r[1] = nullptr;
-    if (fp->zsolve_r[0] && !allow((const void*)fp->zsolve_r[v], fp->smem_z_r))
-      fp->zsolve_r[0] = fp->zsolve_r[1] = nullptr;
+  }
+  {
+    // keep the z candidates whose shared memory fits
+    int kept = 0;
+    for (int i = 0; i < fp->nzc; ++i)
+      if (allow((const void*)fp->zc[i].k[0], fp->zc[i].smem) && allow((const void*)fp->zc[i].k[1], fp->zc[i].smem))
+        fp->zc[kept++] = fp->zc[i];
+    fp->nzc = kept;
+    if (kept) use_zcand(fp, 0);
+    else fp->zsolve_r[0] = fp->zsolve_r[1] = nullptr;
   }
   cudaGetLastError();
   // the tables went up with plain copies on the default stream; the step
@@ -940,6 +992,40 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
   else
     fp->zsolve[0]<<<gz, kFftThreads, fp->smem_z, s>>>(B.src(), Rep{}, fp->rz, fp->twz, fp->sx, fp->sy,
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
+}
+
+// Times the z-pass tile candidates on the class's own spectra (an in-place
+// transform and solve of whatever they hold: the next step rewrites them) and
+// keeps the fastest.  Every candidate computes the same bits, so the choice
+// does not change results.  Once per plan, outside graph capture.
+void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s) {
+  if (!fp || fp->tuned) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  fp->tuned = true;
+  if (fp->nzc < 2 || B.nrep == 0 || B.prec == PREC_F64 || !fp->zsolve_r[0]) return;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    cudaGetLastError();
+    return;
+  }
+  int best = 0;
+  for (int i = 0; i < fp->nzc; ++i) {
+    use_zcand(fp, i);
+    zsolve(B, fp, dim3(1), s);  // warm-up
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; ++r) zsolve(B, fp, dim3(1), s);
+    cudaEventRecord(e1, s);
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = 1e9f;
+    fp->zc_us[i] = ms * 1000.f / 3.f;
+    if (fp->zc_us[i] < fp->zc_us[best]) best = i;
+  }
+  use_zcand(fp, best);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
 }
 
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,

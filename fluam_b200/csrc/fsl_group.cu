@@ -676,6 +676,9 @@ void group_enqueue_step(Group& g) {
     return;
   }
   const int pk = B.max_np > 0 ? 1 : 0;
+  // the z-pass tile of this size class, timed on its own buffers (first
+  // uncaptured step only)
+  if (g.key.scheme <= FSL_SCHEME_FIRST_ORDER) fft_autotune(g.fft, B, s);
   // remembers the first stage whose launch was refused, for the message
   auto chk = [&](const char* stage) {
     if (!g.fail_stage && cudaPeekAtLastError() != cudaSuccess) g.fail_stage = stage;

@@ -648,6 +648,9 @@ void fft_plan_destroy(FftPlan* fp);
 // v = solve(W).  W = f + nfac div(stress 1 [+ stress 2 when nsets == 2]) is
 // built from the spread field (which is cleared on the way) and the noise
 // into Rep::wbuf, unless w_given, in which case Rep::wbuf already holds W.
+// Picks the fastest z-pass tile of the plan's candidates on B's buffers
+// (once per plan; no-op under stream capture).
+void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s);
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof = nullptr);
 }  // namespace fsl
