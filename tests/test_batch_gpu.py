@@ -160,3 +160,35 @@ def test_batch_large_planes_equal_alone(fsl):
         qa, Fa, _ = run_alone(fsl, cfg, q, 2)
         np.testing.assert_array_equal(b.positions(i), qa)
     b.close()
+
+
+def test_batch_mixed_pair_paths_equal_alone(fsl):
+    """One size class holding a Verlet-list instance (soft), a cell-list one
+    (LJ table, on a lattice), one without pair forces and a dense soft one
+    that overflows its list into cell mode: every instance bitwise equal to
+    the same instance alone, over steps with list rebuilds."""
+    L = (20.0,) * 3
+    g = np.arange(6) * 3.3 - 8.25
+    lattice = np.stack(np.meshgrid(g, g, g, indexing="ij")).reshape(3, -1)
+    rng = np.random.default_rng(5)
+    dense = rng.uniform(-3.0, 3.0, (3, 600))
+    cases = [
+        (fsl.make_config((20,) * 3, L, kT=1.0, dt=0.02, cutoff=1.5, kernel=4, pair=fsl.PAIR_SOFT, seed=31),
+         rng.uniform(-10, 10, (3, 300))),
+        (fsl.make_config((20,) * 3, L, kT=0.01, dt=0.01, cutoff=1.5, kernel=4, pair=fsl.PAIR_TABLE_LJ, seed=32),
+         lattice),
+        (fsl.make_config((20,) * 3, L, kT=0.01, dt=0.01, cutoff=1.5, kernel=4, pair=fsl.PAIR_NONE, seed=33),
+         rng.uniform(-10, 10, (3, 100))),
+        (fsl.make_config((20,) * 3, L, kT=0.01, dt=0.01, cutoff=1.5, kernel=4, pair=fsl.PAIR_SOFT, seed=34),
+         dense),
+    ]
+    b = fsl.Batch([c for c, _ in cases], [q for _, q in cases])
+    assert b.info()["classes"] == 1
+    b.step(12)
+    b.sync()
+    for i, (cfg, q) in enumerate(cases):
+        qa, Fa, sa = run_alone(fsl, cfg, q, 12)
+        np.testing.assert_array_equal(b.positions(i), qa)
+        np.testing.assert_array_equal(b.forces(i), Fa)
+        assert b.status(i)["error_bits"] == 0 and sa["error_bits"] == 0
+    b.close()
