@@ -229,19 +229,6 @@ __device__ __forceinline__ int stencil_base(const Params& P, int d, int face, do
   return cellidx(minimage(r, invL, L), invd, m);
 }
 
-// The grid coordinate that stencil_base truncates (before the int cast of
-// cellidx), for the cheap test of the RFD drift.
-__device__ __forceinline__ double stencil_coord(const Params& P, int d, int face, double posc) {
-  const int m = d == 0 ? P.mx : (d == 1 ? P.my : P.mz);
-  const double h = d == 0 ? P.dx : (d == 1 ? P.dy : P.dz);
-  const double invd = d == 0 ? P.invdx : (d == 1 ? P.invdy : P.invdz);
-  const double L = d == 0 ? P.lx : (d == 1 ? P.ly : P.lz);
-  const double invL = d == 0 ? P.invlx : (d == 1 ? P.invly : P.invlz);
-  const double off = face ? __dmul_rn(0.5, h) : 0.0;
-  double r = P.kernel == 3 ? __dsub_rn(posc, off) : __dsub_rn(__dsub_rn(posc, off), __dmul_rn(0.5, h));
-  return __dadd_rn(__dmul_rn(minimage(r, invL, L), invd), __dmul_rn(0.5, (double)m));
-}
-
 // Warp-shared stencil of one particle for all three components.  Per
 // dimension d there are two node families: cell centres (components with
 // comp != d) and faces (comp == d); with n nodes each that is 6n values,

@@ -854,25 +854,13 @@ __device__ __forceinline__ void rfd_drift(const Params& P, const Rep& R, int i, 
   }
   QuadStencil<KN> S;
   if (P.rfd != 1) {
-    // lane a checks the node families a and a + 4 of the six: first whether
-    // the grid coordinate of q lies farther than the displacement (plus a
-    // margin far above the rounding) from an integer and from the wrap
-    // points, so that both displaced positions truncate to its base; else
-    // the bases of the two displaced positions themselves
+    // lane a checks the node families a and a + 4 of the six
     int same = 1;
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       const int fd = a + 4 * r;
       if (fd < 6) {
         const int f = fd / 3, d = fd - 3 * f;
-        const double xq = d == 0 ? pos[0] : (d == 1 ? pos[1] : pos[2]);
-        const double wd = d == 0 ? W[0] : (d == 1 ? W[1] : W[2]);
-        const double invd = d == 0 ? P.invdx : (d == 1 ? P.invdy : P.invdz);
-        const int m = d == 0 ? P.mx : (d == 1 ? P.my : P.mz);
-        const double u = stencil_coord(P, d, f, xq);
-        const double e = 0.5 * kRfdDelta * fabs(wd) * invd + 1e-9;
-        const double fl = floor(u);
-        if (u - e > fl && u + e < fl + 1.0 && u - e > 0.0 && u + e < (double)m) continue;
         const double x = d == 0 ? pp[0] : (d == 1 ? pp[1] : pp[2]);
         const double y = d == 0 ? pm[0] : (d == 1 ? pm[1] : pm[2]);
         same &= stencil_base(P, d, f, x) == stencil_base(P, d, f, y);
