@@ -20,7 +20,7 @@ EXE = os.path.join(HERE, "fluam")
 CU_SOURCES = ["fsl_particles.cu", "fsl_fft.cu", "fsl_group.cu", "fsl_api.cu", "fsl_batch.cu", "fsl_server.cu", "fsl_noalloc.cu",
               "fsl_fp64.cu", "fsl_q2d.cu", "fsl_inc.cu"]
 CPP_SOURCES = ["fsl_datamain.cpp"]
-HEADERS = ["fsl_internal.cuh", "fsl_group.cuh", "fsl_fft_reg.cuh"]
+HEADERS = ["fsl_internal.cuh", "fsl_group.cuh", "fsl_fft_reg.cuh", "fsl_fft_lines.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

@@ -19,6 +19,8 @@
 // j > m/2 cancels between gradient and shift), so the real-to-complex form
 // equals the reference's Re(IFFT(...)) up to rounding.
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <cstdio>
 #include <vector>
 
@@ -32,6 +34,8 @@ struct Radices {
   int nst;
   int r[14];
 };
+
+constexpr int kMaxZCand = 6;
 
 struct FftPlan {
   Radices rx, ry, rz;
@@ -54,6 +58,16 @@ struct FftPlan {
   void (*plane_inv_r[2])(RepSrc, Rep, const float2*) = {};
   void (*zsolve_r[2])(RepSrc, Rep, const float2*, const float*, const float*, const float*,
                       const float2*, const float2*, const float2*) = {};
+  // the same transform as five passes of warp tasks (fsl_fft_lines.cuh);
+  // null where the edge's lines do not fit in a warp
+  void (*line_xf[2])(RepSrc, Rep, const float2*) = {};
+  void (*line_yf[2])(RepSrc, Rep, const float2*) = {};
+  void (*line_yi[2])(RepSrc, Rep, const float2*) = {};
+  void (*line_xi[2])(RepSrc, Rep, const float2*) = {};
+  int line_lw = 0;          // lines per warp
+  size_t smem_lines = 0;
+  bool use_lines = false;   // the five-pass schedule (picked by fft_autotune)
+  float sched_us[2] = {};   // measured solve transform time: plane, lines
   int plane_pb = 0, plane_threads = 0;      // planes per block, threads per block
   int z_kx = 0, z_ky = 0, z_threads = 0;    // zsolve tile and threads per block
   size_t smem_plane_r = 0, smem_z_r = 0;
@@ -64,10 +78,10 @@ struct FftPlan {
                  const float2*, const float2*);
     int kx, ky, threads;
     size_t smem;
-  } zc[4];
+  } zc[kMaxZCand];
   int nzc = 0;
   bool tuned = false;
-  float zc_us[4] = {};  // measured time per candidate (us per launch)
+  float zc_us[kMaxZCand] = {};  // measured time per candidate (us per launch)
 };
 
 static bool factorize(int n, Radices& R) {
@@ -708,17 +722,43 @@ __global__ void __launch_bounds__(kFftThreads)
 }
 
 #include "fsl_fft_reg.cuh"
+#include "fsl_fft_lines.cuh"
 
 // ------------------------------------------------------------ host side ---
 template <int N, int R, int T, int PB>
 static void pick_plane_r(FftPlan* fp) {
+  fp->plane_pb = PB;
+  fp->plane_threads = PB * (N / 2) * T;
+  if constexpr (T > 1 && 32 % T == 0) {
+    fp->line_xf[0] = k_fft_xf<false, N, R, T>;
+    fp->line_xf[1] = k_fft_xf<true, N, R, T>;
+    fp->line_yf[0] = k_fft_y<false, N, R, T, -1>;
+    fp->line_yf[1] = k_fft_y<true, N, R, T, -1>;
+    fp->line_yi[0] = k_fft_y<false, N, R, T, +1>;
+    fp->line_yi[1] = k_fft_y<true, N, R, T, +1>;
+    fp->line_xi[0] = k_fft_xi<false, N, R, T>;
+    fp->line_xi[1] = k_fft_xi<true, N, R, T>;
+    fp->line_lw = 32 / T;
+    fp->smem_lines = sizeof(float2) * (N + (size_t)kLineWarps * (32 / T) * LineGeom<R, T>::LS);
+  }
   fp->plane_fwd_r[0] = k_plane_fwd_r<false, N, R, T, PB>;
   fp->plane_fwd_r[1] = k_plane_fwd_r<true, N, R, T, PB>;
   fp->plane_inv_r[0] = k_plane_inv_r<false, N, R, T, PB>;
   fp->plane_inv_r[1] = k_plane_inv_r<true, N, R, T, PB>;
-  fp->plane_pb = PB;
-  fp->plane_threads = PB * (N / 2) * T;
   fp->smem_plane_r = sizeof(float2) * (N + (size_t)PB * plane_buf<N, R, T>());
+}
+
+// FLUAMSL_FFT_SCHEDULE=plane or =lines fixes the transform schedule of the
+// register path (0: picked by fft_autotune, 1: plane kernels, 2: five passes)
+static int sched_env() {
+  static const int v = [] {
+    const char* e = getenv("FLUAMSL_FFT_SCHEDULE");
+    if (!e) return 0;
+    if (!strcmp(e, "plane")) return 1;
+    if (!strcmp(e, "lines")) return 2;
+    return 0;
+  }();
+  return v;
 }
 
 static void use_zcand(FftPlan* fp, int i) {
@@ -733,7 +773,7 @@ static void use_zcand(FftPlan* fp, int i) {
 
 template <int MZ, int R, int T, int KX, int KY>
 static void pick_z_r(FftPlan* fp) {
-  if (fp->nzc >= 4) return;
+  if (fp->nzc >= kMaxZCand) return;
   FftPlan::ZCand& c = fp->zc[fp->nzc++];
   c.k[0] = k_zsolve_r<false, MZ, R, T, KX, KY>;
   c.k[1] = k_zsolve_r<true, MZ, R, T, KX, KY>;
@@ -792,6 +832,8 @@ static void pick_register_kernels(const Params& P, FftPlan* fp) {
       pick_z_r<128, 16, 8, 8, 2>(fp);
       pick_z_r<128, 16, 8, 13, 1>(fp);
       pick_z_r<128, 16, 8, 4, 2>(fp);
+      pick_z_r<128, 16, 8, 4, 1>(fp);
+      pick_z_r<128, 16, 8, 2, 2>(fp);
       break;
     case 256:
       pick_z_r<256, 16, 16, 8, 1>(fp);
@@ -941,6 +983,12 @@ FftPlan* fft_plan_create(const Params& P) {
           allow((const void*)fp->plane_inv_r[v], fp->smem_plane_r)))
       fp->plane_fwd_r[0] = fp->plane_fwd_r[1] = fp->plane_inv_r[0] = fp->plane_inv_r[1] = nullptr;
   }
+  for (int v = 0; v < 2; ++v) {
+    if (fp->line_xf[0] &&
+        !(allow((const void*)fp->line_xf[v], fp->smem_lines) && allow((const void*)fp->line_yf[v], fp->smem_lines) &&
+          allow((const void*)fp->line_yi[v], fp->smem_lines) && allow((const void*)fp->line_xi[v], fp->smem_lines)))
+      fp->line_xf[0] = fp->line_xf[1] = nullptr;
+  }
   {
     // keep the z candidates whose shared memory fits
     int kept = 0;
@@ -951,6 +999,11 @@ FftPlan* fft_plan_create(const Params& P) {
     if (kept) use_zcand(fp, 0);
     else fp->zsolve_r[0] = fp->zsolve_r[1] = nullptr;
   }
+  // the five-pass schedule needs the register plane shapes (the same
+  // packing) and the register z pass; it starts as the default where it
+  // exists, and fft_autotune keeps whichever is faster
+  if (!fp->plane_fwd_r[0] || !fp->zsolve_r[0]) fp->line_xf[0] = fp->line_xf[1] = nullptr;
+  fp->use_lines = fp->line_xf[0] != nullptr && sched_env() != 1;
   cudaGetLastError();
   // the tables went up with plain copies on the default stream; the step
   // runs on other streams
@@ -995,16 +1048,63 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
                                                      fp->sz, fp->ex, fp->ey, fp->ez);
 }
 
+// The register path's transforms and solve with the plan's schedule: the
+// plane kernels (3 launches) or the five passes of warp tasks.
+static void reg_transform(const Batch& B, const FftPlan* fp, cudaStream_t s, Prof& pr) {
+  const int nrep = B.nrep;
+  if (fp->use_lines) {
+    const long lines = 3L * B.mz * (B.mx / 2);
+    const long per_block = (long)kLineWarps * fp->line_lw;
+    const dim3 g((unsigned)((lines + per_block - 1) / per_block), 1, nrep);
+    const int tb = kLineWarps * 32;
+    const size_t sm = fp->smem_lines;
+    auto go = [&](void (*const* k)(RepSrc, Rep, const float2*)) {
+      if (B.one) k[1]<<<g, tb, sm, s>>>(RepSrc{}, *B.one, fp->twx);
+      else k[0]<<<g, tb, sm, s>>>(B.src(), Rep{}, fp->twx);
+    };
+    pr.mark(s, "fft_x");
+    go(fp->line_xf);
+    pr.mark(s, "fft_y");
+    go(fp->line_yf);
+    pr.mark(s, "zsolve");
+    zsolve(B, fp, dim3(1), s);
+    pr.mark(s, "fft_y");
+    go(fp->line_yi);
+    pr.mark(s, "fft_x");
+    go(fp->line_xi);
+    pr.count(5);
+    return;
+  }
+  dim3 gp((3 * B.mz + fp->plane_pb - 1) / fp->plane_pb, 1, nrep);
+  const int tb = fp->plane_threads;
+  pr.mark(s, "plane_fwd");
+  if (B.one)
+    fp->plane_fwd_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
+  else
+    fp->plane_fwd_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
+  pr.mark(s, "zsolve");
+  zsolve(B, fp, dim3((B.mxh + kZTile - 1) / kZTile, B.my, nrep), s);
+  pr.mark(s, "plane_inv");
+  if (B.one)
+    fp->plane_inv_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
+  else
+    fp->plane_inv_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
+  pr.count(3);
+}
+
 // Times the z-pass tile candidates on the class's own spectra (an in-place
 // transform and solve of whatever they hold: the next step rewrites them) and
-// keeps the fastest.  Every candidate computes the same bits, so the choice
-// does not change results.  Once per plan, outside graph capture.
+// keeps the fastest; then, where the edge has both, the plane schedule
+// against the five-pass one (on the class's W, spectra and velocity buffers,
+// which the step rewrites before reading).  Every candidate computes the
+// same bits, so the choice does not change results.  Once per plan, outside
+// graph capture.
 void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s) {
   if (!fp || fp->tuned) return;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
   fp->tuned = true;
-  if (fp->nzc < 2 || B.nrep == 0 || B.prec == PREC_F64 || !fp->zsolve_r[0]) return;
+  if (B.nrep == 0 || B.prec == PREC_F64 || !fp->zsolve_r[0]) return;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
     if (e0) cudaEventDestroy(e0);
@@ -1014,7 +1114,7 @@ void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s) {
   // three rounds over the candidates in turn (clock ramp-up and cold caches
   // hit every candidate alike), five launches each, the fastest round kept
   for (int i = 0; i < fp->nzc; ++i) fp->zc_us[i] = 1e30f;
-  for (int round = 0; round < 3; ++round)
+  for (int round = 0; round < 3 && fp->nzc > 1; ++round)
     for (int i = 0; i < fp->nzc; ++i) {
       use_zcand(fp, i);
       zsolve(B, fp, dim3(1), s);  // warm-up
@@ -1029,6 +1129,22 @@ void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s) {
   for (int i = 1; i < fp->nzc; ++i)
     if (fp->zc_us[i] < fp->zc_us[best]) best = i;
   use_zcand(fp, best);
+  if (fp->line_xf[0] && sched_env() == 0) {
+    Prof none;
+    fp->sched_us[0] = fp->sched_us[1] = 1e30f;
+    for (int round = 0; round < 3; ++round)
+      for (int sc = 0; sc < 2; ++sc) {
+        fp->use_lines = sc == 1;
+        reg_transform(B, fp, s, none);  // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 5; ++r) reg_transform(B, fp, s, none);
+        cudaEventRecord(e1, s);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = 1e9f;
+        fp->sched_us[sc] = std::min(fp->sched_us[sc], ms * 1000.f / 5.f);
+      }
+    fp->use_lines = fp->sched_us[1] < fp->sched_us[0];
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaGetLastError();
@@ -1057,21 +1173,7 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_giv
     pr.count(1);
   }
   if (fp->plane_fwd_r[0]) {
-    dim3 gp((3 * B.mz + fp->plane_pb - 1) / fp->plane_pb, 1, nrep);
-    const int tb = fp->plane_threads;
-    pr.mark(s, "plane_fwd");
-    if (B.one)
-      fp->plane_fwd_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
-    else
-      fp->plane_fwd_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
-    pr.mark(s, "zsolve");
-    zsolve(B, fp, dim3((B.mxh + kZTile - 1) / kZTile, B.my, nrep), s);
-    pr.mark(s, "plane_inv");
-    if (B.one)
-      fp->plane_inv_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
-    else
-      fp->plane_inv_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
-    pr.count(3);
+    reg_transform(B, fp, s, pr);
     return;
   }
   if (fp->use_plane) {

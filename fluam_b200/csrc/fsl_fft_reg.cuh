@@ -513,3 +513,31 @@ __global__ void __launch_bounds__(3 * KX * KY * T)
     }
   }
 }
+
+// ------------------------------------------------------ warp-local lines ---
+// Helpers of the passes whose lines are held by T consecutive lanes of one
+// warp (T divides 32, fsl_fft_lines.cuh).
+
+// lanes of this thread's line within its warp
+template <int T>
+__device__ __forceinline__ unsigned line_mask() {
+  if constexpr (T >= 32) return 0xffffffffu;
+  else return ((1u << T) - 1u) << ((threadIdx.x & 31) & ~(T - 1));
+}
+
+// Stores of one real row segment: the RT consecutive (EVEN layout) values
+// out[0..RT)[b] of component sel (0: .x, 1: .y) at x0.
+template <int RT, int T>
+__device__ __forceinline__ void store_row_run(float* dst, const float2 (&out)[RT][T], int b, int sel) {
+  float s[RT];
+#pragma unroll
+  for (int j = 0; j < RT; ++j) s[j] = sel ? out[j][b].y : out[j][b].x;
+  if constexpr (RT == 2) {
+    *reinterpret_cast<float2*>(dst) = make_float2(s[0], s[1]);
+  } else if constexpr (RT == 4) {
+    *reinterpret_cast<float4*>(dst) = make_float4(s[0], s[1], s[2], s[3]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < RT; ++j) dst[j] = s[j];
+  }
+}
