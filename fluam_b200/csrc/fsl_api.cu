@@ -293,7 +293,7 @@ int fsl_set_step(fsl_handle* h, uint64_t step) {
 int fsl_clear_errors(fsl_handle* h) {
   if (!h) return errorf(FSL_E_ARG, "null handle");
   FSL_TRY(cudaSetDevice(h->exec.device));
-  FSL_TRY(cudaMemsetAsync(rep(h).err, 0, sizeof(int) * 4, h->exec.stream));
+  if (int rc = fsl::slot_clear_errors(h->slot, h->exec.stream)) return rc;
   FSL_TRY(cudaStreamSynchronize(h->exec.stream));
   return FSL_OK;
 }

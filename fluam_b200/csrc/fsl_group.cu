@@ -398,6 +398,13 @@ int slot_read_observables(const Slot& s, cudaStream_t st, fsl_observables* out) 
   return FSL_OK;
 }
 
+int slot_clear_errors(Slot& s, cudaStream_t st) {
+  FSL_TRY(cudaMemsetAsync(s.r.err, 0, sizeof(int) * 4, st));
+  launch_reset_lists(s.r, st);
+  FSL_TRY(cudaGetLastError());
+  return slot_force_lists(s, st);
+}
+
 int slot_force_lists(Slot& s, cudaStream_t st) {
   static const uint64_t flags[3] = {0, 0, 1};
   FSL_TRY(cudaMemcpyAsync(s.r.vl_flag, flags, sizeof(flags), cudaMemcpyHostToDevice, st));
@@ -459,6 +466,7 @@ int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, c
   else
     FSL_TRY(cudaMemsetAsync(r.v, 0, sizeof(float) * 3 * (size_t)P.nc, st));
   FSL_TRY(cudaMemsetAsync(r.err, 0, sizeof(int) * 4, st));
+  if (r.bar) FSL_TRY(cudaMemsetAsync(r.bar, 0, sizeof(unsigned) * 2, st));
   FSL_TRY(cudaMemsetAsync(r.t, 0, sizeof(uint64_t), st));
   if (int rc = slot_reset_observables(s, st)) return rc;
   if (int rc = slot_force_lists(s, st)) return rc;
@@ -687,7 +695,7 @@ void group_enqueue_step(Group& g) {
     pr.mark(s, "cells");
     // (one cooperative launch for a single instance; on the Verlet path the
     // list kernels return at once unless a rebuild is due)
-    launch_pair_lists(B, which, s);
+    if (launch_pair_lists(B, which, s) != cudaSuccess && !g.fail_stage) g.fail_stage = "cells";
     pr.count(!pk ? 0 : (B.one && B.one->bar) ? 1 : 5 + (B.has_vl ? 1 : 0));
     chk("cells");
     pr.mark(s, "forces");

@@ -70,6 +70,9 @@ int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, c
 // launch_pair_lists builds the cell list whatever the path (the component
 // entry points).
 int slot_force_lists(Slot& s, cudaStream_t st);
+// error word cleared, cell-list counters and barrier reset, lists rebuilt at
+// the next force evaluation
+int slot_clear_errors(Slot& s, cudaStream_t st);
 int slot_mark_moved(Slot& s, cudaStream_t st);
 int slot_request_lists(Slot& s, cudaStream_t st);
 // q0 := q, observables accumulators cleared (enqueued on st).

@@ -614,7 +614,10 @@ bool tile_eligible(const Params& P);
 void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStream_t s);
 // The cell list of force evaluation `which` and, for Verlet-list
 // instances, the pair list (each only where list_needed says so).
-void launch_pair_lists(const Batch& B, int which, cudaStream_t s);
+cudaError_t launch_pair_lists(const Batch& B, int which, cudaStream_t s);
+// The cell-list counters and the single-launch build's barrier cleared
+// (after an error, before lists are built again)
+void launch_reset_lists(const Rep& r, cudaStream_t s);
 // After positions were replaced from the host: flag a Verlet-list rebuild if
 // a particle moved more than skin / 2 from its reference position.
 void launch_moved_check(const Rep& r, cudaStream_t s);

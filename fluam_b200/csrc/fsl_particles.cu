@@ -7,6 +7,8 @@
 // through the block-offset table.  ONE = true compiles the single-instance
 // form, whose instance is a by-value parameter.
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 
 #include "fsl_internal.cuh"
 
@@ -189,10 +191,15 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(FSL_KARGS, int which)
   if (threadIdx.x == 0 && tile == (n + kScanTile - 1) / kScanTile - 1) start[n] = prefix + R.bsum[tile];
 }
 
+// The slot checks below keep every write inside the cell's bucket even when
+// the counts and starts disagree (a single-launch build whose grid barrier
+// gave up leaves them so); such a write is skipped and flagged.
 __device__ __forceinline__ void cell_scatter_one(const Rep& R, int i, int which) {
   const int* start = which && R.start1 ? R.start1 : R.start;
   int c = R.cell_of[i];
-  R.tmp[start[c] + atomicAdd(&R.fill[c], 1)] = i;
+  const int k = start[c] + atomicAdd(&R.fill[c], 1);
+  if (k >= start[c] && k < start[c + 1]) R.tmp[k] = i;
+  else set_err(R.err, 4);
 }
 
 template <bool ONE>
@@ -215,8 +222,12 @@ __device__ __forceinline__ void cell_rank_one(const Rep& R, int i, int which) {
   int s = start[c], e = start[c + 1];
   int rank = 0;
   for (int k = s; k < e; ++k) rank += R.tmp[k] < i;
-  sorted[s + rank] = i;
   R.fill[c] = 0;  // the scatter's slot counters, cleared for the next build
+  if (s + rank >= e) {  // counts and starts disagree (see cell_scatter_one)
+    set_err(R.err, 4);
+    return;
+  }
+  sorted[s + rank] = i;
   if (ws) {  // wrapped positions in cell order for the pair loop
     ws[s + rank] = R.qw[i];
     ws[P.np + s + rank] = R.qw[P.np + i];
@@ -488,17 +499,30 @@ void launch_moved_check(const Rep& r, cudaStream_t s) {
 // The cell list (and the Verlet list) of one instance in one cooperative
 // launch: the phases of the kernels above separated by grid barriers, so a
 // force evaluation that needs no rebuild costs one near-empty launch instead
-// of six.  The barrier spins with a bound; if it ever gives up (the blocks
-// are co-resident by the cooperative launch, so it should not) the instance's
-// error word gets FSL_ERRBIT_GRID.
+// of six.  The barrier spins with a bound (spin_limit waits of 64 ns); if it
+// gives up (the blocks are co-resident by the cooperative launch, so it
+// should not) the block sets FSL_ERRBIT_GRID in the instance's error word and
+// stops, and every other block stops at its next barrier.  The lists are then
+// incomplete but every access stays in bounds (the slot checks of the scatter
+// and rank phases); the build is skipped while the bit is set, and
+// fsl_clear_errors clears the counters and the barrier and requests a fresh
+// build.
 constexpr int kCoopThreads = 256;
+constexpr long kCoopSpinLimit = 20000000L;  // about a second
 
-__device__ void grid_barrier(const Rep& R) {
+__device__ __forceinline__ bool grid_aborted(const Rep& R) {
+  return (reinterpret_cast<volatile int*>(R.err)[ERR_BITS] & 4) != 0;
+}
+
+// false: this block must stop (its own wait gave up, or another block's did)
+__device__ bool grid_barrier(const Rep& R, long spin_limit) {
+  __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* gen = R.bar + 1;
     const unsigned g = *gen;
     __threadfence();
+    int ok = 1;
     if (atomicAdd(R.bar, 1u) == gridDim.x - 1) {
       R.bar[0] = 0u;
       __threadfence();
@@ -506,25 +530,29 @@ __device__ void grid_barrier(const Rep& R) {
     } else {
       long spins = 0;
       while (*gen == g) {
-        if (++spins > 20000000L) {  // about seconds: give up, flag it
+        if (++spins > spin_limit) {
           set_err(R.err, 4);
+          ok = 0;
           break;
         }
         __nanosleep(64);
       }
     }
     __threadfence();
+    s_ok = ok && !grid_aborted(R);
   }
   __syncthreads();
+  return s_ok != 0;
 }
 
-__global__ void __launch_bounds__(kCoopThreads) k_lists_coop(const __grid_constant__ Rep R, int which) {
+__global__ void __launch_bounds__(kCoopThreads) k_lists_coop(const __grid_constant__ Rep R, int which,
+                                                             long spin_limit) {
   const Params& P = R.P;
-  if (!R.active || P.np == 0 || !list_needed(R, which)) return;
+  if (!R.active || P.np == 0 || !list_needed(R, which) || grid_aborted(R)) return;
   const int np = P.np, nb = gridDim.x;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = nb * blockDim.x;
   for (int i = tid; i < np; i += nth) cell_count_one(R, i, which);
-  grid_barrier(R);
+  if (!grid_barrier(R, spin_limit)) return;
   // exclusive scan of the counts: block b takes a contiguous chunk, the
   // block totals go through bsum, the counts are cleared behind the read
   int* start = which && R.start1 ? R.start1 : R.start;
@@ -551,7 +579,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_lists_coop(const __grid_consta
     btot += wsum[w];
   }
   if (threadIdx.x == 0) R.bsum[blockIdx.x] = btot;
-  grid_barrier(R);
+  if (!grid_barrier(R, spin_limit)) return;
   if (threadIdx.x == 0) {
     int off = 0;
     for (int b = 0; b < (int)blockIdx.x; ++b) off += R.bsum[b];
@@ -566,12 +594,12 @@ __global__ void __launch_bounds__(kCoopThreads) k_lists_coop(const __grid_consta
     R.cnt[c] = 0;
     run += v;
   }
-  grid_barrier(R);
+  if (!grid_barrier(R, spin_limit)) return;
   for (int i = tid; i < np; i += nth) cell_scatter_one(R, i, which);
-  grid_barrier(R);
+  if (!grid_barrier(R, spin_limit)) return;
   for (int i = tid; i < np; i += nth) cell_rank_one(R, i, which);
   if (!P.verlet) return;
-  grid_barrier(R);
+  if (!grid_barrier(R, spin_limit)) return;
   if (R.vl_flag[2] == 3) return;  // cell mode: no pair list
   for (int i = tid; i < np; i += nth) vl_build_one(R, i, which);
 }
@@ -676,24 +704,35 @@ void launch_forces(const Batch& B, int which, cudaStream_t s) {
   if (B.has_vl) FSL_GO(k_forces_vl, part_blocks(B, KIND_T4), kPartThreads, 0, s, B, which);
 }
 
-// Blocks of the cooperative build: all co-resident (cached per device).
+// Blocks of the cooperative build: all co-resident, computed once per device
+// (host threads on different devices each read their own entry).
 static unsigned coop_blocks() {
-  static int dev_cached = -1;
-  static unsigned blocks = 0;
+  constexpr int kMaxDev = 64;
+  static std::atomic<unsigned> cache[kMaxDev];
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev != dev_cached) {
-    int per_sm = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lists_coop, kCoopThreads, 0);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    long b = (long)per_sm * sms;
-    blocks = (unsigned)std::max(1L, std::min(b, (long)kCoopMaxBlocks));
-    dev_cached = dev;
+  if (dev >= 0 && dev < kMaxDev) {
+    const unsigned c = cache[dev].load(std::memory_order_relaxed);
+    if (c) return c;
   }
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lists_coop, kCoopThreads, 0);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long b = (long)per_sm * sms;
+  const unsigned blocks = (unsigned)std::max(1L, std::min(b, (long)kCoopMaxBlocks));
+  if (dev >= 0 && dev < kMaxDev) cache[dev].store(blocks, std::memory_order_relaxed);
   return blocks;
 }
 
-void launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
+// The wait bound of the cooperative build's grid barriers; the variable
+// FLUAMSL_COOP_SPIN_LIMIT overrides it (the failure-path test sets 0, so that
+// every wait gives up at once).
+static long coop_spin_limit() {
+  const char* e = getenv("FLUAMSL_COOP_SPIN_LIMIT");
+  return e && *e ? atol(e) : kCoopSpinLimit;
+}
+
+cudaError_t launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
   if (B.one && B.one->bar && B.max_np > 0) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(coop_blocks());
@@ -704,11 +743,32 @@ void launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_lists_coop, *B.one, which);
-    return;
+    return cudaLaunchKernelEx(&cfg, k_lists_coop, *B.one, which, coop_spin_limit());
   }
   launch_cells(B, which, s, false);
   if (B.max_np > 0 && B.has_vl) FSL_GO(k_vl_build, part_blocks(B, KIND_T1), kPartThreads, 0, s, B, which);
+  return cudaPeekAtLastError();
+}
+
+// After an error: the cell-list counters and the grid barrier of the
+// single-launch build back to zero (a build that gave up leaves them
+// partial).
+__global__ void k_reset_lists(const __grid_constant__ Rep R) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.P.mN; c += gridDim.x * blockDim.x) {
+    R.cnt[c] = 0;
+    R.fill[c] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && R.bar) {
+    R.bar[0] = 0u;
+    R.bar[1] = 0u;
+  }
+}
+
+void launch_reset_lists(const Rep& r, cudaStream_t s) {
+  if (!r.cnt) return;
+  unsigned b = blocks_for(r.P.mN, 256);
+  if (b > 1024) b = 1024;
+  k_reset_lists<<<std::max(b, 1u), 256, 0, s>>>(r);
 }
 
 // ------------------------------------------------------------ quad layout ---

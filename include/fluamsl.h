@@ -189,6 +189,11 @@ int fsl_get_observables(fsl_handle* h, fsl_observables* out);
 int fsl_reset_observables(fsl_handle* h);
 
 int fsl_set_step(fsl_handle* h, uint64_t step);
+/* Clears the error word.  It also clears the cell-list counters and the grid
+ * barrier of the single-launch list build and requests fresh lists at the
+ * next force evaluation, so an instance whose list build gave up
+ * (FSL_ERRBIT_GRID: the build is skipped until the bit is cleared) steps
+ * normally again afterwards. */
 int fsl_clear_errors(fsl_handle* h);
 /* Capture one step into a CUDA graph and replay it from then on (on by
  * default once the first step has run; 0 turns it off). */

@@ -93,3 +93,44 @@ def test_verlet_overflow_falls_back_to_cells(fsl):
             np.testing.assert_allclose(b.positions(), qa, rtol=0, atol=1e-12 * max(1.0, np.abs(qa).max()))
             Fa = a.forces()
             np.testing.assert_allclose(b.forces(), Fa, rtol=0, atol=1e-11 * max(1.0, np.abs(Fa).max()))
+
+
+def test_list_barrier_give_up_is_reported_and_recovers(fsl, monkeypatch):
+    """The single-launch list build's grid barrier waits with a bound.  With
+    the bound at zero (FLUAMSL_COOP_SPIN_LIMIT=0, read when the step is
+    enqueued) every wait gives up at once: the build stops in every block,
+    the instance reports FSL_ERRBIT_GRID through fsl_sync (FSL_E_KERNEL), and
+    after fsl_clear_errors the same instance steps to the same bits as a
+    fresh one."""
+    L = (32.0,) * 3
+    q = uniform_positions(256, L, 41)
+
+    def make():
+        cfg = fsl.make_config((32, 32, 32), L, kT=0.01, dt=0.01, cutoff=1.5, kernel=3,
+                              pair=fsl.PAIR_SOFT, seed=5)
+        g = fsl.StokesLimit(cfg, q)
+        g.set_graph(False)
+        return g
+
+    ref = make()
+    ref.step(1)
+    ref.sync()
+    q1 = ref.positions()
+    ref.close()
+
+    g = make()
+    monkeypatch.setenv("FLUAMSL_COOP_SPIN_LIMIT", "0")
+    g.step(1)
+    with pytest.raises(fsl._lib.FslError) as e:
+        g.sync()
+    assert e.value.code == -4
+    assert g.status()["error_bits"] & 4
+    monkeypatch.delenv("FLUAMSL_COOP_SPIN_LIMIT")
+    g.clear_errors()
+    g.set_positions(q)
+    g.set_step(0)
+    g.step(1)
+    g.sync()
+    assert g.status()["error_bits"] == 0
+    np.testing.assert_array_equal(g.positions(), q1)
+    g.close()
