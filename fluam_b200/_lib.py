@@ -20,7 +20,7 @@ PRECISION_FIXED64, PRECISION_FLOAT_ATOMIC, PRECISION_FP64 = 0, 1, 2
 
 # Every symbol include/fluamsl.h declares.
 EXPORTS = [
-    "fsl_config_defaults", "fsl_create", "fsl_load_bonds", "fsl_step", "fsl_sync",
+    "fsl_config_defaults", "fsl_create", "fsl_load_bonds", "fsl_load_bonds_directed", "fsl_step", "fsl_sync",
     "fsl_get_positions", "fsl_set_positions", "fsl_get_forces", "fsl_get_velocity",
     "fsl_get_velocity_f64", "fsl_set_velocity_f64",
     "fsl_get_status", "fsl_get_observables", "fsl_reset_observables", "fsl_set_step", "fsl_clear_errors", "fsl_set_graph", "fsl_stream",
@@ -140,6 +140,7 @@ def load(path=None):
     L.fsl_config_defaults.argtypes = [ctypes.POINTER(Config)]
     L.fsl_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int64, _D, ctypes.POINTER(_VP)]
     L.fsl_load_bonds.argtypes = [_VP, ctypes.c_int64, _I, _I, _D, _D, ctypes.c_int64, _I, _D, _D, _D]
+    L.fsl_load_bonds_directed.argtypes = L.fsl_load_bonds.argtypes
     L.fsl_step.argtypes = [_VP, ctypes.c_int64]
     L.fsl_sync.argtypes = [_VP]
     L.fsl_get_positions.argtypes = [_VP, _D]

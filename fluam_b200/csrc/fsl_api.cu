@@ -128,6 +128,17 @@ int fsl_load_bonds(fsl_handle* h, int64_t nbonds, const int32_t* bi, const int32
   return rc;
 }
 
+int fsl_load_bonds_directed(fsl_handle* h, int64_t nentries, const int32_t* bi, const int32_t* bj,
+                            const double* k, const double* r0, int64_t nfixed, const int32_t* fi,
+                            const double* fk, const double* fr0, const double* fxyz) {
+  if (!h) return errorf(FSL_E_ARG, "null handle");
+  FSL_TRY(cudaSetDevice(h->exec.device));
+  int rc = fsl::slot_bonds(h->slot, nentries, bi, bj, k, r0, nfixed, fi, fk, fr0, fxyz, h->exec.stream,
+                           true);
+  h->group.dirty = true;
+  return rc;
+}
+
 int fsl_set_graph(fsl_handle* h, int enable) {
   if (!h) return errorf(FSL_E_ARG, "null handle");
   h->exec.use_graph = enable != 0;

@@ -41,6 +41,7 @@ struct Run {
   int loadparticles = 0;
   std::string coordinates, outputname, bondfile;
   bool bonded = false;
+  int bond_version = 0;  // bondedForcesVersion: nonzero = the old file format
   // fluid output: saveFluid, saveVTK, savefreq, densfluid, pressureparameters
   int save_fluid = 0, save_vtk = 0;
   int64_t savefreq = 0;
@@ -180,10 +181,7 @@ int parse(const char* path, Run& r, std::string& err) {
         r.bonded = true;
         r.bondfile = vals[0];
       } else if (word == "bondedForcesVersion") {
-        if (I(0) != 0) {
-          err = "bondedForcesVersion != 0 (old bond file format) is not supported";
-          return FSL_E_INPUT;
-        }
+        r.bond_version = (int)I(0);
       } else if (word == "computeNonBondedForces") {
         c.nonbonded = (int)I(0);
       } else if (word == "extraMobility") {
@@ -392,6 +390,67 @@ bool read_bonds(const std::string& file, Bonds& b) {
     b.fxyz.push_back(y);
     b.fxyz.push_back(z);
   }
+  return (bool)f;
+}
+
+// The old bond-file format (bondedForcesVersion != 0,
+// src/initializeBondedForcesOldVersion.cpp:41-238): the particle-particle
+// count counts every bond twice, each line "i j k r0" acts on i only and the
+// lines are sorted by i; then the tethers "i k r0 x y z".  Deliberate
+// differences: an unsorted particle-particle list is an input error here
+// (the reference prints "bad sorting" and goes on with tables it never
+// filled), and a particle's tethers are grouped in file order (the
+// reference's first pass never updates its running index, so it misplaces
+// a particle's second and later tethers).
+bool read_bonds_old(const std::string& file, Bonds& b, std::string& why) {
+  std::ifstream f(file);
+  if (!f) {
+    why = "cannot open";
+    return false;
+  }
+  int64_t n = 0;
+  f >> n;
+  if (!f || n < 0) {
+    why = "bad particle-particle count";
+    return false;
+  }
+  int prev = -1;
+  for (int64_t k = 0; k < n; ++k) {
+    int i1, i2;
+    double ks, r0;
+    f >> i1 >> i2 >> ks >> r0;
+    if (!f) {
+      why = "short particle-particle list";
+      return false;
+    }
+    if (i1 < prev) {
+      why = "bad sorting in bonded Forces Particle-Particle";
+      return false;
+    }
+    prev = i1;
+    b.bi.push_back(i1);
+    b.bj.push_back(i2);
+    b.k.push_back(ks);
+    b.r0.push_back(r0);
+  }
+  int64_t nf = 0;
+  f >> nf;
+  if (!f || nf < 0) {
+    why = "bad particle-fixed point count";
+    return false;
+  }
+  for (int64_t k = 0; k < nf; ++k) {
+    int i1;
+    double ks, r0, x, y, z;
+    f >> i1 >> ks >> r0 >> x >> y >> z;
+    b.fi.push_back(i1);
+    b.fk.push_back(ks);
+    b.fr0.push_back(r0);
+    b.fxyz.push_back(x);
+    b.fxyz.push_back(y);
+    b.fxyz.push_back(z);
+  }
+  if (!f) why = "short particle-fixed point list";
   return (bool)f;
 }
 
@@ -696,14 +755,16 @@ extern "C" int fsl_run_data_main(const char* path) {
   }
   if (r.bonded) {
     Bonds b;
-    if (!read_bonds(r.bondfile, b)) {
-      std::cout << "ERROR reading bondedForces file " << r.bondfile << std::endl;
+    std::string why;
+    if (r.bond_version ? !read_bonds_old(r.bondfile, b, why) : !read_bonds(r.bondfile, b)) {
+      std::cout << "ERROR reading bondedForces file " << r.bondfile << (why.empty() ? "" : ": ")
+                << why << std::endl;
       fsl_destroy(h);
       return FSL_E_IO;
     }
-    rc = fsl_load_bonds(h, (int64_t)b.bi.size(), b.bi.data(), b.bj.data(), b.k.data(),
-                        b.r0.data(), (int64_t)b.fi.size(), b.fi.data(), b.fk.data(),
-                        b.fr0.data(), b.fxyz.data());
+    rc = (r.bond_version ? fsl_load_bonds_directed : fsl_load_bonds)(
+        h, (int64_t)b.bi.size(), b.bi.data(), b.bj.data(), b.k.data(), b.r0.data(),
+        (int64_t)b.fi.size(), b.fi.data(), b.fk.data(), b.fr0.data(), b.fxyz.data());
     if (rc) {
       std::cout << "ERROR: " << fsl_last_error() << std::endl;
       fsl_destroy(h);

@@ -476,7 +476,7 @@ int slot_reset(Slot& s, const Params& P, const double* q, const fsl_config& c, c
 
 int slot_bonds(Slot& s, int64_t nbonds, const int32_t* bi, const int32_t* bj, const double* k,
                const double* r0, int64_t nfixed, const int32_t* fi, const double* fk,
-               const double* fr0, const double* fxyz, cudaStream_t st) {
+               const double* fr0, const double* fxyz, cudaStream_t st, bool directed) {
   Rep& r = s.r;
   const int np = r.P.np;
   if (nbonds < 0 || nfixed < 0) return errorf(FSL_E_ARG, "negative bond count");
@@ -488,25 +488,29 @@ int slot_bonds(Slot& s, int64_t nbonds, const int32_t* bi, const int32_t* bj, co
   for (int64_t b = 0; b < nfixed; ++b)
     if (fi[b] < 0 || fi[b] >= np)
       return errorf(FSL_E_ARG, "tether %lld: particle index out of range", (long long)b);
-  // both endpoints store each particle-particle bond, in file order
+  // both endpoints store each particle-particle bond, in file order; a
+  // directed entry (the old bond-file format) is stored by bi only
   std::vector<int> pc(np, 0), po(np, 0), fc(np, 0), fo(np, 0), tmp(np, 0);
   for (int64_t b = 0; b < nbonds; ++b) {
     pc[bi[b]]++;
-    pc[bj[b]]++;
+    if (!directed) pc[bj[b]]++;
   }
   for (int64_t b = 0; b < nfixed; ++b) fc[fi[b]]++;
   for (int i = 1; i < np; ++i) {
     po[i] = po[i - 1] + pc[i - 1];
     fo[i] = fo[i - 1] + fc[i - 1];
   }
-  std::vector<int> idx(2 * nbonds);
-  std::vector<double> kk(2 * nbonds), rr(2 * nbonds);
+  const int64_t nent = directed ? nbonds : 2 * nbonds;  // stored entries
+  std::vector<int> idx(nent);
+  std::vector<double> kk(nent), rr(nent);
   for (int64_t b = 0; b < nbonds; ++b) {
     int i1 = bi[b], i2 = bj[b];
-    int p1 = po[i1] + tmp[i1]++, p2 = po[i2] + tmp[i2]++;
+    int p1 = po[i1] + tmp[i1]++;
     idx[p1] = i2;
     kk[p1] = k[b];
     rr[p1] = r0[b];
+    if (directed) continue;
+    int p2 = po[i2] + tmp[i2]++;
     idx[p2] = i1;
     kk[p2] = k[b];
     rr[p2] = r0[b];
@@ -523,7 +527,7 @@ int slot_bonds(Slot& s, int64_t nbonds, const int32_t* bi, const int32_t* bj, co
     fxx[3 * p + 2] = fxyz[3 * b + 2];
   }
   // one allocation for the tables: idx | k | r0 | fk | fr0 | fxyz
-  const size_t nb2 = (size_t)2 * nbonds, nf = (size_t)nfixed;
+  const size_t nb2 = (size_t)nent, nf = (size_t)nfixed;
   const size_t o_idx = 0, o_k = align_up(sizeof(int) * nb2), o_r0 = o_k + align_up(sizeof(double) * nb2),
                o_fk = o_r0 + align_up(sizeof(double) * nb2), o_fr0 = o_fk + align_up(sizeof(double) * nf),
                o_fx = o_fr0 + align_up(sizeof(double) * nf), total = o_fx + align_up(sizeof(double) * 3 * nf);

@@ -80,9 +80,10 @@ int slot_reset_observables(Slot& s, cudaStream_t st);
 // The accumulators of the slot (synchronises st).
 int slot_read_observables(const Slot& s, cudaStream_t st, fsl_observables* out);
 // Bond tables in the reference's CSR (src/initializeBondedForces.cpp:31-150).
+// directed: entry b acts on particle bi[b] only (the old bond-file format)
 int slot_bonds(Slot& s, int64_t nbonds, const int32_t* bi, const int32_t* bj, const double* k,
                const double* r0, int64_t nfixed, const int32_t* fi, const double* fk,
-               const double* fr0, const double* fxyz, cudaStream_t st);
+               const double* fr0, const double* fxyz, cudaStream_t st, bool directed = false);
 
 struct Group {
   ClassKey key{};

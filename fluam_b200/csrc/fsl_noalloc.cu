@@ -2,8 +2,6 @@
 //
 // fsl_cell_list needs a handle, and fsl_create allocates the handle's device
 // buffers with cudaMalloc.  Some callers cannot do that:
-//   * code that is recording a CUDA graph with global capture mode, where a
-//     cudaMalloc call is an error;
 //   * a host framework that owns all device memory through its own pool and
 //     only hands out buffers it allocated itself;
 //   * a loop that keeps other work in flight on the GPU and must not stall

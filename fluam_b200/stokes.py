@@ -82,7 +82,10 @@ class StokesLimit:
         self.close()
 
     # -- scheme ------------------------------------------------------------
-    def load_bonds(self, bi, bj, k, r0, fi=None, fk=None, fr0=None, fxyz=None):
+    def load_bonds(self, bi, bj, k, r0, fi=None, fk=None, fr0=None, fxyz=None, directed=False):
+        """Bonds acting on both particles (fsl_load_bonds), or with
+        directed=True entries acting on bi only (fsl_load_bonds_directed, the
+        old bond-file format)."""
         bi = np.ascontiguousarray(bi, dtype=np.int32)
         bj = np.ascontiguousarray(bj, dtype=np.int32)
         k = np.ascontiguousarray(k, dtype=np.float64)
@@ -93,8 +96,9 @@ class StokesLimit:
         fk = np.ascontiguousarray(fk, dtype=np.float64)
         fr0 = np.ascontiguousarray(fr0, dtype=np.float64)
         fxyz = np.ascontiguousarray(fxyz, dtype=np.float64).reshape(-1, 3)
-        check(self.L.fsl_load_bonds(self.h, len(bi), _ip(bi), _ip(bj), _dp(k), _dp(r0), len(fi),
-                                    _ip(fi), _dp(fk), _dp(fr0), _dp(fxyz)))
+        fn = self.L.fsl_load_bonds_directed if directed else self.L.fsl_load_bonds
+        check(fn(self.h, len(bi), _ip(bi), _ip(bj), _dp(k), _dp(r0), len(fi),
+                 _ip(fi), _dp(fk), _dp(fr0), _dp(fxyz)))
 
     def step(self, n=1):
         check(self.L.fsl_step(self.h, int(n)))

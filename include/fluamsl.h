@@ -143,6 +143,18 @@ int fsl_load_bonds(fsl_handle* h, int64_t nbonds, const int32_t* bi, const int32
                    const double* k, const double* r0, int64_t nfixed, const int32_t* fi,
                    const double* fk, const double* fr0, const double* fxyz);
 
+/* Directed bond entries, as the reference holds them in memory and as the
+ * old bond-file format (bondedForcesVersion 1) lists them: entry b adds the
+ * spring (k[b], r0[b]) towards particle bj[b] to the force on bi[b] only, so
+ * a bond appears once from each end (src/initializeBondedForcesOldVersion.cpp:
+ * 41-238; the reference's CSR bondsParticleParticle/Offset,
+ * bondsIndexParticleParticle, kSpring/r0ParticleParticle of
+ * src/initializeBondedForces.cpp:31-170 expands to these entries).  Entries
+ * are grouped by bi in their order.  Tethers as fsl_load_bonds. */
+int fsl_load_bonds_directed(fsl_handle* h, int64_t nentries, const int32_t* bi, const int32_t* bj,
+                            const double* k, const double* r0, int64_t nfixed, const int32_t* fi,
+                            const double* fk, const double* fr0, const double* fxyz);
+
 /* Advance nsteps midpoint steps (the body of the loop in
  * src/runSchemeStokesLimit.cu:163-285).  Runs on the handle's stream; returns
  * after the work is queued unless an error check needs the device. */
@@ -377,8 +389,7 @@ void fsl_server_destroy(fsl_server* s);
 
 /* ---- cell list without device allocation -------------------------------
  * No counterpart in the reference.  The same cell list as fsl_cell_list, for
- * callers that must not allocate device memory: code recording a CUDA graph
- * in global capture mode (where cudaMalloc fails), frameworks that own all
+ * callers that must not allocate device memory: frameworks that own all
  * device memory through their own pool, and loops that keep other GPU work
  * in flight (cudaMalloc/cudaFree can synchronise the whole device).  It takes
  * no handle.  q_dev (np x 3 doubles, SoA), cell_of_dev (np), start_dev (m+1,

@@ -5,18 +5,32 @@ OpenMP, and ``-ffp-contract=off`` (the cell-index formulas of the reference
 must not be fused into multiply-adds).  Also exposes ``build_ref()``, which
 builds the reference's own Stokes-limit sources for the host into
 ``oracle/_ref/`` when the reference tree is present (see ``ref_cpu/``).
+
+Two more builds of the same source serve the CPU baseline timings:
+``real="f32"`` replaces the arithmetic type ``double`` by ``float`` throughout
+(the reference's own single-precision route is the same textual substitution
+of its sources, tools/scriptFloat), and ``native=True`` compiles for the host
+it runs on (``-march=native``; built where it is used, since the library
+travels between machines).  Portable builds use ``-march=x86-64-v3``.
 """
 import os
+import re
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle_fsl.so")
 SRC = os.path.join(HERE, "fsl_oracle.cpp")
 HDR = os.path.join(HERE, "fsl_oracle.h")
 
-CXXFLAGS = ["-O3", "-march=x86-64-v3", "-fopenmp", "-ffp-contract=off", "-fPIC",
+CXXFLAGS = ["-O3", "-fopenmp", "-ffp-contract=off", "-fPIC",
             "-shared", "-std=c++17", "-Wall", "-Wno-unused-function"]
+
+
+def lib_path(real="f64", native=False):
+    return os.path.join(HERE, "liboracle_fsl" + ("_f32" if real == "f32" else "")
+                        + ("_native" if native else "") + ".so")
 
 
 def _stale(target, deps):
@@ -26,13 +40,24 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build_oracle(force=False):
-    if force or _stale(LIB, [SRC, HDR]):
-        tmp = LIB + ".tmp"
-        cmd = ["g++"] + CXXFLAGS + [SRC, "-o", tmp]
-        subprocess.run(cmd, check=True)
-        os.replace(tmp, LIB)
-    return LIB
+def build_oracle(force=False, real="f64", native=False):
+    lib = lib_path(real, native)
+    if not (force or _stale(lib, [SRC, HDR])):
+        return lib
+    arch = ["-march=native"] if native else ["-march=x86-64-v3"]
+    with tempfile.TemporaryDirectory() as tmpdir:
+        src = SRC
+        if real == "f32":
+            for f in (SRC, HDR):
+                with open(f) as fh:
+                    text = re.sub(r"\bdouble\b", "float", fh.read())
+                with open(os.path.join(tmpdir, os.path.basename(f)), "w") as fh:
+                    fh.write(text)
+            src = os.path.join(tmpdir, os.path.basename(SRC))
+        tmp = lib + ".tmp"
+        subprocess.run(["g++"] + CXXFLAGS + arch + [src, "-o", tmp], check=True)
+        os.replace(tmp, lib)
+    return lib
 
 
 def build_ref(force=False):
@@ -47,3 +72,4 @@ def build_ref(force=False):
 
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
+    print(build_oracle(force="--force" in sys.argv, real="f32"))

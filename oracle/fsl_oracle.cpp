@@ -1406,21 +1406,25 @@ orc_state* orc_create(const orc_config* cfg, int64_t np, const double* q) {
 
 void orc_destroy(orc_state* s) { delete s; }
 
-int orc_set_bonds(orc_state* s, int64_t nbonds, const int32_t* bi, const int32_t* bj,
-                  const double* bk, const double* br0, int64_t nfixed, const int32_t* fi,
-                  const double* fk, const double* fr0, const double* fxyz) {
-  // CSR exactly as src/initializeBondedForces.cpp:31-150: both endpoints
-  // store each particle-particle bond, in file order.
+// Directed entries: entry b acts on particle bi[b] only, as a line of the
+// old bond-file format (bondedForcesVersion 1) does; the CSR groups the
+// entries by bi in their order, which for the sorted files the reference
+// accepts is its own CSR (src/initializeBondedForcesOldVersion.cpp:41-238).
+// Tethers as in orc_set_bonds.
+static int set_bonds_csr(orc_state* s, int64_t nbonds, const int32_t* bi, const int32_t* bj,
+                         const double* bk, const double* br0, int64_t nfixed, const int32_t* fi,
+                         const double* fk, const double* fr0, const double* fxyz, bool directed) {
   int np = s->np;
   for (int64_t b = 0; b < nbonds; ++b)
     if (bi[b] < 0 || bi[b] >= np || bj[b] < 0 || bj[b] >= np) return -1;
   for (int64_t b = 0; b < nfixed; ++b)
     if (fi[b] < 0 || fi[b] >= np) return -1;
+  const int64_t nent = directed ? nbonds : 2 * nbonds;
   s->bpp_cnt.assign(np, 0);
   s->bfp_cnt.assign(np, 0);
   for (int64_t b = 0; b < nbonds; ++b) {
     s->bpp_cnt[bi[b]]++;
-    s->bpp_cnt[bj[b]]++;
+    if (!directed) s->bpp_cnt[bj[b]]++;
   }
   for (int64_t b = 0; b < nfixed; ++b) s->bfp_cnt[fi[b]]++;
   s->bpp_off.assign(np, 0);
@@ -1429,21 +1433,21 @@ int orc_set_bonds(orc_state* s, int64_t nbonds, const int32_t* bi, const int32_t
     s->bpp_off[i] = s->bpp_off[i - 1] + s->bpp_cnt[i - 1];
     s->bfp_off[i] = s->bfp_off[i - 1] + s->bfp_cnt[i - 1];
   }
-  s->bpp_idx.assign(2 * nbonds, 0);
-  s->bpp_k.assign(2 * nbonds, 0.0);
-  s->bpp_r0.assign(2 * nbonds, 0.0);
+  s->bpp_idx.assign(nent, 0);
+  s->bpp_k.assign(nent, 0.0);
+  s->bpp_r0.assign(nent, 0.0);
   std::vector<int> tmp(np, 0);
   for (int64_t b = 0; b < nbonds; ++b) {
     int i1 = bi[b], i2 = bj[b];
-    int p1 = s->bpp_off[i1] + tmp[i1], p2 = s->bpp_off[i2] + tmp[i2];
+    int p1 = s->bpp_off[i1] + tmp[i1]++;
     s->bpp_idx[p1] = i2;
     s->bpp_k[p1] = bk[b];
     s->bpp_r0[p1] = br0[b];
+    if (directed) continue;
+    int p2 = s->bpp_off[i2] + tmp[i2]++;
     s->bpp_idx[p2] = i1;
     s->bpp_k[p2] = bk[b];
     s->bpp_r0[p2] = br0[b];
-    tmp[i1]++;
-    tmp[i2]++;
   }
   std::fill(tmp.begin(), tmp.end(), 0);
   s->bfp_k.assign(nfixed, 0.0);
@@ -1461,6 +1465,20 @@ int orc_set_bonds(orc_state* s, int64_t nbonds, const int32_t* bi, const int32_t
   }
   s->bonded = (nbonds + nfixed) > 0;
   return 0;
+}
+
+int orc_set_bonds(orc_state* s, int64_t nbonds, const int32_t* bi, const int32_t* bj,
+                  const double* bk, const double* br0, int64_t nfixed, const int32_t* fi,
+                  const double* fk, const double* fr0, const double* fxyz) {
+  // CSR exactly as src/initializeBondedForces.cpp:31-150: both endpoints
+  // store each particle-particle bond, in file order.
+  return set_bonds_csr(s, nbonds, bi, bj, bk, br0, nfixed, fi, fk, fr0, fxyz, false);
+}
+
+int orc_set_bonds_directed(orc_state* s, int64_t nentries, const int32_t* bi, const int32_t* bj,
+                           const double* bk, const double* br0, int64_t nfixed, const int32_t* fi,
+                           const double* fk, const double* fr0, const double* fxyz) {
+  return set_bonds_csr(s, nentries, bi, bj, bk, br0, nfixed, fi, fk, fr0, fxyz, true);
 }
 
 int orc_step(orc_state* s, int64_t nsteps) {

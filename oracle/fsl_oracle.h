@@ -75,6 +75,13 @@ void orc_destroy(orc_state* s);
 int orc_set_bonds(orc_state* s, int64_t nbonds, const int32_t* bi, const int32_t* bj,
                   const double* bk, const double* br0, int64_t nfixed, const int32_t* fi,
                   const double* fk, const double* fr0, const double* fxyz);
+/* Directed entries of the old bond-file format (bondedForcesVersion 1,
+ * src/initializeBondedForcesOldVersion.cpp:41-238): entry b adds the spring
+ * (bk, br0) towards particle bj[b] to particle bi[b] only (the file lists a
+ * bond once from each end).  Tethers as orc_set_bonds. */
+int orc_set_bonds_directed(orc_state* s, int64_t nentries, const int32_t* bi, const int32_t* bj,
+                           const double* bk, const double* br0, int64_t nfixed, const int32_t* fi,
+                           const double* fk, const double* fr0, const double* fxyz);
 int orc_step(orc_state* s, int64_t nsteps);
 void orc_get_positions(const orc_state* s, double* out);
 void orc_set_positions(orc_state* s, const double* in);

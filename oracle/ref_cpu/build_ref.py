@@ -59,7 +59,8 @@ HOST_FILES = [
     "gauss.cu", "schemeStokesLimit.cu", "schemeStokesLimitFirstOrder.cu", "schemeQuasi2D.cu",
     "schemeIncompressible.cu", "temperature.cu", "saveFluidFinalConfiguration.cu",
     "createCells.cpp", "createParticles.cpp",
-    "simpleCubic.cpp", "initializeBondedForces.cpp", "initializeFluid.cpp", "modu.cu",
+    "simpleCubic.cpp", "initializeBondedForces.cpp", "initializeBondedForcesOldVersion.cpp",
+    "initializeFluid.cpp", "modu.cu",
     "saveSeed.cpp", "saveTime.cpp", "saveParticles.cu", "freeParticles.cu", "random_frenk.cu",
 ]
 

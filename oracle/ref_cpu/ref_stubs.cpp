@@ -38,7 +38,6 @@ bool freeBondedForces() { return 1; }
 
 bool createBoundaries() { return not_built("boundary (fileboundary) input"); }
 bool freeBoundaries() { return 1; }
-bool initializeBondedForcesOldVersion() { return not_built("bondedForcesVersion 1"); }
 
 #define FLUAM_SCHEME_STUB(name) \
   bool name() { return not_built(#name); }

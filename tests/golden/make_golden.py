@@ -117,6 +117,30 @@ numsteps 4
 samplefreq 2
 dt 0.01
 """, chains=(6, 8, (16.0, 24.0, 32.0), 9)),
+    # the old bond-file format (bondedForcesVersion 1,
+    # src/initializeBondedForcesOldVersion.cpp): every bond listed from both
+    # ends and sorted by the first index, two springs listed from one end
+    # only (each pulls its own particle alone; an even line count, because
+    # the reference copies 2 (count / 2) lines to the device,
+    # src/createBondedForcesGPU.cu:62-78), one tether per particle (the
+    # reference misplaces a particle's second tether in this format)
+    "bonds_old_format": dict(old_bonds=True, text="""loadparticles 1
+coordinates start.coor
+bondedForces bonds.dat
+bondedForcesVersion 1
+computeNonBondedForces 0
+cutoff 1.5
+extraMobility 0.1
+shearviscosity 1.2
+temperature 0.02
+cells 24 16 20
+celldimension 24 16 20
+seed 33
+numstepsRelaxation 1
+numsteps 4
+samplefreq 2
+dt 0.01
+""", chains=(5, 7, (24.0, 16.0, 20.0), 15)),
     # the first-order scheme (keyword stokesLimitFirstOrder, which takes
     # precedence over stokesLimit, src/main.cpp:94-99) with LJ forces.  The
     # stokesLimit keyword stays in the file: without it the reference never
@@ -274,10 +298,27 @@ def make_case(name, spec):
         q, bonds = (chains2d if spec.get("dim") == 2 else chains)(nch, beads, box, seed)
         write_coor(os.path.join(d, "start.coor"), q)
         with open(os.path.join(d, "bonds.dat"), "w") as f:
-            f.write(f"{len(bonds)}\n")
-            for k, (a, b) in enumerate(bonds):
-                f.write(f"{a} {b} {10.0 if k % 2 else 4.0} {1.0 if k % 3 else 0.0}\n")
-            f.write("2\n0 2.0 0.0 0.0 0.0 0.0\n5 1.5 0.5 1.0 -2.0 3.0\n")
+            if spec.get("old_bonds"):
+                # each bond from both ends, sorted by the first index; the
+                # last chain's first bead is pulled towards bead 2 of chain
+                # 0, and bead 10 towards bead 30, by springs listed from one
+                # end only
+                ent = []
+                for k, (a, b) in enumerate(bonds):
+                    ks, r0 = (10.0 if k % 2 else 4.0), (1.0 if k % 3 else 0.0)
+                    ent += [(a, b, ks, r0), (b, a, ks, r0)]
+                ent.append((nch * beads - beads, 2, 3.0, 2.0))
+                ent.append((10, 30, 2.5, 1.5))
+                ent.sort(key=lambda e: e[0])
+                f.write(f"{len(ent)}\n")
+                for a, b, ks, r0 in ent:
+                    f.write(f"{a} {b} {ks} {r0}\n")
+                f.write("2\n0 2.0 0.0 0.0 0.0 0.0\n5 1.5 0.5 1.0 -2.0 3.0\n")
+            else:
+                f.write(f"{len(bonds)}\n")
+                for k, (a, b) in enumerate(bonds):
+                    f.write(f"{a} {b} {10.0 if k % 2 else 4.0} {1.0 if k % 3 else 0.0}\n")
+                f.write("2\n0 2.0 0.0 0.0 0.0 0.0\n5 1.5 0.5 1.0 -2.0 3.0\n")
     r = subprocess.run([FLUAM_REF, "data.main"], cwd=d, capture_output=True, text=True,
                        timeout=600)
     if "END" not in r.stdout:

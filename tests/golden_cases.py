@@ -109,9 +109,12 @@ def load(name):
             bb = np.array([f.readline().split() for _ in range(nb)], dtype=float).reshape(nb, 4)
             nf = int(f.readline())
             ff = np.array([f.readline().split() for _ in range(nf)], dtype=float).reshape(nf, 6)
+        # bondedForcesVersion != 0: the old format, one line per bond end
+        k = words.index("bondedForcesVersion") if "bondedForcesVersion" in words else -1
+        directed = k >= 0 and int(words[k + 1]) != 0
         bonds = dict(bi=bb[:, 0].astype(np.int32), bj=bb[:, 1].astype(np.int32), k=bb[:, 2],
                      r0=bb[:, 3], fi=ff[:, 0].astype(np.int32), fk=ff[:, 1], fr0=ff[:, 2],
-                     fxyz=ff[:, 3:6])
+                     fxyz=ff[:, 3:6], directed=directed)
     _, pos = read_particles(os.path.join(d, "out.particles"))
     # the first-order scheme and quasi2D write no .velocityParticles
     # (src/saveParticles.cu:43-46); stokesLimit2D writes zeros there (its

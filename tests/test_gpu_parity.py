@@ -102,6 +102,34 @@ def test_bonded_forces(fsl, oracle):
     g.close()
 
 
+def test_bonded_forces_directed(fsl, oracle):
+    """Directed entries (the old bond-file format): each acts on its first
+    particle only; the same entries listed from both ends equal the bonds."""
+    L = (24.0, 24.0, 24.0)
+    q, bi, bj = chains(10, 8, L, 14)
+    g, o = make_pair(fsl, oracle, (24, 24, 24), L, q, pair="soft")
+    k = 4.0 + np.arange(len(bi)) % 3
+    r0 = np.where(np.arange(len(bi)) % 2 == 0, 1.0, 0.5)
+    # both ends of every bond, sorted by the first index, plus two one-sided springs
+    ei = np.concatenate([bi, bj, [3, 40]]).astype(np.int32)
+    ej = np.concatenate([bj, bi, [70, 1]]).astype(np.int32)
+    ek = np.concatenate([k, k, [2.0, 5.0]])
+    er = np.concatenate([r0, r0, [1.5, 0.0]])
+    order = np.argsort(ei, kind="stable")
+    ei, ej, ek, er = ei[order], ej[order], ek[order], er[order]
+    g.load_bonds(ei, ej, ek, er, directed=True)
+    o.set_bonds(ei, ej, ek, er, directed=True)
+    Fd = g.compute_forces()
+    assert rel_inf(Fd, o.compute_forces(q)) < 1e-12
+    # without the one-sided springs the directed entries are the bonds
+    keep = ~(((ei == 3) & (ej == 70)) | ((ei == 40) & (ej == 1)))
+    g.load_bonds(ei[keep], ej[keep], ek[keep], er[keep], directed=True)
+    Fsym = g.compute_forces()
+    g.load_bonds(bi, bj, k, r0)
+    assert rel_inf(Fsym, g.compute_forces()) < 1e-12
+    g.close()
+
+
 @pytest.mark.parametrize("kernel", [3, 4])
 def test_spread(fsl, oracle, kernel):
     L = (16.0, 12.0, 20.0)

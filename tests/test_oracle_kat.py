@@ -229,3 +229,16 @@ def test_step_statistics_free_particles(oracle):
     expect = 2 * 0.01 * mu * 0.01
     # 64 particles x 40 steps x 3 components; hydrodynamic correlations widen it
     assert abs(d2 / expect - 1) < 0.12
+
+
+def test_fp32_build_tracks_fp64(oracle):
+    """The FP32 build of the restatement (the CPU timing baseline in single
+    precision, `double` replaced by `float` as the reference's own FP32 route
+    does) follows the FP64 build: 3 midpoint steps of 256 particles at 32^3."""
+    q = uniform_positions(256, (32.0,) * 3, 5)
+    a = oracle.Oracle(32, 32, 32, 32.0, 32.0, 32.0, q, kernel=3, seed=3)
+    b = oracle.Oracle(32, 32, 32, 32.0, 32.0, 32.0, q, kernel=3, seed=3, real="f32")
+    a.step(3)
+    b.step(3)
+    assert b.positions().dtype == np.float32
+    assert rel_inf(b.positions() - q, a.positions() - q) < 1e-3

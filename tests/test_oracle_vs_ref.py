@@ -18,6 +18,17 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 FLUAM_REF = os.path.join(ROOT, "oracle", "_ref", "fluam_ref")
 
 
+def _reference_sources():
+    """The reference's source tree as the build recipe finds it (the
+    FLUAM_REFERENCE variable, else the recipe's default location)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "_build_ref", os.path.join(ROOT, "oracle", "ref_cpu", "build_ref.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.REF_SRC
+
+
 def _oracle_for(oracle, c):
     cfg = c["cfg"]
     o = oracle.Oracle(cfg.mx, cfg.my, cfg.mz, cfg.lx, cfg.ly, cfg.lz, c["q0"],
@@ -30,7 +41,8 @@ def _oracle_for(oracle, c):
                       shear_amp=cfg.shear_amp)
     if c["bonds"] is not None:
         b = c["bonds"]
-        o.set_bonds(b["bi"], b["bj"], b["k"], b["r0"], b["fi"], b["fk"], b["fr0"], b["fxyz"])
+        o.set_bonds(b["bi"], b["bj"], b["k"], b["r0"], b["fi"], b["fk"], b["fr0"], b["fxyz"],
+                    directed=b["directed"])
     return o
 
 
@@ -64,7 +76,7 @@ def test_oracle_reproduces_reference(oracle, name):
 def test_golden_files_regenerate_identically(tmp_path, name):
     """Where the reference sources are present, rerun the reference and get
     the committed fixture back byte for byte."""
-    if not (os.path.exists(FLUAM_REF) and os.path.isdir("/root/reference/src")):
+    if not (os.path.exists(FLUAM_REF) and os.path.isdir(_reference_sources())):
         pytest.skip("reference host build not available here")
     src = os.path.join(G.GOLDEN, name)
     for f in os.listdir(src):
@@ -98,7 +110,7 @@ def test_oracle_reproduces_reference_fluid(oracle, name):
 
 @pytest.mark.parametrize("name", G.fluid_cases())
 def test_fluid_golden_files_regenerate_identically(tmp_path, name):
-    if not (os.path.exists(FLUAM_REF) and os.path.isdir("/root/reference/src")):
+    if not (os.path.exists(FLUAM_REF) and os.path.isdir(_reference_sources())):
         pytest.skip("reference host build not available here")
     src = os.path.join(G.GOLDEN, name)
     shutil.copy(os.path.join(src, "data.main"), tmp_path / "data.main")

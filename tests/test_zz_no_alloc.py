@@ -1,6 +1,6 @@
 """fsl_cell_list_noalloc: the cell list for callers that cannot allocate device
-memory (graph capture in global mode, frameworks that own the device memory,
-loops that must not stall in-flight GPU work).  Its output must equal the
+memory (frameworks that own the device memory, loops that must not stall
+in-flight GPU work).  Its output must equal the
 handle-based fsl_cell_list exactly (cell lists are integer results, compared
 bit for bit), on two calls in a row that share the library's scratch array.
 
