@@ -695,17 +695,27 @@ void group_enqueue_step(Group& g) {
   auto chk = [&](const char* stage) {
     if (!g.fail_stage && cudaPeekAtLastError() != cudaSuccess) g.fail_stage = stage;
   };
-  auto cells_forces = [&](int which) {
+  // fused: the Verlet-list forces are left to the spread that follows at
+  // the same positions (launch_spread with forces = true);
+  // FLUAMSL_FUSED_FORCES=0 keeps them in their own launch, for comparison
+  static const bool fuse_ok = [] {
+    const char* e = getenv("FLUAMSL_FUSED_FORCES");
+    return !(e && e[0] == '0');
+  }();
+  // (the FP64 form spreads in its own kernels, which read F)
+  const bool fuse = fuse_ok && B.prec != PREC_F64 && !B.tiled;
+  auto cells_forces = [&](int which, bool fused) {
+    fused = fused && fuse;
     pr.mark(s, "cells");
     // (one cooperative launch for a single instance; on the Verlet path the
     // list kernels return at once unless a rebuild is due)
     if (launch_pair_lists(B, which, s) != cudaSuccess && !g.fail_stage) g.fail_stage = "cells";
     pr.count(!pk ? 0 : (B.one && B.one->bar) ? 1 : 5 + (B.has_vl ? 1 : 0));
     chk("cells");
-    pr.mark(s, "forces");
-    launch_forces(B, which, s);
+    if (!(fused && !B.has_cl)) pr.mark(s, "forces");
+    launch_forces(B, which, s, !fused);
     chk("forces");
-    pr.count(pk ? (B.has_vl ? 1 : 0) + (B.has_cl ? 1 : 0) : 0);
+    pr.count(pk ? (B.has_vl && !fused ? 1 : 0) + (B.has_cl ? 1 : 0) : 0);
   };
   g.fail_stage = nullptr;
   chk("before the step");
@@ -795,7 +805,7 @@ void group_enqueue_step(Group& g) {
     // src/runSchemeStokesLimitFirstOrder.cu:163-241: f = S(q^n) F^n + RFD
     // drift, one solve with noise factor 1, predictor, forces at q^{n+1/2}
     // only with extraMobility (k_forces returns at once otherwise), corrector
-    cells_forces(0);
+    cells_forces(0, !B.tiled);
     join_noise();
     if (B.tiled) {
       pr.mark(s, "spread_w");
@@ -804,7 +814,7 @@ void group_enqueue_step(Group& g) {
       pr.count(1);
     } else {
       pr.mark(s, "spread_rfd");
-      launch_spread(B, 2, 1, s);
+      launch_spread(B, 2, 1, s, fuse);
       chk("spread_rfd");
       pr.count(pk);
     }
@@ -814,7 +824,7 @@ void group_enqueue_step(Group& g) {
     launch_interp_update(B, 1, s);
     chk("interp_update");
     pr.count(pk);
-    cells_forces(1);
+    cells_forces(1, false);
     pr.mark(s, "interp_update");
     launch_interp_update(B, 2, s);
     chk("interp_update");
@@ -831,7 +841,7 @@ void group_enqueue_step(Group& g) {
   // option 0: F^n, f = S(q^n) F^n; solve 1 with sqrt(2) stress 1.  The
   // spread field is all zeros here: it starts cleared and every W build
   // clears what it reads.
-  cells_forces(0);
+  cells_forces(0, !B.tiled);
   if (B.tiled) {
     join_noise();
     pr.mark(s, "spread_w");
@@ -840,7 +850,7 @@ void group_enqueue_step(Group& g) {
     pr.count(1);
   } else {
     pr.mark(s, "spread");
-    launch_spread(B, 0, 1, s);
+    launch_spread(B, 0, 1, s, fuse);
     chk("spread");
     pr.count(pk);
     join_noise();
@@ -853,7 +863,7 @@ void group_enqueue_step(Group& g) {
   launch_interp_update(B, 1, s);
   chk("interp_update");
   pr.count(pk);
-  cells_forces(1);
+  cells_forces(1, !B.tiled);
   if (B.tiled) {
     pr.mark(s, "spread_w_rfd");
     launch_spread_w(B, 1, 2, 0.70710678118654752440, s);
@@ -861,7 +871,7 @@ void group_enqueue_step(Group& g) {
     pr.count(1);
   } else {
     pr.mark(s, "spread_rfd");
-    launch_spread(B, 1, 1, s);
+    launch_spread(B, 1, 1, s, fuse);
     chk("spread_rfd");
     pr.count(pk);
   }

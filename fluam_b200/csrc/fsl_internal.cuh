@@ -597,11 +597,15 @@ void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t cou
 // count and fill arrays cleared; zero_first clears them (and start, for an
 // instance without particles) first, for callers that cannot rely on that.
 void launch_cells(const Batch& B, int which, cudaStream_t s, bool zero_first = true);
-void launch_forces(const Batch& B, int which, cudaStream_t s);
+// vl = false leaves the Verlet-list instances' forces to the spread that
+// follows (launch_spread with forces = true)
+void launch_forces(const Batch& B, int which, cudaStream_t s, bool vl = true);
 // drift = 0: spread F at q (cell-list order when ordered != 0);
 // drift = 1: spread F at q^{n+1/2} and the RFD drift at q;
-// drift = 2: spread F at q and the RFD drift at q (first-order scheme)
-void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s);
+// drift = 2: spread F at q and the RFD drift at q (first-order scheme).
+// forces: the Verlet-list instances compute F at the spread's positions in
+// the spread kernel (and store it) instead of reading it.
+void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s, bool forces = false);
 void launch_interp_update(const Batch& B, int stage, cudaStream_t s);
 void launch_interp(const Batch& B, cudaStream_t s);  // u = J(q) v
 void launch_step_counter(const Batch& B, cudaStream_t s);

@@ -604,31 +604,20 @@ __global__ void __launch_bounds__(kCoopThreads) k_lists_coop(const __grid_consta
   for (int i = tid; i < np; i += nth) vl_build_one(R, i, which);
 }
 
-// Pair forces from the Verlet list (soft repulsion with the cutoff test and
-// arithmetic of k_forces, on the minimum image of the unwrapped positions as
-// the reference takes it) plus the bonded forces; one quad per particle, lane
-// a taking list entries and bonds a, a + 4, ..., the partial forces summed
-// in a fixed butterfly order.  Also the force kernel of instances without
-// pair forces (bonds only).
-template <bool ONE>
-__global__ void k_forces_vl(FSL_KARGS, int which) {
-  FSL_REP_FLAT(KIND_T4);
-  long e;
-  int a, qb;
+// The pair (Verlet list, or the 27 cells of the current cell list in cell
+// mode) and bonded force on particle i by its quad: lane a takes list
+// entries and bonds a, a + 4, ...; the partial forces are summed in a fixed
+// butterfly order, every lane of the quad gets the sum.  Every lane of the
+// warp calls this (shuffles); lanes with on == false contribute nothing.
+__device__ __forceinline__ void quad_force_vl(const Params& P, const Rep& R, int i, int a, int which,
+                                              bool on, bool cell_mode, double& fx, double& fy,
+                                              double& fz) {
   const int np = P.np;
-  if (!(P.verlet || P.nolist)) return;
-  const bool cell_mode = P.verlet && R.vl_flag[2] == 3;
-  __syncthreads();  // every thread has read the word before it is cleared
-  if (blk == 0 && threadIdx.x == 0 && R.vl_flag && !cell_mode) R.vl_flag[2] = 0;  // rebuilt by now
-  if (!quad_of(blk, np, e, a, qb)) return;
-  // first-order scheme: forces at q^{n+1/2} only with extraMobility
-  // (src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:170-180)
-  if (which == 1 && P.scheme == 1 && !P.has_extra) return;
-  const bool on = e < np;
-  const int i = on ? (int)e : 0;
   const double* __restrict__ q = which ? R.qp : R.q;
   const double rx = q[i], ry = q[np + i], rz = q[2 * np + i];
-  double fx = 0.0, fy = 0.0, fz = 0.0;
+  fx = 0.0;
+  fy = 0.0;
+  fz = 0.0;
   if (P.bonded && on) {
     int nb = R.bpp_cnt[i], off = R.bpp_off[i];
     for (int j = a; j < nb; j += 4) {
@@ -691,6 +680,40 @@ __global__ void k_forces_vl(FSL_KARGS, int which) {
     fy += __shfl_xor_sync(0xffffffffu, fy, o);
     fz += __shfl_xor_sync(0xffffffffu, fz, o);
   }
+}
+
+// Whether the instance is in cell mode, read by every thread of the block
+// before block 0 clears the rebuild request (the lists were rebuilt by the
+// launch before); all threads of the block call this.
+__device__ __forceinline__ bool vl_state(const Rep& R, int blk) {
+  const bool cell_mode = R.P.verlet && R.vl_flag[2] == 3;
+  __syncthreads();  // every thread has read the word before it is cleared
+  if (blk == 0 && threadIdx.x == 0 && R.vl_flag && !cell_mode) R.vl_flag[2] = 0;  // rebuilt by now
+  return cell_mode;
+}
+
+// Pair forces from the Verlet list (soft repulsion with the cutoff test and
+// arithmetic of k_forces, on the minimum image of the unwrapped positions as
+// the reference takes it) plus the bonded forces; one quad per particle
+// (quad_force_vl).  Also the force kernel of instances without pair forces
+// (bonds only).  Where a spread follows at the same positions, k_spread
+// computes these forces itself instead.
+template <bool ONE>
+__global__ void k_forces_vl(FSL_KARGS, int which) {
+  FSL_REP_FLAT(KIND_T4);
+  long e;
+  int a, qb;
+  const int np = P.np;
+  if (!(P.verlet || P.nolist)) return;
+  const bool cell_mode = vl_state(R, blk);
+  if (!quad_of(blk, np, e, a, qb)) return;
+  // first-order scheme: forces at q^{n+1/2} only with extraMobility
+  // (src/boundaryParticlesFunctionStokesLimitFirstOrder.cu:170-180)
+  if (which == 1 && P.scheme == 1 && !P.has_extra) return;
+  const bool on = e < np;
+  const int i = on ? (int)e : 0;
+  double fx, fy, fz;
+  quad_force_vl(P, R, i, a, which, on, cell_mode, fx, fy, fz);
   if (!on || a != 0) return;
   if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) set_err(R.err, 2);
   R.F[i] = fx;
@@ -698,10 +721,10 @@ __global__ void k_forces_vl(FSL_KARGS, int which) {
   R.F[2 * np + i] = fz;
 }
 
-void launch_forces(const Batch& B, int which, cudaStream_t s) {
+void launch_forces(const Batch& B, int which, cudaStream_t s, bool vl) {
   if (B.max_np == 0) return;
   if (B.has_cl) FSL_GO(k_forces, part_blocks(B, KIND_T8), kPartThreads, 0, s, B, which);
-  if (B.has_vl) FSL_GO(k_forces_vl, part_blocks(B, KIND_T4), kPartThreads, 0, s, B, which);
+  if (B.has_vl && vl) FSL_GO(k_forces_vl, part_blocks(B, KIND_T4), kPartThreads, 0, s, B, which);
 }
 
 // Blocks of the cooperative build: all co-resident, computed once per device
@@ -896,14 +919,22 @@ __device__ __forceinline__ void quad_interp(const Params& P, const QuadStencil<K
 // the same nodes the two fixed-point spreads are exact negatives of each
 // other (same weights, opposite values, symmetric rounding), so they are
 // skipped without changing the result.  Every lane of the warp calls this.
-template <int KN, class Add>
-__device__ __forceinline__ void rfd_drift(const Params& P, const Rep& R, int i, int a, int qb,
-                                          bool on, Add&& add) {
+__device__ __forceinline__ void rfd_inputs(const Params& P, const Rep& R, int i, double W[3],
+                                           double pos[3]) {
   const int np = P.np;
   const size_t wbase = (size_t)6 * P.nc;
-  double W[3] = {(double)R.noise[wbase + i], (double)R.noise[wbase + np + i],
-                 (double)R.noise[wbase + 2 * np + i]};
-  double pos[3] = {R.q[i], R.q[np + i], R.q[2 * np + i]};
+  W[0] = (double)R.noise[wbase + i];
+  W[1] = (double)R.noise[wbase + np + i];
+  W[2] = (double)R.noise[wbase + 2 * np + i];
+  pos[0] = R.q[i];
+  pos[1] = R.q[np + i];
+  pos[2] = R.q[2 * np + i];
+}
+
+// W: the particle's RFD noise, pos: q^n (rfd_inputs)
+template <int KN, class Add>
+__device__ __forceinline__ void rfd_drift_at(const Params& P, const double W[3], const double pos[3],
+                                             int a, int qb, bool on, Add&& add) {
   double pp[3], pm[3], vp[3], vm[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -942,6 +973,123 @@ __device__ __forceinline__ void rfd_drift(const Params& P, const Rep& R, int i, 
   }
 }
 
+template <int KN, class Add>
+__device__ __forceinline__ void rfd_drift(const Params& P, const Rep& R, int i, int a, int qb,
+                                          bool on, Add&& add) {
+  double W[3], pos[3];
+  rfd_inputs(P, R, i, W, pos);
+  rfd_drift_at<KN>(P, W, pos, a, qb, on, add);
+}
+
+// ------------------------------------------------- warp-aggregated spread ---
+// The fixed-point spread of a warp's eight particles gathered in a shared
+// box before it reaches the L2: consecutive particles (a chain's beads, or
+// cell-ordered particles) share most stencil nodes, and the L2 takes 64-bit
+// atomic adds at a limited rate.  Per component the warp finds the box of
+// kBox^3 nodes that holds the stencils of its live particles (relative to
+// the first particle's nodes, periodic); each product goes into the box as
+// two 32-bit shared atomics (low word, then high word plus the carry of the
+// low one: exact integer arithmetic mod 2^64, so every node's sum is the
+// same integer whatever the order); the box is then flushed with one 64-bit
+// global atomic per non-zero node and left cleared.  A warp whose particles do not fit in the box, and
+// grids with fewer than kBox cells along an axis, take the per-particle
+// atomics of quad_spread.  Same products (w = wx (wy wz) times the
+// fixed-point value), same integer sums: bitwise equal to quad_spread.
+constexpr int kBox = 8;
+constexpr int kBoxNodes = kBox * kBox * kBox;
+
+// d wrapped into [-m/2, m/2)
+__device__ __forceinline__ int rel_wrap(int d, int m) {
+  if (2 * d >= m) d -= m;
+  else if (2 * d < -m) d += m;
+  return d;
+}
+
+template <int KN>
+__device__ __forceinline__ void warp_spread(const Params& P, const QuadStencil<KN>& S, int a,
+                                            const double val[3], bool on,
+                                            unsigned long long* __restrict__ grid, bool& sat,
+                                            unsigned* __restrict__ blo, unsigned* __restrict__ bhi) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const bool small = P.mx < kBox || P.my < kBox || P.mz < kBox;
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    // first node of the quad per dimension: x of lane 0 of the quad, y and z
+    // shared by the quad's lanes
+    const int x0 = __shfl_sync(full, S.jx[comp == 0], lane & ~3);
+    const int y0 = S.jy[comp == 1][0], z0 = S.jz[comp == 2][0];
+    const int X0 = __shfl_sync(full, x0, 0), Y0 = __shfl_sync(full, y0, 0),
+              Z0 = __shfl_sync(full, z0, 0);
+    const int dx = rel_wrap(x0 - X0, P.mx), dy = rel_wrap(y0 - Y0, P.my), dz = rel_wrap(z0 - Z0, P.mz);
+    constexpr int kBig = 1 << 28;
+    const int lx = __reduce_min_sync(full, on ? dx : kBig), hx = __reduce_max_sync(full, on ? dx : -kBig);
+    const int ly = __reduce_min_sync(full, on ? dy : kBig), hy = __reduce_max_sync(full, on ? dy : -kBig);
+    const int lz = __reduce_min_sync(full, on ? dz : kBig), hz = __reduce_max_sync(full, on ? dz : -kBig);
+    const bool fits = !small && hx - lx + KN <= kBox && hy - ly + KN <= kBox && hz - lz + KN <= kBox;
+    const double vs = val[comp] * kFixedScale;
+    if (!fits) {  // warp-uniform
+      if (on && a < KN) {
+        unsigned long long* gc = grid + (size_t)comp * P.nc;
+        const int x = S.jx[comp == 0];
+        const float wx = S.wx[comp == 0];
+#pragma unroll
+        for (int b = 0; b < KN; ++b)
+#pragma unroll
+          for (int c = 0; c < KN; ++c) {
+            const int at = x + P.mx * (S.jy[comp == 1][b] + P.my * S.jz[comp == 2][c]);
+            const float w = wx * (S.wy[comp == 1][b] * S.wz[comp == 2][c]);
+            const double v = (double)w * vs;
+            sat |= !(fabs(v) < kFixedMax);
+            const long long iv = sat ? 0ll : __double2ll_rn(v);
+            if (iv != 0) atomicAdd(gc + at, (unsigned long long)iv);
+          }
+      }
+      continue;
+    }
+    if (on && a < KN) {
+      const float wx = S.wx[comp == 0];
+      const int bx = dx - lx + a;
+#pragma unroll
+      for (int b = 0; b < KN; ++b)
+#pragma unroll
+        for (int c = 0; c < KN; ++c) {
+          const float w = wx * (S.wy[comp == 1][b] * S.wz[comp == 2][c]);
+          const double v = (double)w * vs;
+          sat |= !(fabs(v) < kFixedMax);
+          const long long iv = sat ? 0ll : __double2ll_rn(v);
+          if (iv != 0) {
+            const int n = ((dz - lz + c) * kBox + (dy - ly + b)) * kBox + bx;
+            const unsigned lo = (unsigned)(unsigned long long)iv;
+            const unsigned hi = (unsigned)((unsigned long long)iv >> 32);
+            const unsigned old = atomicAdd(blo + n, lo);
+            atomicAdd(bhi + n, hi + (old + lo < old ? 1u : 0u));
+          }
+        }
+    }
+    __syncwarp();
+    // the box's first node, in [0, m); m >= kBox, so one wrap per axis
+    int bx0 = X0 + lx, by0 = Y0 + ly, bz0 = Z0 + lz;
+    bx0 += bx0 < 0 ? P.mx : (bx0 >= P.mx ? -P.mx : 0);
+    by0 += by0 < 0 ? P.my : (by0 >= P.my ? -P.my : 0);
+    bz0 += bz0 < 0 ? P.mz : (bz0 >= P.mz ? -P.mz : 0);
+    unsigned long long* gc = grid + (size_t)comp * P.nc;
+#pragma unroll 4
+    for (int n = lane; n < kBoxNodes; n += 32) {
+      const unsigned lo = blo[n], hi = bhi[n];
+      if ((lo | hi) == 0u) continue;
+      blo[n] = 0u;
+      bhi[n] = 0u;
+      int x = bx0 + (n & (kBox - 1)), y = by0 + ((n / kBox) & (kBox - 1)), z = bz0 + n / (kBox * kBox);
+      x -= x >= P.mx ? P.mx : 0;
+      y -= y >= P.my ? P.my : 0;
+      z -= z >= P.mz ? P.mz : 0;
+      atomicAdd(gc + x + P.mx * (y + P.my * z), ((unsigned long long)hi << 32) | lo);
+    }
+    __syncwarp();
+  }
+}
+
 // ------------------------------------------------------------- spreading ---
 // One quad per particle (in cell order when ordered).  drift = 0: F at q;
 // drift = 1: F at q^{n+1/2}, then the particle's RFD drift (kT/delta) sign
@@ -949,11 +1097,17 @@ __device__ __forceinline__ void rfd_drift(const Params& P, const Rep& R, int i, 
 // drift.  In reference mode the drift's nodes come from the displaced
 // position and its weights from q, as the reference does.
 template <bool ONE, int KN>
-__global__ void k_spread(FSL_KARGS, int drift, int ordered) {
+__global__ void k_spread(FSL_KARGS, int drift, int ordered, int box, int forces) {
   FSL_REP_FLAT(KIND_T4);
+  // the warp's aggregation box (low and high words), kept cleared
+  __shared__ unsigned s_box[kPartThreads / 32][2][kBoxNodes];
   long e;
   int a, qb;
   const int np = P.np;
+  // forces: the Verlet-list and bonded forces at the spread's positions are
+  // computed here (k_forces_vl's arithmetic) and stored, instead of read
+  const bool own_forces = forces && (P.verlet || P.nolist);
+  const bool cell_mode = own_forces ? vl_state(R, blk) : false;
   if (!quad_of(blk, np, e, a, qb)) return;
   const bool on = e < np;  // lanes past the end join the shuffles only
   // cell order on the cell-list path (a list the step has just built)
@@ -964,9 +1118,33 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
   {
     const double* qf = drift == 1 ? R.qp : R.q;
     double pos[3] = {qf[i], qf[np + i], qf[2 * np + i]};
-    double val[3] = {R.F[i], R.F[np + i], R.F[2 * (size_t)np + i]};
+    double val[3];
+    if (own_forces) {
+      quad_force_vl(P, R, i, a, drift == 1 ? 1 : 0, on, cell_mode, val[0], val[1], val[2]);
+      if (on && a == 0) {
+        if (!isfinite(val[0]) || !isfinite(val[1]) || !isfinite(val[2])) set_err(R.err, 2);
+        R.F[i] = val[0];
+        R.F[np + i] = val[1];
+        R.F[2 * (size_t)np + i] = val[2];
+      }
+    } else {
+      val[0] = R.F[i];
+      val[1] = R.F[np + i];
+      val[2] = R.F[2 * (size_t)np + i];
+    }
     quad_stencil<KN>(P, pos, pos, a, qb, S);
-    if (on) quad_spread<KN>(P, S, a, val, R.grid, sat);
+    if (P.prec == PREC_FIXED && box) {
+      unsigned* blo = s_box[threadIdx.x >> 5][0];
+      unsigned* bhi = s_box[threadIdx.x >> 5][1];
+      for (int n = threadIdx.x & 31; n < kBoxNodes; n += 32) {
+        blo[n] = 0u;
+        bhi[n] = 0u;
+      }
+      __syncwarp();
+      warp_spread<KN>(P, S, a, val, on, R.grid, sat, blo, bhi);
+    } else if (on) {
+      quad_spread<KN>(P, S, a, val, R.grid, sat);
+    }
   }
   if (drift) {
     // the RFD drift of the same particle, by the same quad
@@ -977,14 +1155,25 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered) {
   if (sat) set_err(R.err, 1);
 }
 
-void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s) {
+// FLUAMSL_SPREAD_BOX=0 spreads every product with its own global atomic (the
+// same sums, for comparison)
+static int spread_box() {
+  static const int on = [] {
+    const char* e = getenv("FLUAMSL_SPREAD_BOX");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return on;
+}
+
+void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s, bool forces) {
   if (B.max_np == 0) return;
   if (B.prec == PREC_F64) return launch_spread64(B, drift, s);
   const unsigned g = part_blocks(B, KIND_T4);
+  const int f = forces ? 1 : 0;
   if (B.kernel == 4)
-    FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered);
+    FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered, spread_box(), f);
   else
-    FSL_GO_T(k_spread, 3, g, kPartThreads, 0, s, B, drift, ordered);
+    FSL_GO_T(k_spread, 3, g, kPartThreads, 0, s, B, drift, ordered, spread_box(), f);
 }
 
 // ------------------------------------------------ tiled spread + W build ---
