@@ -134,8 +134,11 @@ def stage_bytes(name, P):
 
 
 # --------------------------------------------------------------- cpu side ---
-def cpu_run(workload, seconds, threads=None):
-    """Time the FP64 CPU implementation (oracle) on a bounded sample."""
+def cpu_run(workload, seconds, real="f64", native=True):
+    """Time the CPU implementation of the step (the oracle, built for this
+    host with -march=native, OpenMP over all host threads) on a bounded
+    sample of the workload; real="f32" times the FP32 build of the same
+    source."""
     from oracle import oracle_py as O
     from fluam_b200 import workloads as W
     w = W.WORKLOADS[workload]
@@ -144,8 +147,16 @@ def cpu_run(workload, seconds, threads=None):
         q, bi, bj = W.chains(w["chains"], w["beads"], L, 1, w["r0"])
     else:
         q, bi, bj = W.uniform(w["n"], L, 1), None, None
-    o = O.Oracle(m, m, m, L, L, L, q, eta=w["eta"], kT=w["kT"], dt=w["dt"], cutoff=w["rc"],
-                 kernel=w["kernel"], pair=O.PAIR_SOFT, soft_epsilon=w["eps"], seed=1)
+    try:
+        o = O.Oracle(m, m, m, L, L, L, q, eta=w["eta"], kT=w["kT"], dt=w["dt"], cutoff=w["rc"],
+                     kernel=w["kernel"], pair=O.PAIR_SOFT, soft_epsilon=w["eps"], seed=1,
+                     real=real, native=native)
+        build = "-march=native" if native else "-march=x86-64-v3"
+    except Exception:  # no compiler on this host: the portable build
+        o = O.Oracle(m, m, m, L, L, L, q, eta=w["eta"], kT=w["kT"], dt=w["dt"], cutoff=w["rc"],
+                     kernel=w["kernel"], pair=O.PAIR_SOFT, soft_epsilon=w["eps"], seed=1,
+                     real=real, native=False)
+        build = "-march=x86-64-v3"
     if bi is not None:
         o.set_bonds(bi, bj, np.full(len(bi), w["k"]), np.full(len(bi), w["r0"]))
     o.step(1)  # warm-up (page faults, thread pool)
@@ -158,10 +169,11 @@ def cpu_run(workload, seconds, threads=None):
         if el >= seconds or (n >= 2 and el * (n + 1) / n > 3 * seconds):
             break
     npart = q.shape[1]
+    prec = "FP64" if real == "f64" else "FP32"
     return {"value": npart * n / el, "unit": "particle-steps/s", "cores": O.num_threads(),
-            "kind": "port",
-            "sample": f"{n} steps of {workload} ({m}^3, {npart} particles), FP64 oracle, "
-                      f"{el:.1f} s, OpenMP {O.num_threads()} threads"}
+            "kind": "port", "steps": n, "seconds": el, "precision": prec,
+            "sample": f"{n} steps of {workload} ({m}^3, {npart} particles), {prec} CPU "
+                      f"restatement ({build}), {el:.1f} s, OpenMP {O.num_threads()} threads"}
 
 
 def run_reference(args, rank, world):
@@ -170,17 +182,23 @@ def run_reference(args, rank, world):
     per = max(args.cpu_seconds / max(args.steps, 1), 1.0)
     per = min(per, args.cpu_seconds)
     r = cpu_run(args.workload, per * max(1, min(args.steps, 3)))
+    r32 = cpu_run(args.workload, min(per, 10.0), real="f32")
     line = {
         "metric": "particle-steps/s", "value": r["value"], "unit": "particle-steps/s",
-        "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "impl": "reference", "n_gpus": world, "steps": r["steps"], "warmup": 1,
+        "requested_steps": args.steps, "requested_warmup": args.warmup,
         "higher_is_better": True, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args.workload),
+        "precision": {"fields": "fp64", "positions": "fp64", "spread": "fp64 sums"},
         "cpu_baseline": {"value": r["value"], "unit": r["unit"], "cores": r["cores"],
                          "kind": r["kind"], "sample": r["sample"]},
+        "cpu_fp32": {"value": r32["value"], "unit": r32["unit"], "cores": r32["cores"],
+                     "kind": r32["kind"], "sample": r32["sample"]},
         "e2e": {"value": r["value"], "unit": r["unit"], "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "note": "the reference's CUDA build does not compile with CUDA 12 (legacy texture "
-                "references); this arm times the FP64 CPU restatement of its step",
+                "references); this arm times the CPU restatement of its step (FP64, and its "
+                "FP32 build in cpu_fp32) on the host's cores",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -211,7 +229,6 @@ def workload_config(name):
                         + f", soft repulsion eps={w['eps']} rc={w['rc']}, {w['kernel']}-pt kernel,"
                           f" eta={w['eta']} kT={w['kT']} dt={w['dt']}",
             "cells": w["cells"], "np": w["n"], "kernel": w["kernel"],
-            "fields": "fp32", "positions": "fp64", "spread": "int64 fixed point 2^-40",
             "l2": "flushed between timed steps (256 MiB write)"}
 
 
@@ -221,6 +238,31 @@ def step_bytes(nc, npart):
     fields written and read once per pass, FP64 particle state, noise kept
     in registers)."""
     return 144 * nc + 384 * npart
+
+
+def run_fp64_form(torch, workload, steps=20, warmup=3):
+    """The all-FP64 precision form (noise, spreading, fields, FFTs and
+    interpolation in FP64) on the same workload, device time per step."""
+    from fluam_b200 import StokesLimit, workloads
+    cfg, q, bonds = workloads.build(workload, seed=1)
+    cfg.precision = 2  # FSL_PRECISION_FP64
+    g = StokesLimit(cfg, q)
+    if bonds is not None:
+        g.load_bonds(*bonds)
+    s = torch.cuda.ExternalStream(g.L.fsl_stream(g.h))
+    g.step(warmup)
+    g.sync()
+    a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    g.step(steps)
+    z.record(s)
+    g.sync()
+    ms = a.elapsed_time(z) / steps
+    g.close()
+    return {"value": q.shape[1] / (ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms,
+            "steps": steps,
+            "precision": "fp64 noise, spreading (FP64 atomics), fields, FFTs, interpolation",
+            "l2": "not flushed (the step's FP64 state exceeds the L2)"}
 
 
 def run_batched(torch, steps=20, warmup=3, plain_sample=128):
@@ -311,8 +353,8 @@ def serve_requests(n_per_s, duration, seed, steps_range):
 
 
 # Arrival rates of the serving sweep (requests/s) and how long each stream
-# keeps arriving (s): 20, 60 and 120 requests.
-SERVE_SWEEP = ((10.0, 2.0), (100.0, 0.6), (1000.0, 0.12))
+# keeps arriving (s): about 200 requests per rate.
+SERVE_SWEEP = ((10.0, 20.0), (100.0, 2.0), (1000.0, 0.2))
 
 
 def serve_stream(srv, reqs):
@@ -484,10 +526,11 @@ def main():
                 traffic = tr["stages"][dname]["dram_bytes"]
         except (OSError, KeyError, ValueError):
             traffic = None
-        cpu = None
+        cpu = cpu32 = None
         if not args.no_cpu_baseline:
             try:
                 cpu = cpu_run(args.workload, args.cpu_seconds)
+                cpu32 = cpu_run(args.workload, min(args.cpu_seconds, 10.0), real="f32")
             except Exception as e:  # reported, not fatal
                 cpu = {"value": None, "unit": "particle-steps/s", "cores": 0, "kind": "port",
                        "sample": f"failed: {e}"}
@@ -497,8 +540,9 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(workload_config(args.workload),
-                           parallelism=f"replicas{world}" if world > 1 else "single"),
+            "config": workload_config(args.workload),
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "precision": {"fields": "fp32", "positions": "fp64", "spread": "int64 fixed point 2^-40"},
             "grid_cell_updates_per_s": world * P["nc"] * args.steps / (t_max * 1e-3),
             "e2e": {"value": world * npart * ke / e2e_max, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": 24 * npart, "d2h_bytes_per_step": 24 * npart},
@@ -509,6 +553,7 @@ def main():
             "stages_ms_per_step": {k: v["total_ms"] / args.steps for k, v in sorted(stages.items())},
             "profiled_ms_per_step": prof_ms / args.steps,
             "cpu_baseline": cpu,
+            "cpu_fp32": cpu32,
             "clocks": clk,
             "gpu_launches": st["launches_per_step"] * args.steps,
             "step_roofline": {"bytes_per_step": step_bytes(P["nc"], npart),
@@ -516,6 +561,11 @@ def main():
                               "peak": hbm, "unit": "GB/s",
                               "frac": step_bytes(P["nc"], npart) / (t_max / args.steps * 1e-3) / 1e9 / hbm},
         }
+        if world == 1:
+            try:
+                line["fp64_form"] = run_fp64_form(torch, args.workload)
+            except Exception as e:  # reported, not fatal
+                line["fp64_form"] = {"error": repr(e)}
         if world == 1 and not args.no_batched:
             sim.close()
             for key, fn in (("batched", run_batched), ("served", run_served)):
