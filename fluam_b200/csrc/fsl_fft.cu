@@ -302,29 +302,26 @@ constexpr int kFftThreads = 512;
 
 // W = f + c div(Sigma) of all three components of every cell
 // (src/stokesLimitFunctions.cu:2281-2378, 3922-4069): the fixed-point spread
-// field times 2^-40/dV plus the stochastic stress divergence, with
-// c = sqrt(2) (midpoint, one stress sample), sqrt(1/2) (two samples) or 1
-// (first-order scheme, src/runSchemeStokesLimitFirstOrder.cu:181-190).  The spread
-// field is cleared behind the read, ready for the next spread.  One thread
-// per cell: the loads of a warp are coalesced rows, full occupancy.
+// field times 2^-40/dV plus c times the stochastic stress divergence that
+// k_div wrote (D1 = div Sigma_1 for one stress sample, D12 =
+// div(Sigma_1 + Sigma_2) for two), with c = sqrt(2) (midpoint, one sample),
+// sqrt(1/2) (two samples) or 1 (first-order scheme,
+// src/runSchemeStokesLimitFirstOrder.cu:181-190).  The spread field is
+// cleared behind the read, ready for the next spread.  One thread per cell:
+// the loads of a warp are coalesced rows, full occupancy.
 template <bool ONE>
 __global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
   FSL_REP_AT(blockIdx.y);
   const float scale = (float)(kFixedInv / P.dV);
-  const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
-  const float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
-  const float a4x = (float)P.invdx * f4, a4y = (float)P.invdy * f4, a4z = (float)P.invdz * f4;
-  const float* n1 = R.noise;
-  const float* n2 = R.noise + (size_t)6 * P.nc + (size_t)9 * P.np;
+  const float fac = (float)nfac;
   const size_t nc = (size_t)P.nc;
+  const float* D = R.ndiv + (nsets > 1 ? 3 * nc : 0);
   // float-atomic form: FP32 sums in the first 3 nc floats of the buffer
   const bool fatom = P.prec == PREC_FLOAT;
   float* gf = reinterpret_cast<float*>(R.grid);
   const float fscale = (float)(1.0 / P.dV);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc;
        i += (size_t)gridDim.x * blockDim.x) {
-    int x = (int)(i % P.mx), r = (int)(i / P.mx);
-    int y = r % P.my, z = r / P.my;
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
       float w;
@@ -336,8 +333,7 @@ __global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
         w = (float)((double)g * (double)scale);
         R.grid[comp * nc + i] = 0ull;
       }
-      w += stress_div(P, n1, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
-      if (nsets > 1) w += stress_div(P, n2, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
+      w += fac * __ldg(D + comp * nc + i);
       R.wbuf[comp * nc + i] = w;
     }
   }
@@ -349,24 +345,15 @@ template <bool ONE>
 __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
   FSL_REP_AT(blockIdx.y);
   const float scale = (float)(kFixedInv / P.dV);
-  const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
-  const float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
-  const float a4x = (float)P.invdx * f4, a4y = (float)P.invdy * f4, a4z = (float)P.invdz * f4;
-  const float* n1 = R.noise;
-  const size_t off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
-  const float* n2 = R.noise + off2;
-  const bool al2 = (off2 & 3) == 0;
+  const float fac = (float)nfac;
   const size_t nc = (size_t)P.nc;
-  const int gx = P.mx >> 2;
+  const float* D = R.ndiv + (nsets > 1 ? 3 * nc : 0);
   const size_t ng = nc >> 2;
   const bool fatom = P.prec == PREC_FLOAT;
   float* gf = reinterpret_cast<float*>(R.grid);
   const float fscale = (float)(1.0 / P.dV);
   for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < ng;
        g += (size_t)gridDim.x * blockDim.x) {
-    const int x0 = (int)(g % gx) << 2;
-    const int r = (int)(g / gx);
-    const int y = r % P.my, z = r / P.my;
     const size_t i0 = g << 2;
     float w[3][4];
 #pragma unroll
@@ -388,8 +375,14 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
       w[comp][2] = (float)((double)gb.x * (double)scale);
       w[comp][3] = (float)((double)gb.y * (double)scale);
     }
-    stress_div4(P, n1, true, x0, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
-    if (nsets > 1) stress_div4(P, n2, al2, x0, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      const float4 d = __ldg(reinterpret_cast<const float4*>(D + comp * nc + i0));
+      w[comp][0] += fac * d.x;
+      w[comp][1] += fac * d.y;
+      w[comp][2] += fac * d.z;
+      w[comp][3] += fac * d.w;
+    }
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
       *reinterpret_cast<float4*>(R.wbuf + comp * nc + i0) =

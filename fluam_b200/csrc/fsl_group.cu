@@ -26,7 +26,7 @@ size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 // Byte offsets of one slot's buffers inside its arena.
 struct SlotLayout {
   size_t q, qp, F, u, qw, ws, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
-      bsum, ljtab, noise, grid, spec, v, wbuf, noise64, v64, z64, err, t, q0, obs, obs_part, obs_ticket,
+      bsum, ljtab, noise, ndiv, grid, spec, v, wbuf, noise64, v64, z64, err, t, q0, obs, obs_part, obs_ticket,
       start1, sorted1, ws1, vl_cnt, vl_idx, qref, vl_flag, bar, total;
 };
 
@@ -64,6 +64,8 @@ SlotLayout layout(const Params& P, int np_cap) {
   // form uses its first 3 nc floats)
   const bool f64 = P.prec == FSL_PRECISION_FP64;
   L.noise = take(f64 ? 0 : sizeof(float) * noise);
+  // the stress divergence D1 | D12 of the 3-D Stokes schemes (k_div)
+  L.ndiv = take(!f64 && P.scheme <= FSL_SCHEME_FIRST_ORDER ? sizeof(float) * 6 * nc : 0);
   L.grid = take(sizeof(unsigned long long) * 3 * nc);
   L.spec = take(f64 ? 0 : sizeof(float2) * 3 * (size_t)P.my * P.mz * P.mxh);
   L.v = take(f64 ? 0 : sizeof(float) * 3 * nc);
@@ -344,6 +346,7 @@ int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st) {
   r.bsum = (int*)(base + L.bsum);
   r.ljtab = (float*)(base + L.ljtab);
   r.noise = (float*)(base + L.noise);
+  r.ndiv = (float*)(base + L.ndiv);
   r.grid = (unsigned long long*)(base + L.grid);
   r.spec = (float2*)(base + L.spec);
   r.v = (float*)(base + L.v);
@@ -578,6 +581,7 @@ int group_init(Group& g, const Params& P0) {
   FSL_TRY(cudaStreamCreateWithPriority(&g.side, cudaStreamNonBlocking, lo));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
+  FSL_TRY(cudaEventCreateWithFlags(&g.ev_join2, cudaEventDisableTiming));
   tile_init();
   return FSL_OK;
 }
@@ -589,8 +593,9 @@ void group_destroy(Group& g) {
   }
   if (g.ev_fork) cudaEventDestroy(g.ev_fork);
   if (g.ev_join) cudaEventDestroy(g.ev_join);
+  if (g.ev_join2) cudaEventDestroy(g.ev_join2);
   g.side = nullptr;
-  g.ev_fork = g.ev_join = nullptr;
+  g.ev_fork = g.ev_join = g.ev_join2 = nullptr;
   fft_plan_destroy(g.fft);
   g.fft = nullptr;
   if (g.d_reps) cudaFree(g.d_reps);
@@ -720,23 +725,36 @@ void group_enqueue_step(Group& g) {
   g.fail_stage = nullptr;
   chk("before the step");
   // the noise of step t has no input but the step counter: it runs on the
-  // side stream beside the cell list and the forces, joined before its
-  // first reader (profiled steps keep one stream so that the stage
-  // intervals stay sequential)
+  // side stream beside the cell list, forces and spread (part 0: the
+  // normals and the divergence of stress sample 1, read by the first W
+  // build) and beside the first solve (part 1: the divergence of sample 2,
+  // read by the second W build), joined before their first readers
+  // (profiled steps keep one stream so that the stage intervals stay
+  // sequential)
   const bool fork = !pr.on && g.side;
+  const bool div = B.prec != PREC_F64 && g.key.scheme <= FSL_SCHEME_FIRST_ORDER;
+  const bool two = div && g.key.scheme == FSL_SCHEME_MIDPOINT;
   if (fork) {
     cudaEventRecord(g.ev_fork, s);
     cudaStreamWaitEvent(g.side, g.ev_fork, 0);
-    launch_noise(B, g.side);
+    launch_noise(B, g.side, g.key.scheme, 0);
     cudaEventRecord(g.ev_join, g.side);
+    if (two) {
+      launch_noise(B, g.side, g.key.scheme, 1);
+      cudaEventRecord(g.ev_join2, g.side);
+    }
   } else {
     pr.mark(s, "noise");
-    launch_noise(B, s);
+    launch_noise(B, s, g.key.scheme, 0);
+    if (two) launch_noise(B, s, g.key.scheme, 1);
   }
   chk("noise");
-  pr.count(1);
+  pr.count(1 + (div ? 1 : 0) + (two ? 1 : 0));
   auto join_noise = [&]() {
     if (fork) cudaStreamWaitEvent(s, g.ev_join, 0);
+  };
+  auto join_noise2 = [&]() {
+    if (fork && two) cudaStreamWaitEvent(s, g.ev_join2, 0);
   };
   auto observe = [&]() {
     if (!g.key.observe) return;
@@ -865,6 +883,7 @@ void group_enqueue_step(Group& g) {
   pr.count(pk);
   cells_forces(1, !B.tiled);
   if (B.tiled) {
+    join_noise2();
     pr.mark(s, "spread_w_rfd");
     launch_spread_w(B, 1, 2, 0.70710678118654752440, s);
     chk("spread_w_rfd");
@@ -875,6 +894,7 @@ void group_enqueue_step(Group& g) {
     chk("spread_rfd");
     pr.count(pk);
   }
+  join_noise2();
   launch_solve(B, g.fft, 2, 0.70710678118654752440, B.tiled, s, &pr);
   chk("solve");
   // option 2: corrector

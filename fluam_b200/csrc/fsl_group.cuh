@@ -103,7 +103,7 @@ struct Group {
   // the noise of a step runs beside the cell list and forces on this stream
   // (fork and join events); profiled steps keep everything on `stream`
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;  // noise parts 0, 1
   Prof prof;
   std::map<std::string, std::pair<int64_t, double>> stage_acc;
   int launches = 0;             // kernels of this group in one step

@@ -391,6 +391,9 @@ struct Rep {
   double *bfp_k, *bfp_r0, *bfp_xyz;
   float* ljtab;
   float* noise;
+  // the 3-D Stokes schemes: D1 = div(Sigma_1) | D12 = div(Sigma_1 + Sigma_2),
+  // [3][nc] each (k_div), read by the W build
+  float* ndiv;
   unsigned long long* grid;
   float2* spec;
   float* v;
@@ -590,7 +593,12 @@ inline unsigned part_blocks(const Batch& B, int k) {
   return (unsigned)B.nblk[k];
 }
 
-void launch_noise(const Batch& B, cudaStream_t s);
+// The noise of one step in two parts.  Part 0 draws the normals in the
+// reference's layout; for the 3-D Stokes schemes (scheme 0 midpoint, 1 first
+// order) it also turns stress sample 1 into its divergence D1 (k_div), and
+// part 1 (midpoint only) adds the divergence of sample 2 into D12.  For the
+// other schemes part 1 does nothing.
+void launch_noise(const Batch& B, cudaStream_t s, int scheme, int part);
 void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t count, float* out,
                         cudaStream_t s);
 // which = 0: cell list / forces at q, 1: at q^{n+1/2}.  The build leaves the

@@ -42,7 +42,77 @@ __global__ void k_noise_range(uint64_t seed, uint64_t t, uint64_t first, int64_t
   out[k] = lane == 0 ? v.x : lane == 1 ? v.y : lane == 2 ? v.z : v.w;
 }
 
-void launch_noise(const Batch& B, cudaStream_t s) {
+// ------------------------------------------------- stress divergence noise ---
+// The 3-D Stokes schemes read the stochastic stress only through its
+// divergence (W = f + c div(Sigma), src/stokesLimitFunctions.cu:2281-2378,
+// 3922-4069).  k_div turns the drawn stress samples into that divergence on
+// the noise's side stream, so the W builds on the step's critical path read
+// 3 nc floats instead of 6 nc or 12 nc: set 0 writes D1 = div(Sigma_1) to
+// Rep::ndiv, set 1 writes D12 = D1 + div(Sigma_2) after it.  The terms and
+// their order are those of stress_div (the W build multiplies D by its
+// factor c); one thread per four x cells where mx is a multiple of 4.
+template <bool ONE>
+__global__ void k_div(FSL_KARGS, int set) {
+  FSL_REP_AT(blockIdx.y);
+  const size_t nc = (size_t)P.nc;
+  const float a1x = (float)P.invdx * (float)P.fact1, a1y = (float)P.invdy * (float)P.fact1,
+              a1z = (float)P.invdz * (float)P.fact1;
+  const float a4x = (float)P.invdx * (float)P.fact4, a4y = (float)P.invdy * (float)P.fact4,
+              a4z = (float)P.invdz * (float)P.fact4;
+  const size_t off = set ? (size_t)6 * nc + (size_t)9 * P.np : 0;
+  const float* n = R.noise + off;
+  float* D = R.ndiv + (set ? 3 * nc : 0);
+  if ((P.mx & 3) == 0) {
+    const bool aligned = (off & 3) == 0;
+    const int gx = P.mx >> 2;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < nc >> 2;
+         g += (size_t)gridDim.x * blockDim.x) {
+      const int x0 = (int)(g % gx) << 2;
+      const int r = (int)(g / gx);
+      const int y = r % P.my, z = r / P.my;
+      const size_t i0 = g << 2;
+      float w[3][4] = {};
+      stress_div4(P, n, aligned, x0, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp) {
+        float4 d = make_float4(w[comp][0], w[comp][1], w[comp][2], w[comp][3]);
+        if (set) {
+          const float4 d1 = *reinterpret_cast<const float4*>(R.ndiv + comp * nc + i0);
+          d = make_float4(d1.x + d.x, d1.y + d.y, d1.z + d.z, d1.w + d.w);
+        }
+        *reinterpret_cast<float4*>(D + comp * nc + i0) = d;
+      }
+    }
+    return;
+  }
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % P.mx), r = (int)(i / P.mx);
+    const int y = r % P.my, z = r / P.my;
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      float d = stress_div(P, n, comp, x, y, z, (int)i, a1x, a1y, a1z, a4x, a4y, a4z);
+      if (set) d = R.ndiv[comp * nc + i] + d;
+      D[comp * nc + i] = d;
+    }
+  }
+}
+
+static void launch_div(const Batch& B, int set, cudaStream_t s) {
+  const int tb = 256;
+  const long work = (B.mx & 3) == 0 ? (long)B.nc / 4 : (long)B.nc;
+  long blocks = (work + tb - 1) / tb;
+  const long cap = (148L * 16 + B.nrep - 1) / B.nrep;
+  if (blocks > cap) blocks = cap < 1 ? 1 : cap;
+  FSL_GO(k_div, dim3((unsigned)blocks, B.nrep), tb, 0, s, B, set);
+}
+
+void launch_noise(const Batch& B, cudaStream_t s, int scheme, int part) {
+  const bool div = B.prec != PREC_F64 && scheme <= 1;
+  if (part != 0) {
+    // the second stress sample's divergence, after the first's
+    if (div && scheme == 0) launch_div(B, 1, s);
+    return;
+  }
   if (B.prec == PREC_F64) return launch_noise64(B, s);
   const int tb = 256;
   uint64_t nb = (B.max_noise_n + 3) / 4;
@@ -50,6 +120,7 @@ void launch_noise(const Batch& B, cudaStream_t s) {
   unsigned cap = (unsigned)((148 * 16 + B.nrep - 1) / B.nrep);
   if (bx > cap) bx = cap < 1 ? 1 : cap;
   FSL_GO(k_noise, dim3(bx, B.nrep), tb, 0, s, B);
+  if (div) launch_div(B, 0, s);
 }
 
 void launch_noise_range(const Params& P, uint64_t t, uint64_t first, int64_t count, float* out,
@@ -1413,16 +1484,11 @@ __global__ void __launch_bounds__(kTileThreads) k_spread_w(FSL_KARGS, int drift,
   __syncthreads();
   // W of the tile's cells
   const float scale = (float)(kFixedInv / P.dV);
-  const float f1 = (float)(nfac * P.fact1), f4 = (float)(nfac * P.fact4);
-  const float a1x = (float)P.invdx * f1, a1y = (float)P.invdy * f1, a1z = (float)P.invdz * f1;
-  const float a4x = (float)P.invdx * f4, a4y = (float)P.invdy * f4, a4z = (float)P.invdz * f4;
-  const float* n1 = R.noise;
-  const size_t off2 = (size_t)6 * P.nc + (size_t)9 * P.np;
-  const float* n2 = R.noise + off2;
+  const float fac = (float)nfac;
   const size_t nc = (size_t)P.nc;
+  const float* D = R.ndiv + (nsets > 1 ? 3 * nc : 0);
   const int ex = min(kTileX, P.mx - x0), ey = min(kTileY, P.my - y0), ez = min(kTileZ, P.mz - z0);
   if ((P.mx & 3) == 0) {
-    const bool al2 = (off2 & 3) == 0;
     constexpr int GX = kTileX / 4;
     for (int g = threadIdx.x; g < GX * kTileY * kTileZ; g += blockDim.x) {
       const int lx = 4 * (g % GX), ly = (g / GX) % kTileY, lz = g / (GX * kTileY);
@@ -1436,8 +1502,14 @@ __global__ void __launch_bounds__(kTileThreads) k_spread_w(FSL_KARGS, int drift,
         for (int c = 0; c < 4; ++c)
           w[comp][c] = (float)((double)(long long)acc[comp * kTileCells + (lz * kTileY + ly) * kTileX + lx + c] *
                                (double)scale);
-      stress_div4(P, n1, true, x, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
-      if (nsets > 1) stress_div4(P, n2, al2, x, y, z, i0, a1x, a1y, a1z, a4x, a4y, a4z, w);
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp) {
+        const float4 d = __ldg(reinterpret_cast<const float4*>(D + comp * nc + i0));
+        w[comp][0] += fac * d.x;
+        w[comp][1] += fac * d.y;
+        w[comp][2] += fac * d.z;
+        w[comp][3] += fac * d.w;
+      }
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp)
         *reinterpret_cast<float4*>(R.wbuf + comp * nc + i0) =
@@ -1452,8 +1524,7 @@ __global__ void __launch_bounds__(kTileThreads) k_spread_w(FSL_KARGS, int drift,
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp) {
         float w = (float)((double)(long long)acc[comp * kTileCells + c] * (double)scale);
-        w += stress_div(P, n1, comp, x, y, z, i, a1x, a1y, a1z, a4x, a4y, a4z);
-        if (nsets > 1) w += stress_div(P, n2, comp, x, y, z, i, a1x, a1y, a1z, a4x, a4y, a4z);
+        w += fac * __ldg(D + comp * nc + i);
         R.wbuf[comp * nc + i] = w;
       }
     }
