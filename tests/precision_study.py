@@ -16,8 +16,11 @@ dt = 0.002, soft repulsion eps = 1, rc = 1.5, 200 steps.  Forms:
    the oracle's.
 2. Per-step errors over the whole run: form (c) advances the reference
    trajectory; at every step forms (a) and (b) start from its state and their
-   displacement and velocity are compared with its result.  (c) itself is
-   pinned to the oracle by part 1.
+   displacement and velocity are compared with its result.  Every
+   --oracle-every steps the oracle also takes that step from the same state,
+   and all three forms are compared with it, so the oracle pins the forms
+   along the whole run (an oracle step at 256^3 / 10^6 particles takes some
+   seconds on the host's cores).
 3. Reproducibility: every form runs the whole run twice from the same start
    (graph replay); the final positions are compared bit for bit.
 
@@ -58,6 +61,8 @@ def main(argv=None):
     ap.add_argument("--np", type=int, default=1_000_000)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--oracle-steps", type=int, default=2)
+    ap.add_argument("--oracle-every", type=int, default=10,
+                    help="compare every k-th step of the run with the oracle (0: none)")
     ap.add_argument("--v-every", type=int, default=10, help="compare the velocity fields every k steps")
     ap.add_argument("--dt", type=float, default=0.002)
     ap.add_argument("--seed", type=int, default=2024)
@@ -118,19 +123,40 @@ def main(argv=None):
                              "v_rel_l2": rel_l2(vg, vo)}
             pin.append(row)
             print("oracle pin", json.dumps(row), flush=True)
-        del o
     report["oracle_pin"] = pin
+    o = None
+    if a.oracle_every > 0:
+        o = oracle.Oracle(m, m, m, L[0], L[1], L[2], q0, pair=oracle.PAIR_SOFT, seed=a.seed,
+                          **{k: params[k] for k in ("eta", "kT", "dt", "cutoff", "kernel")})
 
     # 2. per-step errors of (a), (b) against the FP64 form's trajectory
     per = {"fixed64": [], "float_atomic": []}
+    along = []  # every --oracle-every steps: all forms against the oracle
     q = q0.copy()
     for t in range(a.steps):
-        wv = t % a.v_every == 0
+        orc = o is not None and t % a.oracle_every == 0
+        wv = t % a.v_every == 0 or orc
         qc, Fc, vc = teacher_step(inst[2], q, t, wv)
+        got = {2: (qc, Fc, vc)}
         for p in (0, 1):
             qg, Fg, vg = teacher_step(inst[p], q, t, wv)
+            got[p] = (qg, Fg, vg)
             per[FORMS[p]].append([rel_inf(qg - q, qc - q), rel_l2(qg - q, qc - q),
                                   rel_inf(vg, vc) if wv else np.nan, rel_l2(vg, vc) if wv else np.nan])
+        if orc:
+            o.set_positions(q)
+            o.t = t
+            t0 = time.time()
+            o.step(1)
+            t_orc = time.time() - t0
+            qo, Fo, vo = o.positions(), o.forces(), o.velocity()
+            row = {"step": t, "oracle_seconds": t_orc}
+            for p, name in FORMS.items():
+                qg, Fg, vg = got[p]
+                row[name] = {"dq_rel_inf": rel_inf(qg - q, qo - q), "F_rel_inf": rel_inf(Fg, Fo),
+                             "v_rel_inf": rel_inf(vg, vo)}
+            along.append(row)
+            print("oracle along", json.dumps(row), flush=True)
         q = qc
         if t % 20 == 0:
             print("step", t, {k: v[-1] for k, v in per.items()}, flush=True)
@@ -141,6 +167,8 @@ def main(argv=None):
                    "dq_rel_l2_max": float(r[:, 1].max()), "v_rel_inf_max": float(np.nanmax(r[:, 2])),
                    "v_rel_inf_median": float(np.nanmedian(r[:, 2])), "v_rel_l2_max": float(np.nanmax(r[:, 3]))}
     report["per_step_vs_fp64_form"] = summ
+    report["oracle_along_run"] = along
+    report["oracle_every"] = a.oracle_every
     report["per_step_rows"] = {k: [[None if np.isnan(x) else x for x in row] for row in v]
                                for k, v in per.items()}
     report["velocity_every"] = a.v_every
@@ -190,6 +218,17 @@ def markdown(r):
                 e = row[f]
                 s.append(f"| {row['step']} | {f} | {e['dq_rel_inf']:.2e} | {e['dq_rel_l2']:.2e} | "
                          f"{e['F_rel_inf']:.2e} | {e['v_rel_inf']:.2e} | {e['v_rel_l2']:.2e} |\n")
+    if r.get("oracle_along_run"):
+        s.append(f"\n## Against the FP64 oracle along the run (every {r['oracle_every']} steps of the "
+                 "FP64 form's trajectory, teacher forced)\n")
+        s.append("| form | steps compared | dq rel_inf max | dq rel_inf median | F rel_inf max | v rel_inf max |\n"
+                 "|---|---|---|---|---|---|\n")
+        for f in FORMS.values():
+            dq = [row[f]["dq_rel_inf"] for row in r["oracle_along_run"]]
+            fr = [row[f]["F_rel_inf"] for row in r["oracle_along_run"]]
+            vv = [row[f]["v_rel_inf"] for row in r["oracle_along_run"]]
+            s.append(f"| {f} | {len(dq)} | {max(dq):.2e} | {float(np.median(dq)):.2e} | {max(fr):.2e} | "
+                     f"{max(vv):.2e} |\n")
     s.append("\n## Every step against the FP64 form's trajectory (teacher forced; velocity fields "
              f"every {r['velocity_every']} steps)\n")
     s.append("| form | dq rel_inf max | dq rel_inf median | dq rel_l2 max | v rel_inf max | v rel_inf median | v rel_l2 max |\n|---|---|---|---|---|---|---|\n")
