@@ -107,24 +107,35 @@ class ClockSampler:
 # ---------------------------------------------------------- algorithmic bytes
 def stage_bytes(name, P):
     """Algorithmic DRAM bytes of one launch of a stage (FP32 fields, FP64
-    particle state, materialised FP32 noise, int64 fixed-point spread grid)."""
+    particle state, FP32 stress samples and their divergence, int64
+    fixed-point spread grid).  P["fused"]: the Verlet-list forces are
+    computed inside the spread that follows them (the default)."""
     nc, npart, k = P["nc"], P["np"], P["kernel"]
     spec = 3 * 8 * (P["mx"] // 2 + 1) * P["my"] * P["mz"]
     touched = 3 * 8 * min(P["nc"], k ** 3 * npart)
+    # positions read + F written and the pair lists read, when fused;
+    # positions and F read otherwise
+    part = 52 * npart if P.get("fused", True) else 48 * npart
     return {
-        "noise": 4 * (12 * nc + 9 * npart),
+        # three launches per step, averaged: the raw samples and particle
+        # noise written (48 nc + 36 np), the divergence of sample 1
+        # (6 nc read, 3 nc written) and of sample 2 added to it (9 nc read,
+        # 3 nc written)
+        "noise": (48 * nc + 36 * npart + 36 * nc + 48 * nc) // 3,
         "cells": 40 * npart + 12 * P["mN"],
         "forces": 52 * npart + 4 * P["mN"],
         "grid_zero": 24 * nc,
-        "spread": 48 * npart + 2 * touched,
+        "spread": part + 2 * touched,
         # force spread + the drift test (reference mode: the drift spreads
         # cancel and are skipped except at stencil changes)
-        "spread_rfd": 48 * npart + 2 * touched + 36 * npart,
-        # int64 field read + cleared, mean noise of the two solves, W written
-        "wbuild": 24 * nc + 24 * nc + 36 * nc + 12 * nc,
+        "spread_rfd": part + 2 * touched + 36 * npart,
+        # int64 field read + cleared, divergence of the noise read, W written
+        "wbuild": 24 * nc + 24 * nc + 12 * nc + 12 * nc,
         "plane_fwd": 12 * nc + spec,               # W read, half spectrum written
         "plane_inv": spec + 12 * nc,
-        "xfwd": 24 * nc + 36 * nc + spec,
+        "fft_x": 12 * nc + spec,                   # line schedule: x forward or inverse
+        "fft_y": 2 * spec,
+        "xfwd": 12 * nc + spec,                    # general sizes: x forward of W
         "yfft": 2 * spec,
         "zsolve": 2 * spec,
         "xinv": spec + 12 * nc,
@@ -512,7 +523,7 @@ def main():
         hbm, peak_kind = peaks()
         P = {"nc": cfg.mx * cfg.my * cfg.mz, "np": npart, "kernel": cfg.kernel, "mx": cfg.mx,
              "my": cfg.my, "mz": cfg.mz,
-             "mN": int(np.prod(sim.neighbor_grid()))}
+             "mN": int(np.prod(sim.neighbor_grid())), "fused": "forces" not in stages}
         dom = max(stages.items(), key=lambda kv: kv[1]["total_ms"])
         dname, dv = dom
         avg_ms = dv["total_ms"] / max(dv["launches"], 1)

@@ -325,15 +325,14 @@ __global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
       float w;
+      const float d = __ldg(D + comp * nc + i);
       if (fatom) {
-        w = gf[comp * nc + i] * fscale;
+        w = w_float(gf[comp * nc + i], fscale, fac, d);
         gf[comp * nc + i] = 0.0f;
       } else {
-        long long g = (long long)R.grid[comp * nc + i];
-        w = (float)((double)g * (double)scale);
+        w = w_fixed((long long)R.grid[comp * nc + i], scale, fac, d);
         R.grid[comp * nc + i] = 0ull;
       }
-      w += fac * __ldg(D + comp * nc + i);
       R.wbuf[comp * nc + i] = w;
     }
   }
@@ -358,30 +357,23 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
     float w[3][4];
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
+      const float4 d = __ldg(reinterpret_cast<const float4*>(D + comp * nc + i0));
       if (fatom) {
         float4* fp = reinterpret_cast<float4*>(gf + comp * nc + i0);
         const float4 ga = *fp;
-        w[comp][0] = ga.x * fscale;
-        w[comp][1] = ga.y * fscale;
-        w[comp][2] = ga.z * fscale;
-        w[comp][3] = ga.w * fscale;
+        w[comp][0] = w_float(ga.x, fscale, fac, d.x);
+        w[comp][1] = w_float(ga.y, fscale, fac, d.y);
+        w[comp][2] = w_float(ga.z, fscale, fac, d.z);
+        w[comp][3] = w_float(ga.w, fscale, fac, d.w);
         *fp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         continue;
       }
       const longlong2* gp = reinterpret_cast<const longlong2*>(R.grid + comp * nc + i0);
       const longlong2 ga = gp[0], gb = gp[1];
-      w[comp][0] = (float)((double)ga.x * (double)scale);
-      w[comp][1] = (float)((double)ga.y * (double)scale);
-      w[comp][2] = (float)((double)gb.x * (double)scale);
-      w[comp][3] = (float)((double)gb.y * (double)scale);
-    }
-#pragma unroll
-    for (int comp = 0; comp < 3; ++comp) {
-      const float4 d = __ldg(reinterpret_cast<const float4*>(D + comp * nc + i0));
-      w[comp][0] += fac * d.x;
-      w[comp][1] += fac * d.y;
-      w[comp][2] += fac * d.z;
-      w[comp][3] += fac * d.w;
+      w[comp][0] = w_fixed(ga.x, scale, fac, d.x);
+      w[comp][1] = w_fixed(ga.y, scale, fac, d.y);
+      w[comp][2] = w_fixed(gb.x, scale, fac, d.z);
+      w[comp][3] = w_fixed(gb.y, scale, fac, d.w);
     }
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
@@ -973,8 +965,10 @@ FftPlan* fft_plan_create(const Params& P) {
   for (int v = 0; v < 2; ++v) {
     if (fp->plane_fwd_r[0] &&
         !(allow((const void*)fp->plane_fwd_r[v], fp->smem_plane_r) &&
-          allow((const void*)fp->plane_inv_r[v], fp->smem_plane_r)))
-      fp->plane_fwd_r[0] = fp->plane_fwd_r[1] = fp->plane_inv_r[0] = fp->plane_inv_r[1] = nullptr;
+          allow((const void*)fp->plane_inv_r[v], fp->smem_plane_r))) {
+      fp->plane_fwd_r[0] = fp->plane_fwd_r[1] = nullptr;
+      fp->plane_inv_r[0] = fp->plane_inv_r[1] = nullptr;
+    }
   }
   for (int v = 0; v < 2; ++v) {
     if (fp->line_xf[0] &&

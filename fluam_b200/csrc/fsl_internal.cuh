@@ -118,6 +118,19 @@ __device__ inline float4 philox_normal4(uint64_t seed, uint64_t t, uint64_t b) {
   return make_float4(-ra * ca, -ra * sa, -rb * cb, -rb * sb);
 }
 
+// ------------------------------------------------------------ W of a cell ---
+// The solve's right-hand side W of one cell: the spread field's sum over the
+// cell volume (fixed point, scale = 2^-40 / dV, or the FP32 sum of the
+// float-atomic form, fscale = 1 / dV) plus fac times the noise divergence,
+// with one FP32 FMA for the noise term.  Every W builder (the W kernels, the
+// tiled spread, the transforms that read the field directly) rounds alike.
+__device__ __forceinline__ float w_fixed(long long g, float scale, float fac, float d) {
+  return __fmaf_rn(fac, d, (float)((double)g * (double)scale));
+}
+__device__ __forceinline__ float w_float(float g, float fscale, float fac, float d) {
+  return __fmaf_rn(fac, d, __fmul_rn(g, fscale));
+}
+
 // --------------------------------------------------- exact cell indices ---
 __device__ __forceinline__ double dsgn(double r) { return (double)((r > 0) - (r < 0)); }
 
@@ -662,7 +675,8 @@ FftPlan* fft_plan_create(const Params& P);
 void fft_plan_destroy(FftPlan* fp);
 // v = solve(W).  W = f + nfac div(stress 1 [+ stress 2 when nsets == 2]) is
 // built from the spread field (which is cleared on the way) and the noise
-// into Rep::wbuf, unless w_given, in which case Rep::wbuf already holds W.
+// divergence into Rep::wbuf, unless w_given, in which case Rep::wbuf already
+// holds W.
 // Picks the fastest z-pass tile of the plan's candidates on B's buffers
 // (once per plan; no-op under stream capture).
 void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s);

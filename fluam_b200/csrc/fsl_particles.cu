@@ -1129,13 +1129,13 @@ __device__ __forceinline__ void warp_spread(const Params& P, const QuadStencil<K
           const double v = (double)w * vs;
           sat |= !(fabs(v) < kFixedMax);
           const long long iv = sat ? 0ll : __double2ll_rn(v);
-          if (iv != 0) {
-            const int n = ((dz - lz + c) * kBox + (dy - ly + b)) * kBox + bx;
-            const unsigned lo = (unsigned)(unsigned long long)iv;
-            const unsigned hi = (unsigned)((unsigned long long)iv >> 32);
-            const unsigned old = atomicAdd(blo + n, lo);
-            atomicAdd(bhi + n, hi + (old + lo < old ? 1u : 0u));
-          }
+          // unconditional (a zero adds nothing): straight-line code lets
+          // the low-word adds of the stencil issue back to back
+          const int n = ((dz - lz + c) * kBox + (dy - ly + b)) * kBox + bx;
+          const unsigned lo = (unsigned)(unsigned long long)iv;
+          const unsigned hi = (unsigned)((unsigned long long)iv >> 32);
+          const unsigned old = atomicAdd(blo + n, lo);
+          atomicAdd(bhi + n, hi + (old + lo < old ? 1u : 0u));
         }
     }
     __syncwarp();
@@ -1497,18 +1497,13 @@ __global__ void __launch_bounds__(kTileThreads) k_spread_w(FSL_KARGS, int drift,
       const size_t i0 = (size_t)x + (size_t)P.mx * ((size_t)y + (size_t)P.my * z);
       float w[3][4];
 #pragma unroll
-      for (int comp = 0; comp < 3; ++comp)
+      for (int comp = 0; comp < 3; ++comp) {
+        const float4 d4 = __ldg(reinterpret_cast<const float4*>(D + comp * nc + i0));
+        const float d[4] = {d4.x, d4.y, d4.z, d4.w};
 #pragma unroll
         for (int c = 0; c < 4; ++c)
-          w[comp][c] = (float)((double)(long long)acc[comp * kTileCells + (lz * kTileY + ly) * kTileX + lx + c] *
-                               (double)scale);
-#pragma unroll
-      for (int comp = 0; comp < 3; ++comp) {
-        const float4 d = __ldg(reinterpret_cast<const float4*>(D + comp * nc + i0));
-        w[comp][0] += fac * d.x;
-        w[comp][1] += fac * d.y;
-        w[comp][2] += fac * d.z;
-        w[comp][3] += fac * d.w;
+          w[comp][c] = w_fixed((long long)acc[comp * kTileCells + (lz * kTileY + ly) * kTileX + lx + c], scale,
+                               fac, d[c]);
       }
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp)
@@ -1523,9 +1518,7 @@ __global__ void __launch_bounds__(kTileThreads) k_spread_w(FSL_KARGS, int drift,
       const int i = x + P.mx * (y + P.my * z);
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp) {
-        float w = (float)((double)(long long)acc[comp * kTileCells + c] * (double)scale);
-        w += fac * __ldg(D + comp * nc + i);
-        R.wbuf[comp * nc + i] = w;
+        R.wbuf[comp * nc + i] = w_fixed((long long)acc[comp * kTileCells + c], scale, fac, __ldg(D + comp * nc + i));
       }
     }
   }

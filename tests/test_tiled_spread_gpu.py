@@ -56,7 +56,14 @@ def _run(fsl, c, tiled, steps=6):
             s.step(steps)
             st = s.status()
             assert st["error_bits"] == 0
-            return s.positions(), s.forces(), s.velocity(), st["launches_per_step"]
+            out = s.positions(), s.forces(), s.velocity()
+            # the stages of one more (profiled) step, after the state was read
+            s.profile(True)
+            s.step(1)
+            s.sync()
+            stages = set(s.profile_read())
+            s.profile(False)
+            return out + (stages,)
     finally:
         for key, val in zip(("FLUAMSL_TILED_SPREAD", "FLUAMSL_VERLET"), old):
             if val is None:
@@ -67,9 +74,10 @@ def _run(fsl, c, tiled, steps=6):
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_tiled_equals_atomic(fsl, name):
-    q0, F0, v0, n0 = _run(fsl, CASES[name], False)
-    q1, F1, v1, n1 = _run(fsl, CASES[name], True)
-    assert n1 < n0  # the tiled path ran: one launch instead of spread + W build
+    q0, F0, v0, s0 = _run(fsl, CASES[name], False)
+    q1, F1, v1, s1 = _run(fsl, CASES[name], True)
+    # the tiled path ran: its spread writes W, the other spreads into the field
+    assert any(k.startswith("spread_w") for k in s1) and not any(k.startswith("spread_w") for k in s0)
     np.testing.assert_array_equal(q1, q0)
     np.testing.assert_array_equal(F1, F0)
     np.testing.assert_array_equal(v1, v0)
