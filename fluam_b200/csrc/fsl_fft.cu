@@ -1020,11 +1020,11 @@ static void zsolve(const Batch& B, const FftPlan* fp, dim3 gz, cudaStream_t s) {
   if (fp->zsolve_r[0]) {
     dim3 g((B.mxh + fp->z_kx - 1) / fp->z_kx, (B.my + fp->z_ky - 1) / fp->z_ky, B.nrep);
     if (B.one)
-      fp->zsolve_r[1]<<<g, fp->z_threads, fp->smem_z_r, s>>>(RepSrc{}, *B.one, fp->twz, fp->sx, fp->sy,
-                                                             fp->sz, fp->ex, fp->ey, fp->ez);
+      fsl_launch(fp->zsolve_r[1], g, fp->z_threads, fp->smem_z_r, s, RepSrc{}, *B.one, fp->twz, fp->sx,
+                 fp->sy, fp->sz, fp->ex, fp->ey, fp->ez);
     else
-      fp->zsolve_r[0]<<<g, fp->z_threads, fp->smem_z_r, s>>>(B.src(), Rep{}, fp->twz, fp->sx, fp->sy,
-                                                             fp->sz, fp->ex, fp->ey, fp->ez);
+      fsl_launch(fp->zsolve_r[0], g, fp->z_threads, fp->smem_z_r, s, B.src(), Rep{}, fp->twz, fp->sx,
+                 fp->sy, fp->sz, fp->ex, fp->ey, fp->ez);
     return;
   }
   if (B.one)
@@ -1046,8 +1046,8 @@ static void reg_transform(const Batch& B, const FftPlan* fp, cudaStream_t s, Pro
     const int tb = kLineWarps * 32;
     const size_t sm = fp->smem_lines;
     auto go = [&](void (*const* k)(RepSrc, Rep, const float2*)) {
-      if (B.one) k[1]<<<g, tb, sm, s>>>(RepSrc{}, *B.one, fp->twx);
-      else k[0]<<<g, tb, sm, s>>>(B.src(), Rep{}, fp->twx);
+      if (B.one) fsl_launch(k[1], g, tb, sm, s, RepSrc{}, *B.one, fp->twx);
+      else fsl_launch(k[0], g, tb, sm, s, B.src(), Rep{}, fp->twx);
     };
     pr.mark(s, "fft_x");
     go(fp->line_xf);
@@ -1066,16 +1066,16 @@ static void reg_transform(const Batch& B, const FftPlan* fp, cudaStream_t s, Pro
   const int tb = fp->plane_threads;
   pr.mark(s, "plane_fwd");
   if (B.one)
-    fp->plane_fwd_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
+    fsl_launch(fp->plane_fwd_r[1], gp, tb, fp->smem_plane_r, s, RepSrc{}, *B.one, fp->twx);
   else
-    fp->plane_fwd_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
+    fsl_launch(fp->plane_fwd_r[0], gp, tb, fp->smem_plane_r, s, B.src(), Rep{}, fp->twx);
   pr.mark(s, "zsolve");
   zsolve(B, fp, dim3((B.mxh + kZTile - 1) / kZTile, B.my, nrep), s);
   pr.mark(s, "plane_inv");
   if (B.one)
-    fp->plane_inv_r[1]<<<gp, tb, fp->smem_plane_r, s>>>(RepSrc{}, *B.one, fp->twx);
+    fsl_launch(fp->plane_inv_r[1], gp, tb, fp->smem_plane_r, s, RepSrc{}, *B.one, fp->twx);
   else
-    fp->plane_inv_r[0]<<<gp, tb, fp->smem_plane_r, s>>>(B.src(), Rep{}, fp->twx);
+    fsl_launch(fp->plane_inv_r[0], gp, tb, fp->smem_plane_r, s, B.src(), Rep{}, fp->twx);
   pr.count(3);
 }
 

@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 namespace fsl {
@@ -122,8 +123,8 @@ __device__ inline float4 philox_normal4(uint64_t seed, uint64_t t, uint64_t b) {
 // The solve's right-hand side W of one cell: the spread field's sum over the
 // cell volume (fixed point, scale = 2^-40 / dV, or the FP32 sum of the
 // float-atomic form, fscale = 1 / dV) plus fac times the noise divergence,
-// with one FP32 FMA for the noise term.  Every W builder (the W kernels, the
-// tiled spread, the transforms that read the field directly) rounds alike.
+// with one FP32 FMA for the noise term.  Every W builder (the W kernels and
+// the tiled spread) rounds alike.
 __device__ __forceinline__ float w_fixed(long long g, float scale, float fac, float d) {
   return __fmaf_rn(fac, d, (float)((double)g * (double)scale));
 }
@@ -570,34 +571,72 @@ __device__ __forceinline__ const Rep& rep_flat(const RepSrc& src, const Rep& one
 
 #define FSL_KARGS const RepSrc src, const __grid_constant__ Rep one
 
+// Programmatic dependent launch.  The kernels that take their instance
+// through FSL_REP_AT / FSL_REP_FLAT are launched (fsl_launch) so that their
+// blocks may be scheduled while the previous kernel of the stream drains;
+// before anything else each block waits until that kernel has completed
+// and its writes are visible (griddepcontrol.wait, which returns at once
+// for an ordinary launch), then lets the next kernel be scheduled in turn.
+// Every kernel of a chain waits before it can complete, so a kernel sees
+// the writes of all kernels before it in the stream, not only the last.
+__device__ __forceinline__ void fsl_pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 #define FSL_REP_AT(IDX)                                            \
+  fsl_pdl_enter();                                                 \
   __shared__ Rep fsl_sh_rep_;                                      \
   const Rep& R = rep_copy<ONE>(src, one, (int)(IDX), fsl_sh_rep_); \
   if (!R.active) return;                                           \
   const Params& P = R.P
 
 #define FSL_REP_FLAT(KIND)                                         \
+  fsl_pdl_enter();                                                 \
   __shared__ Rep fsl_sh_rep_;                                      \
   int blk;                                                         \
   const Rep& R = rep_flat<ONE>(src, one, (KIND), blk, fsl_sh_rep_); \
   if (!R.active) return;                                           \
   const Params& P = R.P
 
+// Whether launches carry the programmatic-serialisation attribute
+// (FLUAMSL_PDL=0: ordinary launches, for comparison).
+bool pdl_enabled();
+
+// Launch of a kernel that enters through FSL_REP_AT / FSL_REP_FLAT, with
+// programmatic dependent launch where enabled.  Errors are left for
+// cudaPeekAtLastError, as with the <<<>>> syntax.
+template <typename... KArgs, typename... Args>
+inline void fsl_launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 // Launch of a kernel template whose first template argument is ONE.
-#define FSL_GO(KERN, GRID, BLOCK, SMEM, S, B, ...)                                     \
-  do {                                                                                 \
-    if ((B).one)                                                                       \
-      KERN<true><<<(GRID), (BLOCK), (SMEM), (S)>>>(RepSrc{}, *(B).one, ##__VA_ARGS__); \
-    else                                                                               \
-      KERN<false><<<(GRID), (BLOCK), (SMEM), (S)>>>((B).src(), Rep{}, ##__VA_ARGS__);  \
+#define FSL_GO(KERN, GRID, BLOCK, SMEM, S, B, ...)                                          \
+  do {                                                                                      \
+    if ((B).one)                                                                            \
+      fsl_launch(KERN<true>, (GRID), (BLOCK), (SMEM), (S), RepSrc{}, *(B).one, ##__VA_ARGS__); \
+    else                                                                                    \
+      fsl_launch(KERN<false>, (GRID), (BLOCK), (SMEM), (S), (B).src(), Rep{}, ##__VA_ARGS__);  \
   } while (0)
 // ... with a second template argument T
-#define FSL_GO_T(KERN, T, GRID, BLOCK, SMEM, S, B, ...)                                   \
-  do {                                                                                    \
-    if ((B).one)                                                                          \
-      KERN<true, T><<<(GRID), (BLOCK), (SMEM), (S)>>>(RepSrc{}, *(B).one, ##__VA_ARGS__); \
-    else                                                                                  \
-      KERN<false, T><<<(GRID), (BLOCK), (SMEM), (S)>>>((B).src(), Rep{}, ##__VA_ARGS__);  \
+#define FSL_GO_T(KERN, T, GRID, BLOCK, SMEM, S, B, ...)                                        \
+  do {                                                                                         \
+    if ((B).one)                                                                               \
+      fsl_launch(KERN<true, T>, (GRID), (BLOCK), (SMEM), (S), RepSrc{}, *(B).one, ##__VA_ARGS__); \
+    else                                                                                       \
+      fsl_launch(KERN<false, T>, (GRID), (BLOCK), (SMEM), (S), (B).src(), Rep{}, ##__VA_ARGS__);  \
   } while (0)
 
 // Blocks of a particle launch of kind k.

@@ -1533,6 +1533,14 @@ void tile_init() {
   cudaFuncSetAttribute(k_spread_w<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
 }
 
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("FLUAMSL_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 bool tile_eligible(const Params& P) {
   if (P.prec != PREC_FIXED || P.scheme > 1) return false;  // 3-D Stokes schemes
   if (P.verlet || P.nolist) return false;  // needs both cell lists of every step
