@@ -310,7 +310,7 @@ constexpr int kFftThreads = 512;
 // cleared behind the read, ready for the next spread.  One thread per cell:
 // the loads of a warp are coalesced rows, full occupancy.
 template <bool ONE>
-__global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
+__global__ void k_wbuild(FSL_KARGS, int nsets, double nfac, int clear) {
   FSL_REP_AT(blockIdx.y);
   const float scale = (float)(kFixedInv / P.dV);
   const float fac = (float)nfac;
@@ -328,20 +328,33 @@ __global__ void k_wbuild(FSL_KARGS, int nsets, double nfac) {
       const float d = __ldg(D + comp * nc + i);
       if (fatom) {
         w = w_float(gf[comp * nc + i], fscale, fac, d);
-        gf[comp * nc + i] = 0.0f;
+        if (clear) gf[comp * nc + i] = 0.0f;
       } else {
         w = w_fixed((long long)R.grid[comp * nc + i], scale, fac, d);
-        R.grid[comp * nc + i] = 0ull;
+        if (clear) R.grid[comp * nc + i] = 0ull;
       }
       R.wbuf[comp * nc + i] = w;
     }
   }
 }
 
+// Zeroes the spread field (3 nc 64-bit sums, or 3 nc floats of the
+// float-atomic form) with streaming stores, which leave the L2 to the
+// transforms it runs beside.
+template <bool ONE>
+__global__ void k_field_clear(FSL_KARGS) {
+  FSL_REP_AT(blockIdx.y);
+  const size_t bytes = (size_t)3 * P.nc * (P.prec == PREC_FLOAT ? 4 : 8);
+  float4* q = reinterpret_cast<float4*>(R.grid);
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < bytes / 16; i += (size_t)gridDim.x * blockDim.x)
+    __stcs(q + i, z);
+}
+
 // k_wbuild for mx a multiple of 4: one thread per four x cells, 16-byte loads
 // of the fixed-point field, the noise rows and W, and 16-byte clears.
 template <bool ONE>
-__global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
+__global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac, int clear) {
   FSL_REP_AT(blockIdx.y);
   const float scale = (float)(kFixedInv / P.dV);
   const float fac = (float)nfac;
@@ -365,7 +378,7 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
         w[comp][1] = w_float(ga.y, fscale, fac, d.y);
         w[comp][2] = w_float(ga.z, fscale, fac, d.z);
         w[comp][3] = w_float(ga.w, fscale, fac, d.w);
-        *fp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (clear) *fp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         continue;
       }
       const longlong2* gp = reinterpret_cast<const longlong2*>(R.grid + comp * nc + i0);
@@ -379,7 +392,7 @@ __global__ void k_wbuild4(FSL_KARGS, int nsets, double nfac) {
     for (int comp = 0; comp < 3; ++comp) {
       *reinterpret_cast<float4*>(R.wbuf + comp * nc + i0) =
           make_float4(w[comp][0], w[comp][1], w[comp][2], w[comp][3]);
-      if (fatom) continue;  // cleared at the read
+      if (fatom || !clear) continue;  // cleared at the read, or by k_field_clear
       longlong2* gq = reinterpret_cast<longlong2*>(R.grid + comp * nc + i0);
       gq[0] = make_longlong2(0, 0);
       gq[1] = make_longlong2(0, 0);
@@ -1137,8 +1150,16 @@ void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s) {
   cudaGetLastError();
 }
 
+void launch_field_clear(const Batch& B, cudaStream_t s) {
+  if (B.nrep == 0) return;
+  const long cap = (148L * 8 + B.nrep - 1) / B.nrep;
+  long blocks = ((long)3 * B.nc * 8 / 16 + 255) / 256;
+  if (blocks > cap) blocks = cap < 1 ? 1 : cap;
+  FSL_GO(k_field_clear, dim3((unsigned)blocks, B.nrep), 256, 0, s, B);
+}
+
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
-                  Prof* prof) {
+                  Prof* prof, cudaEvent_t w_built) {
   if (B.prec == PREC_F64) return launch_solve64(B, nsets, nfac, s, prof);
   Prof dummy;
   Prof& pr = prof ? *prof : dummy;
@@ -1153,11 +1174,12 @@ void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_giv
     if ((B.mx & 3) == 0) {
       long b4 = ((long)B.nc / 4 + tb - 1) / tb;
       if (b4 > cap) b4 = cap < 1 ? 1 : cap;
-      FSL_GO(k_wbuild4, dim3((unsigned)b4, nrep), tb, 0, s, B, nsets, nfac);
+      FSL_GO(k_wbuild4, dim3((unsigned)b4, nrep), tb, 0, s, B, nsets, nfac, w_built ? 0 : 1);
     } else {
-      FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets, nfac);
+      FSL_GO(k_wbuild, dim3((unsigned)blocks, nrep), tb, 0, s, B, nsets, nfac, w_built ? 0 : 1);
     }
     pr.count(1);
+    if (w_built) cudaEventRecord(w_built, s);
   }
   if (fp->plane_fwd_r[0]) {
     reg_transform(B, fp, s, pr);

@@ -582,6 +582,10 @@ int group_init(Group& g, const Params& P0) {
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   FSL_TRY(cudaEventCreateWithFlags(&g.ev_join2, cudaEventDisableTiming));
+  for (int i = 0; i < 2; ++i) {
+    FSL_TRY(cudaEventCreateWithFlags(&g.ev_w[i], cudaEventDisableTiming));
+    FSL_TRY(cudaEventCreateWithFlags(&g.ev_c[i], cudaEventDisableTiming));
+  }
   tile_init();
   return FSL_OK;
 }
@@ -594,6 +598,11 @@ void group_destroy(Group& g) {
   if (g.ev_fork) cudaEventDestroy(g.ev_fork);
   if (g.ev_join) cudaEventDestroy(g.ev_join);
   if (g.ev_join2) cudaEventDestroy(g.ev_join2);
+  for (int i = 0; i < 2; ++i) {
+    if (g.ev_w[i]) cudaEventDestroy(g.ev_w[i]);
+    if (g.ev_c[i]) cudaEventDestroy(g.ev_c[i]);
+    g.ev_w[i] = g.ev_c[i] = nullptr;
+  }
   g.side = nullptr;
   g.ev_fork = g.ev_join = g.ev_join2 = nullptr;
   fft_plan_destroy(g.fft);
@@ -756,6 +765,22 @@ void group_enqueue_step(Group& g) {
   auto join_noise2 = [&]() {
     if (fork && two) cudaStreamWaitEvent(s, g.ev_join2, 0);
   };
+  // the field clear after a W build goes to the side stream, where its
+  // blocks fill the SMs that the transforms leave idle; the W build then
+  // only reads the field
+  const bool clear_fork = fork && !B.tiled && B.prec != PREC_F64;
+  auto solve = [&](int k, int nsets, double nfac) {
+    launch_solve(B, g.fft, nsets, nfac, B.tiled, s, &pr, clear_fork ? g.ev_w[k] : nullptr);
+    chk("solve");
+    if (!clear_fork) return;
+    cudaStreamWaitEvent(g.side, g.ev_w[k], 0);
+    launch_field_clear(B, g.side);
+    cudaEventRecord(g.ev_c[k], g.side);
+    pr.count(1);
+  };
+  auto join_clear = [&](int k) {
+    if (clear_fork) cudaStreamWaitEvent(s, g.ev_c[k], 0);
+  };
   auto observe = [&]() {
     if (!g.key.observe) return;
     pr.mark(s, "observe");
@@ -836,8 +861,7 @@ void group_enqueue_step(Group& g) {
       chk("spread_rfd");
       pr.count(pk);
     }
-    launch_solve(B, g.fft, 1, 1.0, B.tiled, s, &pr);
-    chk("solve");
+    solve(0, 1, 1.0);
     pr.mark(s, "interp_update");
     launch_interp_update(B, 1, s);
     chk("interp_update");
@@ -852,6 +876,7 @@ void group_enqueue_step(Group& g) {
     launch_step_counter(B, s);
     chk("counter");
     pr.count(1);
+    join_clear(0);
     pr.mark(s, nullptr);
     g.launches = pr.launches;
     return;
@@ -873,8 +898,7 @@ void group_enqueue_step(Group& g) {
     pr.count(pk);
     join_noise();
   }
-  launch_solve(B, g.fft, 1, 1.41421356237309504880, B.tiled, s, &pr);
-  chk("solve");
+  solve(0, 1, 1.41421356237309504880);
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
   // sqrt(1/2) (stress 1 + stress 2)
   pr.mark(s, "interp_update");
@@ -882,6 +906,7 @@ void group_enqueue_step(Group& g) {
   chk("interp_update");
   pr.count(pk);
   cells_forces(1, !B.tiled);
+  join_clear(0);  // the field is spread into again
   if (B.tiled) {
     join_noise2();
     pr.mark(s, "spread_w_rfd");
@@ -895,8 +920,7 @@ void group_enqueue_step(Group& g) {
     pr.count(pk);
   }
   join_noise2();
-  launch_solve(B, g.fft, 2, 0.70710678118654752440, B.tiled, s, &pr);
-  chk("solve");
+  solve(1, 2, 0.70710678118654752440);
   // option 2: corrector
   pr.mark(s, "interp_update");
   launch_interp_update(B, 2, s);
@@ -907,6 +931,7 @@ void group_enqueue_step(Group& g) {
   launch_step_counter(B, s);
   chk("counter");
   pr.count(1);
+  join_clear(1);
   pr.mark(s, nullptr);
   g.launches = pr.launches;
 }

@@ -104,6 +104,9 @@ struct Group {
   // (fork and join events); profiled steps keep everything on `stream`
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;  // noise parts 0, 1
+  // the spread field is cleared on `side` after each W build (ev_w) and
+  // waited for before the next spread or the end of the step (ev_c)
+  cudaEvent_t ev_w[2] = {}, ev_c[2] = {};
   Prof prof;
   std::map<std::string, std::pair<int64_t, double>> stage_acc;
   int launches = 0;             // kernels of this group in one step

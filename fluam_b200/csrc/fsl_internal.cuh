@@ -715,10 +715,14 @@ void fft_plan_destroy(FftPlan* fp);
 // v = solve(W).  W = f + nfac div(stress 1 [+ stress 2 when nsets == 2]) is
 // built from the spread field (which is cleared on the way) and the noise
 // divergence into Rep::wbuf, unless w_given, in which case Rep::wbuf already
-// holds W.
+// holds W.  With w_built, the W build leaves the field as it is and records
+// w_built after itself: the caller clears the field (launch_field_clear)
+// after that event and before the next spread.
 // Picks the fastest z-pass tile of the plan's candidates on B's buffers
 // (once per plan; no-op under stream capture).
 void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s);
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
-                  Prof* prof = nullptr);
+                  Prof* prof = nullptr, cudaEvent_t w_built = nullptr);
+// Zeroes the spread fields of B's instances (streaming stores).
+void launch_field_clear(const Batch& B, cudaStream_t s);
 }  // namespace fsl
