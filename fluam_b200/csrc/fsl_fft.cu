@@ -721,6 +721,7 @@ __global__ void __launch_bounds__(kFftThreads)
 
 #include "fsl_fft_reg.cuh"
 #include "fsl_fft_lines.cuh"
+#include "fsl_fft_v.cuh"
 
 // ------------------------------------------------------------ host side ---
 template <int N, int R, int T, int PB>
@@ -744,6 +745,18 @@ static void pick_plane_r(FftPlan* fp) {
   fp->plane_inv_r[0] = k_plane_inv_r<false, N, R, T, PB>;
   fp->plane_inv_r[1] = k_plane_inv_r<true, N, R, T, PB>;
   fp->smem_plane_r = sizeof(float2) * (N + (size_t)PB * plane_buf<N, R, T>());
+  if constexpr (N == 128 && R == 16 && T == 8 && PB == 1) {
+    // the conflict-free layout of the same arithmetic (fsl_fft_v.cuh);
+    // FLUAMSL_PLANE_V=0 keeps the generic kernels, for comparison
+    const char* e = getenv("FLUAMSL_PLANE_V");
+    if (!(e && e[0] == '0')) {
+      fp->plane_fwd_r[0] = k_plane_fwd_v<false>;
+      fp->plane_fwd_r[1] = k_plane_fwd_v<true>;
+      fp->plane_inv_r[0] = k_plane_inv_v<false>;
+      fp->plane_inv_r[1] = k_plane_inv_v<true>;
+      fp->smem_plane_r = sizeof(float2) * (size_t)kVSmem;
+    }
+  }
 }
 
 // FLUAMSL_FFT_SCHEDULE=plane or =lines fixes the transform schedule of the
