@@ -456,16 +456,25 @@ __global__ void __launch_bounds__(3 * KX * KY * T)
     const float inv_eta = (float)(1.0 / P.eta);
     const float inv_nc = 1.0f / (float)P.nc;
     const float tdx = (float)(2.0 * P.invdx), tdy = (float)(2.0 * P.invdy), tdz = (float)(2.0 * P.invdz);
+    // the block size is a multiple of KX * KY, so a thread's (kx, ky) stays
+    // the same over its modes and only kz moves: the x and y factors are
+    // read once
+    static_assert((3 * KX * KY * T) % (KX * KY) == 0, "fixed (kx, ky) per thread");
+    const int mxl = threadIdx.x % KX, myl = (threadIdx.x / KX) % KY;
+    const int mkx = blockIdx.x * KX + mxl, mky = blockIdx.y * KY + myl;
+    const bool mlive = mkx < mxh && mky < my;
+    const float2 Ex = mlive ? __ldg(ex + mkx) : make_float2(0.f, 0.f);
+    const float2 Ey = mlive ? __ldg(ey + mky) : make_float2(0.f, 0.f);
+    // src/initializePrefactorFourierSpace.cu:48-66: g = 2/h sin(pi j/m)
+    const float gx = mlive ? tdx * __ldg(sx + mkx) : 0.f, gy = mlive ? tdy * __ldg(sy + mky) : 0.f;
     for (int e = threadIdx.x; e < KX * KY * MZ; e += blockDim.x) {
-      const int mxl = e % KX, r2 = e / KX, myl = r2 % KY, kz = r2 / KY;
-      const int mkx = blockIdx.x * KX + mxl, mky = blockIdx.y * KY + myl;
-      if (mkx >= mxh || mky >= my) continue;
+      const int kz = e / (KX * KY);
+      if (!mlive) continue;
       float2* pc[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) pc[a] = buf + ((myl * 3 + a) * KX + mxl) * LS + kz;
-      const float2 E[3] = {__ldg(ex + mkx), __ldg(ey + mky), __ldg(ez + kz)};
-      // src/initializePrefactorFourierSpace.cu:48-66: g = 2/h sin(pi j/m)
-      const float g[3] = {tdx * __ldg(sx + mkx), tdy * __ldg(sy + mky), tdz * __ldg(sz + kz)};
+      const float2 E[3] = {Ex, Ey, __ldg(ez + kz)};
+      const float g[3] = {gx, gy, tdz * __ldg(sz + kz)};
       if (mkx == 0 && mky == 0 && kz == 0) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) *pc[a] = make_float2(0.f, 0.f);

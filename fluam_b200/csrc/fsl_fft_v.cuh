@@ -15,7 +15,9 @@
 //   * the real plane in rows of kVR floats (kVR = 8 mod 32), read one float
 //     per lane without conflicts, and written as 16-byte rows;
 //   * x-pass lines are private to their eight lanes (one quarter warp), so
-//     the x exchange needs a warp barrier, not a block barrier.
+//     the x exchange needs a warp barrier, not a block barrier;
+//   * the inverse's input, the contiguous half-spectrum plane, comes into
+//     shared memory by one bulk copy (fsl_bulk.cuh).
 
 constexpr int kVX = 18;   // exchange row of one t (float2)
 constexpr int kVL = 146;  // line pitch (float2); kVL / 2 odd
@@ -81,7 +83,8 @@ __global__ void __launch_bounds__(512) k_plane_fwd_v(FSL_KARGS, const float2* __
   const bool live = pl < 3 * P.mz;
   const int comp = live ? pl / P.mz : 0, z = live ? pl - comp * P.mz : 0;
   v_twiddles(twt, twn);
-  // the real plane, 16-byte loads into rows of kVR floats
+  // the real plane, 16-byte loads into rows of kVR floats (ordinary loads:
+  // measured faster here than bulk row copies or per-thread async copies)
   float* fb = reinterpret_cast<float*>(buf);
   {
     const float4* W4 = reinterpret_cast<const float4*>(R.wbuf + (size_t)comp * P.nc + (size_t)z * N * N);
@@ -178,8 +181,23 @@ __global__ void __launch_bounds__(512) k_plane_inv_v(FSL_KARGS, const float2* __
   const int pl = blockIdx.x;
   const bool live = pl < 3 * P.mz;
   const int comp = live ? pl / P.mz : 0, z = live ? pl - comp * P.mz : 0;
+  // the half-spectrum plane is contiguous (N rows of H + 1): one bulk copy
+  // into shared memory while the block stages the twiddles
   const float2* in_g = R.spec + ((size_t)comp * P.mz + z) * (size_t)N * (H + 1);
+  constexpr unsigned kPlaneBytes = N * (H + 1) * sizeof(float2);
+  static_assert(kPlaneBytes % 16 == 0 && N * (H + 1) <= 64 * kVL, "plane copy");
+  __shared__ __align__(8) unsigned long long s_bar;
+  if (r == 0) {
+    mbar_init(&s_bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (r == 0 && live) {
+    mbar_arrive_tx(&s_bar, kPlaneBytes);
+    bulk_load(buf, in_g, kPlaneBytes, &s_bar);
+  }
   v_twiddles(twt, twn);
+  if (live) bulk_wait(&s_bar, R.err);
   __syncthreads();
   // y pass: column c (fastest), lane t; rows of the result at pitch kVH
   {
@@ -191,12 +209,13 @@ __global__ void __launch_bounds__(512) k_plane_inv_v(FSL_KARGS, const float2* __
       if (!live) {
         v[k] = make_float2(0.f, 0.f);
       } else if (c == 0) {
-        const float2 f0 = in_g[(size_t)ky * (H + 1)], fh = in_g[(size_t)ky * (H + 1) + H];
+        const float2 f0 = buf[ky * (H + 1)], fh = buf[ky * (H + 1) + H];
         v[k] = make_float2(f0.x - fh.y, f0.y + fh.x);  // F0 + i FH
       } else {
-        v[k] = in_g[(size_t)ky * (H + 1) + c];
+        v[k] = buf[ky * (H + 1) + c];
       }
     }
+    __syncthreads();  // the plane is overwritten by the lines
     float2* lb = buf + c * kVL;
     v_line_a(v, t, lb, twt, +1);
     __syncthreads();
