@@ -26,7 +26,7 @@ size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 // Byte offsets of one slot's buffers inside its arena.
 struct SlotLayout {
   size_t q, qp, F, u, qw, ws, cell_of, tmp, sorted, bpp_cnt, bpp_off, bfp_cnt, bfp_off, cnt, fill, start,
-      bsum, ljtab, noise, ndiv, grid, spec, v, wbuf, noise64, v64, z64, err, t, q0, obs, obs_part, obs_ticket,
+      bsum, ljtab, noise, ndiv, stc, grid, spec, v, wbuf, noise64, v64, z64, err, t, q0, obs, obs_part, obs_ticket,
       start1, sorted1, ws1, vl_cnt, vl_idx, qref, vl_flag, bar, total;
 };
 
@@ -66,6 +66,10 @@ SlotLayout layout(const Params& P, int np_cap) {
   L.noise = take(f64 ? 0 : sizeof(float) * noise);
   // the stress divergence D1 | D12 of the 3-D Stokes schemes (k_div)
   L.ndiv = take(!f64 && P.scheme <= FSL_SCHEME_FIRST_ORDER ? sizeof(float) * 6 * nc : 0);
+  // the midpoint scheme's stencil cache: every spread stores the nodes and
+  // weights of its quads for the interpolation at the same positions
+  // (3 x 16 bytes per lane, 4 lanes per particle)
+  L.stc = take(!f64 && P.scheme == FSL_SCHEME_MIDPOINT ? sizeof(uint4) * 3 * 4 * np : 0);
   L.grid = take(sizeof(unsigned long long) * 3 * nc);
   L.spec = take(f64 ? 0 : sizeof(float2) * 3 * (size_t)P.my * P.mz * P.mxh);
   L.v = take(f64 ? 0 : sizeof(float) * 3 * nc);
@@ -347,6 +351,7 @@ int slot_alloc(Slot& s, const Params& P, int np_cap, cudaStream_t st) {
   r.ljtab = (float*)(base + L.ljtab);
   r.noise = (float*)(base + L.noise);
   r.ndiv = (float*)(base + L.ndiv);
+  r.stc = P.prec != FSL_PRECISION_FP64 && P.scheme == FSL_SCHEME_MIDPOINT ? (uint4*)(base + L.stc) : nullptr;
   r.grid = (unsigned long long*)(base + L.grid);
   r.spec = (float2*)(base + L.spec);
   r.v = (float*)(base + L.v);
@@ -883,7 +888,10 @@ void group_enqueue_step(Group& g) {
   }
   // option 0: F^n, f = S(q^n) F^n; solve 1 with sqrt(2) stress 1.  The
   // spread field is all zeros here: it starts cleared and every W build
-  // clears what it reads.
+  // clears what it reads.  Each spread leaves its nodes and weights in the
+  // stencil cache for the interpolation at the same positions (q^n, then
+  // q^{n+1/2}) unless the tiled spread, which keeps none, runs.
+  const bool stc = !B.tiled;
   cells_forces(0, !B.tiled);
   if (B.tiled) {
     join_noise();
@@ -893,7 +901,7 @@ void group_enqueue_step(Group& g) {
     pr.count(1);
   } else {
     pr.mark(s, "spread");
-    launch_spread(B, 0, 1, s, fuse);
+    launch_spread(B, 0, 1, s, fuse, stc);
     chk("spread");
     pr.count(pk);
     join_noise();
@@ -902,7 +910,7 @@ void group_enqueue_step(Group& g) {
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
   // sqrt(1/2) (stress 1 + stress 2)
   pr.mark(s, "interp_update");
-  launch_interp_update(B, 1, s);
+  launch_interp_update(B, 1, s, stc);
   chk("interp_update");
   pr.count(pk);
   cells_forces(1, !B.tiled);
@@ -915,7 +923,7 @@ void group_enqueue_step(Group& g) {
     pr.count(1);
   } else {
     pr.mark(s, "spread_rfd");
-    launch_spread(B, 1, 1, s, fuse);
+    launch_spread(B, 1, 1, s, fuse, stc);
     chk("spread_rfd");
     pr.count(pk);
   }
@@ -923,7 +931,7 @@ void group_enqueue_step(Group& g) {
   solve(1, 2, 0.70710678118654752440);
   // option 2: corrector
   pr.mark(s, "interp_update");
-  launch_interp_update(B, 2, s);
+  launch_interp_update(B, 2, s, stc);
   chk("interp_update");
   pr.count(pk);
   observe();

@@ -408,6 +408,10 @@ struct Rep {
   // the 3-D Stokes schemes: D1 = div(Sigma_1) | D12 = div(Sigma_1 + Sigma_2),
   // [3][nc] each (k_div), read by the W build
   float* ndiv;
+  // the midpoint scheme's stencil cache (null elsewhere): planes A, B, C of
+  // 4 np lanes each (lane e 4 + a of particle e), the quad_nodes of that
+  // lane as written by the last spread (QuadLane packing)
+  uint4* stc;
   unsigned long long* grid;
   float2* spec;
   float* v;
@@ -664,9 +668,15 @@ void launch_forces(const Batch& B, int which, cudaStream_t s, bool vl = true);
 // drift = 1: spread F at q^{n+1/2} and the RFD drift at q;
 // drift = 2: spread F at q and the RFD drift at q (first-order scheme).
 // forces: the Verlet-list instances compute F at the spread's positions in
-// the spread kernel (and store it) instead of reading it.
-void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s, bool forces = false);
-void launch_interp_update(const Batch& B, int stage, cudaStream_t s);
+// the spread kernel (and store it) instead of reading it.  cache: the
+// spread stores its quads' nodes and weights in Rep::stc (midpoint scheme)
+// for an interpolation at the same positions.
+void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s, bool forces = false,
+                   bool cache = false);
+// stage 1: q^{n+1/2} = q + dt/2 J(q) v; stage 2: q^{n+1} = q + dt J(q^{n+1/2}) v.
+// cached: the nodes come from Rep::stc, written by the spread at the same
+// positions (midpoint scheme), instead of being computed again.
+void launch_interp_update(const Batch& B, int stage, cudaStream_t s, bool cached = false);
 void launch_interp(const Batch& B, cudaStream_t s);  // u = J(q) v
 void launch_step_counter(const Batch& B, cudaStream_t s);
 // The fixed-point form's spread and W build in one tiled pass (drift as

@@ -879,35 +879,78 @@ struct QuadStencil {
   float wx[2], wy[2][KN], wz[2][KN];
 };
 
-// Every lane of the warp calls this (shuffles); qb is the first lane of the
-// quad.  Node k of family f in dimension d is the stencil_node of component
-// d (faces) or (d + 1) mod 3 (centres).
-template <int KN>
-__device__ __forceinline__ void quad_stencil(const Params& P, const double posc[3],
-                                             const double posw[3], int a, int qb,
-                                             QuadStencil<KN>& S) {
+// The nodes and weights that lane a of a quad computes itself: node a of
+// family f (0: cell centres, 1: faces) in dimension d (zeros for a >= KN).
+struct QuadLane {
   int j[2][3];
   float w[2][3];
+};
+
+template <int KN>
+__device__ __forceinline__ void quad_lane(const Params& P, const double posc[3], const double posw[3], int a,
+                                          QuadLane& L) {
 #pragma unroll
   for (int f = 0; f < 2; ++f)
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      j[f][d] = 0;
-      w[f][d] = 0.0f;
-      if (a < KN) stencil_node(P, d, f == 1 ? d : (d + 1) % 3, posc[d], posw[d], a, j[f][d], w[f][d]);
+      L.j[f][d] = 0;
+      L.w[f][d] = 0.0f;
+      if (a < KN) stencil_node(P, d, f == 1 ? d : (d + 1) % 3, posc[d], posw[d], a, L.j[f][d], L.w[f][d]);
     }
+}
+
+// The quad's stencil from its lanes' own nodes: x stays with its lane, y and
+// z go to every lane of the quad (first lane qb).
+template <int KN>
+__device__ __forceinline__ void quad_share(const QuadLane& L, int qb, QuadStencil<KN>& S) {
 #pragma unroll
   for (int f = 0; f < 2; ++f) {
-    S.jx[f] = j[f][0];
-    S.wx[f] = w[f][0];
+    S.jx[f] = L.j[f][0];
+    S.wx[f] = L.w[f][0];
 #pragma unroll
     for (int k = 0; k < KN; ++k) {
-      S.jy[f][k] = __shfl_sync(0xffffffffu, j[f][1], qb + k);
-      S.wy[f][k] = __shfl_sync(0xffffffffu, w[f][1], qb + k);
-      S.jz[f][k] = __shfl_sync(0xffffffffu, j[f][2], qb + k);
-      S.wz[f][k] = __shfl_sync(0xffffffffu, w[f][2], qb + k);
+      S.jy[f][k] = __shfl_sync(0xffffffffu, L.j[f][1], qb + k);
+      S.wy[f][k] = __shfl_sync(0xffffffffu, L.w[f][1], qb + k);
+      S.jz[f][k] = __shfl_sync(0xffffffffu, L.j[f][2], qb + k);
+      S.wz[f][k] = __shfl_sync(0xffffffffu, L.w[f][2], qb + k);
     }
   }
+}
+
+template <int KN>
+__device__ __forceinline__ void quad_stencil(const Params& P, const double posc[3],
+                                             const double posw[3], int a, int qb,
+                                             QuadStencil<KN>& S) {
+  QuadLane L;
+  quad_lane<KN>(P, posc, posw, a, L);
+  quad_share<KN>(L, qb, S);
+}
+
+// The stencil cache of the midpoint scheme: lane slot (particle i, lane a)
+// = 4 i + a of 4 np slots per plane, three 16-byte planes
+// A = (j00 j01 j02 j10), B = (j11 j12 w00 w01), C = (w02 w10 w11 w12).
+__device__ __forceinline__ void lane_store(uint4* stc, size_t np4, size_t slot, const QuadLane& L) {
+  stc[slot] = make_uint4((unsigned)L.j[0][0], (unsigned)L.j[0][1], (unsigned)L.j[0][2], (unsigned)L.j[1][0]);
+  stc[np4 + slot] =
+      make_uint4((unsigned)L.j[1][1], (unsigned)L.j[1][2], __float_as_uint(L.w[0][0]), __float_as_uint(L.w[0][1]));
+  stc[2 * np4 + slot] = make_uint4(__float_as_uint(L.w[0][2]), __float_as_uint(L.w[1][0]),
+                                   __float_as_uint(L.w[1][1]), __float_as_uint(L.w[1][2]));
+}
+
+__device__ __forceinline__ void lane_load(const uint4* __restrict__ stc, size_t np4, size_t slot, QuadLane& L) {
+  const uint4 A = __ldg(stc + slot), B = __ldg(stc + np4 + slot), C = __ldg(stc + 2 * np4 + slot);
+  L.j[0][0] = (int)A.x;
+  L.j[0][1] = (int)A.y;
+  L.j[0][2] = (int)A.z;
+  L.j[1][0] = (int)A.w;
+  L.j[1][1] = (int)B.x;
+  L.j[1][2] = (int)B.y;
+  L.w[0][0] = __uint_as_float(B.z);
+  L.w[0][1] = __uint_as_float(B.w);
+  L.w[0][2] = __uint_as_float(C.x);
+  L.w[1][0] = __uint_as_float(C.y);
+  L.w[1][1] = __uint_as_float(C.z);
+  L.w[1][2] = __uint_as_float(C.w);
 }
 
 // One spread of one particle by its quad: every lane adds w * value of its
@@ -1168,7 +1211,7 @@ __device__ __forceinline__ void warp_spread(const Params& P, const QuadStencil<K
 // drift.  In reference mode the drift's nodes come from the displaced
 // position and its weights from q, as the reference does.
 template <bool ONE, int KN>
-__global__ void k_spread(FSL_KARGS, int drift, int ordered, int box, int forces) {
+__global__ void k_spread(FSL_KARGS, int drift, int ordered, int box, int forces, int cache) {
   FSL_REP_FLAT(KIND_T4);
   // the warp's aggregation box (low and high words), kept cleared
   __shared__ unsigned s_box[kPartThreads / 32][2][kBoxNodes];
@@ -1203,7 +1246,13 @@ __global__ void k_spread(FSL_KARGS, int drift, int ordered, int box, int forces)
       val[1] = R.F[np + i];
       val[2] = R.F[2 * (size_t)np + i];
     }
-    quad_stencil<KN>(P, pos, pos, a, qb, S);
+    {
+      QuadLane L;
+      quad_lane<KN>(P, pos, pos, a, L);
+      // the interpolation at the same positions takes these nodes back
+      if (cache && on && R.stc) lane_store(R.stc, (size_t)4 * np, (size_t)4 * i + a, L);
+      quad_share<KN>(L, qb, S);
+    }
     if (P.prec == PREC_FIXED && box) {
       unsigned* blo = s_box[threadIdx.x >> 5][0];
       unsigned* bhi = s_box[threadIdx.x >> 5][1];
@@ -1236,15 +1285,15 @@ static int spread_box() {
   return on;
 }
 
-void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s, bool forces) {
+void launch_spread(const Batch& B, int drift, int ordered, cudaStream_t s, bool forces, bool cache) {
   if (B.max_np == 0) return;
   if (B.prec == PREC_F64) return launch_spread64(B, drift, s);
   const unsigned g = part_blocks(B, KIND_T4);
-  const int f = forces ? 1 : 0;
+  const int f = forces ? 1 : 0, c = cache ? 1 : 0;
   if (B.kernel == 4)
-    FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered, spread_box(), f);
+    FSL_GO_T(k_spread, 4, g, kPartThreads, 0, s, B, drift, ordered, spread_box(), f, c);
   else
-    FSL_GO_T(k_spread, 3, g, kPartThreads, 0, s, B, drift, ordered, spread_box(), f);
+    FSL_GO_T(k_spread, 3, g, kPartThreads, 0, s, B, drift, ordered, spread_box(), f, c);
 }
 
 // ------------------------------------------------ tiled spread + W build ---
@@ -1582,7 +1631,7 @@ void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStre
 //          src/stokesLimitFunctions.cu:3676-3681
 // One quad per particle; lanes 0, 1, 2 of the quad update x, y, z.
 template <bool ONE, int KN>
-__global__ void k_interp_update(FSL_KARGS, int stage) {
+__global__ void k_interp_update(FSL_KARGS, int stage, int cached) {
   FSL_REP_FLAT(KIND_T4);
   long e;
   int a, qb;
@@ -1592,9 +1641,18 @@ __global__ void k_interp_update(FSL_KARGS, int stage) {
   const int i = on ? (int)e : 0;
   const double* qpos = stage == 1 ? R.q : R.qp;
   double* qout = stage == 1 ? R.qp : R.q;
-  double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
   QuadStencil<KN> S;
-  quad_stencil<KN>(P, pos, pos, a, qb, S);
+  {
+    // the nodes of the spread at the same positions, or computed here
+    QuadLane L;
+    if (cached && R.stc) {
+      lane_load(R.stc, (size_t)4 * np, (size_t)4 * i + a, L);
+    } else {
+      double pos[3] = {qpos[i], qpos[np + i], qpos[2 * np + i]};
+      quad_lane<KN>(P, pos, pos, a, L);
+    }
+    quad_share<KN>(L, qb, S);
+  }
   float us[3];
   quad_interp<KN>(P, S, a, R.v, us);
   const int comp = a < 3 ? a : 0;
@@ -1640,14 +1698,15 @@ __global__ void k_interp(FSL_KARGS) {
   if (on && a < 3) R.u[(size_t)a * np + i] = (double)(a == 0 ? us[0] : (a == 1 ? us[1] : us[2]));
 }
 
-void launch_interp_update(const Batch& B, int stage, cudaStream_t s) {
+void launch_interp_update(const Batch& B, int stage, cudaStream_t s, bool cached) {
   if (B.max_np == 0) return;
   if (B.prec == PREC_F64) return launch_interp_update64(B, stage, s);
   const unsigned g = part_blocks(B, KIND_T4);
+  const int c = cached ? 1 : 0;
   if (B.kernel == 4)
-    FSL_GO_T(k_interp_update, 4, g, kPartThreads, 0, s, B, stage);
+    FSL_GO_T(k_interp_update, 4, g, kPartThreads, 0, s, B, stage, c);
   else
-    FSL_GO_T(k_interp_update, 3, g, kPartThreads, 0, s, B, stage);
+    FSL_GO_T(k_interp_update, 3, g, kPartThreads, 0, s, B, stage, c);
 }
 
 void launch_interp(const Batch& B, cudaStream_t s) {
