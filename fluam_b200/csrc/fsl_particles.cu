@@ -968,9 +968,10 @@ __device__ __forceinline__ void quad_spread(const Params& P, const QuadStencil<K
   const bool fatom = P.prec == PREC_FLOAT;
 #pragma unroll
   for (int comp = 0; comp < 3; ++comp) {
+    const double vc = val[comp];
+    if (vc == 0.0) continue;  // every product is zero: nothing to add
     const int x = S.jx[comp == 0];
     const float wx = S.wx[comp == 0];
-    const double vc = val[comp];
     const double vs = vc * kFixedScale;
     unsigned long long* gc = grid + (size_t)comp * P.nc;
 #pragma unroll
@@ -1059,8 +1060,9 @@ __device__ __forceinline__ void rfd_drift_at(const Params& P, const double W[3],
   }
   QuadStencil<KN> S;
   if (P.rfd != 1) {
-    // lane a checks the node families a and a + 4 of the six
-    int same = 1;
+    // lane a checks the node families a and a + 4 of the six (bit f 3 + d
+    // of chg: family f of dimension d picks another first node)
+    int chg = 0;
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       const int fd = a + 4 * r;
@@ -1068,12 +1070,22 @@ __device__ __forceinline__ void rfd_drift_at(const Params& P, const double W[3],
         const int f = fd / 3, d = fd - 3 * f;
         const double x = d == 0 ? pp[0] : (d == 1 ? pp[1] : pp[2]);
         const double y = d == 0 ? pm[0] : (d == 1 ? pm[1] : pm[2]);
-        same &= stencil_base(P, d, f, x) == stencil_base(P, d, f, y);
+        if (stencil_base(P, d, f, x) != stencil_base(P, d, f, y)) chg |= 1 << fd;
       }
     }
-    same &= __shfl_xor_sync(0xffffffffu, same, 1);
-    same &= __shfl_xor_sync(0xffffffffu, same, 2);
+    chg |= __shfl_xor_sync(0xffffffffu, chg, 1);
+    chg |= __shfl_xor_sync(0xffffffffu, chg, 2);
+    const bool same = chg == 0;
     if (!__all_sync(0xffffffffu, same || !on)) {
+      // component c reads the face family of dimension c and the centre
+      // families of the other two; a component none of whose families
+      // changed has the same nodes and weights in both spreads, which then
+      // cancel exactly: its values are left at zero (quad_spread skips them)
+      constexpr int fam[3] = {(1 << 3) | (1 << 1) | (1 << 2), (1 << 4) | (1 << 0) | (1 << 2),
+                              (1 << 5) | (1 << 0) | (1 << 1)};
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if (!(chg & fam[c])) vp[c] = vm[c] = 0.0;
       quad_stencil<KN>(P, pp, pos, a, qb, S);
       if (on && !same) add(S, vp);
       quad_stencil<KN>(P, pm, pos, a, qb, S);
