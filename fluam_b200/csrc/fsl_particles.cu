@@ -1223,7 +1223,7 @@ __device__ __forceinline__ void warp_spread(const Params& P, const QuadStencil<K
 // drift.  In reference mode the drift's nodes come from the displaced
 // position and its weights from q, as the reference does.
 template <bool ONE, int KN>
-__global__ void k_spread(FSL_KARGS, int drift, int ordered, int box, int forces, int cache) {
+__global__ void __launch_bounds__(kPartThreads, 4) k_spread(FSL_KARGS, int drift, int ordered, int box, int forces, int cache) {
   FSL_REP_FLAT(KIND_T4);
   // the warp's aggregation box (low and high words), kept cleared
   __shared__ unsigned s_box[kPartThreads / 32][2][kBoxNodes];
