@@ -383,9 +383,15 @@ struct Prof {
   void mark(cudaStream_t s, const char* n) {
     if (!on || used >= kMax) return;
     if (!ev[used]) cudaEventCreate(&ev[used]);
-    // External: under stream capture this becomes an event-record node of
-    // the graph (a plain record would only express a dependency).
-    cudaEventRecordWithFlags(ev[used], s, cudaEventRecordExternal);
+    // External under stream capture, so that the record becomes an
+    // event-record node of the graph (a plain record would only express a
+    // dependency); the flag is refused outside capture (the eager first step
+    // of an instance, or steps without graphs), where a plain record does
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+      cudaEventRecordWithFlags(ev[used], s, cudaEventRecordExternal);
+    else
+      cudaEventRecord(ev[used], s);
     name[used++] = n;
   }
   void count(int k) { launches += k; }

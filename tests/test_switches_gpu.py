@@ -1,0 +1,91 @@
+"""Every alternative kernel schedule gives the bits of the default one.
+
+The library reads these switches once per process, so each case runs the
+128^3 benchmark workload (65,536 chain beads, 4-point kernel, the Verlet
+list, the 128-point plane passes) for a few steps in a fresh process and
+compares positions, forces and the velocity field bit for bit with the
+default process:
+
+* FLUAMSL_PDL=0: ordinary launches instead of programmatic dependent ones;
+* FLUAMSL_PLANE_V=0: the generic register plane passes instead of the
+  conflict-free 128-point ones;
+* FLUAMSL_FFT_SCHEDULE=lines / plane: the five-pass schedule, or the plane
+  schedule, instead of the autotuner's pick;
+* FLUAMSL_FUSED_FORCES=0: the Verlet-list forces in their own launch
+  instead of inside the spread;
+* FLUAMSL_SPREAD_BOX=0: one global atomic per product instead of the
+  warp's shared box.
+
+A further case compares the default step with the per-stage profiled step,
+which keeps everything on one stream (the noise, and the field clear that
+the W build then does itself).
+"""
+import hashlib
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+STEPS = 4
+
+_SCRIPT = r"""
+import hashlib, json, sys
+sys.path.insert(0, sys.argv[1])
+from fluam_b200 import StokesLimit, workloads
+cfg, q, bonds = workloads.build("plain_128", seed=3)
+sim = StokesLimit(cfg, q)
+if bonds is not None:
+    sim.load_bonds(*bonds)
+profiled = sys.argv[3] == "1"
+if profiled:
+    sim.profile(True)
+sim.step(int(sys.argv[2]))
+sim.sync()
+st = sim.status()
+out = {k: hashlib.sha1(a.tobytes()).hexdigest()
+       for k, a in (("q", sim.positions()), ("F", sim.forces()), ("v", sim.velocity()))}
+out["errors"] = st["error_bits"]
+print(json.dumps(out))
+sim.close()
+"""
+
+
+def _run(env_extra, profiled=False):
+    env = dict(os.environ)
+    for k in ("FLUAMSL_PDL", "FLUAMSL_PLANE_V", "FLUAMSL_FFT_SCHEDULE", "FLUAMSL_FUSED_FORCES",
+              "FLUAMSL_SPREAD_BOX"):
+        env.pop(k, None)
+    env.update(env_extra)
+    r = subprocess.run([sys.executable, "-c", _SCRIPT, ROOT, str(STEPS), "1" if profiled else "0"],
+                       capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out.pop("errors") == 0
+    return out
+
+
+@pytest.fixture(scope="module")
+def default_run():
+    return _run({})
+
+
+@pytest.mark.parametrize("env", [
+    {"FLUAMSL_PDL": "0"},
+    {"FLUAMSL_PLANE_V": "0"},
+    {"FLUAMSL_FFT_SCHEDULE": "lines"},
+    {"FLUAMSL_FFT_SCHEDULE": "plane"},
+    {"FLUAMSL_FUSED_FORCES": "0"},
+    {"FLUAMSL_SPREAD_BOX": "0"},
+], ids=lambda e: ",".join(f"{k}={v}" for k, v in e.items()))
+def test_switch_gives_same_bits(default_run, env):
+    assert _run(env) == default_run
+
+
+def test_profiled_step_gives_same_bits(default_run):
+    assert _run({}, profiled=True) == default_run
