@@ -262,6 +262,7 @@ int make_params(const fsl_config& c, int64_t np, Params& P) {
   P.fact4 = std::sqrt((2. * c.temperature * c.shearviscosity) / (P.dV * c.dt));
   P.fact2 = std::sqrt(c.temperature * c.extra_mobility * c.dt);
   P.seed = c.seed;
+  P.keys = philox_keys(P.seed);
   if (two_d) {
     // src/createCellsQuasi2DGPU.cu:49-79: blob variance by scheme, stencil
     // half-width int(3 a mx / lx) + 1 (at most mx / 2), stochastic prefactor

@@ -32,6 +32,11 @@ enum { ERR_ANY = 0, ERR_BITS = 1 };
 // Params::prec, the values of FSL_PRECISION_* (include/fluamsl.h)
 enum { PREC_FIXED = 0, PREC_FLOAT = 1, PREC_F64 = 2 };
 
+// The ten round keys of Philox4x32-10 for one seed (philox_keys).
+struct PhiloxKeys {
+  uint32_t k0[10], k1[10];
+};
+
 // Everything a kernel needs about one instance, passed by value.
 struct Params {
   // fluid grid
@@ -58,6 +63,7 @@ struct Params {
   double cutoff, cutoff2, invcut2, soft_eps;
   double eta, kT, dt, extra_mob, fact1, fact2, fact4;
   uint64_t seed;
+  PhiloxKeys keys;   // the round keys of seed (set with it on the host)
   uint64_t noise_n;  // 12 nc + 9 np; quasi-2D family 4 (nc + mx + my) + 2 np nDrift
   // quasi-2D family: Gaussian variance, stencil half-width, stochastic
   // prefactor, options
@@ -97,12 +103,33 @@ __host__ __device__ inline uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
   return c;
 }
 
-// The four normal deviates with noise indices 4b .. 4b+3 of draw t.  Word w
-// becomes the uniform (2 (w >> 9) + 1) 2^-24 in (0,1), exact in FP32;
-// Box-Muller on the pairs (u0,u1) and (u2,u3).
-__device__ inline float4 philox_normal4(uint64_t seed, uint64_t t, uint64_t b) {
-  uint4 c = make_uint4((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)t, (uint32_t)(t >> 32));
-  uint4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+// The same rounds with the key schedule computed beforehand (the round keys
+// depend on the seed only; Params::keys holds the instance's).
+__host__ __device__ inline PhiloxKeys philox_keys(uint64_t seed) {
+  PhiloxKeys K;
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  for (int r = 0; r < 10; ++r) {
+    K.k0[r] = k0;
+    K.k1[r] = k1;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return K;
+}
+__host__ __device__ inline uint4 philox4x32_10(uint4 c, const PhiloxKeys& K) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0 = mulhi32(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    uint32_t hi1 = mulhi32(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ K.k0[r], lo1, hi0 ^ c.w ^ K.k1[r], lo0);
+  }
+  return c;
+}
+
+// The four normal deviates of one Philox output r.  Word w becomes the
+// uniform (2 (w >> 9) + 1) 2^-24 in (0,1), exact in FP32; Box-Muller on the
+// pairs (u0,u1) and (u2,u3).
+__device__ inline float4 philox_box_muller(uint4 r) {
   const float s24 = 5.9604644775390625e-08f;  // 2^-24
   float u0 = (float)(2u * (r.x >> 9) + 1u) * s24;
   float u1 = (float)(2u * (r.y >> 9) + 1u) * s24;
@@ -117,6 +144,19 @@ __device__ inline float4 philox_normal4(uint64_t seed, uint64_t t, uint64_t b) {
   __sincosf(6.28318530717958647692f * (u1 - 0.5f), &sa, &ca);
   __sincosf(6.28318530717958647692f * (u3 - 0.5f), &sb, &cb);
   return make_float4(-ra * ca, -ra * sa, -rb * cb, -rb * sb);
+}
+
+// philox_normal4 with the key schedule K of the seed (philox_keys)
+__device__ inline float4 philox_normal4(const PhiloxKeys& K, uint64_t t, uint64_t b) {
+  const uint4 c = make_uint4((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)t, (uint32_t)(t >> 32));
+  return philox_box_muller(philox4x32_10(c, K));
+}
+
+// The four normal deviates with noise indices 4b .. 4b+3 of draw t
+// (philox_box_muller of the Philox output of counter (b, t) keyed by seed).
+__device__ inline float4 philox_normal4(uint64_t seed, uint64_t t, uint64_t b) {
+  const uint4 c = make_uint4((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)t, (uint32_t)(t >> 32));
+  return philox_box_muller(philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32)));
 }
 
 // ------------------------------------------------------------ W of a cell ---

@@ -29,7 +29,7 @@ __global__ void k_noise(FSL_KARGS) {
   float4* out = reinterpret_cast<float4*>(R.noise);
   for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < nb;
        b += (uint64_t)gridDim.x * blockDim.x)
-    out[b] = philox_normal4(P.seed, t, b);
+    out[b] = philox_normal4(P.keys, t, b);  // the round keys of P.seed
 }
 
 __global__ void k_noise_range(uint64_t seed, uint64_t t, uint64_t first, int64_t count,
