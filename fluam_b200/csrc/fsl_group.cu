@@ -727,10 +727,11 @@ void group_enqueue_step(Group& g) {
   auto cells_forces = [&](int which, bool fused) {
     fused = fused && fuse;
     pr.mark(s, "cells");
-    // (one cooperative launch for a single instance; on the Verlet path the
+    // (one cooperative launch for a single instance, one launch of a block
+    // per instance for a batch of small instances; on the Verlet path the
     // list kernels return at once unless a rebuild is due)
     if (launch_pair_lists(B, which, s) != cudaSuccess && !g.fail_stage) g.fail_stage = "cells";
-    pr.count(!pk ? 0 : (B.one && B.one->bar) ? 1 : 5 + (B.has_vl ? 1 : 0));
+    pr.count(!pk ? 0 : ((B.one && B.one->bar) || block_lists(B)) ? 1 : 5 + (B.has_vl ? 1 : 0));
     chk("cells");
     if (!(fused && !B.has_cl)) pr.mark(s, "forces");
     launch_forces(B, which, s, !fused);

@@ -735,6 +735,10 @@ void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStre
 // The cell list of force evaluation `which` and, for Verlet-list
 // instances, the pair list (each only where list_needed says so).
 cudaError_t launch_pair_lists(const Batch& B, int which, cudaStream_t s);
+// Whether launch_pair_lists builds the lists of this batch in one launch of
+// one block per instance (batches of small instances; FLUAMSL_BLOCK_LISTS=0
+// keeps the separate kernels)
+bool block_lists(const Batch& B);
 // The cell-list counters and the single-launch build's barrier cleared
 // (after an error, before lists are built again)
 void launch_reset_lists(const Rep& r, cudaStream_t s);

@@ -678,6 +678,69 @@ __global__ void __launch_bounds__(kCoopThreads) k_lists_coop(const __grid_consta
   for (int i = tid; i < np; i += nth) vl_build_one(R, i, which);
 }
 
+// ------------------------------------------- block-per-instance list build ---
+// The lists of every instance of a batch of small instances in one launch:
+// block r runs the phases of the separate kernels above for instance r, with
+// block barriers between them (count, exclusive scan tile by tile with a
+// running carry, scatter, rank, Verlet list).  Each phase leaves the words
+// the separate kernels leave (the rank phase orders every cell by particle
+// index whatever order the scatter's atomics took), so the lists are the
+// same, and a force evaluation of a batch costs one launch instead of six.
+// Taken for batches whose instances have at most kBlockListsMaxNp particles
+// and kBlockListsMaxCells cells (a block of 1024 threads per instance keeps
+// each phase to a few passes); larger instances keep the separate kernels,
+// whose grids spread an instance over many blocks.
+constexpr int kBlockListsMaxNp = 8192;
+constexpr int kBlockListsMaxCells = 1 << 18;
+
+template <bool ONE>
+__global__ void __launch_bounds__(kScanThreads) k_lists_block(FSL_KARGS, int which) {
+  FSL_REP_AT(blockIdx.x);
+  if (!list_needed(R, which)) return;
+  const int np = P.np, n = P.mN;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) cell_count_one(R, i, which);
+  __syncthreads();
+  int* start = which && R.start1 ? R.start1 : R.start;
+  __shared__ int warp_tot[33];
+  int carry = 0;
+  for (int tile = 0; tile < n; tile += kScanTile) {
+    const int base = tile + threadIdx.x * kScanItems;
+    int v[kScanItems];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < n) ? R.cnt[base + k] : 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+      if (base + k < n) R.cnt[base + k] = 0;
+    int run, sum, total;
+    block_scan(v, run, sum, warp_tot, total);
+    run += carry;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      if (base + k < n) start[base + k] = run;
+      run += v[k];
+    }
+    carry += total;
+    __syncthreads();  // every thread has read warp_tot before the next tile writes it
+  }
+  if (threadIdx.x == 0) start[n] = carry;
+  __syncthreads();
+  for (int i = threadIdx.x; i < np; i += blockDim.x) cell_scatter_one(R, i, which);
+  __syncthreads();
+  for (int i = threadIdx.x; i < np; i += blockDim.x) cell_rank_one(R, i, which);
+  if (!P.verlet) return;
+  __syncthreads();
+  if (R.vl_flag[2] == 3) return;  // cell mode: no pair list
+  for (int i = threadIdx.x; i < np; i += blockDim.x) vl_build_one(R, i, which);
+}
+
+bool block_lists(const Batch& B) {
+  static const bool on = [] {
+    const char* e = getenv("FLUAMSL_BLOCK_LISTS");
+    return !(e && e[0] == '0');
+  }();
+  return on && !B.one && B.max_np > 0 && B.max_np <= kBlockListsMaxNp && B.mN <= kBlockListsMaxCells;
+}
+
 // The pair (Verlet list, or the 27 cells of the current cell list in cell
 // mode) and bonded force on particle i by its quad: lane a takes list
 // entries and bonds a, a + 4, ...; the partial forces are summed in a fixed
@@ -841,6 +904,10 @@ cudaError_t launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, k_lists_coop, *B.one, which, coop_spin_limit());
+  }
+  if (block_lists(B)) {
+    FSL_GO(k_lists_block, dim3(B.nrep), kScanThreads, 0, s, B, which);
+    return cudaPeekAtLastError();
   }
   launch_cells(B, which, s, false);
   if (B.max_np > 0 && B.has_vl) FSL_GO(k_vl_build, part_blocks(B, KIND_T1), kPartThreads, 0, s, B, which);

@@ -18,7 +18,10 @@ default process:
 
 A further case compares the default step with the per-stage profiled step,
 which keeps everything on one stream (the noise, and the field clear that
-the W build then does itself).
+the W build then does itself).  A batch of small instances of several size
+classes (Verlet-list, cell-mode and empty instances among them) compares
+FLUAMSL_BLOCK_LISTS=0, the separate list kernels, with the default build of
+one block per instance.
 """
 import hashlib
 import json
@@ -56,13 +59,47 @@ sim.close()
 """
 
 
-def _run(env_extra, profiled=False):
+_BATCH_SCRIPT = r"""
+import hashlib, json, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import fluam_b200 as fsl
+rng = np.random.default_rng(11)
+cfgs, qs = [], []
+for i in range(24):
+    m = int(rng.choice((16, 24, 32)))
+    n = 0 if i == 5 else int(round(np.exp(rng.uniform(np.log(8), np.log(3000)))))
+    if i == 7:  # dense: the Verlet list overflows into cell mode
+        q = rng.uniform(-2.0, 2.0, (3, 500))
+    else:
+        q = rng.uniform(-0.5, 0.5, (3, n)) * m
+    cfgs.append(fsl.make_config((m, m, m), (float(m),) * 3, eta=float(rng.uniform(0.5, 2.0)), kT=0.01,
+                                dt=0.01, cutoff=1.5, kernel=int(rng.choice((3, 4))), pair=fsl.PAIR_SOFT,
+                                seed=500 + i))
+    qs.append(q)
+b = fsl.Batch(cfgs, qs)
+b.step(int(sys.argv[2]))
+b.sync()
+h = hashlib.sha1()
+errors = 0
+for i in range(len(cfgs)):
+    h.update(b.positions(i).tobytes())
+    h.update(b.forces(i).tobytes())
+    errors |= b.status(i)["error_bits"]
+print(json.dumps({"qF": h.hexdigest(), "errors": errors}))
+b.close()
+"""
+
+_SWITCHES = ("FLUAMSL_PDL", "FLUAMSL_PLANE_V", "FLUAMSL_FFT_SCHEDULE", "FLUAMSL_FUSED_FORCES",
+             "FLUAMSL_SPREAD_BOX", "FLUAMSL_BLOCK_LISTS")
+
+
+def _run(env_extra, profiled=False, script=_SCRIPT):
     env = dict(os.environ)
-    for k in ("FLUAMSL_PDL", "FLUAMSL_PLANE_V", "FLUAMSL_FFT_SCHEDULE", "FLUAMSL_FUSED_FORCES",
-              "FLUAMSL_SPREAD_BOX"):
+    for k in _SWITCHES:
         env.pop(k, None)
     env.update(env_extra)
-    r = subprocess.run([sys.executable, "-c", _SCRIPT, ROOT, str(STEPS), "1" if profiled else "0"],
+    r = subprocess.run([sys.executable, "-c", script, ROOT, str(STEPS), "1" if profiled else "0"],
                        capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     out = json.loads(r.stdout.strip().splitlines()[-1])
@@ -89,3 +126,7 @@ def test_switch_gives_same_bits(default_run, env):
 
 def test_profiled_step_gives_same_bits(default_run):
     assert _run({}, profiled=True) == default_run
+
+
+def test_batch_list_build_gives_same_bits():
+    assert _run({"FLUAMSL_BLOCK_LISTS": "0"}, script=_BATCH_SCRIPT) == _run({}, script=_BATCH_SCRIPT)
