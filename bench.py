@@ -282,6 +282,15 @@ def run_fp64_form(torch, workload, steps=20, warmup=3):
             "l2": "not flushed (the step's FP64 state exceeds the L2)"}
 
 
+def compact_tuning(t):
+    """The picks of one size class's tuner (made at its first step), for the
+    JSON line."""
+    return {"cells": t["mx"], "instances": t["n"], "fft_schedule": t["fft_schedule"],
+            "schedule_us": [round(u, 2) for u in t["schedule_us"]],
+            "z_tile": [t["z_tile_kx"], t["z_tile_ky"]], "z_us": [round(u, 2) for u in t["z_us"]],
+            "list_build": t["list_build"], "list_us": [round(u, 2) for u in t["list_us"]]}
+
+
 def run_batched(torch, steps=20, warmup=3, plain_sample=128):
     """The mixed 1,024-replica workload as one batch (one launch per stage and
     size class, one graph per step), next to the same replicas stepped one at
@@ -294,6 +303,7 @@ def run_batched(torch, steps=20, warmup=3, plain_sample=128):
     stream = torch.cuda.ExternalStream(b.stream())
     b.step(warmup)
     b.sync()
+    tuning = [compact_tuning(t) for t in b.class_tuning()]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     b.step(steps)
@@ -347,6 +357,7 @@ def run_batched(torch, steps=20, warmup=3, plain_sample=128):
                                           "each, device time"},
         "speedup_vs_plain": value / plain,
         "gpu_launches_per_step": launches,
+        "autotune": tuning,
         "l2": "inputs (device state of all replicas) far larger than L2",
     }
 
@@ -475,6 +486,7 @@ def main():
 
     sim.step(max(args.warmup, 3))
     sim.sync()
+    tuning = compact_tuning(sim.tuning())
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -577,6 +589,7 @@ def main():
             "cpu_fp32": cpu32,
             "clocks": clk,
             "gpu_launches": launches_a * args.steps,
+            "autotune": tuning,
             "step_roofline": {"bytes_per_step": step_bytes(P["nc"], npart),
                               "achieved": step_bytes(P["nc"], npart) / (t_max / args.steps * 1e-3) / 1e9,
                               "peak": hbm, "unit": "GB/s",

@@ -35,6 +35,7 @@ EXPORTS = [
     "fsl_batch_get_positions_packed", "fsl_batch_set_positions_packed",
     "fsl_batch_get_positions_packed_async", "fsl_batch_set_positions_packed_async",
     "fsl_batch_set_graph", "fsl_batch_get_info", "fsl_batch_stream", "fsl_batch_destroy",
+    "fsl_batch_get_class_tuning", "fsl_get_tuning",
     "fsl_server_config_defaults", "fsl_server_create", "fsl_server_submit", "fsl_server_poll",
     "fsl_server_wait", "fsl_server_result", "fsl_server_get_stats", "fsl_server_destroy",
 ]
@@ -93,6 +94,28 @@ class BatchInfo(ctypes.Structure):
         ("launches_per_step", ctypes.c_int32), ("np_total", ctypes.c_int64),
         ("nc_total", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
     ]
+
+
+class ClassTuning(ctypes.Structure):
+    _fields_ = [
+        ("mx", ctypes.c_int32), ("my", ctypes.c_int32), ("mz", ctypes.c_int32),
+        ("kernel", ctypes.c_int32), ("precision", ctypes.c_int32), ("scheme", ctypes.c_int32),
+        ("n", ctypes.c_int32), ("tuned", ctypes.c_int32), ("fft_schedule", ctypes.c_int32),
+        ("z_tile_kx", ctypes.c_int32), ("z_tile_ky", ctypes.c_int32), ("z_threads", ctypes.c_int32),
+        ("z_candidates", ctypes.c_int32), ("z_us", ctypes.c_float * 8),
+        ("schedule_us", ctypes.c_float * 2), ("list_build", ctypes.c_int32),
+        ("list_us", ctypes.c_float * 2),
+    ]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["z_us"] = list(self.z_us)[:self.z_candidates]
+        d["schedule_us"] = list(self.schedule_us)
+        d["list_us"] = list(self.list_us)
+        d["fft_schedule"] = {0: "plane", 1: "lines"}.get(self.fft_schedule, "other")
+        d["list_build"] = {0: "separate", 1: "block_per_instance", 2: "cooperative"}.get(
+            self.list_build, "none")
+        return d
 
 
 class ServerConfig(ctypes.Structure):
@@ -197,6 +220,8 @@ def load(path=None):
     L.fsl_batch_set_positions_packed_async.argtypes = [_VP, _VP]
     L.fsl_batch_set_graph.argtypes = [_VP, ctypes.c_int]
     L.fsl_batch_get_info.argtypes = [_VP, ctypes.POINTER(BatchInfo)]
+    L.fsl_batch_get_class_tuning.argtypes = [_VP, ctypes.c_int32, ctypes.POINTER(ClassTuning)]
+    L.fsl_get_tuning.argtypes = [_VP, ctypes.POINTER(ClassTuning)]
     L.fsl_batch_stream.argtypes = [_VP]
     L.fsl_batch_stream.restype = _VP
     L.fsl_batch_destroy.argtypes = [_VP]

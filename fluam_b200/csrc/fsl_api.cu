@@ -262,6 +262,12 @@ int fsl_set_velocity_f64(fsl_handle* h, const double* in) {
   return FSL_OK;
 }
 
+int fsl_get_tuning(fsl_handle* h, fsl_class_tuning* out) {
+  if (!h || !out) return errorf(FSL_E_ARG, "null argument");
+  fsl::group_tuning(h->group, out);
+  return FSL_OK;
+}
+
 int fsl_get_status(fsl_handle* h, fsl_status* st) {
   if (!h || !st) return errorf(FSL_E_ARG, "null argument");
   FSL_TRY(cudaSetDevice(h->exec.device));

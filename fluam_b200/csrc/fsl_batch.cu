@@ -3,6 +3,7 @@
 // launch per stage on its own stream, the whole step captured in one graph.
 #include <algorithm>
 #include <cstring>
+#include <iterator>
 #include <map>
 #include <memory>
 #include <string>
@@ -337,6 +338,15 @@ int fsl_batch_get_info(fsl_batch* b, fsl_batch_info* info) {
   for (const auto& s : b->slots) bytes += (int64_t)s->bytes;
   bytes += (int64_t)sizeof(double) * b->packed_n;
   info->device_bytes = bytes;
+  return FSL_OK;
+}
+
+int fsl_batch_get_class_tuning(fsl_batch* b, int32_t k, fsl_class_tuning* out) {
+  if (!b || !out) return errorf(FSL_E_ARG, "null argument");
+  if (k < 0 || k >= (int32_t)b->groups.size()) return errorf(FSL_E_ARG, "no size class %d", (int)k);
+  auto it = b->groups.begin();
+  std::advance(it, k);
+  fsl::group_tuning(*it->second, out);
   return FSL_OK;
 }
 

@@ -1164,6 +1164,20 @@ void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s) {
   cudaGetLastError();
 }
 
+void fft_tuning(const FftPlan* fp, FftTuning& out) {
+  out = FftTuning{};
+  out.schedule = -1;
+  if (!fp) return;
+  out.tuned = fp->tuned ? 1 : 0;
+  if (fp->plane_fwd_r[0]) out.schedule = fp->use_lines ? 1 : 0;
+  out.z_kx = fp->z_kx;
+  out.z_ky = fp->z_ky;
+  out.z_threads = fp->z_threads;
+  out.nz = std::min(fp->nzc, 8);
+  for (int i = 0; i < out.nz; ++i) out.z_us[i] = fp->zc_us[i] < 1e29f ? fp->zc_us[i] : 0.f;
+  for (int k = 0; k < 2; ++k) out.sched_us[k] = fp->sched_us[k] < 1e29f ? fp->sched_us[k] : 0.f;
+}
+
 void launch_field_clear(const Batch& B, cudaStream_t s) {
   if (B.nrep == 0) return;
   const long cap = (148L * 8 + B.nrep - 1) / B.nrep;

@@ -695,6 +695,32 @@ int group_upload(Group& g) {
   return FSL_OK;
 }
 
+void group_tuning(const Group& g, fsl_class_tuning* out) {
+  std::memset(out, 0, sizeof(*out));
+  out->mx = g.key.mx;
+  out->my = g.key.my;
+  out->mz = g.key.mz;
+  out->kernel = g.key.kernel;
+  out->precision = g.key.prec;
+  out->scheme = g.key.scheme;
+  out->n = (int32_t)g.slots.size();
+  FftTuning t;
+  fft_tuning(g.fft, t);
+  out->tuned = t.tuned;
+  out->fft_schedule = t.schedule;
+  out->z_tile_kx = t.z_kx;
+  out->z_tile_ky = t.z_ky;
+  out->z_threads = t.z_threads;
+  out->z_candidates = t.nz;
+  for (int i = 0; i < 8; ++i) out->z_us[i] = t.z_us[i];
+  out->schedule_us[0] = t.sched_us[0];
+  out->schedule_us[1] = t.sched_us[1];
+  const Batch& B = g.B;
+  out->list_build = B.max_np == 0 ? -1 : (B.one && B.one->bar) ? 2 : block_lists(B) ? 1 : 0;
+  out->list_us[0] = g.lists_us[0];
+  out->list_us[1] = g.lists_us[1];
+}
+
 // One midpoint step (src/runSchemeStokesLimit.cu:163-275) of every active
 // instance of the group.
 void group_enqueue_step(Group& g) {
@@ -894,6 +920,24 @@ void group_enqueue_step(Group& g) {
   // stencil cache for the interpolation at the same positions (q^n, then
   // q^{n+1/2}) unless the tiled spread, which keeps none, runs.
   const bool stc = !B.tiled;
+  // The list build of a batch of small instances: one block per instance or
+  // the separate kernels, whichever builds this class's lists faster.  Timed
+  // once (first uncaptured step) after the first force evaluation, where a
+  // build costs what it costs at most evaluations: the Verlet lists whose
+  // rebuild was due are rebuilt by then (the spread that computed the
+  // forces has taken the request), the cell lists of the cell-list path and
+  // of cell mode rebuild in full.  Both builds give the same lists, and a
+  // build at unchanged positions leaves the lists as they are, so the timed
+  // builds change no result.
+  auto tune_lists = [&]() {
+    if (g.lists_tuned || !pk || !block_lists_eligible(B) || block_lists_env() >= 0) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+    g.lists_tuned = true;
+    pr.mark(s, "autotune");
+    lists_autotune(B, s, g.lists_us);
+    g.B.lists_pick = g.lists_us[1] <= g.lists_us[0] ? 1 : 0;
+  };
   cells_forces(0, !B.tiled);
   if (B.tiled) {
     join_noise();
@@ -908,6 +952,7 @@ void group_enqueue_step(Group& g) {
     pr.count(pk);
     join_noise();
   }
+  tune_lists();
   solve(0, 1, 1.41421356237309504880);
   // option 1: predictor, F^{n+1/2}, f = S F + RFD; solve 2 with
   // sqrt(1/2) (stress 1 + stress 2)

@@ -110,6 +110,10 @@ struct Group {
   Prof prof;
   std::map<std::string, std::pair<int64_t, double>> stage_acc;
   int launches = 0;             // kernels of this group in one step
+  // the list build of a batch of small instances, timed at the class's first
+  // uncaptured step (us per build: separate kernels, block per instance)
+  bool lists_tuned = false;
+  float lists_us[2] = {};
   const char* fail_stage = nullptr;  // first stage whose launch failed
 };
 
@@ -120,6 +124,8 @@ void group_destroy(Group& g);  // plan, table, events; not the slots
 int group_upload(Group& g);
 void group_enqueue_step(Group& g);  // one midpoint step of every active slot
 int group_prof_collect(Group& g);
+// The class's tuner picks and timings (fsl_batch_get_class_tuning)
+void group_tuning(const Group& g, fsl_class_tuning* out);
 
 struct Exec {
   int device = 0;

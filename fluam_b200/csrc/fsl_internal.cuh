@@ -570,6 +570,10 @@ struct Batch {
   int has_vl, has_cl;  // instances on the Verlet path / on the cell-list pair path
   int nblk[NKIND];  // total blocks of each particle launch kind
   const Rep* one;   // host copy of the single instance (nrep == 1), else null
+  // list build of a batch of small instances, as the class's tuner picked it
+  // (-1: not tuned, the block-per-instance build; 0: the separate kernels;
+  // 1: the block-per-instance build)
+  int lists_pick = -1;
   RepSrc src() const { return RepSrc{reps, boff, nrep}; }
 };
 
@@ -736,9 +740,18 @@ void launch_spread_w(const Batch& B, int drift, int nsets, double nfac, cudaStre
 // instances, the pair list (each only where list_needed says so).
 cudaError_t launch_pair_lists(const Batch& B, int which, cudaStream_t s);
 // Whether launch_pair_lists builds the lists of this batch in one launch of
-// one block per instance (batches of small instances; FLUAMSL_BLOCK_LISTS=0
-// keeps the separate kernels)
+// one block per instance: batches of small instances (block_lists_eligible),
+// unless the class's tuner picked the separate kernels.
+// FLUAMSL_BLOCK_LISTS=0 / =1 fixes the separate kernels / the block build.
+bool block_lists_eligible(const Batch& B);
 bool block_lists(const Batch& B);
+// -1: the tuner decides; 0, 1: fixed by FLUAMSL_BLOCK_LISTS
+int block_lists_env();
+// Times both list builds of force evaluation 0 of an eligible batch (three
+// rounds of three builds each, the fastest round kept) and returns the us
+// per build: us[0] the separate kernels, us[1] the block per instance.  A
+// build at unchanged positions leaves the lists as they are.
+void lists_autotune(const Batch& B, cudaStream_t s, float us[2]);
 // The cell-list counters and the single-launch build's barrier cleared
 // (after an error, before lists are built again)
 void launch_reset_lists(const Rep& r, cudaStream_t s);
@@ -772,15 +785,23 @@ void launch_q2_update(const Batch& B, int stage, cudaStream_t s);
 struct FftPlan;  // defined in fsl_fft.cu
 FftPlan* fft_plan_create(const Params& P);
 void fft_plan_destroy(FftPlan* fp);
+// Picks the fastest z-pass tile of the plan's candidates, then the faster
+// of the plane and five-pass transform schedules, on B's buffers (once per
+// plan; no-op under stream capture).
+void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s);
+// What the plan's tuner picked and measured (schedule -1: the plan has no
+// register path; z tile 0 x 0: no candidates)
+struct FftTuning {
+  int tuned, schedule, z_kx, z_ky, z_threads, nz;
+  float z_us[8], sched_us[2];
+};
+void fft_tuning(const FftPlan* fp, FftTuning& out);
 // v = solve(W).  W = f + nfac div(stress 1 [+ stress 2 when nsets == 2]) is
 // built from the spread field (which is cleared on the way) and the noise
 // divergence into Rep::wbuf, unless w_given, in which case Rep::wbuf already
 // holds W.  With w_built, the W build leaves the field as it is and records
 // w_built after itself: the caller clears the field (launch_field_clear)
 // after that event and before the next spread.
-// Picks the fastest z-pass tile of the plan's candidates on B's buffers
-// (once per plan; no-op under stream capture).
-void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s);
 void launch_solve(const Batch& B, FftPlan* fp, int nsets, double nfac, int w_given, cudaStream_t s,
                   Prof* prof = nullptr, cudaEvent_t w_built = nullptr);
 // Zeroes the spread fields of B's instances (streaming stores).

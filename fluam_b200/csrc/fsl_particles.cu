@@ -733,12 +733,57 @@ __global__ void __launch_bounds__(kScanThreads) k_lists_block(FSL_KARGS, int whi
   for (int i = threadIdx.x; i < np; i += blockDim.x) vl_build_one(R, i, which);
 }
 
-bool block_lists(const Batch& B) {
-  static const bool on = [] {
+int block_lists_env() {
+  static const int v = [] {
     const char* e = getenv("FLUAMSL_BLOCK_LISTS");
-    return !(e && e[0] == '0');
+    return !e || !*e ? -1 : e[0] == '0' ? 0 : 1;
   }();
-  return on && !B.one && B.max_np > 0 && B.max_np <= kBlockListsMaxNp && B.mN <= kBlockListsMaxCells;
+  return v;
+}
+
+bool block_lists_eligible(const Batch& B) {
+  return !B.one && B.max_np > 0 && B.max_np <= kBlockListsMaxNp && B.mN <= kBlockListsMaxCells;
+}
+
+bool block_lists(const Batch& B) {
+  const int env = block_lists_env();
+  if (!block_lists_eligible(B) || env == 0) return false;
+  return env == 1 || B.lists_pick != 0;
+}
+
+static void lists_separate(const Batch& B, int which, cudaStream_t s);
+
+void lists_autotune(const Batch& B, cudaStream_t s, float us[2]) {
+  us[0] = us[1] = 0.f;
+  if (!block_lists_eligible(B)) return;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    cudaGetLastError();
+    return;
+  }
+  // three rounds over the two builds in turn, three builds each after one
+  // untimed, the fastest round kept
+  float best[2] = {1e30f, 1e30f};
+  for (int round = 0; round < 3; ++round)
+    for (int k = 0; k < 2; ++k) {
+      auto build = [&] {
+        if (k) FSL_GO(k_lists_block, dim3(B.nrep), kScanThreads, 0, s, B, 0);
+        else lists_separate(B, 0, s);
+      };
+      build();
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < 3; ++r) build();
+      cudaEventRecord(e1, s);
+      float ms = 0.f;
+      if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = 1e9f;
+      best[k] = std::min(best[k], ms * 1000.f / 3.f);
+    }
+  us[0] = best[0];
+  us[1] = best[1];
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
 }
 
 // The pair (Verlet list, or the 27 cells of the current cell list in cell
@@ -909,9 +954,13 @@ cudaError_t launch_pair_lists(const Batch& B, int which, cudaStream_t s) {
     FSL_GO(k_lists_block, dim3(B.nrep), kScanThreads, 0, s, B, which);
     return cudaPeekAtLastError();
   }
+  lists_separate(B, which, s);
+  return cudaPeekAtLastError();
+}
+
+static void lists_separate(const Batch& B, int which, cudaStream_t s) {
   launch_cells(B, which, s, false);
   if (B.max_np > 0 && B.has_vl) FSL_GO(k_vl_build, part_blocks(B, KIND_T1), kPartThreads, 0, s, B, which);
-  return cudaPeekAtLastError();
 }
 
 // After an error: the cell-list counters and the grid barrier of the

@@ -156,6 +156,12 @@ class StokesLimit:
         return {"step": st.step, "error_bits": st.error_bits, "np": st.np, "nc": st.nc,
                 "graph": bool(st.graph), "launches_per_step": st.launches_per_step}
 
+    def tuning(self):
+        """The autotuner's picks and timings (after the first step)."""
+        t = _lib.ClassTuning()
+        check(self.L.fsl_get_tuning(self.h, ctypes.byref(t)))
+        return t.as_dict()
+
     def profile(self, enable=True):
         """Per-stage CUDA-event timing of every step (clears the totals)."""
         check(self.L.fsl_profile(self.h, 1 if enable else 0))
@@ -327,6 +333,16 @@ class Batch:
         b = _lib.BatchInfo()
         check(self.L.fsl_batch_get_info(self.h, ctypes.byref(b)))
         return {f: getattr(b, f) for f, _ in _lib.BatchInfo._fields_}
+
+    def class_tuning(self):
+        """Per size class: the autotuner's picks and timings (after the
+        first step)."""
+        out = []
+        for k in range(self.info()["classes"]):
+            t = _lib.ClassTuning()
+            check(self.L.fsl_batch_get_class_tuning(self.h, k, ctypes.byref(t)))
+            out.append(t.as_dict())
+        return out
 
     def stream(self):
         return self.L.fsl_batch_stream(self.h)

@@ -180,6 +180,9 @@ int fsl_get_velocity_f64(fsl_handle* h, double* out);
  * first step (src/runSchemeIncompressible.cu:82-96). */
 int fsl_set_velocity_f64(fsl_handle* h, const double* in);
 int fsl_get_status(fsl_handle* h, fsl_status* st);
+/* The autotuner's picks for this instance (fsl_class_tuning, below). */
+struct fsl_class_tuning;
+int fsl_get_tuning(fsl_handle* h, struct fsl_class_tuning* out);
 
 /* FP64 accumulators kept on the device when fsl_config.observables is 1
  * (3-D Stokes schemes).  No counterpart in the reference, which computes no
@@ -325,6 +328,37 @@ int fsl_batch_get_positions_packed_async(fsl_batch* b, double* host);
 int fsl_batch_set_positions_packed_async(fsl_batch* b, const double* host);
 int fsl_batch_set_graph(fsl_batch* b, int enable);
 int fsl_batch_get_info(fsl_batch* b, fsl_batch_info* info);
+
+/* What the autotuner of one size class picked and measured.  A class (the
+ * instances with the same cells, kernel, scheme and precision) is tuned at
+ * its first step outside graph capture: the z-pass tile of the transform,
+ * the transform schedule, and for a batch of small instances the list
+ * build.  Every choice computes the same bits, so the picks change speed
+ * only.  No counterpart in the reference, whose launch shape is a fixed
+ * heuristic on the particle count (src/runSchemeStokesLimit.cu:24-68). */
+typedef struct fsl_class_tuning {
+  int32_t mx, my, mz;            /* cells                                      */
+  int32_t kernel;                /* 3- or 4-point                              */
+  int32_t precision;             /* FSL_PRECISION_*                            */
+  int32_t scheme;                /* FSL_SCHEME_*                               */
+  int32_t n;                     /* instances in the class                     */
+  int32_t tuned;                 /* 1 once the class's first step has run      */
+  int32_t fft_schedule;          /* 0 plane passes, 1 five passes, -1 other    */
+  int32_t z_tile_kx, z_tile_ky;  /* z-pass tile picked (0: no register z pass) */
+  int32_t z_threads;             /* threads per block of that tile             */
+  int32_t z_candidates;          /* z tiles timed (at most 8)                  */
+  float z_us[8];                 /* us per z-pass launch of each candidate     */
+  float schedule_us[2];          /* us per transform: plane, five passes
+                                    (0: not timed)                             */
+  int32_t list_build;            /* 0 separate kernels, 1 one block per
+                                    instance, 2 cooperative single launch,
+                                    -1 no particles                            */
+  float list_us[2];              /* us per build: separate, block per
+                                    instance (0: not timed)                    */
+} fsl_class_tuning;
+
+/* Size class k of the batch, 0 <= k < fsl_batch_info.classes. */
+int fsl_batch_get_class_tuning(fsl_batch* b, int32_t k, fsl_class_tuning* out);
 void* fsl_batch_stream(fsl_batch* b);
 void fsl_batch_destroy(fsl_batch* b);
 

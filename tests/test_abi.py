@@ -36,6 +36,15 @@ def test_config_layout_matches_header():
     # fsl_config: 4 int32, 9 doubles, 1 uint64, 10 int32, 5 doubles
     assert ctypes.sizeof(_lib.Config) == 4 * 4 + 9 * 8 + 8 + 10 * 4 + 5 * 8
     assert ctypes.sizeof(_lib.Status) == 8 + 4 + 4 + 8 + 4 + 4
+    # fsl_class_tuning: 13 int32, 8 + 2 floats, 1 int32, 2 floats
+    assert ctypes.sizeof(_lib.ClassTuning) == 13 * 4 + 10 * 4 + 4 + 2 * 4
+
+
+def test_tuning_query_checks_arguments():
+    L = _lib.load()
+    t = _lib.ClassTuning()
+    assert L.fsl_batch_get_class_tuning(None, 0, ctypes.byref(t)) == -1
+    assert L.fsl_get_tuning(None, ctypes.byref(t)) == -1
 
 
 def test_defaults_follow_reference():

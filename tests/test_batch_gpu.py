@@ -192,3 +192,39 @@ def test_batch_mixed_pair_paths_equal_alone(fsl):
         np.testing.assert_array_equal(b.forces(i), Fa)
         assert b.status(i)["error_bits"] == 0 and sa["error_bits"] == 0
     b.close()
+
+
+def test_class_tuning_reports_picks(fsl):
+    """Every size class reports the tuner's picks after its first step: the
+    z-pass tile among the timed candidates, the faster transform schedule
+    and, for a batch of small instances, the faster list build; a single
+    instance reports the cooperative list build."""
+    inst = mixed_set(fsl, n=12, np_max=2000)
+    b = fsl.Batch([c for c, _ in inst], [q for _, q in inst])
+    b.step(2)
+    b.sync()
+    tun = b.class_tuning()
+    assert len(tun) == b.info()["classes"]
+    assert sum(t["n"] for t in tun) == len(inst)
+    for t in tun:
+        assert t["tuned"] == 1
+        assert t["fft_schedule"] in ("plane", "lines")
+        assert t["z_tile_kx"] > 0 and t["z_tile_ky"] > 0 and t["z_threads"] > 0
+        assert len(t["z_us"]) == t["z_candidates"] >= 1
+        if t["z_candidates"] > 1:  # a single candidate is not timed
+            assert all(u > 0 for u in t["z_us"])
+        plane_us, lines_us = t["schedule_us"]
+        if plane_us > 0 and lines_us > 0:  # both schedules exist for this edge
+            assert t["fft_schedule"] == ("lines" if lines_us < plane_us else "plane")
+        if t["n"] > 1:
+            us_sep, us_blk = t["list_us"]
+            assert us_sep > 0 and us_blk > 0
+            assert t["list_build"] == ("block_per_instance" if us_blk <= us_sep else "separate")
+    b.close()
+    cfg, q = inst[0]
+    g = fsl.StokesLimit(cfg, q)
+    g.step(1)
+    g.sync()
+    t = g.tuning()
+    assert t["tuned"] == 1 and t["list_build"] == "cooperative" and t["n"] == 1
+    g.close()

@@ -20,8 +20,8 @@ A further case compares the default step with the per-stage profiled step,
 which keeps everything on one stream (the noise, and the field clear that
 the W build then does itself).  A batch of small instances of several size
 classes (Verlet-list, cell-mode and empty instances among them) compares
-FLUAMSL_BLOCK_LISTS=0, the separate list kernels, with the default build of
-one block per instance.
+FLUAMSL_BLOCK_LISTS=0 and =1, the separate list kernels and the build of
+one block per instance, with the default, where each class's tuner picks.
 """
 import hashlib
 import json
@@ -128,5 +128,11 @@ def test_profiled_step_gives_same_bits(default_run):
     assert _run({}, profiled=True) == default_run
 
 
-def test_batch_list_build_gives_same_bits():
-    assert _run({"FLUAMSL_BLOCK_LISTS": "0"}, script=_BATCH_SCRIPT) == _run({}, script=_BATCH_SCRIPT)
+@pytest.fixture(scope="module")
+def default_batch_run():
+    return _run({}, script=_BATCH_SCRIPT)
+
+
+@pytest.mark.parametrize("value", ["0", "1"])
+def test_batch_list_build_gives_same_bits(default_batch_run, value):
+    assert _run({"FLUAMSL_BLOCK_LISTS": value}, script=_BATCH_SCRIPT) == default_batch_run
