@@ -288,6 +288,7 @@ def compact_tuning(t):
     return {"cells": t["mx"], "instances": t["n"], "fft_schedule": t["fft_schedule"],
             "schedule_us": [round(u, 2) for u in t["schedule_us"]],
             "z_tile": [t["z_tile_kx"], t["z_tile_ky"]], "z_us": [round(u, 2) for u in t["z_us"]],
+            "planes_per_block": t["plane_pb"], "plane_us": [round(u, 2) for u in t["plane_us"]],
             "list_build": t["list_build"], "list_us": [round(u, 2) for u in t["list_us"]]}
 
 

@@ -104,7 +104,8 @@ class ClassTuning(ctypes.Structure):
         ("z_tile_kx", ctypes.c_int32), ("z_tile_ky", ctypes.c_int32), ("z_threads", ctypes.c_int32),
         ("z_candidates", ctypes.c_int32), ("z_us", ctypes.c_float * 8),
         ("schedule_us", ctypes.c_float * 2), ("list_build", ctypes.c_int32),
-        ("list_us", ctypes.c_float * 2),
+        ("list_us", ctypes.c_float * 2), ("plane_pb", ctypes.c_int32),
+        ("plane_candidates", ctypes.c_int32), ("plane_us", ctypes.c_float * 4),
     ]
 
     def as_dict(self):
@@ -112,6 +113,7 @@ class ClassTuning(ctypes.Structure):
         d["z_us"] = list(self.z_us)[:self.z_candidates]
         d["schedule_us"] = list(self.schedule_us)
         d["list_us"] = list(self.list_us)
+        d["plane_us"] = list(self.plane_us)[:self.plane_candidates]
         d["fft_schedule"] = {0: "plane", 1: "lines"}.get(self.fft_schedule, "other")
         d["list_build"] = {0: "separate", 1: "block_per_instance", 2: "cooperative"}.get(
             self.list_build, "none")

@@ -36,6 +36,7 @@ struct Radices {
 };
 
 constexpr int kMaxZCand = 6;
+constexpr int kMaxPCand = 4;
 
 struct FftPlan {
   Radices rx, ry, rz;
@@ -82,6 +83,17 @@ struct FftPlan {
   int nzc = 0;
   bool tuned = false;
   float zc_us[kMaxZCand] = {};  // measured time per candidate (us per launch)
+  // planes-per-block candidates of the register plane passes (same
+  // arithmetic, another number of independent planes per block); the first
+  // is the default, fft_autotune picks one
+  struct PCand {
+    void (*fwd[2])(RepSrc, Rep, const float2*);
+    void (*inv[2])(RepSrc, Rep, const float2*);
+    int pb, threads;
+    size_t smem;
+  } pc[kMaxPCand];
+  int npc = 0;
+  float pc_us[kMaxPCand] = {};  // measured plane-schedule transform per candidate (us)
 };
 
 static bool factorize(int n, Radices& R) {
@@ -725,10 +737,38 @@ __global__ void __launch_bounds__(kFftThreads)
 #include "fsl_fft_v.cuh"
 
 // ------------------------------------------------------------ host side ---
+static void use_pcand(FftPlan* fp, int i) {
+  const FftPlan::PCand& c = fp->pc[i];
+  fp->plane_fwd_r[0] = c.fwd[0];
+  fp->plane_fwd_r[1] = c.fwd[1];
+  fp->plane_inv_r[0] = c.inv[0];
+  fp->plane_inv_r[1] = c.inv[1];
+  fp->plane_pb = c.pb;
+  fp->plane_threads = c.threads;
+  fp->smem_plane_r = c.smem;
+}
+
+// One planes-per-block candidate of the register plane passes.
 template <int N, int R, int T, int PB>
+static void add_pcand(FftPlan* fp) {
+  if (fp->npc >= kMaxPCand) return;
+  FftPlan::PCand& c = fp->pc[fp->npc++];
+  c.fwd[0] = k_plane_fwd_r<false, N, R, T, PB>;
+  c.fwd[1] = k_plane_fwd_r<true, N, R, T, PB>;
+  c.inv[0] = k_plane_inv_r<false, N, R, T, PB>;
+  c.inv[1] = k_plane_inv_r<true, N, R, T, PB>;
+  c.pb = PB;
+  c.threads = PB * (N / 2) * T;
+  c.smem = sizeof(float2) * (N + (size_t)PB * plane_buf<N, R, T>());
+}
+
+// The register plane passes of edge N (N = R x T), with planes-per-block
+// candidates PB, PBS... (the first is the default), and the five-pass
+// line kernels of the same shape.
+template <int N, int R, int T, int PB, int... PBS>
 static void pick_plane_r(FftPlan* fp) {
-  fp->plane_pb = PB;
-  fp->plane_threads = PB * (N / 2) * T;
+  add_pcand<N, R, T, PB>(fp);
+  (add_pcand<N, R, T, PBS>(fp), ...);
   if constexpr (T > 1 && 32 % T == 0) {
     fp->line_xf[0] = k_fft_xf<false, N, R, T>;
     fp->line_xf[1] = k_fft_xf<true, N, R, T>;
@@ -741,23 +781,31 @@ static void pick_plane_r(FftPlan* fp) {
     fp->line_lw = 32 / T;
     fp->smem_lines = sizeof(float2) * (N + (size_t)kLineWarps * (32 / T) * LineGeom<R, T>::LS);
   }
-  fp->plane_fwd_r[0] = k_plane_fwd_r<false, N, R, T, PB>;
-  fp->plane_fwd_r[1] = k_plane_fwd_r<true, N, R, T, PB>;
-  fp->plane_inv_r[0] = k_plane_inv_r<false, N, R, T, PB>;
-  fp->plane_inv_r[1] = k_plane_inv_r<true, N, R, T, PB>;
-  fp->smem_plane_r = sizeof(float2) * (N + (size_t)PB * plane_buf<N, R, T>());
-  if constexpr (N == 128 && R == 16 && T == 8 && PB == 1) {
+  if constexpr (N == 128 && R == 16 && T == 8 && PB == 1 && sizeof...(PBS) == 0) {
     // the conflict-free layout of the same arithmetic (fsl_fft_v.cuh);
     // FLUAMSL_PLANE_V=0 keeps the generic kernels, for comparison
     const char* e = getenv("FLUAMSL_PLANE_V");
     if (!(e && e[0] == '0')) {
-      fp->plane_fwd_r[0] = k_plane_fwd_v<false>;
-      fp->plane_fwd_r[1] = k_plane_fwd_v<true>;
-      fp->plane_inv_r[0] = k_plane_inv_v<false>;
-      fp->plane_inv_r[1] = k_plane_inv_v<true>;
-      fp->smem_plane_r = sizeof(float2) * (size_t)kVSmem;
+      FftPlan::PCand& c = fp->pc[0];
+      c.fwd[0] = k_plane_fwd_v<false>;
+      c.fwd[1] = k_plane_fwd_v<true>;
+      c.inv[0] = k_plane_inv_v<false>;
+      c.inv[1] = k_plane_inv_v<true>;
+      c.smem = sizeof(float2) * (size_t)kVSmem;
     }
   }
+  use_pcand(fp, 0);
+}
+
+// FLUAMSL_PLANE_CAND=i fixes the planes-per-block candidate i of the
+// register plane passes (0: the default; past the last: the last) instead
+// of letting fft_autotune time them (-1)
+static int pcand_env() {
+  static const int v = [] {
+    const char* e = getenv("FLUAMSL_PLANE_CAND");
+    return e && *e ? std::max(0, atoi(e)) : -1;
+  }();
+  return v;
 }
 
 // FLUAMSL_FFT_SCHEDULE=plane or =lines fixes the transform schedule of the
@@ -800,17 +848,17 @@ static void pick_z_r(FftPlan* fp) {
 static void pick_register_kernels(const Params& P, FftPlan* fp) {
   if (P.mx == P.my) {
     switch (P.mx) {
-      case 16: pick_plane_r<16, 16, 1, 16>(fp); break;
-      case 24: pick_plane_r<24, 24, 1, 16>(fp); break;
-      case 32: pick_plane_r<32, 16, 2, 4>(fp); break;
+      case 16: pick_plane_r<16, 16, 1, 16, 8, 32>(fp); break;
+      case 24: pick_plane_r<24, 24, 1, 16, 8, 32>(fp); break;
+      case 32: pick_plane_r<32, 16, 2, 4, 2, 8>(fp); break;
       case 40: pick_plane_r<40, 8, 5, 4>(fp); break;
-      case 48: pick_plane_r<48, 12, 4, 2>(fp); break;
+      case 48: pick_plane_r<48, 12, 4, 2, 1, 4>(fp); break;
       case 56: pick_plane_r<56, 8, 7, 2>(fp); break;
-      case 64: pick_plane_r<64, 16, 4, 2>(fp); break;
+      case 64: pick_plane_r<64, 16, 4, 2, 1, 4>(fp); break;
       case 72: pick_plane_r<72, 12, 6, 1>(fp); break;
       case 80: pick_plane_r<80, 20, 4, 1>(fp); break;
       case 88: pick_plane_r<88, 8, 11, 1>(fp); break;
-      case 96: pick_plane_r<96, 24, 4, 1>(fp); break;
+      case 96: pick_plane_r<96, 24, 4, 1, 2>(fp); break;
       case 128: pick_plane_r<128, 16, 8, 1>(fp); break;
       default: break;
     }
@@ -989,10 +1037,20 @@ FftPlan* fft_plan_create(const Params& P) {
                       allow((const void*)fp->plane_inv[v], fp->smem_plane);
   }
   pick_register_kernels(P, fp);
-  for (int v = 0; v < 2; ++v) {
-    if (fp->plane_fwd_r[0] &&
-        !(allow((const void*)fp->plane_fwd_r[v], fp->smem_plane_r) &&
-          allow((const void*)fp->plane_inv_r[v], fp->smem_plane_r))) {
+  {
+    // keep the planes-per-block candidates whose shared memory fits
+    int kept = 0;
+    for (int i = 0; i < fp->npc; ++i) {
+      const FftPlan::PCand& c = fp->pc[i];
+      bool fits = true;
+      for (int v = 0; v < 2; ++v)
+        fits = fits && allow((const void*)c.fwd[v], c.smem) && allow((const void*)c.inv[v], c.smem);
+      if (fits) fp->pc[kept++] = c;
+    }
+    fp->npc = kept;
+    if (kept) {
+      use_pcand(fp, pcand_env() < 0 ? 0 : std::min(pcand_env(), kept - 1));
+    } else {
       fp->plane_fwd_r[0] = fp->plane_fwd_r[1] = nullptr;
       fp->plane_inv_r[0] = fp->plane_inv_r[1] = nullptr;
     }
@@ -1143,6 +1201,30 @@ void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s) {
   for (int i = 1; i < fp->nzc; ++i)
     if (fp->zc_us[i] < fp->zc_us[best]) best = i;
   use_zcand(fp, best);
+  // planes per block of the plane schedule: the whole transform timed per
+  // candidate, as the z tiles
+  if (fp->npc > 1 && pcand_env() < 0 && sched_env() != 2) {
+    const bool lines = fp->use_lines;
+    fp->use_lines = false;
+    Prof none;
+    for (int i = 0; i < fp->npc; ++i) fp->pc_us[i] = 1e30f;
+    for (int round = 0; round < 3; ++round)
+      for (int i = 0; i < fp->npc; ++i) {
+        use_pcand(fp, i);
+        reg_transform(B, fp, s, none);  // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 5; ++r) reg_transform(B, fp, s, none);
+        cudaEventRecord(e1, s);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = 1e9f;
+        fp->pc_us[i] = std::min(fp->pc_us[i], ms * 1000.f / 5.f);
+      }
+    int pbest = 0;
+    for (int i = 1; i < fp->npc; ++i)
+      if (fp->pc_us[i] < fp->pc_us[pbest]) pbest = i;
+    use_pcand(fp, pbest);
+    fp->use_lines = lines;
+  }
   if (fp->line_xf[0] && sched_env() == 0) {
     Prof none;
     fp->sched_us[0] = fp->sched_us[1] = 1e30f;
@@ -1176,6 +1258,9 @@ void fft_tuning(const FftPlan* fp, FftTuning& out) {
   out.nz = std::min(fp->nzc, 8);
   for (int i = 0; i < out.nz; ++i) out.z_us[i] = fp->zc_us[i] < 1e29f ? fp->zc_us[i] : 0.f;
   for (int k = 0; k < 2; ++k) out.sched_us[k] = fp->sched_us[k] < 1e29f ? fp->sched_us[k] : 0.f;
+  out.plane_pb = fp->plane_fwd_r[0] ? fp->plane_pb : 0;
+  out.npc = std::min(fp->npc, 4);
+  for (int i = 0; i < out.npc; ++i) out.plane_us[i] = fp->pc_us[i] < 1e29f ? fp->pc_us[i] : 0.f;
 }
 
 void launch_field_clear(const Batch& B, cudaStream_t s) {

@@ -715,6 +715,9 @@ void group_tuning(const Group& g, fsl_class_tuning* out) {
   for (int i = 0; i < 8; ++i) out->z_us[i] = t.z_us[i];
   out->schedule_us[0] = t.sched_us[0];
   out->schedule_us[1] = t.sched_us[1];
+  out->plane_pb = t.plane_pb;
+  out->plane_candidates = t.npc;
+  for (int i = 0; i < 4; ++i) out->plane_us[i] = t.plane_us[i];
   const Batch& B = g.B;
   out->list_build = B.max_np == 0 ? -1 : (B.one && B.one->bar) ? 2 : block_lists(B) ? 1 : 0;
   out->list_us[0] = g.lists_us[0];

@@ -785,15 +785,18 @@ void launch_q2_update(const Batch& B, int stage, cudaStream_t s);
 struct FftPlan;  // defined in fsl_fft.cu
 FftPlan* fft_plan_create(const Params& P);
 void fft_plan_destroy(FftPlan* fp);
-// Picks the fastest z-pass tile of the plan's candidates, then the faster
-// of the plane and five-pass transform schedules, on B's buffers (once per
-// plan; no-op under stream capture).
+// Picks the fastest z-pass tile of the plan's candidates, the fastest
+// planes-per-block candidate of the plane passes, then the faster of the
+// plane and five-pass transform schedules, on B's buffers (once per plan;
+// no-op under stream capture).
 void fft_autotune(FftPlan* fp, const Batch& B, cudaStream_t s);
 // What the plan's tuner picked and measured (schedule -1: the plan has no
 // register path; z tile 0 x 0: no candidates)
 struct FftTuning {
   int tuned, schedule, z_kx, z_ky, z_threads, nz;
   float z_us[8], sched_us[2];
+  int plane_pb, npc;
+  float plane_us[4];
 };
 void fft_tuning(const FftPlan* fp, FftTuning& out);
 // v = solve(W).  W = f + nfac div(stress 1 [+ stress 2 when nsets == 2]) is

@@ -332,8 +332,8 @@ int fsl_batch_get_info(fsl_batch* b, fsl_batch_info* info);
 /* What the autotuner of one size class picked and measured.  A class (the
  * instances with the same cells, kernel, scheme and precision) is tuned at
  * its first step outside graph capture: the z-pass tile of the transform,
- * the transform schedule, and for a batch of small instances the list
- * build.  Every choice computes the same bits, so the picks change speed
+ * the planes per block of its plane passes, the transform schedule, and for
+ * a batch of small instances the list build.  Every choice computes the same bits, so the picks change speed
  * only.  No counterpart in the reference, whose launch shape is a fixed
  * heuristic on the particle count (src/runSchemeStokesLimit.cu:24-68). */
 typedef struct fsl_class_tuning {
@@ -355,6 +355,11 @@ typedef struct fsl_class_tuning {
                                     -1 no particles                            */
   float list_us[2];              /* us per build: separate, block per
                                     instance (0: not timed)                    */
+  int32_t plane_pb;              /* planes per block of the plane passes
+                                    picked (0: no register plane passes)       */
+  int32_t plane_candidates;      /* planes-per-block candidates (at most 4)    */
+  float plane_us[4];             /* us per plane-schedule transform of each
+                                    candidate (0: not timed)                   */
 } fsl_class_tuning;
 
 /* Size class k of the batch, 0 <= k < fsl_batch_info.classes. */

@@ -36,8 +36,8 @@ def test_config_layout_matches_header():
     # fsl_config: 4 int32, 9 doubles, 1 uint64, 10 int32, 5 doubles
     assert ctypes.sizeof(_lib.Config) == 4 * 4 + 9 * 8 + 8 + 10 * 4 + 5 * 8
     assert ctypes.sizeof(_lib.Status) == 8 + 4 + 4 + 8 + 4 + 4
-    # fsl_class_tuning: 13 int32, 8 + 2 floats, 1 int32, 2 floats
-    assert ctypes.sizeof(_lib.ClassTuning) == 13 * 4 + 10 * 4 + 4 + 2 * 4
+    # fsl_class_tuning: 13 int32, 8 + 2 floats, 1 int32, 2 floats, 2 int32, 4 floats
+    assert ctypes.sizeof(_lib.ClassTuning) == 13 * 4 + 10 * 4 + 4 + 2 * 4 + 2 * 4 + 4 * 4
 
 
 def test_tuning_query_checks_arguments():

@@ -213,6 +213,11 @@ def test_class_tuning_reports_picks(fsl):
         assert len(t["z_us"]) == t["z_candidates"] >= 1
         if t["z_candidates"] > 1:  # a single candidate is not timed
             assert all(u > 0 for u in t["z_us"])
+        assert len(t["plane_us"]) == t["plane_candidates"] >= 1
+        if t["plane_candidates"] > 1:
+            assert all(u > 0 for u in t["plane_us"])
+            best = min(range(t["plane_candidates"]), key=lambda i: t["plane_us"][i])
+            assert t["plane_pb"] > 0 and t["plane_us"][best] == min(t["plane_us"])
         plane_us, lines_us = t["schedule_us"]
         if plane_us > 0 and lines_us > 0:  # both schedules exist for this edge
             assert t["fft_schedule"] == ("lines" if lines_us < plane_us else "plane")

@@ -21,7 +21,10 @@ which keeps everything on one stream (the noise, and the field clear that
 the W build then does itself).  A batch of small instances of several size
 classes (Verlet-list, cell-mode and empty instances among them) compares
 FLUAMSL_BLOCK_LISTS=0 and =1, the separate list kernels and the build of
-one block per instance, with the default, where each class's tuner picks.
+one block per instance, with the default, where each class's tuner picks;
+the same batch and an instance at 64^3 compare FLUAMSL_PLANE_CAND=0, 1, 2
+(the planes-per-block candidates of the plane passes) with the tuner's
+pick.
 """
 import hashlib
 import json
@@ -90,8 +93,29 @@ print(json.dumps({"qF": h.hexdigest(), "errors": errors}))
 b.close()
 """
 
+# one instance at 64^3 (20,000 particles, 4-point kernel, soft repulsion):
+# the edge whose plane passes have three planes-per-block candidates
+_SCRIPT64 = r"""
+import hashlib, json, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import fluam_b200 as fsl
+rng = np.random.default_rng(17)
+q = rng.uniform(-32.0, 32.0, (3, 20000))
+cfg = fsl.make_config((64, 64, 64), (64.0,) * 3, kT=0.01, dt=0.01, cutoff=1.5, kernel=4,
+                      pair=fsl.PAIR_SOFT, seed=77)
+sim = fsl.StokesLimit(cfg, q)
+sim.step(int(sys.argv[2]))
+sim.sync()
+out = {k: hashlib.sha1(a.tobytes()).hexdigest()
+       for k, a in (("q", sim.positions()), ("F", sim.forces()), ("v", sim.velocity()))}
+out["errors"] = sim.status()["error_bits"]
+print(json.dumps(out))
+sim.close()
+"""
+
 _SWITCHES = ("FLUAMSL_PDL", "FLUAMSL_PLANE_V", "FLUAMSL_FFT_SCHEDULE", "FLUAMSL_FUSED_FORCES",
-             "FLUAMSL_SPREAD_BOX", "FLUAMSL_BLOCK_LISTS")
+             "FLUAMSL_SPREAD_BOX", "FLUAMSL_BLOCK_LISTS", "FLUAMSL_PLANE_CAND")
 
 
 def _run(env_extra, profiled=False, script=_SCRIPT):
@@ -136,3 +160,13 @@ def default_batch_run():
 @pytest.mark.parametrize("value", ["0", "1"])
 def test_batch_list_build_gives_same_bits(default_batch_run, value):
     assert _run({"FLUAMSL_BLOCK_LISTS": value}, script=_BATCH_SCRIPT) == default_batch_run
+
+
+@pytest.mark.parametrize("value", ["0", "1", "2"])
+def test_batch_planes_per_block_gives_same_bits(default_batch_run, value):
+    assert _run({"FLUAMSL_PLANE_CAND": value}, script=_BATCH_SCRIPT) == default_batch_run
+
+
+@pytest.mark.parametrize("value", ["0", "1", "2"])
+def test_planes_per_block_gives_same_bits_64(value):
+    assert _run({"FLUAMSL_PLANE_CAND": value}, script=_SCRIPT64) == _run({}, script=_SCRIPT64)
