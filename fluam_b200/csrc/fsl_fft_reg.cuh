@@ -99,6 +99,52 @@ struct LineGeom {
   static constexpr int RT = (R + T - 1) / T;
 };
 
+// Exchange layout of the plane kernels' x pass, whose warps hold 32 / T
+// lines (row pairs) of T lanes each: line pitch LS, a-row pitch XP and, with
+// SW, lane t's value of row a in slot (t + a / RT) mod T of its a-row.
+// Chosen so that the exchange write and its read-back each take the
+// minimum two wavefronts per warp instruction (8-byte accesses, 16 lanes
+// per 128 bytes); with the y-pass geometry the write of the 64 edge took
+// eight.  Where and in which slot a value waits changes nothing of the
+// arithmetic.
+template <int R, int T>
+struct XLineGeom {
+  static constexpr int XP = LineGeom<R, T>::XP, LS = LineGeom<R, T>::LS;
+  static constexpr bool SW = false;
+};
+template <>
+struct XLineGeom<16, 2> {  // edge 32
+  static constexpr int XP = 2, LS = 34;
+  static constexpr bool SW = true;
+};
+template <>
+struct XLineGeom<12, 4> {  // edge 48
+  static constexpr int XP = 5, LS = 60;
+  static constexpr bool SW = false;
+};
+template <>
+struct XLineGeom<16, 4> {  // edge 64
+  static constexpr int XP = 4, LS = 68;
+  static constexpr bool SW = true;
+};
+template <>
+struct XLineGeom<20, 4> {  // edge 80
+  static constexpr int XP = 5, LS = 100;
+  static constexpr bool SW = false;
+};
+template <>
+struct XLineGeom<24, 4> {  // edge 96
+  static constexpr int XP = 4, LS = 100;
+  static constexpr bool SW = true;
+};
+
+// slot of lane t's value of a-row a (see XLineGeom)
+template <int R, int T, bool SW>
+__device__ __forceinline__ int ex_slot(int t, int a) {
+  if constexpr (SW) return (t + a / LineGeom<R, T>::RT) % T;
+  return t;
+}
+
 template <int R, int T>
 __device__ __forceinline__ int line_a(int t, int j) {
   return LineGeom<R, T>::EVEN ? t * LineGeom<R, T>::RT + j : t + T * j;
@@ -121,10 +167,11 @@ __host__ __device__ constexpr int plane_buf() {
 // Steps 1-2 and the exchange write: v holds z[t + T k]; afterwards the line's
 // exchange area holds Y_t[a] W_N^{a t}.  tw[i] = exp(-2 pi i i / N) (smem).
 // With T == 1 the transform is complete here and v holds X[f] in order.
-template <int R, int T>
+template <int R, int T, int XP = LineGeom<R, T>::XP, bool SW = false>
 __device__ __forceinline__ void line_fft_a(float2 (&v)[R], int t, float2* ex,
                                            const float2* __restrict__ tw, int dir) {
   using G = LineGeom<R, T>;
+  static_assert(!SW || G::EVEN, "the slot rotation assumes T divides R");
   RDft<R>::run(v, dir);
   if constexpr (T > 1) {
 #pragma unroll
@@ -134,13 +181,13 @@ __device__ __forceinline__ void line_fft_a(float2 (&v)[R], int t, float2* ex,
       v[a] = cmul(v[a], w);
     }
 #pragma unroll
-    for (int a = 0; a < R; ++a) ex[a * G::XP + t] = v[a];
+    for (int a = 0; a < R; ++a) ex[a * XP + ex_slot<R, T, SW>(t, a)] = v[a];
   }
 }
 
 // Step 3 after a barrier: thread t takes its a values (line_a, j < RT) and
 // all T values of each; out[j][b] = X[a + R b] (zero where line_has fails).
-template <int R, int T>
+template <int R, int T, int XP = LineGeom<R, T>::XP, bool SW = false>
 __device__ __forceinline__ void line_fft_b(const float2* ex, int t, int dir,
                                            float2 (&out)[LineGeom<R, T>::RT][T]) {
   using G = LineGeom<R, T>;
@@ -153,7 +200,7 @@ __device__ __forceinline__ void line_fft_b(const float2* ex, int t, int dir,
       continue;
     }
 #pragma unroll
-    for (int tt = 0; tt < T; ++tt) out[j][tt] = ex[a * G::XP + tt];
+    for (int tt = 0; tt < T; ++tt) out[j][tt] = ex[a * XP + ex_slot<R, T, SW>(tt, a)];
     RDft<T>::run(out[j], dir);
   }
 }
@@ -205,10 +252,13 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
       const int x = t + T * k;
       v[k] = live ? make_float2(W[(2 * p) * N + x], W[(2 * p + 1) * N + x]) : make_float2(0.f, 0.f);
     }
-    line_fft_a<RR, T>(v, t, buf + p * LS, stw, -1);
+    using XG = XLineGeom<RR, T>;
+    static_assert(XG::XP >= T && (RR - 1) * XG::XP + T <= XG::LS && H * XG::LS <= plane_buf<N, RR, T>(),
+                  "x-pass exchange fits its line pitch and the plane buffer");
+    line_fft_a<RR, T, XG::XP, XG::SW>(v, t, buf + p * XG::LS, stw, -1);
     __syncthreads();
     float2 out[G::RT][T];
-    line_fft_b<RR, T>(buf + p * LS, t, -1, out);
+    line_fft_b<RR, T, XG::XP, XG::SW>(buf + p * XG::LS, t, -1, out);
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < G::RT; ++j)
@@ -383,10 +433,13 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
       fb[(2 * p + 1) * (N + 1) + x] = v[x].y;
     }
   } else {
-    line_fft_a<RR, T>(v, t, buf + p * LS, stw, +1);
+    using XG = XLineGeom<RR, T>;
+    static_assert(XG::XP >= T && (RR - 1) * XG::XP + T <= XG::LS && H * XG::LS <= plane_buf<N, RR, T>(),
+                  "x-pass exchange fits its line pitch and the plane buffer");
+    line_fft_a<RR, T, XG::XP, XG::SW>(v, t, buf + p * XG::LS, stw, +1);
     __syncthreads();
     float2 out[G::RT][T];
-    line_fft_b<RR, T>(buf + p * LS, t, +1, out);
+    line_fft_b<RR, T, XG::XP, XG::SW>(buf + p * XG::LS, t, +1, out);
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < G::RT; ++j)
