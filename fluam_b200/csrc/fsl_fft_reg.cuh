@@ -107,35 +107,44 @@ struct LineGeom {
 // per 128 bytes); with the y-pass geometry the write of the 64 edge took
 // eight.  Where and in which slot a value waits changes nothing of the
 // arithmetic.
+// The inverse's x pass also reads the rows of the half-spectrum plane
+// (float2, row pitch PR >= N / 2 + 1) and writes the rows of the real plane
+// (float, row pitch PRF >= N); their pitches are chosen the same way.
 template <int R, int T>
 struct XLineGeom {
   static constexpr int XP = LineGeom<R, T>::XP, LS = LineGeom<R, T>::LS;
   static constexpr bool SW = false;
+  static constexpr int PR = R * T / 2 + 1, PRF = R * T + 1;
 };
 template <>
 struct XLineGeom<16, 2> {  // edge 32
   static constexpr int XP = 2, LS = 34;
   static constexpr bool SW = true;
+  static constexpr int PR = 17, PRF = 33;
 };
 template <>
 struct XLineGeom<12, 4> {  // edge 48
   static constexpr int XP = 5, LS = 60;
   static constexpr bool SW = false;
+  static constexpr int PR = 26, PRF = 50;
 };
 template <>
 struct XLineGeom<16, 4> {  // edge 64
   static constexpr int XP = 4, LS = 68;
   static constexpr bool SW = true;
+  static constexpr int PR = 34, PRF = 67;
 };
 template <>
 struct XLineGeom<20, 4> {  // edge 80
   static constexpr int XP = 5, LS = 100;
   static constexpr bool SW = false;
+  static constexpr int PR = 42, PRF = 82;
 };
 template <>
 struct XLineGeom<24, 4> {  // edge 96
   static constexpr int XP = 4, LS = 100;
   static constexpr bool SW = true;
+  static constexpr int PR = 50, PRF = 98;
 };
 
 // slot of lane t's value of a-row a (see XLineGeom)
@@ -344,7 +353,12 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
     k_plane_inv_r(FSL_KARGS, const float2* __restrict__ twn) {
   FSL_REP_AT(blockIdx.z);
   using G = LineGeom<RR, T>;
-  constexpr int H = N / 2, TPP = H * T, LS = G::LS, PR = H + 1;  // PR: row pitch of the plane
+  // PR: row pitch of the half-spectrum plane, PRF: of the real plane
+  constexpr int H = N / 2, TPP = H * T, LS = G::LS, PR = XLineGeom<RR, T>::PR,
+                PRF = XLineGeom<RR, T>::PRF;
+  static_assert(PR >= H + 1 && N * PR <= plane_buf<N, RR, T>() && PRF >= N &&
+                    N * PRF <= 2 * plane_buf<N, RR, T>(),
+                "plane rows fit the plane buffer");
   extern __shared__ float2 smem[];
   float2* stw = smem;
   const int lp = threadIdx.x / TPP, r = threadIdx.x - lp * TPP;
@@ -424,13 +438,13 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
     v[k] = make_float2(e.x - o.y, e.y + o.x);  // X_2p + i X_2p+1
   }
   __syncthreads();
-  float* fb = reinterpret_cast<float*>(buf);  // the real plane, row pitch N + 1
+  float* fb = reinterpret_cast<float*>(buf);  // the real plane, row pitch PRF
   if constexpr (T == 1) {
     RDft<RR>::run(v, +1);
 #pragma unroll
     for (int x = 0; x < N; ++x) {
-      fb[(2 * p) * (N + 1) + x] = v[x].x;
-      fb[(2 * p + 1) * (N + 1) + x] = v[x].y;
+      fb[(2 * p) * PRF + x] = v[x].x;
+      fb[(2 * p + 1) * PRF + x] = v[x].y;
     }
   } else {
     using XG = XLineGeom<RR, T>;
@@ -447,14 +461,14 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
 #pragma unroll
         for (int b = 0; b < T; ++b) {
         const int x = line_freq<RR, T>(t, j, b);
-        fb[(2 * p) * (N + 1) + x] = out[j][b].x;
-        fb[(2 * p + 1) * (N + 1) + x] = out[j][b].y;
+        fb[(2 * p) * PRF + x] = out[j][b].x;
+        fb[(2 * p + 1) * PRF + x] = out[j][b].y;
       }
   }
   __syncthreads();
   if (live) {
     float* out_g = R.v + (size_t)comp * P.nc + (size_t)z * N * N;
-    for (int i = r; i < N * N; i += TPP) out_g[i] = fb[i + i / N];
+    for (int i = r; i < N * N; i += TPP) out_g[i] = fb[(i / N) * PRF + i % N];
   }
 }
 
