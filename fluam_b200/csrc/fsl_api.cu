@@ -206,6 +206,38 @@ int fsl_set_positions(fsl_handle* h, const double* in) {
   return FSL_OK;
 }
 
+// whether p is page-locked host memory (a copy from or to it can be a node
+// of a CUDA graph)
+static bool pinned_host(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+int fsl_step_io(fsl_handle* h, const double* in, double* out) {
+  if (!h || !in || !out) return errorf(FSL_E_ARG, "null argument");
+  FSL_TRY(cudaSetDevice(h->exec.device));
+  if (!pinned_host(in) || !pinned_host(out)) {
+    // pageable buffers: the copies stay outside the step's graph
+    if (int rc = fsl_set_positions(h, in)) return rc;
+    if (int rc = fsl_step(h, 1)) return rc;
+    return fsl_get_positions(h, out);
+  }
+  fsl::Group& g = h->group;
+  g.io_in = in;
+  g.io_out = out;
+  g.io_bytes = sizeof(double) * 3 * (size_t)params(h).np;
+  const int rc = fsl::exec_step(h->exec, 1);
+  g.io_in = nullptr;
+  g.io_out = nullptr;
+  if (rc) return rc;
+  FSL_TRY(cudaStreamSynchronize(h->exec.stream));
+  return FSL_OK;
+}
+
 int fsl_get_forces(fsl_handle* h, double* out) {
   if (!h || !out) return errorf(FSL_E_ARG, "null argument");
   FSL_TRY(cudaSetDevice(h->exec.device));

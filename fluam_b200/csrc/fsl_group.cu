@@ -795,6 +795,14 @@ void group_enqueue_step(Group& g) {
   }
   chk("noise");
   pr.count(1 + (div ? 1 : 0) + (two ? 1 : 0));
+  // the positions of an input/output step, copied in from pinned host
+  // memory beside the noise (which reads no position), then the Verlet-list
+  // check of fsl_set_positions
+  if (g.io_in && !g.slots.empty()) {
+    cudaMemcpyAsync(g.slots[0]->r.q, g.io_in, g.io_bytes, cudaMemcpyHostToDevice, s);
+    launch_moved_check(g.slots[0]->r, s);
+    chk("positions in");
+  }
   auto join_noise = [&]() {
     if (fork) cudaStreamWaitEvent(s, g.ev_join, 0);
   };
@@ -1070,6 +1078,8 @@ int exec_prepare(Exec& e) {
     shape.push_back(g.B.max_np);
     shape.push_back((long long)g.B.max_noise_n);
     shape.push_back(g.prof.on ? 1 : 0);
+    shape.push_back((long long)(uintptr_t)g.io_in);
+    shape.push_back((long long)(uintptr_t)g.io_out);
     for (int k = 0; k < NKIND; ++k) shape.push_back(g.B.nblk[k]);
     // a single instance is a by-value kernel argument: any change to it
     // needs a new capture
@@ -1094,8 +1104,12 @@ int exec_prepare(Exec& e) {
 void exec_enqueue(Exec& e) {
   const size_t ng = e.groups.size();
   if (ng == 1) {
-    group_enqueue_step(*e.groups[0]);
-    e.launches_per_step = e.groups[0]->launches;
+    Group& g = *e.groups[0];
+    group_enqueue_step(g);
+    e.launches_per_step = g.launches;
+    // the positions after the step of an input/output step
+    if (g.io_out && !g.slots.empty())
+      cudaMemcpyAsync(g.io_out, g.slots[0]->r.q, g.io_bytes, cudaMemcpyDeviceToHost, e.stream);
     return;
   }
   // fork: every group on its own stream, joined back into the main one

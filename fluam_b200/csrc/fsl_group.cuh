@@ -114,6 +114,12 @@ struct Group {
   // uncaptured step (us per build: separate kernels, block per instance)
   bool lists_tuned = false;
   float lists_us[2] = {};
+  // an input/output step of a single instance (fsl_step_io): the positions
+  // come from pinned host memory io_in at the start of the step and go to
+  // io_out at its end, both inside the step's graph (null: a plain step)
+  const double* io_in = nullptr;
+  double* io_out = nullptr;
+  size_t io_bytes = 0;
   const char* fail_stage = nullptr;  // first stage whose launch failed
 };
 

@@ -156,6 +156,17 @@ class StokesLimit:
         return {"step": st.step, "error_bits": st.error_bits, "np": st.np, "nc": st.nc,
                 "graph": bool(st.graph), "launches_per_step": st.launches_per_step}
 
+    def step_io(self, q_in, q_out):
+        """One step with its positions in and out (fsl_step_io): q_in, q_out
+        are host addresses of 3 x np doubles (page-locked for the in-graph
+        copies), or (3, np) float64 arrays."""
+        def addr(a):
+            if isinstance(a, np.ndarray):
+                assert a.dtype == np.float64 and a.size == 3 * self.np and a.flags.c_contiguous
+                return a.ctypes.data
+            return int(a)
+        check(self.L.fsl_step_io(self.h, ctypes.c_void_p(addr(q_in)), ctypes.c_void_p(addr(q_out))))
+
     def tuning(self):
         """The autotuner's picks and timings (after the first step)."""
         t = _lib.ClassTuning()

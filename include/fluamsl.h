@@ -166,6 +166,16 @@ int fsl_sync(fsl_handle* h);
 /* Particle positions q^n (gpuToHostStokesLimit, src/gpuToHostStokesLimit.cu:36-38). */
 int fsl_get_positions(fsl_handle* h, double* out);
 int fsl_set_positions(fsl_handle* h, const double* in);
+/* One step with its positions in and out: fsl_set_positions(in),
+ * fsl_step(1), fsl_get_positions(out) with the same results, bit for bit
+ * (in may equal out).  With page-locked host buffers both copies are nodes
+ * of the step's CUDA graph and the copy in runs beside the step's noise,
+ * which reads no position; the graph is kept for the same pair of buffers,
+ * and a plain fsl_step in between captures it again.  Pageable buffers
+ * take the three calls.  The reference moves positions between host and
+ * device around its step loop (src/runSchemeStokesLimit.cu:163-285,
+ * src/gpuToHostStokesLimit.cu). */
+int fsl_step_io(fsl_handle* h, const double* in, double* out);
 /* Particle forces F^{n+1/2} of the last step: what the reference writes to
  * <out>.velocityParticles (src/gpuToHostStokesLimit.cu:41-43). */
 int fsl_get_forces(fsl_handle* h, double* out);
