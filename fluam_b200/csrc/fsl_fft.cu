@@ -731,9 +731,9 @@ __global__ void __launch_bounds__(kFftThreads)
   }
 }
 
+#include "fsl_bulk.cuh"
 #include "fsl_fft_reg.cuh"
 #include "fsl_fft_lines.cuh"
-#include "fsl_bulk.cuh"
 #include "fsl_fft_v.cuh"
 
 // ------------------------------------------------------------ host side ---

@@ -359,16 +359,40 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
   static_assert(PR >= H + 1 && N * PR <= plane_buf<N, RR, T>() && PRF >= N &&
                     N * PRF <= 2 * plane_buf<N, RR, T>(),
                 "plane rows fit the plane buffer");
-  extern __shared__ float2 smem[];
+  extern __shared__ __align__(16) float2 smem[];
   float2* stw = smem;
   const int lp = threadIdx.x / TPP, r = threadIdx.x - lp * TPP;
   float2* buf = smem + N + lp * plane_buf<N, RR, T>();
-  for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twn[i];
   const int pl = blockIdx.x * PB + lp;
   const bool live = pl < 3 * P.mz;
   const int comp = live ? pl / P.mz : 0, z = live ? pl - comp * P.mz : 0;
-  const float2* in_g = R.spec + ((size_t)comp * P.mz + z) * (size_t)N * (H + 1);
+  // The half-spectrum planes are contiguous (N rows of H + 1, plane pl at
+  // pl N (H + 1)): one bulk copy per live plane of the block into the
+  // plane's buffer, completed on the block's mbarrier (bounded wait), while
+  // the twiddles are staged.  Plane bytes, plane offsets and buffer starts
+  // are multiples of 16 bytes.
+  constexpr unsigned kPlaneBytes = sizeof(float2) * N * (H + 1);
+  static_assert(kPlaneBytes % 16 == 0 && N % 2 == 0 && plane_buf<N, RR, T>() % 2 == 0 &&
+                    PB * kPlaneBytes < (1u << 20),
+                "bulk copies of whole half-spectrum planes");
+  __shared__ __align__(8) unsigned long long s_bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    mbar_fence_init();
+  }
   __syncthreads();
+  if (threadIdx.x == 0) {
+    // blockIdx.x PB < 3 mz, so the block has at least one live plane
+    const int nlive = min(PB, 3 * P.mz - (int)blockIdx.x * PB);
+    mbar_arrive_tx(&s_bar, kPlaneBytes * (unsigned)nlive);
+    for (int q = 0; q < nlive; ++q)
+      bulk_load(smem + N + q * plane_buf<N, RR, T>(),
+                R.spec + (size_t)(blockIdx.x * PB + q) * (size_t)N * (H + 1), kPlaneBytes, &s_bar);
+  }
+  for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twn[i];
+  bulk_wait(&s_bar, R.err);
+  __syncthreads();
+  const float2* in_s = buf;  // this thread's plane, row pitch H + 1
   // y pass: column c (fastest), thread t
   {
     const int c = r % H, t = r / H;
@@ -379,12 +403,13 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
       if (!live) {
         v[k] = make_float2(0.f, 0.f);
       } else if (c == 0) {
-        const float2 f0 = in_g[(size_t)ky * (H + 1)], fh = in_g[(size_t)ky * (H + 1) + H];
+        const float2 f0 = in_s[ky * (H + 1)], fh = in_s[ky * (H + 1) + H];
         v[k] = make_float2(f0.x - fh.y, f0.y + fh.x);  // F0 + i FH
       } else {
-        v[k] = in_g[(size_t)ky * (H + 1) + c];
+        v[k] = in_s[ky * (H + 1) + c];
       }
     }
+    __syncthreads();  // the staged plane is overwritten from here on
     if constexpr (T == 1) {
       RDft<RR>::run(v, +1);
       // rows y: X_y[c], or X_y[0] + i X_y[H] for the packed column
