@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
   FSL_REP_AT(blockIdx.z);
   using G = LineGeom<RR, T>;
   constexpr int H = N / 2, TPP = H * T, LS = G::LS;
-  extern __shared__ float2 smem[];
+  extern __shared__ __align__(16) float2 smem[];
   float2* stw = smem;
   const int lp = threadIdx.x / TPP, r = threadIdx.x - lp * TPP;
   float2* buf = smem + N + lp * plane_buf<N, RR, T>();
@@ -254,13 +254,43 @@ __global__ void __launch_bounds__(PB * (N / 2) * T)
 #pragma unroll
     for (int f = 0; f < N; ++f) buf[p * LS + f] = v[f];
   } else {
+    // The W planes come into the planes' buffers row by row (N floats at
+    // pitch PW = N + 4; rows, pitch and buffer starts are multiples of 16
+    // bytes) by bulk copies on the block's mbarrier (bounded wait), and the
+    // x pass reads them from shared memory: at pitch N + 4 a warp load takes
+    // two wavefronts (four at edge 32) where reading the rows from global
+    // memory touched eight row segments.
+    constexpr int PW = N + 4;
+    constexpr unsigned kRowBytes = sizeof(float) * N;
+    static_assert(kRowBytes % 16 == 0 && (PW * sizeof(float)) % 16 == 0 && N * PW <= 2 * plane_buf<N, RR, T>() &&
+                      plane_buf<N, RR, T>() % 2 == 0 && PB * N * kRowBytes < (1u << 20),
+                  "row-wise bulk copies of the W planes");
+    __shared__ __align__(8) unsigned long long s_bar;
+    if (threadIdx.x == 0) {
+      mbar_init(&s_bar, 1);
+      mbar_fence_init();
+    }
     __syncthreads();
+    // blockIdx.x PB < 3 mz, so the block has at least one live plane
+    const int nlive = min(PB, 3 * P.mz - (int)blockIdx.x * PB);
+    if (threadIdx.x == 0) mbar_arrive_tx(&s_bar, kRowBytes * (unsigned)(N * nlive));
+    __syncthreads();
+    for (int i = threadIdx.x; i < N * nlive; i += blockDim.x) {
+      const int q = i / N, row = i - q * N;
+      const int plq = blockIdx.x * PB + q, cq = plq / P.mz, zq = plq - cq * P.mz;
+      bulk_load(reinterpret_cast<float*>(smem + N + q * plane_buf<N, RR, T>()) + row * PW,
+                R.wbuf + (size_t)cq * P.nc + ((size_t)zq * N + row) * N, kRowBytes, &s_bar);
+    }
+    bulk_wait(&s_bar, R.err);
+    __syncthreads();
+    const float* fw = reinterpret_cast<const float*>(buf);  // this thread's plane
     const int p = r / T, t = r - p * T;
 #pragma unroll
     for (int k = 0; k < RR; ++k) {
       const int x = t + T * k;
-      v[k] = live ? make_float2(W[(2 * p) * N + x], W[(2 * p + 1) * N + x]) : make_float2(0.f, 0.f);
+      v[k] = live ? make_float2(fw[(2 * p) * PW + x], fw[(2 * p + 1) * PW + x]) : make_float2(0.f, 0.f);
     }
+    __syncthreads();  // the staged plane is overwritten by the exchange
     using XG = XLineGeom<RR, T>;
     static_assert(XG::XP >= T && (RR - 1) * XG::XP + T <= XG::LS && H * XG::LS <= plane_buf<N, RR, T>(),
                   "x-pass exchange fits its line pitch and the plane buffer");
