@@ -35,7 +35,7 @@ EXPORTS = [
     "fsl_batch_get_positions_packed", "fsl_batch_set_positions_packed",
     "fsl_batch_get_positions_packed_async", "fsl_batch_set_positions_packed_async",
     "fsl_batch_set_graph", "fsl_batch_get_info", "fsl_batch_stream", "fsl_batch_destroy",
-    "fsl_batch_get_class_tuning", "fsl_get_tuning", "fsl_step_io",
+    "fsl_batch_get_class_tuning", "fsl_get_tuning", "fsl_step_io", "fsl_batch_step_io",
     "fsl_server_config_defaults", "fsl_server_create", "fsl_server_submit", "fsl_server_poll",
     "fsl_server_wait", "fsl_server_result", "fsl_server_get_stats", "fsl_server_destroy",
 ]
@@ -225,6 +225,7 @@ def load(path=None):
     L.fsl_batch_get_class_tuning.argtypes = [_VP, ctypes.c_int32, ctypes.POINTER(ClassTuning)]
     L.fsl_get_tuning.argtypes = [_VP, ctypes.POINTER(ClassTuning)]
     L.fsl_step_io.argtypes = [_VP, _VP, _VP]
+    L.fsl_batch_step_io.argtypes = [_VP, _VP, _VP]
     L.fsl_batch_stream.argtypes = [_VP]
     L.fsl_batch_stream.restype = _VP
     L.fsl_batch_destroy.argtypes = [_VP]

@@ -206,21 +206,10 @@ int fsl_set_positions(fsl_handle* h, const double* in) {
   return FSL_OK;
 }
 
-// whether p is page-locked host memory (a copy from or to it can be a node
-// of a CUDA graph)
-static bool pinned_host(const void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeHost;
-}
-
 int fsl_step_io(fsl_handle* h, const double* in, double* out) {
   if (!h || !in || !out) return errorf(FSL_E_ARG, "null argument");
   FSL_TRY(cudaSetDevice(h->exec.device));
-  if (!pinned_host(in) || !pinned_host(out)) {
+  if (!fsl::pinned_host(in) || !fsl::pinned_host(out)) {
     // pageable buffers: the copies stay outside the step's graph
     if (int rc = fsl_set_positions(h, in)) return rc;
     if (int rc = fsl_step(h, 1)) return rc;

@@ -101,10 +101,14 @@ int check_index(const fsl_batch* b, int32_t i) {
   return FSL_OK;
 }
 
-int pack(fsl_batch* b, int dir) {
-  if (b->slots.empty() || b->max_np == 0) return FSL_OK;
+void pack_on(fsl_batch* b, int dir, cudaStream_t st) {
+  if (b->slots.empty() || b->max_np == 0) return;
   unsigned bx = (unsigned)std::min<long long>((3ll * b->max_np + 255) / 256, 64);
-  k_pack<<<dim3(bx, (unsigned)b->slots.size()), 256, 0, b->exec.stream>>>(b->d_ents, b->d_packed, dir);
+  k_pack<<<dim3(bx, (unsigned)b->slots.size()), 256, 0, st>>>(b->d_ents, b->d_packed, dir);
+}
+
+int pack(fsl_batch* b, int dir) {
+  pack_on(b, dir, b->exec.stream);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fsl::cuda_fail(e, "pack kernel");
   return FSL_OK;
@@ -303,6 +307,36 @@ int fsl_batch_set_positions_packed_async(fsl_batch* b, const double* host) {
     FSL_TRY(cudaMemcpyAsync(b->d_packed, host, sizeof(double) * b->packed_n, cudaMemcpyHostToDevice,
                             b->exec.stream));
   return pack(b, 1);
+}
+
+int fsl_batch_step_io(fsl_batch* b, const double* in, double* out) {
+  if (!b || !in || !out) return errorf(FSL_E_ARG, "null argument");
+  FSL_TRY(cudaSetDevice(b->exec.device));
+  if (!fsl::pinned_host(in) || !fsl::pinned_host(out)) {
+    // pageable buffers: the copies stay outside the step's graph
+    if (int rc = fsl_batch_set_positions_packed(b, in)) return rc;
+    if (int rc = fsl_batch_step(b, 1)) return rc;
+    return fsl_batch_get_positions_packed(b, out);
+  }
+  const size_t bytes = sizeof(double) * (size_t)b->packed_n;
+  fsl::Exec& e = b->exec;
+  e.io_in = [b, in, bytes](cudaStream_t st) {
+    if (bytes) cudaMemcpyAsync(b->d_packed, in, bytes, cudaMemcpyHostToDevice, st);
+    pack_on(b, 1, st);
+  };
+  e.io_out = [b, out, bytes](cudaStream_t st) {
+    pack_on(b, 0, st);
+    if (bytes) cudaMemcpyAsync(out, b->d_packed, bytes, cudaMemcpyDeviceToHost, st);
+  };
+  e.io_key[0] = in;
+  e.io_key[1] = out;
+  const int rc = fsl::exec_step(e, 1);
+  e.io_in = nullptr;
+  e.io_out = nullptr;
+  e.io_key[0] = e.io_key[1] = nullptr;
+  if (rc) return rc;
+  FSL_TRY(cudaStreamSynchronize(e.stream));
+  return FSL_OK;
 }
 
 int fsl_batch_get_positions_packed(fsl_batch* b, double* out) {

@@ -798,6 +798,7 @@ void group_enqueue_step(Group& g) {
   // the positions of an input/output step, copied in from pinned host
   // memory beside the noise (which reads no position), then the Verlet-list
   // check of fsl_set_positions
+  if (g.io_wait) cudaStreamWaitEvent(s, g.io_wait, 0);
   if (g.io_in && !g.slots.empty()) {
     cudaMemcpyAsync(g.slots[0]->r.q, g.io_in, g.io_bytes, cudaMemcpyHostToDevice, s);
     launch_moved_check(g.slots[0]->r, s);
@@ -1037,9 +1038,26 @@ void exec_drop_graph(Exec& e) {
   e.shape.clear();
 }
 
+bool pinned_host(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 void exec_destroy(Exec& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
   exec_drop_graph(e);
+  if (e.io_stream) {
+    cudaStreamSynchronize(e.io_stream);
+    cudaStreamDestroy(e.io_stream);
+    e.io_stream = nullptr;
+  }
+  if (e.io_fork) cudaEventDestroy(e.io_fork);
+  if (e.io_ev) cudaEventDestroy(e.io_ev);
+  e.io_fork = e.io_ev = nullptr;
   for (cudaStream_t s : e.side) {
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
@@ -1068,6 +1086,13 @@ int exec_prepare(Exec& e) {
     e.ev.push_back(ev);
   }
   std::vector<long long> shape;
+  shape.push_back((long long)(uintptr_t)e.io_key[0]);
+  shape.push_back((long long)(uintptr_t)e.io_key[1]);
+  if (e.io_in && !e.io_stream) {
+    FSL_TRY(cudaStreamCreateWithFlags(&e.io_stream, cudaStreamNonBlocking));
+    FSL_TRY(cudaEventCreateWithFlags(&e.io_fork, cudaEventDisableTiming));
+    FSL_TRY(cudaEventCreateWithFlags(&e.io_ev, cudaEventDisableTiming));
+  }
   for (size_t i = 0; i < ng; ++i) {
     Group& g = *e.groups[i];
     g.stream = i == 0 ? e.stream : e.side[i - 1];
@@ -1101,7 +1126,7 @@ int exec_prepare(Exec& e) {
   return FSL_OK;
 }
 
-void exec_enqueue(Exec& e) {
+void exec_enqueue_groups(Exec& e) {
   const size_t ng = e.groups.size();
   if (ng == 1) {
     Group& g = *e.groups[0];
@@ -1125,6 +1150,25 @@ void exec_enqueue(Exec& e) {
     cudaStreamWaitEvent(e.stream, e.ev[i], 0);
   }
   e.launches_per_step = total;
+}
+
+void exec_enqueue(Exec& e) {
+  const bool io = e.io_in && e.io_stream;
+  if (io) {
+    // the inputs of an input/output step on the io stream, beside the
+    // groups' noise; every group's main branch waits for them
+    cudaEventRecord(e.io_fork, e.stream);
+    cudaStreamWaitEvent(e.io_stream, e.io_fork, 0);
+    e.io_in(e.io_stream);
+    cudaEventRecord(e.io_ev, e.io_stream);
+    for (Group* g : e.groups) g->io_wait = e.io_ev;
+  }
+  exec_enqueue_groups(e);
+  if (io) {
+    for (Group* g : e.groups) g->io_wait = nullptr;
+    cudaStreamWaitEvent(e.stream, e.io_ev, 0);
+  }
+  if (e.io_out) e.io_out(e.stream);
 }
 
 }  // namespace

@@ -10,6 +10,7 @@
 //           whole step captured in one CUDA graph.
 #pragma once
 
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -120,6 +121,10 @@ struct Group {
   const double* io_in = nullptr;
   double* io_out = nullptr;
   size_t io_bytes = 0;
+  // an input/output step of a batch: the step's main branch waits for this
+  // event (the inputs copied in and scattered on the Exec's io stream)
+  // after forking its noise
+  cudaEvent_t io_wait = nullptr;
   const char* fail_stage = nullptr;  // first stage whose launch failed
 };
 
@@ -146,7 +151,20 @@ struct Exec {
   uint64_t steps = 0;
   int launches_per_step = 0;
   int64_t captures = 0;               // graphs captured so far
+  // an input/output step of a batch (fsl_batch_step_io): io_in enqueues the
+  // copy in and scatter on io_stream, forked at the start of the step so
+  // that the groups' noise runs beside it; io_out enqueues the gather and
+  // copy out on the main stream after the join.  io_key (the host buffers)
+  // is part of the captured graph's shape.  Unset: a plain step.
+  std::function<void(cudaStream_t)> io_in, io_out;
+  const void* io_key[2] = {};
+  cudaStream_t io_stream = nullptr;
+  cudaEvent_t io_fork = nullptr, io_ev = nullptr;
 };
+
+// Whether p is page-locked host memory (a copy from or to it can be a node
+// of a CUDA graph).
+bool pinned_host(const void* p);
 
 int exec_init(Exec& e, int device);
 void exec_destroy(Exec& e);

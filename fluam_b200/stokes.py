@@ -345,6 +345,17 @@ class Batch:
         check(self.L.fsl_batch_get_info(self.h, ctypes.byref(b)))
         return {f: getattr(b, f) for f, _ in _lib.BatchInfo._fields_}
 
+    def step_io(self, q_in, q_out):
+        """One step of every instance with the packed positions in and out
+        (fsl_batch_step_io): host addresses of offsets[-1] doubles
+        (page-locked for the in-graph copies), or float64 arrays."""
+        def addr(a):
+            if isinstance(a, np.ndarray):
+                assert a.dtype == np.float64 and a.size == int(self.offsets[-1]) and a.flags.c_contiguous
+                return a.ctypes.data
+            return int(a)
+        check(self.L.fsl_batch_step_io(self.h, ctypes.c_void_p(addr(q_in)), ctypes.c_void_p(addr(q_out))))
+
     def class_tuning(self):
         """Per size class: the autotuner's picks and timings (after the
         first step)."""

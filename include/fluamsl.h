@@ -336,6 +336,16 @@ int fsl_batch_set_positions_packed(fsl_batch* b, const double* in);
  * reaches the copy. */
 int fsl_batch_get_positions_packed_async(fsl_batch* b, double* host);
 int fsl_batch_set_positions_packed_async(fsl_batch* b, const double* host);
+/* One step of every instance with all positions in and out in the packed
+ * layout: fsl_batch_set_positions_packed(in), fsl_batch_step(1),
+ * fsl_batch_get_positions_packed(out) with the same results, bit for bit
+ * (in may equal out).  With page-locked host buffers the copies and the
+ * scatter and gather kernels are nodes of the step's CUDA graph: the copy
+ * in and the scatter on a stream of their own beside every size class's
+ * noise, the gather and the copy out after the join; the graph is kept
+ * while the same pair of buffers comes back.  Pageable buffers take the
+ * three calls. */
+int fsl_batch_step_io(fsl_batch* b, const double* in, double* out);
 int fsl_batch_set_graph(fsl_batch* b, int enable);
 int fsl_batch_get_info(fsl_batch* b, fsl_batch_info* info);
 

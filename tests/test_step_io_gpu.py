@@ -83,3 +83,42 @@ def test_step_io_then_plain_steps(fsl):
         qa[...] = a.positions() + rng.normal(0.0, 0.01, qa.shape)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("pinned", [True, False], ids=["pinned", "pageable"])
+def test_batch_step_io_equals_set_step_get(fsl, pinned):
+    """The batched form: every instance of a batch over three size classes
+    (one instance empty) bit for bit as the packed set, step and get."""
+    import torch
+    rng = np.random.default_rng(9)
+    cfgs, qs = [], []
+    for i in range(9):
+        m = (16, 24, 32)[i % 3]
+        n = 0 if i == 4 else 200 + 150 * i
+        cfgs.append(fsl.make_config((m, m, m), (float(m),) * 3, kT=0.01, dt=0.01, cutoff=1.5,
+                                    kernel=3 + i % 2, pair=fsl.PAIR_SOFT, seed=60 + i))
+        qs.append(uniform_positions(n, (m, m, m), 20 + i))
+    a = fsl.Batch(cfgs, qs)
+    b = fsl.Batch(cfgs, qs)
+    n = int(a.offsets[-1])
+    if pinned:
+        buf = torch.empty(n, dtype=torch.float64).pin_memory()
+        qa = buf.numpy()
+    else:
+        qa = np.empty(n)
+    a.positions_packed(qa)
+    qb = qa.copy()
+    for k in range(6):
+        a.step_io(qa, qa)
+        b.set_positions_packed(qb)
+        b.step(1)
+        b.positions_packed(qb)
+        np.testing.assert_array_equal(qa, qb)
+        moves = rng.normal(0.0, 0.01, n)
+        qa += moves
+        qb += moves
+    for i in range(len(cfgs)):
+        np.testing.assert_array_equal(a.forces(i), b.forces(i))
+        assert a.status(i)["error_bits"] == b.status(i)["error_bits"] == 0
+    a.close()
+    b.close()
