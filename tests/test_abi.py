@@ -47,6 +47,15 @@ def test_tuning_query_checks_arguments():
     assert L.fsl_get_tuning(None, ctypes.byref(t)) == -1
 
 
+def test_step_io_checks_arguments():
+    """The input/output steps refuse a missing handle or buffer before they
+    touch a device."""
+    L = _lib.load()
+    buf = (ctypes.c_double * 6)()
+    assert L.fsl_step_io(None, buf, buf) == -1
+    assert L.fsl_batch_step_io(None, buf, buf) == -1
+
+
 def test_defaults_follow_reference():
     c = _lib.Config()
     _lib.load().fsl_config_defaults(ctypes.byref(c))
